@@ -1,0 +1,321 @@
+#!/usr/bin/env python3
+"""Traversal benchmark: Mrays/s of incoherent closest-hit rays on the
+2,097,152-triangle traversal set (512 noisy spheres x 4096 triangles in a 100^3
+box; 7,997,584 rays per step, origins uniform in the box, directions uniform).
+
+One step = one closest-hit trace of all 7,997,584 rays through the reference's
+SAH BVH (same layout as BuildBvh). Inputs (256 MB of rays, 128 MB of hits,
+~150 MB of BVH) exceed the 126 MB L2, so no L2 flush is needed between steps.
+
+  value      device throughput: rays resident in HBM, K launches timed with
+             CUDA events on the launching stream (max over ranks).
+  e2e        the same metric through the C ABI's host entry point
+             (yrc_trace_host): pinned host rays in, host hits out, the copies
+             inside the timed region.
+  roofline   algorithmic bytes per launch = sum over rays of
+             32 * node_tests + 48 * triangle_tests + 32 (ray) + 16 (hit),
+             with the reference's own BvhTraceStats counts, / kernel time,
+             against the measured HBM copy bandwidth.
+  cpu_baseline  the reference CPU traversal (IntersectBvh, compiled from the
+             reference sources) on this host's cores, on a bounded sample.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Multi-GPU (weak scaling, replicas: each rank traces its own ray set):
+  python -m torch.distributed.run --nproc-per-node N bench.py --gpus N ...
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s traversal"
+UNIT = "Mrays/s"
+WORKLOAD = "traversal-2M-tris-incoherent-closest-hit"
+RAYS_PER_STEP = 2828 * 2828
+PROFILE_SUMMARY = ROOT / "profiles" / "trace_closest_incoherent_2M.md"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([c.strip() for c in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the trace kernel from the committed ncu summary."""
+    if PROFILE_SUMMARY.exists():
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", PROFILE_SUMMARY.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def cpu_baseline(geom, rays, seconds: float = 10.0):
+    """Times the reference CPU traversal (oracle/_ref, else the C oracle port)
+    on all host threads over repeated 1M-ray chunks for ~`seconds`."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    threads = os.cpu_count() or 1
+    chunk = rays[: 1 << 20]
+    if oracle.ref_available():
+        scene = oracle.RefScene(geom, threads=threads)
+        run = lambda: scene.trace_count(chunk, any_hit=False, threads=threads)  # noqa: E731
+        kind = "reference"
+    else:
+        from yaoray_b200 import accel
+        scene = oracle.OracleScene(geom, accel.build_bvh(geom))
+        run = lambda: scene.trace(chunk, threads=threads, stats=False)  # noqa: E731
+        kind = "port"
+    run()  # warm-up
+    done = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        run()
+        done += chunk.shape[0]
+    dt = time.perf_counter() - t0
+    return {"value": done / dt / 1e6, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{done} incoherent closest-hit rays ({done // chunk.shape[0]} x 1M-ray chunks of the same "
+                      f"workload) in {dt:.1f} s on {threads} threads"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's own CPU IntersectBvh on all host
+    threads, each step a bounded 1M-ray sample of the workload."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from yaoray_b200 import scenes
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    geom = scenes.traversal_scene()
+    rays = scenes.incoherent_rays(seed=2)
+    threads = os.cpu_count() or 1
+    sample = 1 << 20
+    if oracle.ref_available():
+        scene = oracle.RefScene(geom, threads=threads)
+        kind = "reference"
+        step = lambda i: scene.trace_count(rays[(i * sample) % len(rays):][:sample], False, threads)  # noqa: E731
+    else:
+        from yaoray_b200 import accel
+        scene = oracle.OracleScene(geom, accel.build_bvh(geom))
+        kind = "port"
+        step = lambda i: scene.trace(rays[(i * sample) % len(rays):][:sample], threads=threads, stats=False)  # noqa
+    for i in range(args.warmup):
+        step(i)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        step(args.warmup + i)
+    dt = time.perf_counter() - t0
+    value = args.steps * sample / dt / 1e6
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "impl": "reference", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "triangles": geom.triangle_count, "rays_per_step": sample,
+                       "threads": threads},
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"{sample} of the {len(rays)} incoherent rays per step"},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    from yaoray_b200 import accel, scenes
+
+    geom = scenes.traversal_scene()
+    bvh = accel.build_bvh(geom)
+    acc = accel.DeviceAccelerator(geom, bvh)
+    rays_np = scenes.incoherent_rays(seed=2 + 1000 * rank)
+    n = rays_np.shape[0]
+    rays = torch.from_numpy(rays_np).to(dev)
+    hits = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    # Algorithmic bytes per launch from the per-ray BvhTraceStats counts.
+    with torch.cuda.stream(stream):
+        st = acc.trace_stats(rays, stream=stream)
+    stream.synchronize()
+    node_tests = int(st[0].to(torch.int64).sum().item())
+    tri_tests = int(st[1].to(torch.int64).sum().item())
+    algo_bytes = 32 * node_tests + 48 * tri_tests + (32 + 16) * n
+    del st
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        acc.intersect(rays, hits=hits, stream=stream)
+    stream.synchronize()
+    acc.check()
+
+    gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[local]) \
+        if os.environ.get("CUDA_VISIBLE_DEVICES") else local
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(gpu_index) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            acc.intersect(rays, hits=hits, stream=stream)
+        end.record(stream)
+        end.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    elapsed_ms = start.elapsed_time(end)
+    acc.check()
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    per_launch_s = elapsed_ms / 1e3 / args.steps
+    value = ws * n * args.steps / (max_ms / 1e3) / 1e6
+
+    # End to end through the C ABI host path (pinned host buffers).
+    host_rays = torch.from_numpy(rays_np).pin_memory().numpy()
+    host_hits = torch.empty((n, 4), dtype=torch.float32).pin_memory().numpy()
+    for _ in range(max(1, args.warmup // 2)):
+        acc.intersect_host(host_rays, out=host_hits)
+    e_steps = max(1, args.steps // 2)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        acc.intersect_host(host_rays, out=host_hits)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = ws * n * e_steps / float(te.item()) / 1e6
+
+    peak, peak_kind = measured_peak()
+    achieved = algo_bytes / per_launch_s / 1e9
+    traffic = profiled_traffic()
+    base = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(geom, rays_np, seconds=args.cpu_seconds)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "triangles": geom.triangle_count, "bvh_nodes": int(len(bvh.nodes)),
+                       "rays_per_step_per_gpu": n, "ray_set": "incoherent: origin U[0,100]^3, direction uniform",
+                       "l2": "inputs larger than L2 (rays 256 MB + hits 128 MB + BVH), no flush",
+                       "parallelism": f"replicas x{ws}"},
+            "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": n * 32,
+                    "d2h_bytes_per_step": n * 16},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": algo_bytes,
+                         "node_tests_per_ray": round(node_tests / n, 2),
+                         "triangle_tests_per_ray": round(tri_tests / n, 2)},
+            "cpu_baseline": base,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,388 @@
+"""TEST ORACLE — Python access to (1) the C restatement of the reference's hot
+path (oracle/liboracle.so, built from yr_oracle.c) and (2) the reference
+implementation itself (oracle/_ref/libyaoray_ref.so, compiled from the
+reference sources by oracle/Makefile, with ref_shim.cpp as its C shim).
+
+Only the tests, ``__graft_entry__.smoke()`` and the benchmark's CPU-baseline
+leg use this module, and only as the checker / the timed CPU reference. The
+product (yaoray_b200, libyrcuda) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libyaoray_ref.so"
+REFERENCE_SRC = Path(os.environ.get("YAORAY_REFERENCE", "/root/reference"))
+
+P, I64, I32, U64 = C.c_void_p, C.c_int64, C.c_int32, C.c_uint64
+
+
+def build(reference: bool = True) -> None:
+    """Builds liboracle.so and, when the reference sources are present, _ref."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
+    if reference and REFERENCE_SRC.exists():
+        jobs = str(min(16, os.cpu_count() or 4))
+        subprocess.run(["make", "-s", "-C", str(HERE), f"-j{jobs}", "ref", f"REF={REFERENCE_SRC}"], check=True)
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+# --------------------------------------------------------- C restatement
+
+class YoGeometry(C.Structure):
+    _fields_ = [("positions", P), ("vertex_count", I64), ("vertex_stride", I64), ("indices", P),
+                ("index_count", I64), ("prim_first_count", P), ("primitive_count", I32), ("spheres", P),
+                ("sphere_count", I32)]
+
+
+class YoBvh(C.Structure):
+    _fields_ = [("nodes", P), ("node_count", I64), ("primitive_indices", P), ("primitive_index_count", I64),
+                ("primitives", P), ("primitive_count", I64)]
+
+
+class YoTwoLevel(C.Structure):
+    _fields_ = [("blases", P), ("blas_count", I32), ("instance_blas", P), ("instance_w2o", P),
+                ("instance_count", I32), ("tlas_nodes", P), ("tlas_node_count", I64),
+                ("tlas_primitive_indices", P), ("tlas_primitive_index_count", I64), ("tlas_primitives", P),
+                ("tlas_primitive_count", I64)]
+
+
+YO_HIT_DTYPE = np.dtype([("hit", "<i4"), ("t", "<f4"), ("triangle_index", "<i4"), ("mesh_primitive", "<i4"),
+                         ("instance", "<i4"), ("sphere", "<i4"), ("u", "<f4"), ("v", "<f4")])
+
+
+def _p(a):
+    return None if a is None or a.size == 0 else a.ctypes.data
+
+
+_ORACLE = None
+
+
+def oracle_lib() -> C.CDLL:
+    global _ORACLE
+    if _ORACLE is None:
+        if not ORACLE_SO.exists():
+            build(reference=False)
+        L = C.CDLL(str(ORACLE_SO))
+        L.yo_trace_flat.argtypes = [P, P, P, I64, P, P, P, P, C.c_int]
+        L.yo_trace_two_level.argtypes = [P, P, P, I64, P, P, P, P, C.c_int]
+        L.yo_probe.argtypes = [P, P, P, P, I64, P, P, P, P]
+        L.yo_sampler.argtypes = [C.c_int, U64, C.c_int, P, I64, C.c_int, P]
+        L.yo_seed_for_pixel_sample.argtypes = [U64, C.c_int, C.c_int, C.c_int]
+        L.yo_seed_for_pixel_sample.restype = U64
+        L.yo_rng_floats.argtypes = [U64, C.c_int, P]
+        L.yo_camera_rays.argtypes = [P, C.c_int, C.c_int, P, P, I64, P]
+        L.yo_film_accumulate.argtypes = [C.c_int, C.c_int, P, I64, P]
+        L.yo_film_accumulate.restype = U64
+        _ORACLE = L
+    return _ORACLE
+
+
+class OracleScene:
+    """Geometry + BVH arrays held for the C restatement."""
+
+    def __init__(self, geometry, accel):
+        self.g_pos = np.ascontiguousarray(geometry.positions, np.float32)
+        self.g_idx = np.ascontiguousarray(geometry.indices, np.uint32)
+        self.g_prims = np.ascontiguousarray(
+            np.stack([geometry.primitives["first_index"], geometry.primitives["index_count"]], 1)
+            if geometry.primitives.size else np.zeros((0, 2)), np.uint32)
+        sp = geometry.spheres
+        self.g_sph = np.ascontiguousarray(
+            np.concatenate([sp["center"], sp["radius"][:, None]], 1) if sp.size else np.zeros((0, 4)), np.float32)
+        self.geo = YoGeometry(_p(self.g_pos), self.g_pos.shape[0], 12, _p(self.g_idx), self.g_idx.size,
+                              _p(self.g_prims), self.g_prims.shape[0], _p(self.g_sph), self.g_sph.shape[0])
+        self._keep = []
+        self.two_level = hasattr(accel, "blases")
+        if self.two_level:
+            blases = (YoBvh * max(len(accel.blases), 1))()
+            for k, (_, _, b) in enumerate(accel.blases):
+                blases[k] = self._bvh(b)
+            self._keep.append(blases)
+            inst = accel.instances
+            self.i_blas = np.ascontiguousarray(inst["blas_index"], np.int32)
+            self.i_w2o = np.ascontiguousarray(inst["world_to_object"].reshape(-1, 16), np.float32)
+            tp = accel.tlas_primitives
+            self.t_prims = np.ascontiguousarray(
+                np.stack([tp["kind"], tp["instance"], tp["sphere"]], 1) if tp.size else np.zeros((0, 3)), np.int32)
+            t = accel.tlas
+            self.t_nodes = np.ascontiguousarray(t.nodes)
+            self.t_pi = np.ascontiguousarray(t.primitive_indices, np.int32)
+            self.tl = YoTwoLevel(C.addressof(blases), len(accel.blases), _p(self.i_blas), _p(self.i_w2o),
+                                 self.i_blas.size, _p(self.t_nodes), self.t_nodes.size, _p(self.t_pi), self.t_pi.size,
+                                 _p(self.t_prims), self.t_prims.shape[0])
+        else:
+            self.bvh = self._bvh(accel)
+
+    def _bvh(self, b) -> YoBvh:
+        nodes = np.ascontiguousarray(b.nodes)
+        pi = np.ascontiguousarray(b.primitive_indices, np.int32)
+        prims = np.ascontiguousarray(b.primitives)
+        self._keep += [nodes, pi, prims]
+        return YoBvh(_p(nodes), nodes.size, _p(pi), pi.size, _p(prims), prims.size)
+
+    def trace(self, rays: np.ndarray, threads: int = 0, stats: bool = True):
+        """Closest hit for (N, 8) rays -> (YO_HIT_DTYPE array, stats (3, N))."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        hits = np.empty(n, YO_HIT_DTYPE)
+        st = np.zeros((3, n), np.uint32) if stats else None
+        threads = threads or (os.cpu_count() or 1)
+        L = oracle_lib()
+        sp = [None, None, None] if st is None else [st[0].ctypes.data, st[1].ctypes.data, st[2].ctypes.data]
+        if self.two_level:
+            L.yo_trace_two_level(C.byref(self.geo), C.byref(self.tl), rays.ctypes.data, n, hits.ctypes.data, *sp,
+                                 threads)
+        else:
+            L.yo_trace_flat(C.byref(self.geo), C.byref(self.bvh), rays.ctypes.data, n, hits.ctypes.data, *sp,
+                            threads)
+        return hits, st
+
+    def probe(self, rays: np.ndarray, targets: np.ndarray):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        tg = np.ascontiguousarray(targets[:, :3], np.int32)
+        counts = np.zeros(n, np.int32)
+        ex = np.zeros(n, np.uint8)
+        hits = np.zeros((n, 64), YO_HIT_DTYPE)
+        oracle_lib().yo_probe(C.byref(self.geo), None if self.two_level else C.byref(self.bvh),
+                              C.byref(self.tl) if self.two_level else None, rays.ctypes.data, n, tg.ctypes.data,
+                              counts.ctypes.data, ex.ctypes.data, hits.ctypes.data)
+        return hits, counts, ex
+
+
+def oracle_sampler(kind: int, seed: int, spp: int, queries: np.ndarray, two_d: bool) -> np.ndarray:
+    q = np.ascontiguousarray(queries, np.int32).reshape(-1, 6)
+    out = np.empty(q.shape[0] * (2 if two_d else 1), np.float32)
+    oracle_lib().yo_sampler(kind, seed, spp, q.ctypes.data, q.shape[0], int(two_d), out.ctypes.data)
+    return out.reshape(-1, 2) if two_d else out
+
+
+def oracle_rng(seed: int, count: int) -> np.ndarray:
+    out = np.empty(count, np.float32)
+    oracle_lib().yo_rng_floats(seed, count, out.ctypes.data)
+    return out
+
+
+def oracle_seed_for_pixel_sample(seed: int, x: int, y: int, sample: int) -> int:
+    return int(oracle_lib().yo_seed_for_pixel_sample(seed, x, y, sample))
+
+
+def oracle_camera_rays(camera: np.ndarray, width: int, height: int, pixels: np.ndarray, samples: np.ndarray):
+    cam = np.ascontiguousarray(camera, np.float32)
+    px = np.ascontiguousarray(pixels, np.int32)
+    sm = np.ascontiguousarray(samples, np.float32)
+    out = np.empty((px.shape[0], 6), np.float32)
+    oracle_lib().yo_camera_rays(cam.ctypes.data, width, height, px.ctypes.data, sm.ctypes.data, px.shape[0],
+                                out.ctypes.data)
+    return out
+
+
+FILM_PIXEL_DTYPE = np.dtype([("sum", "<f4", 3), ("samples", "<u4"), ("luminance_mean", "<f4"),
+                             ("luminance_m2", "<f4"), ("albedo_sum", "<f4", 3), ("normal_sum", "<f4", 3),
+                             ("depth_sum", "<f4"), ("aov_samples", "<u4")])
+assert FILM_PIXEL_DTYPE.itemsize == 56
+
+
+def oracle_film(width: int, height: int, samples: np.ndarray):
+    s = np.ascontiguousarray(samples, np.float32).reshape(-1, 13)
+    px = np.zeros(width * height, FILM_PIXEL_DTYPE)
+    bad = oracle_lib().yo_film_accumulate(width, height, s.ctypes.data, s.shape[0], px.ctypes.data)
+    return px, int(bad)
+
+
+# ----------------------------------------------------- compiled reference
+
+_REF = None
+
+
+def ref_lib() -> C.CDLL:
+    global _REF
+    if _REF is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"{REF_SO} not built (needs the reference sources; see oracle/Makefile)")
+        L = C.CDLL(str(REF_SO))
+        L.yrref_last_error.restype = C.c_char_p
+        L.yrref_scene_create.restype = P
+        L.yrref_scene_create.argtypes = [P, I64, P, I64, P, C.c_int, P, C.c_int, P, P, C.c_int]
+        L.yrref_scene_destroy.argtypes = [P]
+        L.yrref_scene_build.argtypes = [P, C.c_int, C.c_int, C.c_int]
+        L.yrref_scene_is_two_level.argtypes = [P]
+        L.yrref_flat_counts.argtypes = [P, P]
+        L.yrref_flat_copy.argtypes = [P, P, P, P]
+        L.yrref_two_level_counts.argtypes = [P, P]
+        L.yrref_blas_counts.argtypes = [P, C.c_int, P]
+        L.yrref_blas_copy.argtypes = [P, C.c_int, P, P, P, P, P]
+        L.yrref_instances_copy.argtypes = [P, P, P, P, P, P]
+        L.yrref_tlas_copy.argtypes = [P, P, P, P]
+        L.yrref_trace.argtypes = [P, P, I64, P, P, P, P, P, P, P, P, P, P, P, C.c_int]
+        L.yrref_trace_count.argtypes = [P, P, I64, C.c_int, P, P, C.c_int]
+        L.yrref_trace_count.restype = I64
+        L.yrref_probe.argtypes = [P, P, I64, P, P, P, P, P, P, P, P, P, P, C.c_int]
+        L.yrref_sampler.argtypes = [C.c_int, U64, C.c_int, P, I64, C.c_int, P]
+        L.yrref_seed_for_pixel_sample.argtypes = [U64, C.c_int, C.c_int, C.c_int]
+        L.yrref_seed_for_pixel_sample.restype = U64
+        L.yrref_rng_floats.argtypes = [U64, C.c_int, P]
+        L.yrref_camera_rays.argtypes = [P, C.c_int, C.c_int, P, P, I64, P]
+        L.yrref_film_accumulate.argtypes = [C.c_int, C.c_int, P, I64, P]
+        L.yrref_film_accumulate.restype = U64
+        _REF = L
+    return _REF
+
+
+class RefScene:
+    """The reference's own RenderSceneIR geometry + RenderAcceleration."""
+
+    def __init__(self, geometry, split_method: str = "sah", max_leaf: int = 4, threads: int = 0):
+        L = ref_lib()
+        self._pos = np.ascontiguousarray(geometry.positions, np.float32)
+        self._idx = np.ascontiguousarray(geometry.indices, np.uint32)
+        prims = geometry.primitives
+        self._prims = np.ascontiguousarray(
+            np.stack([prims["first_index"], prims["index_count"]], 1) if prims.size else np.zeros((0, 2)), np.uint32)
+        sp = geometry.spheres
+        self._sph = np.ascontiguousarray(
+            np.concatenate([sp["center"], sp["radius"][:, None]], 1) if sp.size else np.zeros((0, 4)), np.float32)
+        inst = geometry.instances
+        self._ip = np.ascontiguousarray(inst["primitive"], np.int32)
+        self._im = np.ascontiguousarray(inst["object_to_world"].reshape(-1, 16), np.float32)
+        self.h = L.yrref_scene_create(_p(self._pos), self._pos.shape[0], _p(self._idx), self._idx.size,
+                                      _p(self._prims), self._prims.shape[0], _p(self._sph), self._sph.shape[0],
+                                      _p(self._ip), _p(self._im), self._ip.size)
+        self.errors = L.yrref_scene_build(self.h, 1 if split_method == "median" else 0, max_leaf, threads)
+        self.error = L.yrref_last_error().decode() if self.errors else ""
+        self.two_level = bool(L.yrref_scene_is_two_level(self.h))
+
+    def __del__(self):
+        try:
+            ref_lib().yrref_scene_destroy(self.h)
+        except Exception:
+            pass
+
+    @staticmethod
+    def _bvh_arrays(counts):
+        from yaoray_b200._lib import BVH_PRIM_DTYPE, NODE_DTYPE
+        return (np.zeros(counts[0], NODE_DTYPE), np.zeros(counts[1], np.int32), np.zeros(counts[2], BVH_PRIM_DTYPE))
+
+    def flat_bvh(self):
+        """(nodes, primitive_indices, primitives, max_depth) of the flat BVH."""
+        L = ref_lib()
+        c = np.zeros(4, np.int64)
+        L.yrref_flat_counts(self.h, c.ctypes.data)
+        nodes, pi, prims = self._bvh_arrays(c)
+        L.yrref_flat_copy(self.h, _p(nodes), _p(pi), _p(prims))
+        return nodes, pi, prims, int(c[3])
+
+    def two_level_bvh(self):
+        """dict with blases, instances and tlas arrays of the TwoLevelBvh."""
+        from yaoray_b200._lib import NODE_DTYPE
+        L = ref_lib()
+        c = np.zeros(6, np.int64)
+        L.yrref_two_level_counts(self.h, c.ctypes.data)
+        blases = []
+        for b in range(int(c[0])):
+            bc = np.zeros(4, np.int64)
+            L.yrref_blas_counts(self.h, b, bc.ctypes.data)
+            nodes, pi, prims = self._bvh_arrays(bc)
+            bounds = np.zeros(6, np.float32)
+            mp = np.zeros(1, np.int32)
+            L.yrref_blas_copy(self.h, b, _p(nodes), _p(pi), _p(prims), bounds.ctypes.data, mp.ctypes.data)
+            blases.append((int(mp[0]), bounds.reshape(2, 3), nodes, pi, prims, int(bc[3])))
+        n = int(c[1])
+        ip = np.zeros(n, np.int32)
+        ib = np.zeros(n, np.int32)
+        o2w = np.zeros((n, 16), np.float32)
+        w2o = np.zeros((n, 16), np.float32)
+        wb = np.zeros((n, 6), np.float32)
+        if n:
+            L.yrref_instances_copy(self.h, ip.ctypes.data, ib.ctypes.data, o2w.ctypes.data, w2o.ctypes.data,
+                                   wb.ctypes.data)
+        tn = np.zeros(int(c[2]), NODE_DTYPE)
+        tpi = np.zeros(int(c[3]), np.int32)
+        tpr = np.zeros((int(c[4]), 3), np.int32)
+        L.yrref_tlas_copy(self.h, _p(tn), _p(tpi), _p(tpr))
+        return {"blases": blases, "instance_primitive": ip, "instance_blas": ib, "object_to_world": o2w,
+                "world_to_object": w2o, "world_bounds": wb, "tlas_nodes": tn, "tlas_primitive_indices": tpi,
+                "tlas_primitives": tpr, "tlas_max_depth": int(c[5])}
+
+    def trace(self, rays: np.ndarray, threads: int = 0):
+        """IntersectAcceleration over (N, 8) rays -> dict of per-ray arrays."""
+        L = ref_lib()
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        out = {k: np.empty(n, dt) for k, dt in [("t", np.float32), ("triangle_index", np.int32),
+                                                ("sphere", np.int32), ("mesh_primitive", np.int32),
+                                                ("instance", np.int32), ("u", np.float32), ("v", np.float32),
+                                                ("hit", np.uint8), ("node_tests", np.uint32),
+                                                ("triangle_tests", np.uint32), ("sphere_tests", np.uint32)]}
+        L.yrref_trace(self.h, rays.ctypes.data, n, *[out[k].ctypes.data for k in
+                      ["t", "triangle_index", "sphere", "mesh_primitive", "instance", "u", "v", "hit",
+                       "node_tests", "triangle_tests", "sphere_tests"]], threads)
+        return out
+
+    def trace_count(self, rays: np.ndarray, any_hit: bool, threads: int = 0, t_out=None, id_out=None) -> int:
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        return int(ref_lib().yrref_trace_count(self.h, rays.ctypes.data, rays.shape[0], int(any_hit),
+                                               _p(t_out), _p(id_out), threads))
+
+    def probe(self, rays: np.ndarray, targets: np.ndarray, threads: int = 1):
+        L = ref_lib()
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        tp = np.ascontiguousarray(targets[:, 0], np.int32)
+        ti = np.ascontiguousarray(targets[:, 1], np.int32)
+        ts = np.ascontiguousarray(targets[:, 2], np.int32)
+        counts = np.zeros(n, np.int32)
+        ex = np.zeros(n, np.uint8)
+        t = np.zeros((n, 64), np.float32)
+        tri = np.full((n, 64), -1, np.int32)
+        inst = np.full((n, 64), -1, np.int32)
+        u = np.zeros((n, 64), np.float32)
+        v = np.zeros((n, 64), np.float32)
+        L.yrref_probe(self.h, rays.ctypes.data, n, tp.ctypes.data, ti.ctypes.data, ts.ctypes.data, counts.ctypes.data,
+                      ex.ctypes.data, t.ctypes.data, tri.ctypes.data, inst.ctypes.data, u.ctypes.data, v.ctypes.data,
+                      threads)
+        return {"count": counts, "exhausted": ex, "t": t, "triangle_index": tri, "instance": inst, "u": u, "v": v}
+
+
+def ref_sampler(kind: int, seed: int, spp: int, queries: np.ndarray, two_d: bool) -> np.ndarray:
+    q = np.ascontiguousarray(queries, np.int32).reshape(-1, 6)
+    out = np.empty(q.shape[0] * (2 if two_d else 1), np.float32)
+    ref_lib().yrref_sampler(kind, seed, spp, q.ctypes.data, q.shape[0], int(two_d), out.ctypes.data)
+    return out.reshape(-1, 2) if two_d else out
+
+
+def ref_rng(seed: int, count: int) -> np.ndarray:
+    out = np.empty(count, np.float32)
+    ref_lib().yrref_rng_floats(seed, count, out.ctypes.data)
+    return out
+
+
+def ref_seed_for_pixel_sample(seed: int, x: int, y: int, sample: int) -> int:
+    return int(ref_lib().yrref_seed_for_pixel_sample(seed, x, y, sample))
+
+
+def ref_camera_rays(camera, width, height, pixels, samples):
+    cam = np.ascontiguousarray(camera, np.float32)
+    px = np.ascontiguousarray(pixels, np.int32)
+    sm = np.ascontiguousarray(samples, np.float32)
+    out = np.empty((px.shape[0], 6), np.float32)
+    ref_lib().yrref_camera_rays(cam.ctypes.data, width, height, px.ctypes.data, sm.ctypes.data, px.shape[0],
+                                out.ctypes.data)
+    return out
+
+
+def ref_film(width: int, height: int, samples: np.ndarray):
+    s = np.ascontiguousarray(samples, np.float32).reshape(-1, 13)
+    px = np.zeros(width * height, FILM_PIXEL_DTYPE)
+    bad = ref_lib().yrref_film_accumulate(width, height, s.ctypes.data, s.shape[0], px.ctypes.data)
+    return px, int(bad)

@@ -1,0 +1,607 @@
+// Device accelerator: converts the reference's RenderBvh / TwoLevelBvh arrays
+// into the traversal layout of device_layout.cuh, uploads it, and runs the
+// trace kernels for device- or host-resident ray batches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "device_layout.cuh"
+#include "trace_kernels.hpp"
+#include "yrc_internal.hpp"
+
+namespace yrc {
+namespace {
+
+constexpr int32_t kUnassigned = INT32_MIN + 1;
+
+struct Layout {
+    std::vector<NodePair> pairs;
+    std::vector<Record> records;
+    std::vector<Instance> instances;
+};
+
+Record SkipRecord(int32_t kind) {
+    Record r{};
+    r.v1.w = IntBits(kind << 1);
+    return r;
+}
+
+// Builds the traversal records for one BVH. `slot_record` converts one
+// primitive slot (an index into primitive_indices) into a Record.
+template <typename SlotFn>
+bool AddBvh(const yrc_bvh_node* nodes, int64_t node_count, SlotFn slot_record, Layout& out, int32_t& root_ref,
+            float root_lo[3], float root_hi[3], int32_t& depth, std::string& error) {
+    root_ref = kAbsentRef;
+    depth = 0;
+    if (node_count <= 0) {
+        for (int a = 0; a < 3; ++a) root_lo[a] = root_hi[a] = 0.0f;
+        return true;
+    }
+    for (int a = 0; a < 3; ++a) {
+        root_lo[a] = nodes[0].bounds_min[a];
+        root_hi[a] = nodes[0].bounds_max[a];
+    }
+    const size_t n = static_cast<size_t>(node_count);
+    std::vector<int32_t> ref(n, kUnassigned);
+    std::vector<int32_t> sub_depth(n, 0);
+    std::vector<uint8_t> color(n, 0);  // 0 white, 1 on the DFS path, 2 done
+    struct Frame {
+        int32_t node;
+        bool expanded;
+    };
+    std::vector<Frame> stack;
+    stack.push_back({0, false});
+    auto child_of = [&](int32_t i, int which) -> int32_t {
+        const int64_t c = which == 0 ? static_cast<int64_t>(i) + 1 : nodes[i].payload_offset;
+        return (c >= 0 && c < node_count) ? static_cast<int32_t>(c) : -1;
+    };
+    while (!stack.empty()) {
+        Frame& f = stack.back();
+        const int32_t i = f.node;
+        if (!f.expanded) {
+            if (color[i] == 2) {
+                stack.pop_back();
+                continue;
+            }
+            color[i] = 1;
+            f.expanded = true;
+            const yrc_bvh_node& node = nodes[i];
+            if (node.primitive_count > 0) {
+                const int32_t first = static_cast<int32_t>(out.records.size());
+                for (int32_t k = 0; k < node.primitive_count; ++k) {
+                    out.records.push_back(slot_record(static_cast<int64_t>(node.payload_offset) + k));
+                }
+                Record& last = out.records.back();
+                last.v1.w = IntBits(FloatBits(last.v1.w) | kRecLast);
+                ref[i] = ~first;
+                color[i] = 2;
+                stack.pop_back();
+                continue;
+            }
+            ref[i] = static_cast<int32_t>(out.pairs.size());
+            out.pairs.push_back(NodePair{});
+            for (int which = 1; which >= 0; --which) {  // left ends on top
+                const int32_t c = child_of(i, which);
+                if (c < 0) continue;
+                if (color[c] == 1) {
+                    error = "BVH node graph contains a cycle";
+                    return false;
+                }
+                if (color[c] == 0) stack.push_back({c, false});
+            }
+            continue;
+        }
+        // Post-order: both children have refs now.
+        const int32_t l = child_of(i, 0);
+        const int32_t r = child_of(i, 1);
+        NodePair& p = out.pairs[static_cast<size_t>(ref[i])];
+        const float* L = l >= 0 ? nodes[l].bounds_min : nullptr;
+        const float* R = r >= 0 ? nodes[r].bounds_min : nullptr;
+        float lb[6] = {0, 0, 0, 0, 0, 0}, rb[6] = {0, 0, 0, 0, 0, 0};
+        if (L) std::memcpy(lb, L, sizeof(lb));
+        if (R) std::memcpy(rb, R, sizeof(rb));
+        p.a = make_float4(lb[0], lb[1], lb[2], lb[3]);
+        p.b = make_float4(lb[4], lb[5], rb[0], rb[1]);
+        p.c = make_float4(rb[2], rb[3], rb[4], rb[5]);
+        p.d = make_int4(l >= 0 ? ref[l] : kAbsentRef, r >= 0 ? ref[r] : kAbsentRef, 0, 0);
+        int32_t d = 0;
+        if (l >= 0) d = std::max(d, sub_depth[l]);
+        if (r >= 0) d = std::max(d, sub_depth[r]);
+        sub_depth[i] = d + 1;
+        color[i] = 2;
+        stack.pop_back();
+    }
+    root_ref = ref[0];
+    depth = sub_depth[0];
+    return true;
+}
+
+Record TriangleOrSphereRecord(const yrc_geometry& g, const yrc_bvh_view& bvh, int64_t slot) {
+    if (slot < 0 || slot >= bvh.primitive_index_count) return SkipRecord(kRecSkip);
+    const int32_t pi = bvh.primitive_indices[slot];
+    if (pi < 0 || pi >= bvh.primitive_count) return SkipRecord(kRecSkip);
+    const yrc_bvh_primitive& p = bvh.primitives[pi];
+    Record rec{};
+    if (p.kind == 0) {
+        if (p.mesh_primitive < 0 || p.mesh_primitive >= g.primitive_count || p.local_triangle < 0) {
+            return SkipRecord(kRecSkipCountTriangle);
+        }
+        const uint32_t base =
+            g.primitives[p.mesh_primitive].first_index + static_cast<uint32_t>(p.local_triangle) * 3u;
+        if (static_cast<uint64_t>(base) + 2 >= static_cast<uint64_t>(g.index_count)) {
+            return SkipRecord(kRecSkipCountTriangle);
+        }
+        const uint32_t i0 = g.indices[base], i1 = g.indices[base + 1], i2 = g.indices[base + 2];
+        const uint64_t nv = static_cast<uint64_t>(g.vertex_count);
+        if (i0 >= nv || i1 >= nv || i2 >= nv) return SkipRecord(kRecSkipCountTriangle);
+        const float* a = VertexPosition(g, i0);
+        const float* b = VertexPosition(g, i1);
+        const float* c = VertexPosition(g, i2);
+        rec.v0 = make_float4(a[0], a[1], a[2], IntBits(p.flat_triangle_index));
+        rec.v1 = make_float4(b[0] - a[0], b[1] - a[1], b[2] - a[2], IntBits(kRecTriangle << 1));
+        rec.v2 = make_float4(c[0] - a[0], c[1] - a[1], c[2] - a[2], IntBits(p.mesh_primitive));
+        return rec;
+    }
+    if (p.sphere < 0 || p.sphere >= g.sphere_count) return SkipRecord(kRecSkipCountSphere);
+    const yrc_sphere& s = g.spheres[p.sphere];
+    rec.v0 = make_float4(s.center[0], s.center[1], s.center[2], IntBits(p.sphere));
+    rec.v1 = make_float4(s.radius, 0.0f, 0.0f, IntBits(kRecSphere << 1));
+    rec.v2 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    return rec;
+}
+
+Record SphereRecord(const yrc_geometry& g, int32_t sphere) {
+    if (sphere < 0 || sphere >= g.sphere_count) return SkipRecord(kRecSkipCountSphere);
+    const yrc_sphere& s = g.spheres[sphere];
+    Record rec{};
+    rec.v0 = make_float4(s.center[0], s.center[1], s.center[2], IntBits(sphere));
+    rec.v1 = make_float4(s.radius, 0.0f, 0.0f, IntBits(kRecSphere << 1));
+    return rec;
+}
+
+bool CheckGeometry(const yrc_geometry* g, std::string& error) {
+    if (!g) {
+        error = "null geometry";
+        return false;
+    }
+    if (g->vertex_count < 0 || g->index_count < 0 || g->primitive_count < 0 || g->sphere_count < 0 ||
+        g->instance_count < 0) {
+        error = "negative geometry count";
+        return false;
+    }
+    if ((g->vertex_count > 0 && !g->positions) || (g->index_count > 0 && !g->indices) ||
+        (g->primitive_count > 0 && !g->primitives) || (g->sphere_count > 0 && !g->spheres) ||
+        (g->instance_count > 0 && !g->instances)) {
+        error = "null geometry array with a non-zero count";
+        return false;
+    }
+    if (g->vertex_count > 0 && g->vertex_stride < 12) {
+        error = "vertex_stride must be at least 12 bytes";
+        return false;
+    }
+    return true;
+}
+
+bool CheckBvh(const yrc_bvh_view* b, std::string& error) {
+    if (!b) {
+        error = "null BVH view";
+        return false;
+    }
+    if (b->node_count < 0 || b->primitive_index_count < 0 || b->primitive_count < 0) {
+        error = "negative BVH count";
+        return false;
+    }
+    if ((b->node_count > 0 && !b->nodes) || (b->primitive_index_count > 0 && !b->primitive_indices) ||
+        (b->primitive_count > 0 && !b->primitives)) {
+        error = "null BVH array with a non-zero count";
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+// Host pipeline resources for yrc_trace_host (allocated on first use).
+struct HostPipeline {
+    static constexpr int kStreams = 3;
+    int64_t chunk = 0;
+    cudaStream_t streams[kStreams] = {};
+    void* d_rays[kStreams] = {};
+    void* d_out[kStreams] = {};
+    int32_t* d_inst[kStreams] = {};
+    uint32_t* d_stats[kStreams] = {};
+    unsigned long long* d_counters = nullptr;
+};
+
+}  // namespace yrc
+
+struct yrc_accel {
+    int device = 0;
+    int sm_count = 148;
+    yrc::NodePair* d_pairs = nullptr;
+    yrc::Record* d_records = nullptr;
+    yrc::Instance* d_instances = nullptr;
+    unsigned long long* d_counter = nullptr;
+    int* d_error = nullptr;
+    yrc::AccelParams params{};
+    int64_t device_bytes = 0;
+    yrc::HostPipeline pipe;
+    std::mutex mutex;
+};
+
+namespace yrc {
+namespace {
+
+yrc_status CudaFail(cudaError_t err, const char* what) {
+    return Fail(err == cudaErrorMemoryAllocation ? YRC_ERR_OUT_OF_MEMORY : YRC_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+template <typename T>
+cudaError_t Upload(T** dst, const std::vector<T>& src, int64_t& bytes) {
+    const size_t n = std::max<size_t>(src.size(), 1);
+    cudaError_t err = cudaMalloc(reinterpret_cast<void**>(dst), n * sizeof(T));
+    if (err != cudaSuccess) return err;
+    bytes += static_cast<int64_t>(n * sizeof(T));
+    if (!src.empty()) err = cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return err;
+}
+
+void FreeAccel(yrc_accel* a) {
+    if (!a) return;
+    cudaSetDevice(a->device);
+    cudaFree(a->d_pairs);
+    cudaFree(a->d_records);
+    cudaFree(a->d_instances);
+    cudaFree(a->d_counter);
+    cudaFree(a->d_error);
+    HostPipeline& p = a->pipe;
+    for (int s = 0; s < HostPipeline::kStreams; ++s) {
+        cudaFree(p.d_rays[s]);
+        cudaFree(p.d_out[s]);
+        cudaFree(p.d_inst[s]);
+        cudaFree(p.d_stats[s]);
+        if (p.streams[s]) cudaStreamDestroy(p.streams[s]);
+    }
+    cudaFree(p.d_counters);
+    delete a;
+}
+
+yrc_status Finalize(Layout& layout, int32_t root_ref, const float lo[3], const float hi[3], int32_t two_level,
+                    int32_t depth, yrc_accel** out) {
+    if (depth + 1 > kMaxTraceStack) {
+        return Fail(YRC_ERR_UNSUPPORTED, "BVH too deep for the device traversal stack (" + std::to_string(depth) +
+                                             " levels, limit " + std::to_string(kMaxTraceStack - 1) + ")");
+    }
+    auto* a = new (std::nothrow) yrc_accel();
+    if (!a) return Fail(YRC_ERR_OUT_OF_MEMORY, "host allocation failed");
+    cudaError_t err = cudaGetDevice(&a->device);
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&a->sm_count, cudaDevAttrMultiProcessorCount, a->device);
+    if (err == cudaSuccess) err = Upload(&a->d_pairs, layout.pairs, a->device_bytes);
+    if (err == cudaSuccess) err = Upload(&a->d_records, layout.records, a->device_bytes);
+    if (err == cudaSuccess) err = Upload(&a->d_instances, layout.instances, a->device_bytes);
+    if (err == cudaSuccess) err = cudaMalloc(reinterpret_cast<void**>(&a->d_counter), sizeof(unsigned long long));
+    if (err == cudaSuccess) err = cudaMalloc(reinterpret_cast<void**>(&a->d_error), sizeof(int));
+    if (err == cudaSuccess) err = cudaMemset(a->d_error, 0, sizeof(int));
+    if (err != cudaSuccess) {
+        FreeAccel(a);
+        return CudaFail(err, "accelerator upload");
+    }
+    AccelParams& p = a->params;
+    p.pairs = a->d_pairs;
+    p.records = a->d_records;
+    p.instances = a->d_instances;
+    for (int k = 0; k < 3; ++k) {
+        p.root_lo[k] = lo[k];
+        p.root_hi[k] = hi[k];
+    }
+    p.root_ref = root_ref;
+    p.two_level = two_level;
+    p.stack_limit = depth + 1;
+    *out = a;
+    return Ok();
+}
+
+yrc_status LaunchInternal(yrc_accel* a, const yrc_ray* rays, int64_t count, int32_t flags, yrc_hit* hits,
+                          int32_t* instances, uint8_t* occluded, uint32_t* nt, uint32_t* tt, uint32_t* st,
+                          unsigned long long* counter, cudaStream_t stream) {
+    if (count <= 0) return Ok();
+    TraceArgs args{};
+    args.accel = a->params;
+    args.rays = reinterpret_cast<const float4*>(rays);
+    args.count = count;
+    args.hits = hits;
+    args.instances = instances;
+    args.occluded = occluded;
+    args.node_tests = nt;
+    args.triangle_tests = tt;
+    args.sphere_tests = st;
+    args.counter = counter;
+    args.error = a->d_error;
+    cudaError_t err = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
+    if (err != cudaSuccess) return CudaFail(err, "trace counter reset");
+    const bool any = (flags & YRC_TRACE_ANY) != 0;
+    const bool stats = (flags & YRC_TRACE_STATS) != 0;
+    err = LaunchTrace(args, any, stats, stream, a->sm_count);
+    if (err != cudaSuccess) return CudaFail(err, "trace launch");
+    return Ok();
+}
+
+}  // namespace
+
+yrc_status CheckDeviceError(yrc_accel* a) {
+    int status = 0;
+    cudaError_t err = cudaMemcpy(&status, a->d_error, sizeof(int), cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return CudaFail(err, "reading the device status word");
+    if (status != 0) {
+        cudaMemset(a->d_error, 0, sizeof(int));
+        if (status & kTraceErrorStackOverflow) return Fail(YRC_ERR_DEVICE_FAULT, "traversal stack overflow");
+        return Fail(YRC_ERR_DEVICE_FAULT, "device status word " + std::to_string(status));
+    }
+    return Ok();
+}
+
+}  // namespace yrc
+
+extern "C" {
+
+yrc_status yrc_accel_create_flat(const yrc_geometry* geometry, const yrc_bvh_view* bvh, yrc_accel** out) {
+    using namespace yrc;
+    if (!out) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_create_flat: null output");
+    *out = nullptr;
+    std::string error;
+    if (!CheckGeometry(geometry, error) || !CheckBvh(bvh, error)) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_create_flat: " + error);
+    }
+    Layout layout;
+    int32_t root = kAbsentRef, depth = 0;
+    float lo[3], hi[3];
+    try {
+        auto slot = [&](int64_t s) { return TriangleOrSphereRecord(*geometry, *bvh, s); };
+        if (!AddBvh(bvh->nodes, bvh->node_count, slot, layout, root, lo, hi, depth, error)) {
+            return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_create_flat: " + error);
+        }
+    } catch (const std::bad_alloc&) {
+        return Fail(YRC_ERR_OUT_OF_MEMORY, "yrc_accel_create_flat: host allocation failed");
+    }
+    return Finalize(layout, root, lo, hi, 0, depth, out);
+}
+
+yrc_status yrc_accel_create_two_level(const yrc_geometry* geometry, const yrc_two_level_view* tl, yrc_accel** out) {
+    using namespace yrc;
+    if (!out) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_create_two_level: null output");
+    *out = nullptr;
+    std::string error;
+    if (!CheckGeometry(geometry, error)) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_create_two_level: " + error);
+    if (!tl || tl->blas_count < 0 || tl->instance_count < 0 || (tl->blas_count > 0 && !tl->blases) ||
+        (tl->instance_count > 0 && !tl->instances) || (tl->tlas_node_count > 0 && !tl->tlas_nodes) ||
+        (tl->tlas_primitive_index_count > 0 && !tl->tlas_primitive_indices) ||
+        (tl->tlas_primitive_count > 0 && !tl->tlas_primitives)) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_create_two_level: invalid two-level view");
+    }
+    Layout layout;
+    int32_t tlas_root = kAbsentRef, tlas_depth = 0;
+    float lo[3], hi[3];
+    try {
+        // BLASes first so their refs are known when instances are written.
+        std::vector<int32_t> blas_root(static_cast<size_t>(tl->blas_count), kAbsentRef);
+        std::vector<std::array<float, 6>> blas_box(static_cast<size_t>(tl->blas_count));
+        int32_t blas_depth = 0;
+        for (int32_t b = 0; b < tl->blas_count; ++b) {
+            const yrc_bvh_view& v = tl->blases[b].bvh;
+            if (!CheckBvh(&v, error)) return Fail(YRC_ERR_INVALID_ARGUMENT, "BLAS " + std::to_string(b) + ": " + error);
+            auto slot = [&](int64_t s) { return TriangleOrSphereRecord(*geometry, v, s); };
+            float blo[3], bhi[3];
+            int32_t d = 0;
+            if (!AddBvh(v.nodes, v.node_count, slot, layout, blas_root[b], blo, bhi, d, error)) {
+                return Fail(YRC_ERR_INVALID_ARGUMENT, "BLAS " + std::to_string(b) + ": " + error);
+            }
+            blas_depth = std::max(blas_depth, d);
+            blas_box[b] = {blo[0], blo[1], blo[2], bhi[0], bhi[1], bhi[2]};
+        }
+        layout.instances.resize(static_cast<size_t>(tl->instance_count));
+        for (int32_t i = 0; i < tl->instance_count; ++i) {
+            const yrc_prepared_instance& src = tl->instances[i];
+            Instance& dst = layout.instances[static_cast<size_t>(i)];
+            const float* m = src.world_to_object;
+            dst.row0 = make_float4(m[0], m[4], m[8], m[12]);
+            dst.row1 = make_float4(m[1], m[5], m[9], m[13]);
+            dst.row2 = make_float4(m[2], m[6], m[10], m[14]);
+            const bool valid = src.blas_index >= 0 && src.blas_index < tl->blas_count;
+            const std::array<float, 6> box = valid ? blas_box[src.blas_index] : std::array<float, 6>{};
+            dst.box_a = make_float4(box[0], box[1], box[2], box[3]);
+            dst.box_b = make_float4(box[4], box[5], IntBits(valid ? blas_root[src.blas_index] : kAbsentRef),
+                                    0.0f);
+        }
+        auto tlas_slot = [&](int64_t s) -> Record {
+            if (s < 0 || s >= tl->tlas_primitive_index_count) return SkipRecord(kRecSkip);
+            const int32_t pi = tl->tlas_primitive_indices[s];
+            if (pi < 0 || pi >= tl->tlas_primitive_count) return SkipRecord(kRecSkip);
+            const yrc_tlas_primitive& p = tl->tlas_primitives[pi];
+            if (p.kind == 1) return SphereRecord(*geometry, p.sphere);
+            if (p.instance < 0 || p.instance >= tl->instance_count) return SkipRecord(kRecSkip);
+            const int32_t b = tl->instances[p.instance].blas_index;
+            if (b < 0 || b >= tl->blas_count) return SkipRecord(kRecSkip);
+            Record r{};
+            r.v0 = make_float4(0.0f, 0.0f, 0.0f, IntBits(p.instance));
+            r.v1 = make_float4(0.0f, 0.0f, 0.0f, IntBits(kRecInstance << 1));
+            return r;
+        };
+        if (!AddBvh(tl->tlas_nodes, tl->tlas_node_count, tlas_slot, layout, tlas_root, lo, hi, tlas_depth, error)) {
+            return Fail(YRC_ERR_INVALID_ARGUMENT, "TLAS: " + error);
+        }
+        tlas_depth += blas_depth;
+    } catch (const std::bad_alloc&) {
+        return Fail(YRC_ERR_OUT_OF_MEMORY, "yrc_accel_create_two_level: host allocation failed");
+    }
+    return Finalize(layout, tlas_root, lo, hi, 1, tlas_depth, out);
+}
+
+void yrc_accel_destroy(yrc_accel* accel) { yrc::FreeAccel(accel); }
+
+int64_t yrc_accel_device_bytes(const yrc_accel* accel) { return accel ? accel->device_bytes : 0; }
+
+yrc_status yrc_trace_device(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags, yrc_hit* hits,
+                            int32_t* instances, uint8_t* occluded, void* stream) {
+    using namespace yrc;
+    if (!accel || count < 0 || (count > 0 && !rays)) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_trace_device: bad argument");
+    const bool any = (flags & YRC_TRACE_ANY) != 0;
+    if (count > 0 && ((any && !occluded) || (!any && !hits))) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_trace_device: missing output buffer");
+    }
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    cudaSetDevice(accel->device);
+    return LaunchInternal(accel, rays, count, flags & ~YRC_TRACE_STATS, hits, instances, occluded, nullptr, nullptr,
+                          nullptr, accel->d_counter, static_cast<cudaStream_t>(stream));
+}
+
+yrc_status yrc_trace_stats_device(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags,
+                                  uint32_t* node_tests, uint32_t* triangle_tests, uint32_t* sphere_tests,
+                                  void* stream) {
+    using namespace yrc;
+    if (!accel || count < 0 || (count > 0 && !rays)) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_trace_stats_device: bad argument");
+    }
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    cudaSetDevice(accel->device);
+    const bool any = (flags & YRC_TRACE_ANY) != 0;
+    // The stats kernel still writes its primary output; route it to scratch.
+    void* scratch = nullptr;
+    cudaError_t err = cudaMallocAsync(&scratch, static_cast<size_t>(std::max<int64_t>(count, 1)) * (any ? 1 : 16),
+                                      static_cast<cudaStream_t>(stream));
+    if (err != cudaSuccess) return CudaFail(err, "stats scratch");
+    yrc_status s = LaunchInternal(accel, rays, count, flags | YRC_TRACE_STATS, any ? nullptr : static_cast<yrc_hit*>(scratch),
+                                  nullptr, any ? static_cast<uint8_t*>(scratch) : nullptr, node_tests, triangle_tests,
+                                  sphere_tests, accel->d_counter, static_cast<cudaStream_t>(stream));
+    cudaFreeAsync(scratch, static_cast<cudaStream_t>(stream));
+    return s;
+}
+
+yrc_status yrc_trace_host(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags, yrc_hit* hits,
+                          int32_t* instances, uint8_t* occluded, yrc_trace_stats* stats) {
+    using namespace yrc;
+    if (!accel || count < 0 || (count > 0 && !rays)) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_trace_host: bad argument");
+    const bool any = (flags & YRC_TRACE_ANY) != 0;
+    const bool want_stats = (flags & YRC_TRACE_STATS) != 0 && stats != nullptr;
+    if (count > 0 && ((any && !occluded) || (!any && !hits))) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_trace_host: missing output buffer");
+    }
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    cudaSetDevice(accel->device);
+    HostPipeline& p = accel->pipe;
+    cudaError_t err = cudaSuccess;
+    if (p.chunk == 0) {
+        p.chunk = int64_t{1} << 21;  // 2M rays = 64 MiB of rays per chunk
+        err = cudaMalloc(reinterpret_cast<void**>(&p.d_counters), sizeof(unsigned long long) * HostPipeline::kStreams);
+        for (int s = 0; s < HostPipeline::kStreams && err == cudaSuccess; ++s) {
+            err = cudaStreamCreateWithFlags(&p.streams[s], cudaStreamNonBlocking);
+            if (err == cudaSuccess) err = cudaMalloc(&p.d_rays[s], static_cast<size_t>(p.chunk) * sizeof(yrc_ray));
+            if (err == cudaSuccess) err = cudaMalloc(&p.d_out[s], static_cast<size_t>(p.chunk) * sizeof(yrc_hit));
+            if (err == cudaSuccess)
+                err = cudaMalloc(reinterpret_cast<void**>(&p.d_inst[s]), static_cast<size_t>(p.chunk) * sizeof(int32_t));
+            if (err == cudaSuccess)
+                err = cudaMalloc(reinterpret_cast<void**>(&p.d_stats[s]), static_cast<size_t>(p.chunk) * 3 * sizeof(uint32_t));
+        }
+        if (err != cudaSuccess) {
+            p.chunk = 0;
+            return CudaFail(err, "yrc_trace_host pipeline setup");
+        }
+    }
+    std::vector<uint32_t> host_stats;
+    if (want_stats) host_stats.resize(static_cast<size_t>(std::min(count, p.chunk)) * 3);
+    yrc_trace_stats total{0, 0, 0, static_cast<uint64_t>(count)};
+    int64_t done = 0;
+    int chunk_id = 0;
+    while (done < count && err == cudaSuccess) {
+        const int s = chunk_id % HostPipeline::kStreams;
+        const int64_t n = std::min(p.chunk, count - done);
+        cudaStream_t st = p.streams[s];
+        if (want_stats) err = cudaStreamSynchronize(st);  // host_stats buffer is reused per chunk
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(p.d_rays[s], rays + done, static_cast<size_t>(n) * sizeof(yrc_ray),
+                                  cudaMemcpyHostToDevice, st);
+        if (err != cudaSuccess) break;
+        uint32_t* ds = p.d_stats[s];
+        yrc_status ls = LaunchInternal(accel, static_cast<const yrc_ray*>(p.d_rays[s]), n,
+                                       want_stats ? flags : (flags & ~YRC_TRACE_STATS),
+                                       any ? nullptr : static_cast<yrc_hit*>(p.d_out[s]), instances ? p.d_inst[s] : nullptr,
+                                       any ? static_cast<uint8_t*>(p.d_out[s]) : nullptr, want_stats ? ds : nullptr,
+                                       want_stats ? ds + n : nullptr, want_stats ? ds + 2 * n : nullptr,
+                                       p.d_counters + s, st);
+        if (ls != YRC_OK) return ls;
+        if (any) {
+            err = cudaMemcpyAsync(occluded + done, p.d_out[s], static_cast<size_t>(n), cudaMemcpyDeviceToHost, st);
+        } else {
+            err = cudaMemcpyAsync(hits + done, p.d_out[s], static_cast<size_t>(n) * sizeof(yrc_hit),
+                                  cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess && instances)
+                err = cudaMemcpyAsync(instances + done, p.d_inst[s], static_cast<size_t>(n) * sizeof(int32_t),
+                                      cudaMemcpyDeviceToHost, st);
+        }
+        if (want_stats && err == cudaSuccess) {
+            err = cudaMemcpyAsync(host_stats.data(), ds, static_cast<size_t>(n) * 3 * sizeof(uint32_t),
+                                  cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+            for (int64_t i = 0; i < n && err == cudaSuccess; ++i) {
+                total.node_tests += host_stats[static_cast<size_t>(i)];
+                total.triangle_tests += host_stats[static_cast<size_t>(n + i)];
+                total.sphere_tests += host_stats[static_cast<size_t>(2 * n + i)];
+            }
+        }
+        done += n;
+        ++chunk_id;
+    }
+    for (int s = 0; s < HostPipeline::kStreams; ++s) {
+        const cudaError_t e2 = cudaStreamSynchronize(p.streams[s]);
+        if (err == cudaSuccess) err = e2;
+    }
+    if (err != cudaSuccess) return CudaFail(err, "yrc_trace_host");
+    if (want_stats) *stats = total;
+    return CheckDeviceError(accel);
+}
+
+yrc_status yrc_probe_device(yrc_accel* accel, const yrc_ray* rays, const yrc_probe_target* targets, int64_t count,
+                            yrc_hit* hits, int32_t* instances, int32_t* counts, uint8_t* exhausted, void* stream) {
+    using namespace yrc;
+    if (!accel || count < 0 || (count > 0 && (!rays || !targets || !hits || !counts || !exhausted))) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_probe_device: bad argument");
+    }
+    if (count == 0) return Ok();
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    cudaSetDevice(accel->device);
+    ProbeArgs args{};
+    args.accel = accel->params;
+    args.rays = reinterpret_cast<const float4*>(rays);
+    args.targets = targets;
+    args.count = count;
+    args.hits = hits;
+    args.instances = instances;
+    args.counts = counts;
+    args.exhausted = exhausted;
+    args.error = accel->d_error;
+    const cudaError_t err = LaunchProbe(args, static_cast<cudaStream_t>(stream), accel->sm_count);
+    if (err != cudaSuccess) return CudaFail(err, "probe launch");
+    return Ok();
+}
+
+yrc_status yrc_accel_check(yrc_accel* accel) {
+    if (!accel) return yrc::Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_check: null accelerator");
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    cudaSetDevice(accel->device);
+    const cudaError_t err = cudaDeviceSynchronize();
+    if (err != cudaSuccess) return yrc::Fail(YRC_ERR_CUDA, std::string("synchronize: ") + cudaGetErrorString(err));
+    return yrc::CheckDeviceError(accel);
+}
+
+yrc_status yrc_stream_synchronize(void* stream) {
+    const cudaError_t err = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    if (err != cudaSuccess) return yrc::Fail(YRC_ERR_CUDA, std::string("stream synchronize: ") + cudaGetErrorString(err));
+    return yrc::Ok();
+}
+
+}  // extern "C"

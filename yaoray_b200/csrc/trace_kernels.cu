@@ -1,0 +1,437 @@
+// Closest-hit / any-hit / probe traversal kernels for the flat and two-level
+// BVH.
+//
+// Semantics are those of IntersectBvh (src/accel/bvh_traversal.cpp:253-345),
+// IntersectTwoLevelBvh (src/accel/two_level_bvh.cpp:365-481) and
+// IntersectAccelerationProbe (src/accel/acceleration.cpp:63-108), including
+// the exact visiting order: depth-first, both children box-tested against the
+// current nearest t, the nearer child (left on a tie) taken next and the other
+// pushed, popped entries culled when their entry t exceeds the nearest t.
+// Following the same order with the same IEEE operations makes the hit IDs and
+// t values bit-identical to the CPU reference, not merely close.
+//
+// Execution model (sm_100a):
+//  * persistent grid sized from the occupancy calculator (a multiple of the SM
+//    count); each lane owns one ray and fetches a new one as soon as its ray
+//    finishes (warp-aggregated atomicAdd on a global ray counter), checked
+//    every kSteps node visits so lanes with short rays do not idle;
+//  * traversal stack: the first kShortStack entries of each thread live in
+//    shared memory laid out [depth][thread] (bank-conflict free), deeper
+//    entries in a per-thread local array; the host picks a kernel whose
+//    total depth covers the BVH's longest root-to-leaf path;
+//  * nodes and leaf records are read with 128-bit read-only loads.
+#include "device_layout.cuh"
+#include "trace_kernels.hpp"
+
+#include <cuda_runtime.h>
+
+namespace yrc {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+struct Traversal {
+    RayPre r;        // current ray (world, or object space inside a BLAS)
+    float tmin;
+    Nearest best;    // world (flat) nearest
+    Nearest local;   // BLAS-local nearest while inside an instance
+    int32_t best_inst;
+    int32_t cur;        // node pair (>= 0) or leaf (~first record)
+    int32_t sp;
+    int32_t level;      // 0: root level (flat BVH or TLAS), 1: inside a BLAS
+    int32_t blas_base;  // stack pointer when the BLAS was entered
+    int32_t tl_resume;  // TLAS record to resume after the BLAS, -1 = none
+    int32_t cur_inst;   // instance being traversed
+    uint32_t nodes, tris, spheres;  // BvhTraceStats
+};
+
+__device__ __forceinline__ float4 Ld(const float4* p) { return __ldg(p); }
+
+template <int kTotal>
+struct StackStore {
+    static constexpr int kLocal = kTotal > kShortStack ? kTotal - kShortStack : 1;
+    int2 local[kLocal];
+
+    __device__ __forceinline__ void Put(int2* col, int sp, int2 e) {
+        if (sp < kShortStack) {
+            col[sp * kTraceBlock] = e;
+        } else {
+            local[sp - kShortStack] = e;
+        }
+    }
+    __device__ __forceinline__ int2 Get(const int2* col, int sp) const {
+        return sp < kShortStack ? col[sp * kTraceBlock] : local[sp - kShortStack];
+    }
+};
+
+// Sets the world-space origin/direction of ray i (not t_min / t_max).
+__device__ __forceinline__ void LoadWorldRay(const float4* rays, int64_t i, Traversal& s) {
+    const float4 a = Ld(rays + 2 * i);
+    const float4 b = Ld(rays + 2 * i + 1);
+    s.r.o[0] = a.x;
+    s.r.o[1] = a.y;
+    s.r.o[2] = a.z;
+    s.r.d[0] = b.x;
+    s.r.d[1] = b.y;
+    s.r.d[2] = b.z;
+    Precompute(s.r);
+}
+
+// Begins a traversal of ray i over [tmin, tmax]; returns false when the ray
+// already finished at the root (empty BVH or root box missed).
+__device__ __forceinline__ bool Begin(const AccelParams& a, const float4* rays, int64_t i, float tmin, float tmax,
+                                      Traversal& s) {
+    LoadWorldRay(rays, i, s);
+    s.tmin = tmin;
+    s.best.t = tmax;
+    s.best.id = -1;
+    s.best.prim = -1;
+    s.best.u = 0.0f;
+    s.best.v = 0.0f;
+    s.best.hit = false;
+    s.best_inst = -1;
+    s.sp = 0;
+    s.level = 0;
+    s.tl_resume = -1;
+    s.nodes = s.tris = s.spheres = 0;
+    if (a.root_ref == kAbsentRef) return false;
+    s.nodes = 1;
+    float entry;
+    if (!SlabTest(s.r, a.root_lo[0], a.root_lo[1], a.root_lo[2], a.root_hi[0], a.root_hi[1], a.root_hi[2], s.tmin,
+                  s.best.t, entry)) {
+        return false;
+    }
+    s.cur = a.root_ref;
+    return true;
+}
+
+// Pops the next live stack entry into s.cur (culled against the nearest t of
+// the current level) and closes finished BLAS traversals. Returns false when
+// the ray's traversal is complete.
+template <bool kAny, bool kTwo, int kTotal>
+__device__ __forceinline__ bool Pop(const float4* rays, int64_t ray, Traversal& s, StackStore<kTotal>& st,
+                                    const int2* col) {
+    for (;;) {
+        if (kTwo && s.level == 1 && s.sp == s.blas_base) {
+            // IntersectTwoLevelBvh accepts the BLAS hit only if strictly nearer.
+            if (s.local.hit && s.local.t < s.best.t) {
+                s.best = s.local;
+                s.best_inst = s.cur_inst;
+            }
+            s.level = 0;
+            LoadWorldRay(rays, ray, s);
+            if (kAny && s.best.hit) return false;
+            if (s.tl_resume >= 0) {
+                s.cur = ~s.tl_resume;
+                return true;
+            }
+            continue;
+        }
+        if (s.sp == 0) return false;
+        --s.sp;
+        const int2 e = st.Get(col, s.sp);
+        const float limit = (kTwo && s.level == 1) ? s.local.t : s.best.t;
+        if (__int_as_float(e.y) > limit) continue;
+        s.cur = e.x;
+        return true;
+    }
+}
+
+// One traversal step: an interior node (test both children) or a leaf (test
+// its records). Returns false when the ray's traversal is complete.
+template <bool kAny, bool kStats, bool kTwo, int kTotal>
+__device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, int64_t ray, Traversal& s,
+                                     StackStore<kTotal>& st, int2* col, int* error) {
+    const bool in_blas = kTwo && s.level == 1;
+    if (s.cur >= 0) {
+        const float4* p = reinterpret_cast<const float4*>(a.pairs + s.cur);
+        const float4 pa = Ld(p), pb = Ld(p + 1), pc = Ld(p + 2);
+        const int4 pd = __ldg(reinterpret_cast<const int4*>(p + 3));
+        const float limit = in_blas ? s.local.t : s.best.t;
+        float le = 0.0f, re = 0.0f;
+        bool hl = false, hr = false;
+        if (pd.x != kAbsentRef) {
+            if (kStats) ++s.nodes;
+            hl = SlabTest(s.r, pa.x, pa.y, pa.z, pa.w, pb.x, pb.y, s.tmin, limit, le);
+        }
+        if (pd.y != kAbsentRef) {
+            if (kStats) ++s.nodes;
+            hr = SlabTest(s.r, pb.z, pb.w, pc.x, pc.y, pc.z, pc.w, s.tmin, limit, re);
+        }
+        if (hl && hr) {
+            const bool left_first = le <= re;
+            if (s.sp >= kTotal) {  // unreachable when the host's depth bound holds
+                atomicOr(error, kTraceErrorStackOverflow);
+                s.best.hit = false;
+                return false;
+            }
+            st.Put(col, s.sp, left_first ? make_int2(pd.y, __float_as_int(re)) : make_int2(pd.x, __float_as_int(le)));
+            ++s.sp;
+            s.cur = left_first ? pd.x : pd.y;
+            return true;
+        }
+        if (hl) {
+            s.cur = pd.x;
+            return true;
+        }
+        if (hr) {
+            s.cur = pd.y;
+            return true;
+        }
+        return Pop<kAny, kTwo, kTotal>(rays, ray, s, st, col);
+    }
+
+    // Leaf: a run of records ending at the one flagged kRecLast.
+    int32_t rec = ~s.cur;
+    for (;;) {
+        const float4* q = reinterpret_cast<const float4*>(a.records + rec);
+        const float4 v0 = Ld(q), v1 = Ld(q + 1);
+        const int32_t flags = __float_as_int(v1.w);
+        const int32_t kind = (flags >> 1) & 7;
+        if (kind == kRecTriangle) {
+            const float4 v2 = Ld(q + 2);
+            if (kStats) ++s.tris;
+            if (in_blas) {
+                const bool acc = TriangleTest(s.r, v0, v1, v2, s.tmin, s.local);
+                if (kAny && acc && s.local.t < s.best.t) {
+                    s.best = s.local;
+                    s.best_inst = s.cur_inst;
+                    return false;
+                }
+            } else {
+                const bool acc = TriangleTest(s.r, v0, v1, v2, s.tmin, s.best);
+                if (kAny && acc) return false;
+            }
+        } else if (kind == kRecSphere) {
+            if (kStats) ++s.spheres;
+            if (in_blas) {
+                const bool acc = SphereTest(s.r, v0, v1, s.tmin, s.local);
+                if (kAny && acc && s.local.t < s.best.t) {
+                    s.best = s.local;
+                    s.best_inst = s.cur_inst;
+                    return false;
+                }
+            } else {
+                const bool acc = SphereTest(s.r, v0, v1, s.tmin, s.best);
+                if (acc) s.best_inst = -1;
+                if (kAny && acc) return false;
+            }
+        } else if (kTwo && kind == kRecInstance) {
+            // Descend into the instance's BLAS with the ray in object space
+            // (TransformPoint / TransformVector by world_to_object; the
+            // direction is not normalised, so t stays in world units).
+            const int32_t inst = __float_as_int(v0.w);
+            const float4* ip = reinterpret_cast<const float4*>(a.instances + inst);
+            const float4 m0 = Ld(ip), m1 = Ld(ip + 1), m2 = Ld(ip + 2), ba = Ld(ip + 3), bb = Ld(ip + 4);
+            const float4 rows[3] = {m0, m1, m2};
+            RayPre obj;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float4 m = rows[k];
+                obj.o[k] = __fadd_rn(
+                    __fadd_rn(__fadd_rn(__fmul_rn(m.x, s.r.o[0]), __fmul_rn(m.y, s.r.o[1])), __fmul_rn(m.z, s.r.o[2])),
+                    m.w);
+                obj.d[k] =
+                    __fadd_rn(__fadd_rn(__fmul_rn(m.x, s.r.d[0]), __fmul_rn(m.y, s.r.d[1])), __fmul_rn(m.z, s.r.d[2]));
+            }
+            Precompute(obj);
+            const int32_t root = __float_as_int(bb.z);
+            if (root != kAbsentRef) {
+                if (kStats) ++s.nodes;
+                float entry;
+                if (SlabTest(obj, ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, s.tmin, s.best.t, entry)) {
+                    s.local.t = s.best.t;
+                    s.local.id = -1;
+                    s.local.prim = -1;
+                    s.local.u = 0.0f;
+                    s.local.v = 0.0f;
+                    s.local.hit = false;
+                    s.level = 1;
+                    s.blas_base = s.sp;
+                    s.cur_inst = inst;
+                    s.tl_resume = (flags & kRecLast) ? -1 : rec + 1;
+                    s.r = obj;
+                    s.cur = root;
+                    return true;
+                }
+            }
+        } else if (kStats) {
+            if (kind == kRecSkipCountTriangle) ++s.tris;
+            if (kind == kRecSkipCountSphere) ++s.spheres;
+        }
+        if (flags & kRecLast) break;
+        ++rec;
+    }
+    return Pop<kAny, kTwo, kTotal>(rays, ray, s, st, col);
+}
+
+template <bool kAny, bool kStats>
+__device__ __forceinline__ void WriteResult(const TraceArgs& args, int64_t ray, const Traversal& s) {
+    if (kAny) {
+        args.occluded[ray] = s.best.hit ? 1 : 0;
+    } else {
+        reinterpret_cast<float4*>(args.hits)[ray] =
+            make_float4(s.best.t, __int_as_float(s.best.hit ? s.best.id : -1), s.best.u, s.best.v);
+        if (args.instances) args.instances[ray] = s.best.hit ? s.best_inst : -1;
+    }
+    if (kStats) {
+        if (args.node_tests) args.node_tests[ray] = s.nodes;
+        if (args.triangle_tests) args.triangle_tests[ray] = s.tris;
+        if (args.sphere_tests) args.sphere_tests[ray] = s.spheres;
+    }
+}
+
+template <bool kAny, bool kStats, bool kTwo, int kTotal>
+__global__ void __launch_bounds__(kTraceBlock) TraceKernel(TraceArgs args) {
+    __shared__ int2 s_stack[kShortStack * kTraceBlock];
+    int2* col = s_stack + threadIdx.x;
+    StackStore<kTotal> st;
+    Traversal s;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    int64_t ray = -1;
+    bool alive = false;
+    bool exhausted = false;
+
+    for (;;) {
+        const unsigned need = __ballot_sync(kFull, !alive && !exhausted);
+        if (need) {
+            unsigned long long base = 0;
+            const int leader = __ffs(need) - 1;
+            if (static_cast<int>(lane) == leader) {
+                base = atomicAdd(args.counter, static_cast<unsigned long long>(__popc(need)));
+            }
+            base = __shfl_sync(kFull, base, leader);
+            if (!alive && !exhausted) {
+                const unsigned long long idx = base + __popc(need & lt_mask);
+                if (idx >= static_cast<unsigned long long>(args.count)) {
+                    exhausted = true;
+                } else {
+                    ray = static_cast<int64_t>(idx);
+                    const float4 b = Ld(args.rays + 2 * ray + 1);
+                    const float tmin = Ld(args.rays + 2 * ray).w;
+                    alive = Begin(args.accel, args.rays, ray, tmin, b.w, s);
+                    if (!alive) WriteResult<kAny, kStats>(args, ray, s);
+                }
+            }
+        }
+        if (!__any_sync(kFull, alive)) {
+            if (__all_sync(kFull, exhausted)) break;
+            continue;
+        }
+        for (int k = 0; k < kSteps && alive; ++k) {
+            alive = Step<kAny, kStats, kTwo, kTotal>(args.accel, args.rays, ray, s, st, col, args.error);
+            if (!alive) WriteResult<kAny, kStats>(args, ray, s);
+        }
+    }
+}
+
+// IntersectAccelerationProbe: one thread per probe ray iterating closest-hit
+// queries with an advancing cursor; target hits are appended in t order.
+template <bool kTwo, int kTotal>
+__global__ void __launch_bounds__(kTraceBlock) ProbeKernel(ProbeArgs args) {
+    __shared__ int2 s_stack[kShortStack * kTraceBlock];
+    int2* col = s_stack + threadIdx.x;
+    StackStore<kTotal> st;
+    Traversal s;
+    for (int64_t ray = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; ray < args.count;
+         ray += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int4 target = __ldg(reinterpret_cast<const int4*>(args.targets) + ray);
+        const float t_min = Ld(args.rays + 2 * ray).w;
+        const float t_max = Ld(args.rays + 2 * ray + 1).w;
+        int32_t count = 0;
+        uint8_t exhausted = 0;
+        float cursor = t_min;
+        for (int iter = 0; iter < kProbeMaxIterations; ++iter) {
+            bool alive = Begin(args.accel, args.rays, ray, cursor, t_max, s);
+            while (alive) alive = Step<false, false, kTwo, kTotal>(args.accel, args.rays, ray, s, st, col, args.error);
+            if (!s.best.hit) break;
+            const bool inst_ok = !kTwo || target.y < 0 || s.best_inst == target.y;
+            const bool is_target = (target.x >= 0 && s.best.id >= 0 && s.best.prim == target.x && inst_ok) ||
+                                   (target.z >= 0 && s.best.id == -2 - target.z);
+            if (is_target) {
+                if (count < kProbeMaxHits) {
+                    const int64_t o = ray * kProbeMaxHits + count;
+                    reinterpret_cast<float4*>(args.hits)[o] =
+                        make_float4(s.best.t, __int_as_float(s.best.id), s.best.u, s.best.v);
+                    if (args.instances) args.instances[o] = s.best_inst;
+                    ++count;
+                } else {
+                    exhausted = 1;
+                    break;
+                }
+            }
+            float next = __fadd_rn(s.best.t, __fmul_rn(1.0e-4f, __fadd_rn(1.0f, fabsf(s.best.t))));
+            if (!(next > cursor)) next = __fadd_rn(cursor, 1.0e-4f);
+            cursor = next;
+            if (cursor >= t_max) break;
+        }
+        args.counts[ray] = count;
+        args.exhausted[ray] = exhausted;
+    }
+}
+
+template <typename Kernel>
+cudaError_t PersistentGrid(Kernel kernel, int64_t count, int sm_count, int64_t& blocks) {
+    int per_sm = 0;
+    const cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTraceBlock, 0);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) per_sm = 1;
+    blocks = static_cast<int64_t>(per_sm) * sm_count;
+    const int64_t needed = (count + kTraceBlock - 1) / kTraceBlock;
+    if (blocks > needed) blocks = needed < 1 ? 1 : needed;
+    return cudaSuccess;
+}
+
+template <bool kAny, bool kStats, bool kTwo, int kTotal>
+cudaError_t LaunchOne(const TraceArgs& args, cudaStream_t stream, int sm_count) {
+    auto kernel = TraceKernel<kAny, kStats, kTwo, kTotal>;
+    int64_t blocks = 0;
+    const cudaError_t err = PersistentGrid(kernel, args.count, sm_count, blocks);
+    if (err != cudaSuccess) return err;
+    kernel<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
+    return cudaGetLastError();
+}
+
+template <bool kAny, bool kStats, bool kTwo>
+cudaError_t LaunchDepth(const TraceArgs& args, cudaStream_t stream, int sm_count) {
+    if (args.accel.stack_limit <= 64) return LaunchOne<kAny, kStats, kTwo, 64>(args, stream, sm_count);
+    return LaunchOne<kAny, kStats, kTwo, kMaxTraceStack>(args, stream, sm_count);
+}
+
+template <bool kTwo, int kTotal>
+cudaError_t LaunchProbeOne(const ProbeArgs& args, cudaStream_t stream, int sm_count) {
+    auto kernel = ProbeKernel<kTwo, kTotal>;
+    int64_t blocks = 0;
+    const cudaError_t err = PersistentGrid(kernel, args.count, sm_count, blocks);
+    if (err != cudaSuccess) return err;
+    kernel<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, cudaStream_t stream, int sm_count) {
+    const bool two = args.accel.two_level != 0;
+    if (any_hit) {
+        if (two) return stats ? LaunchDepth<true, true, true>(args, stream, sm_count)
+                              : LaunchDepth<true, false, true>(args, stream, sm_count);
+        return stats ? LaunchDepth<true, true, false>(args, stream, sm_count)
+                     : LaunchDepth<true, false, false>(args, stream, sm_count);
+    }
+    if (two) return stats ? LaunchDepth<false, true, true>(args, stream, sm_count)
+                          : LaunchDepth<false, false, true>(args, stream, sm_count);
+    return stats ? LaunchDepth<false, true, false>(args, stream, sm_count)
+                 : LaunchDepth<false, false, false>(args, stream, sm_count);
+}
+
+cudaError_t LaunchProbe(const ProbeArgs& args, cudaStream_t stream, int sm_count) {
+    const bool two = args.accel.two_level != 0;
+    const bool deep = args.accel.stack_limit > 64;
+    if (two) return deep ? LaunchProbeOne<true, kMaxTraceStack>(args, stream, sm_count)
+                         : LaunchProbeOne<true, 64>(args, stream, sm_count);
+    return deep ? LaunchProbeOne<false, kMaxTraceStack>(args, stream, sm_count)
+                : LaunchProbeOne<false, 64>(args, stream, sm_count);
+}
+
+}  // namespace yrc

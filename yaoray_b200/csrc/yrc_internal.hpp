@@ -1,0 +1,65 @@
+// Internal host-side helpers shared by the libyrcuda translation units.
+#pragma once
+
+#include "yrcuda.h"
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace yrc {
+
+// Records `message` as this thread's last error and returns `status`.
+yrc_status Fail(yrc_status status, const std::string& message);
+// Clears this thread's last error and returns YRC_OK.
+yrc_status Ok();
+
+struct Vec3 {
+    float x = 0.0f, y = 0.0f, z = 0.0f;
+};
+
+// Bounds3f (include/yaoray/core/bounds.hpp:12-25): an empty box is
+// (+inf, -inf) so the first union takes the operand.
+struct Box {
+    Vec3 lo{__builtin_inff(), __builtin_inff(), __builtin_inff()};
+    Vec3 hi{-__builtin_inff(), -__builtin_inff(), -__builtin_inff()};
+};
+
+// Host copy of one RenderBvh (bvh.hpp:72-81).
+struct HostBvh {
+    std::vector<yrc_bvh_node> nodes;
+    std::vector<int32_t> primitive_indices;
+    std::vector<yrc_bvh_primitive> primitives;
+    int32_t max_depth = 0;
+    int32_t total_triangles = 0;
+    int32_t total_spheres = 0;
+};
+
+yrc_bvh_view ViewOf(const HostBvh& bvh);
+
+// Position of vertex `i` of a yrc_geometry.
+inline const float* VertexPosition(const yrc_geometry& g, uint64_t i) {
+    return reinterpret_cast<const float*>(reinterpret_cast<const char*>(g.positions) +
+                                          static_cast<int64_t>(i) * g.vertex_stride);
+}
+
+// One object handed to the hierarchy builder: a triangle, a sphere, or (for
+// the TLAS) an instance's world box.
+struct BuildRef {
+    int32_t flat_index;
+    Box bounds;
+    Vec3 centroid;
+};
+
+// Builds the binary hierarchy over `refs` (reordered in place) into `bvh`'s
+// nodes / primitive_indices / max_depth. Returns false with `error` set on a
+// build error.
+bool BuildHierarchy(std::vector<BuildRef>& refs, const yrc_bvh_options& options, HostBvh& bvh,
+                    std::string& error);
+
+// Builds a flat BVH (primitives + hierarchy) over a geometry's triangles and
+// spheres, as BuildBvh does.
+bool BuildFlatBvh(const yrc_geometry& geometry, const yrc_bvh_options& options, HostBvh& bvh,
+                  std::string& error);
+
+}  // namespace yrc
