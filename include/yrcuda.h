@@ -278,6 +278,21 @@ yrc_status yrc_trace_stats_device(yrc_accel* accel, const yrc_ray* rays, int64_t
                                   uint32_t* node_tests, uint32_t* triangle_tests, uint32_t* sphere_tests,
                                   void* stream);
 
+/*
+ * Autotuner: times every compiled launch shape of the flat closest-hit (or,
+ * with YRC_TRACE_ANY, any-hit) kernel on `count` device rays (results are
+ * discarded) and keeps the fastest for this accelerator. `times_ms`
+ * (optional, YRC_TRACE_SHAPES floats) receives the measured time per shape.
+ * Synchronises `stream`.
+ */
+#define YRC_TRACE_SHAPES 7
+yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags, void* stream,
+                              float* times_ms);
+/* Set / get the launch shape (0..YRC_TRACE_SHAPES-1) used for closest-hit
+ * (any_hit = 0) or any-hit (any_hit = 1) traces; 0 is the default shape. */
+yrc_status yrc_accel_set_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t shape);
+int32_t yrc_accel_get_trace_shape(const yrc_accel* accel, int32_t any_hit);
+
 /* ------------------------------------------------------------------ probe */
 
 #define YRC_PROBE_MAX_HITS 64 /* BvhProbeHits::MaxHits (bvh.hpp:122-127) */

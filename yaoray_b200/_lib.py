@@ -173,6 +173,9 @@ def lib() -> C.CDLL:
         "yrc_trace_stats_device": (C.c_int, [P, P, I64, I32, P, P, P, P]),
         "yrc_probe_device": (C.c_int, [P, P, P, I64, P, P, P, P, P]),
         "yrc_accel_check": (C.c_int, [P]),
+        "yrc_accel_autotune": (C.c_int, [P, P, I64, I32, P, P]),
+        "yrc_accel_set_trace_shape": (C.c_int, [P, I32, I32]),
+        "yrc_accel_get_trace_shape": (I32, [P, I32]),
         "yrc_stream_synchronize": (C.c_int, [P]),
     }
     for name, (res, args) in sig.items():

@@ -287,6 +287,19 @@ class DeviceAccelerator:
     def device_bytes(self) -> int:
         return int(lib().yrc_accel_device_bytes(self._handle))
 
+    def autotune(self, rays, any_hit: bool = False, stream=None) -> dict:
+        """Times every launch shape on `rays` (CUDA tensor) and keeps the
+        fastest; returns {shape: milliseconds} and the chosen shape."""
+        times = (C.c_float * 7)()
+        n = rays.numel() // 8
+        check(lib().yrc_accel_autotune(self._handle, ptr(rays), n, _lib.YRC_TRACE_ANY if any_hit else 0,
+                                       _stream_handle(stream), times))
+        return {"times_ms": [round(float(t), 4) for t in times],
+                "shape": int(lib().yrc_accel_get_trace_shape(self._handle, int(any_hit)))}
+
+    def set_trace_shape(self, shape: int, any_hit: bool = False) -> None:
+        check(lib().yrc_accel_set_trace_shape(self._handle, int(any_hit), shape))
+
     def check(self) -> None:
         """Synchronises and raises if a kernel recorded an error status."""
         check(lib().yrc_accel_check(self._handle))

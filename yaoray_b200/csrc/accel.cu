@@ -229,6 +229,7 @@ struct yrc_accel {
     unsigned long long* d_counter = nullptr;
     int* d_error = nullptr;
     yrc::AccelParams params{};
+    int trace_shape[2] = {0, 0};  // launch shape for closest / any hit (autotuned)
     int64_t device_bytes = 0;
     yrc::HostPipeline pipe;
     std::mutex mutex;
@@ -327,7 +328,7 @@ yrc_status LaunchInternal(yrc_accel* a, const yrc_ray* rays, int64_t count, int3
     if (err != cudaSuccess) return CudaFail(err, "trace counter reset");
     const bool any = (flags & YRC_TRACE_ANY) != 0;
     const bool stats = (flags & YRC_TRACE_STATS) != 0;
-    err = LaunchTrace(args, any, stats, stream, a->sm_count);
+    err = LaunchTrace(args, any, stats, a->trace_shape[any ? 1 : 0], stream, a->sm_count);
     if (err != cudaSuccess) return CudaFail(err, "trace launch");
     return Ok();
 }
@@ -586,6 +587,65 @@ yrc_status yrc_probe_device(yrc_accel* accel, const yrc_ray* rays, const yrc_pro
     args.error = accel->d_error;
     const cudaError_t err = LaunchProbe(args, static_cast<cudaStream_t>(stream), accel->sm_count);
     if (err != cudaSuccess) return CudaFail(err, "probe launch");
+    return Ok();
+}
+
+yrc_status yrc_accel_set_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t shape) {
+    if (!accel || shape < 0 || shape >= yrc::kTraceShapes) {
+        return yrc::Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_set_trace_shape: bad argument");
+    }
+    accel->trace_shape[any_hit ? 1 : 0] = shape;
+    return yrc::Ok();
+}
+
+int32_t yrc_accel_get_trace_shape(const yrc_accel* accel, int32_t any_hit) {
+    return accel ? accel->trace_shape[any_hit ? 1 : 0] : -1;
+}
+
+yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags, void* stream,
+                              float* times_ms) {
+    using namespace yrc;
+    if (!accel || count <= 0 || !rays) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_autotune: bad argument");
+    const bool any = (flags & YRC_TRACE_ANY) != 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    cudaSetDevice(accel->device);
+    void* out = nullptr;
+    cudaError_t err = cudaMallocAsync(&out, static_cast<size_t>(count) * (any ? 1 : 16), st);
+    if (err != cudaSuccess) return CudaFail(err, "autotune scratch");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 0.0f;
+    int best_shape = 0;
+    yrc_status status = Ok();
+    for (int shape = 0; shape < kTraceShapes && status == YRC_OK; ++shape) {
+        accel->trace_shape[any ? 1 : 0] = shape;
+        float total = 0.0f;
+        for (int rep = 0; rep < 3 && status == YRC_OK; ++rep) {  // first repetition warms up
+            cudaEventRecord(e0, st);
+            status = LaunchInternal(accel, rays, count, flags & YRC_TRACE_ANY, any ? nullptr : static_cast<yrc_hit*>(out),
+                                    nullptr, any ? static_cast<uint8_t*>(out) : nullptr, nullptr, nullptr, nullptr,
+                                    accel->d_counter, st);
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) total += ms;
+        }
+        if (times_ms) times_ms[shape] = total / 2.0f;
+        if (shape == 0 || total < best) {
+            best = total;
+            best_shape = shape;
+        }
+    }
+    accel->trace_shape[any ? 1 : 0] = best_shape;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeAsync(out, st);
+    err = cudaStreamSynchronize(st);
+    if (status != YRC_OK) return status;
+    if (err != cudaSuccess) return CudaFail(err, "autotune");
     return Ok();
 }
 

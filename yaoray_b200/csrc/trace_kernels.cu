@@ -47,20 +47,23 @@ struct Traversal {
 
 __device__ __forceinline__ float4 Ld(const float4* p) { return __ldg(p); }
 
-template <int kTotal>
+// Traversal stack of kTotal entries per thread: the first kShortStack in the
+// block's shared memory (column `col`, stride kBlock), the rest local.
+template <int kTotal, int kBlock = kTraceBlock>
 struct StackStore {
+    static constexpr int kTotalEntries = kTotal;
     static constexpr int kLocal = kTotal > kShortStack ? kTotal - kShortStack : 1;
     int2 local[kLocal];
 
     __device__ __forceinline__ void Put(int2* col, int sp, int2 e) {
         if (sp < kShortStack) {
-            col[sp * kTraceBlock] = e;
+            col[sp * kBlock] = e;
         } else {
             local[sp - kShortStack] = e;
         }
     }
     __device__ __forceinline__ int2 Get(const int2* col, int sp) const {
-        return sp < kShortStack ? col[sp * kTraceBlock] : local[sp - kShortStack];
+        return sp < kShortStack ? col[sp * kBlock] : local[sp - kShortStack];
     }
 };
 
@@ -108,9 +111,8 @@ __device__ __forceinline__ bool Begin(const AccelParams& a, const float4* rays, 
 // Pops the next live stack entry into s.cur (culled against the nearest t of
 // the current level) and closes finished BLAS traversals. Returns false when
 // the ray's traversal is complete.
-template <bool kAny, bool kTwo, int kTotal>
-__device__ __forceinline__ bool Pop(const float4* rays, int64_t ray, Traversal& s, StackStore<kTotal>& st,
-                                    const int2* col) {
+template <bool kAny, bool kTwo, typename Stack>
+__device__ __forceinline__ bool Pop(const float4* rays, int64_t ray, Traversal& s, Stack& st, const int2* col) {
     for (;;) {
         if (kTwo && s.level == 1 && s.sp == s.blas_base) {
             // IntersectTwoLevelBvh accepts the BLAS hit only if strictly nearer.
@@ -139,9 +141,9 @@ __device__ __forceinline__ bool Pop(const float4* rays, int64_t ray, Traversal& 
 
 // One traversal step: an interior node (test both children) or a leaf (test
 // its records). Returns false when the ray's traversal is complete.
-template <bool kAny, bool kStats, bool kTwo, int kTotal>
-__device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, int64_t ray, Traversal& s,
-                                     StackStore<kTotal>& st, int2* col, int* error) {
+template <bool kAny, bool kStats, bool kTwo, typename Stack>
+__device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, int64_t ray, Traversal& s, Stack& st,
+                                     int2* col, int* error) {
     const bool in_blas = kTwo && s.level == 1;
     if (s.cur >= 0) {
         const float4* p = reinterpret_cast<const float4*>(a.pairs + s.cur);
@@ -160,7 +162,7 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
         }
         if (hl && hr) {
             const bool left_first = le <= re;
-            if (s.sp >= kTotal) {  // unreachable when the host's depth bound holds
+            if (s.sp >= Stack::kTotalEntries) {  // unreachable when the host's depth bound holds
                 atomicOr(error, kTraceErrorStackOverflow);
                 s.best.hit = false;
                 return false;
@@ -178,7 +180,7 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
             s.cur = pd.y;
             return true;
         }
-        return Pop<kAny, kTwo, kTotal>(rays, ray, s, st, col);
+        return Pop<kAny, kTwo>(rays, ray, s, st, col);
     }
 
     // Leaf: a run of records ending at the one flagged kRecLast.
@@ -262,7 +264,7 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
         if (flags & kRecLast) break;
         ++rec;
     }
-    return Pop<kAny, kTwo, kTotal>(rays, ray, s, st, col);
+    return Pop<kAny, kTwo>(rays, ray, s, st, col);
 }
 
 template <bool kAny, bool kStats>
@@ -281,11 +283,11 @@ __device__ __forceinline__ void WriteResult(const TraceArgs& args, int64_t ray, 
     }
 }
 
-template <bool kAny, bool kStats, bool kTwo, int kTotal>
-__global__ void __launch_bounds__(kTraceBlock) TraceKernel(TraceArgs args) {
-    __shared__ int2 s_stack[kShortStack * kTraceBlock];
+template <bool kAny, bool kStats, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args) {
+    __shared__ int2 s_stack[kShortStack * kBlock];
     int2* col = s_stack + threadIdx.x;
-    StackStore<kTotal> st;
+    StackStore<kTotal, kBlock> st;
     Traversal s;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -319,8 +321,9 @@ __global__ void __launch_bounds__(kTraceBlock) TraceKernel(TraceArgs args) {
             if (__all_sync(kFull, exhausted)) break;
             continue;
         }
-        for (int k = 0; k < kSteps && alive; ++k) {
-            alive = Step<kAny, kStats, kTwo, kTotal>(args.accel, args.rays, ray, s, st, col, args.error);
+#pragma unroll 1
+        for (int k = 0; k < kStepsPerRefill && alive; ++k) {
+            alive = Step<kAny, kStats, kTwo>(args.accel, args.rays, ray, s, st, col, args.error);
             if (!alive) WriteResult<kAny, kStats>(args, ray, s);
         }
     }
@@ -344,7 +347,7 @@ __global__ void __launch_bounds__(kTraceBlock) ProbeKernel(ProbeArgs args) {
         float cursor = t_min;
         for (int iter = 0; iter < kProbeMaxIterations; ++iter) {
             bool alive = Begin(args.accel, args.rays, ray, cursor, t_max, s);
-            while (alive) alive = Step<false, false, kTwo, kTotal>(args.accel, args.rays, ray, s, st, col, args.error);
+            while (alive) alive = Step<false, false, kTwo>(args.accel, args.rays, ray, s, st, col, args.error);
             if (!s.best.hit) break;
             const bool inst_ok = !kTwo || target.y < 0 || s.best_inst == target.y;
             const bool is_target = (target.x >= 0 && s.best.id >= 0 && s.best.prim == target.x && inst_ok) ||
@@ -372,38 +375,54 @@ __global__ void __launch_bounds__(kTraceBlock) ProbeKernel(ProbeArgs args) {
 }
 
 template <typename Kernel>
-cudaError_t PersistentGrid(Kernel kernel, int64_t count, int sm_count, int64_t& blocks) {
+cudaError_t PersistentGrid(Kernel kernel, int block, int64_t count, int sm_count, int64_t& blocks) {
     int per_sm = 0;
-    const cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTraceBlock, 0);
+    const cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
     if (err != cudaSuccess) return err;
     if (per_sm < 1) per_sm = 1;
     blocks = static_cast<int64_t>(per_sm) * sm_count;
-    const int64_t needed = (count + kTraceBlock - 1) / kTraceBlock;
+    const int64_t needed = (count + block - 1) / block;
     if (blocks > needed) blocks = needed < 1 ? 1 : needed;
     return cudaSuccess;
 }
 
-template <bool kAny, bool kStats, bool kTwo, int kTotal>
+template <bool kAny, bool kStats, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks>
 cudaError_t LaunchOne(const TraceArgs& args, cudaStream_t stream, int sm_count) {
-    auto kernel = TraceKernel<kAny, kStats, kTwo, kTotal>;
+    auto kernel = TraceKernel<kAny, kStats, kTwo, kTotal, kBlock, kStepsPerRefill, kMinBlocks>;
     int64_t blocks = 0;
-    const cudaError_t err = PersistentGrid(kernel, args.count, sm_count, blocks);
+    const cudaError_t err = PersistentGrid(kernel, kBlock, args.count, sm_count, blocks);
     if (err != cudaSuccess) return err;
-    kernel<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
+    kernel<<<static_cast<unsigned>(blocks), kBlock, 0, stream>>>(args);
     return cudaGetLastError();
 }
 
+// The tunable launch shapes (block size, node visits between ray refills,
+// minimum resident blocks for the register budget). Index 0 is the default;
+// the autotuner times the rest on the actual accelerator.
+template <bool kAny, bool kStats, bool kTwo, int kTotal>
+cudaError_t LaunchShape(const TraceArgs& args, int shape, cudaStream_t stream, int sm_count) {
+    switch (kStats || kTwo ? 0 : shape) {
+        case 1: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 4, 1>(args, stream, sm_count);
+        case 2: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 16, 1>(args, stream, sm_count);
+        case 3: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 12>(args, stream, sm_count);
+        case 4: return LaunchOne<kAny, kStats, kTwo, kTotal, 64, 8, 1>(args, stream, sm_count);
+        case 5: return LaunchOne<kAny, kStats, kTwo, kTotal, 256, 8, 1>(args, stream, sm_count);
+        case 6: return LaunchOne<kAny, kStats, kTwo, kTotal, 64, 8, 24>(args, stream, sm_count);
+        default: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1>(args, stream, sm_count);
+    }
+}
+
 template <bool kAny, bool kStats, bool kTwo>
-cudaError_t LaunchDepth(const TraceArgs& args, cudaStream_t stream, int sm_count) {
-    if (args.accel.stack_limit <= 64) return LaunchOne<kAny, kStats, kTwo, 64>(args, stream, sm_count);
-    return LaunchOne<kAny, kStats, kTwo, kMaxTraceStack>(args, stream, sm_count);
+cudaError_t LaunchDepth(const TraceArgs& args, int shape, cudaStream_t stream, int sm_count) {
+    if (args.accel.stack_limit <= 64) return LaunchShape<kAny, kStats, kTwo, 64>(args, shape, stream, sm_count);
+    return LaunchShape<kAny, kStats, kTwo, kMaxTraceStack>(args, 0, stream, sm_count);
 }
 
 template <bool kTwo, int kTotal>
 cudaError_t LaunchProbeOne(const ProbeArgs& args, cudaStream_t stream, int sm_count) {
     auto kernel = ProbeKernel<kTwo, kTotal>;
     int64_t blocks = 0;
-    const cudaError_t err = PersistentGrid(kernel, args.count, sm_count, blocks);
+    const cudaError_t err = PersistentGrid(kernel, kTraceBlock, args.count, sm_count, blocks);
     if (err != cudaSuccess) return err;
     kernel<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
     return cudaGetLastError();
@@ -411,18 +430,19 @@ cudaError_t LaunchProbeOne(const ProbeArgs& args, cudaStream_t stream, int sm_co
 
 }  // namespace
 
-cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, cudaStream_t stream, int sm_count) {
+cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, int shape, cudaStream_t stream,
+                        int sm_count) {
     const bool two = args.accel.two_level != 0;
     if (any_hit) {
-        if (two) return stats ? LaunchDepth<true, true, true>(args, stream, sm_count)
-                              : LaunchDepth<true, false, true>(args, stream, sm_count);
-        return stats ? LaunchDepth<true, true, false>(args, stream, sm_count)
-                     : LaunchDepth<true, false, false>(args, stream, sm_count);
+        if (two) return stats ? LaunchDepth<true, true, true>(args, shape, stream, sm_count)
+                              : LaunchDepth<true, false, true>(args, shape, stream, sm_count);
+        return stats ? LaunchDepth<true, true, false>(args, shape, stream, sm_count)
+                     : LaunchDepth<true, false, false>(args, shape, stream, sm_count);
     }
-    if (two) return stats ? LaunchDepth<false, true, true>(args, stream, sm_count)
-                          : LaunchDepth<false, false, true>(args, stream, sm_count);
-    return stats ? LaunchDepth<false, true, false>(args, stream, sm_count)
-                 : LaunchDepth<false, false, false>(args, stream, sm_count);
+    if (two) return stats ? LaunchDepth<false, true, true>(args, shape, stream, sm_count)
+                          : LaunchDepth<false, false, true>(args, shape, stream, sm_count);
+    return stats ? LaunchDepth<false, true, false>(args, shape, stream, sm_count)
+                 : LaunchDepth<false, false, false>(args, shape, stream, sm_count);
 }
 
 cudaError_t LaunchProbe(const ProbeArgs& args, cudaStream_t stream, int sm_count) {

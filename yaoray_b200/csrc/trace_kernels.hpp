@@ -12,7 +12,7 @@ namespace yrc {
 
 constexpr int kTraceBlock = 128;    // threads per block
 constexpr int kShortStack = 12;     // stack entries per thread kept in shared memory
-constexpr int kSteps = 8;           // node visits between ray refills
+constexpr int kTraceShapes = 7;     // launch shapes the autotuner may choose from
 constexpr int kMaxTraceStack = 256; // deepest traversal stack any kernel supports
 
 // Status bits a kernel may set in the accelerator's device error word.
@@ -47,7 +47,10 @@ struct ProbeArgs {
     int* error;
 };
 
-cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, cudaStream_t stream, int sm_count);
+// shape: index of the launch shape (block size / refill interval / register
+// budget) for the flat closest- and any-hit kernels, 0 = default.
+cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, int shape, cudaStream_t stream,
+                        int sm_count);
 cudaError_t LaunchProbe(const ProbeArgs& args, cudaStream_t stream, int sm_count);
 
 }  // namespace yrc
