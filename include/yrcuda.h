@@ -322,6 +322,260 @@ yrc_status yrc_probe_device(yrc_accel* accel, const yrc_ray* rays, const yrc_pro
  */
 yrc_status yrc_accel_check(yrc_accel* accel);
 
+/* ================================================================= render */
+
+/* RenderMaterialKind (include/yaoray/scene/material.hpp:7-19). */
+enum {
+    YRC_MAT_DIFFUSE = 0,
+    YRC_MAT_CONDUCTOR = 1,
+    YRC_MAT_DIELECTRIC = 2,
+    YRC_MAT_THIN_DIELECTRIC = 3,
+    YRC_MAT_COATED_DIFFUSE = 4,
+    YRC_MAT_COATED_CONDUCTOR = 5,
+    YRC_MAT_DIFFUSE_TRANSMISSION = 6,
+    YRC_MAT_MIX = 7,
+    YRC_MAT_MEASURED = 8,
+    YRC_MAT_SUBSURFACE = 9,
+    YRC_MAT_SUBSURFACE_EXIT = 10
+};
+
+/* RenderMaterial (material.hpp:31-65) with texture slots as indices; the
+ * device shades untextured materials (every *_texture / normal_map = -1). */
+typedef struct yrc_material {
+    int32_t kind;
+    float reflectance[3];
+    float eta[3];
+    float k[3];
+    float ior;
+    float uroughness;
+    float vroughness;
+    int32_t remap_roughness;
+    int32_t mix_material_a;
+    int32_t mix_material_b;
+    float mix_amount;
+    float coating_ior;
+    float coating_roughness;
+    float coat_thickness;
+    float coat_absorption[3];
+    int32_t coat_maxdepth;
+    int32_t coat_nsamples;
+    float sigma_a[3];
+    float sigma_s[3];
+    float bssrdf_eta;
+    int32_t bssrdf_index;
+    float emission[3];
+    float alpha;
+    float absorption_color[3];
+    float absorption_distance;
+    int32_t reflectance_texture;
+    int32_t alpha_texture;
+    int32_t normal_map;
+    int32_t measured_index;
+} yrc_material;
+
+/* EmissivePrimitive (include/yaoray/scene/light.hpp:30-34). */
+typedef struct yrc_emissive_primitive {
+    int32_t primitive_index;
+    float radiance[3];
+    float area;
+} yrc_emissive_primitive;
+
+/* AliasTable (light.hpp:47-51); count 0 = no table. */
+typedef struct yrc_alias_table {
+    const float* probability;
+    const int32_t* alias;
+    const float* pmf;
+    int32_t count;
+} yrc_alias_table;
+
+/* AnalyticLight (light.hpp:38-45). kind: 0 point, 1 spot, 2 distant. */
+typedef struct yrc_analytic_light {
+    int32_t kind;
+    float position[3];
+    float direction[3];
+    float intensity[3];
+    float cone_angle;
+    float cone_cos_inner;
+} yrc_analytic_light;
+
+/* RenderEnvironment + its RenderTexture (RGBA32F texels, repeat-wrapped,
+ * bilinear) + RenderEnvironmentDistribution (light.hpp:8-28). */
+typedef struct yrc_environment {
+    int32_t active;
+    float radiance[3];
+    float strength;
+    float rotation_radians;
+    int32_t width;
+    int32_t height;
+    const float* texels;          /* width * height * 4 floats, NULL = none */
+    const float* texel_weights;   /* width * height, NULL = not sampleable */
+    const float* row_weights;     /* height */
+    const float* row_cdf;         /* height */
+    const float* conditional_cdfs;/* width * height */
+    float total_weight;
+} yrc_environment;
+
+/* BSSRDFTable (include/yaoray/shading/bssrdf.hpp). */
+typedef struct yrc_bssrdf_table {
+    int32_t rho_count;
+    int32_t radius_count;
+    const float* rho_samples;    /* rho_count */
+    const float* radius_samples; /* radius_count */
+    const float* profile;        /* rho_count * radius_count */
+    const float* rho_eff;        /* rho_count */
+    const float* profile_cdf;    /* rho_count * radius_count */
+} yrc_bssrdf_table;
+
+/* RenderCamera (include/yaoray/scene/camera.hpp:7-13). */
+typedef struct yrc_camera {
+    float origin[3];
+    float forward[3];
+    float right[3];
+    float up[3];
+    float fov_y_radians;
+} yrc_camera;
+
+/* RenderSettings (include/yaoray/scene/render_options.hpp:38-51). sampler:
+ * RenderSamplerKind (0 independent, 1 stratified, 2 Owen-Sobol, 3 Z-Sobol). */
+typedef struct yrc_render_settings {
+    int32_t width;
+    int32_t height;
+    int32_t spp;
+    int32_t max_depth;
+    uint64_t seed;
+    int32_t sampler;
+    float radiance_clamp;
+    int32_t adaptive_enabled;
+    int32_t adaptive_min_spp;
+    float adaptive_relative_error;
+    float adaptive_absolute_error;
+    float adaptive_confidence;
+} yrc_render_settings;
+
+/*
+ * A RenderSceneIR plus its prepared acceleration structure. Vertex shading
+ * normals (RenderVertex.normal) come from `normals` with `normal_stride`
+ * bytes between vertices (NULL when no primitive has normals). Exactly one of
+ * `flat` / `two_level` is non-NULL.
+ */
+typedef struct yrc_scene_desc {
+    yrc_geometry geometry;
+    const float* normals;
+    int64_t normal_stride;
+    const yrc_material* materials;
+    int32_t material_count;
+    const yrc_emissive_primitive* emissive;
+    int32_t emissive_count;
+    yrc_alias_table emissive_power;
+    const yrc_analytic_light* analytic;
+    int32_t analytic_count;
+    yrc_alias_table analytic_power;
+    yrc_environment environment;
+    const yrc_bssrdf_table* bssrdf_tables;
+    int32_t bssrdf_count;
+    yrc_camera camera;
+    yrc_render_settings settings;
+    const yrc_bvh_view* flat;
+    const yrc_two_level_view* two_level;
+} yrc_scene_desc;
+
+/* FilmPixel (include/yaoray/film/film.hpp:19-28), byte-identical, 56 bytes. */
+typedef struct yrc_film_pixel {
+    float sum[3];
+    uint32_t samples;
+    float luminance_mean;
+    float luminance_m2;
+    float albedo_sum[3];
+    float normal_sum[3];
+    float depth_sum;
+    uint32_t aov_samples;
+} yrc_film_pixel;
+
+/* RenderProgress (include/yaoray/runtime/backend.hpp:16-25). */
+typedef struct yrc_render_progress {
+    int32_t completed_spp;
+    int32_t target_spp;
+    uint64_t completed_samples;
+    uint64_t target_samples;
+    uint64_t active_pixels;
+    uint64_t converged_pixels;
+    uint64_t rays_traced;
+    double elapsed_seconds;
+} yrc_render_progress;
+
+/*
+ * Progress callback, called on the calling thread after each complete pass
+ * with the film so far (host memory, width * height pixels) and the number of
+ * non-finite samples dropped. Return non-zero to cancel the render; `error`
+ * (capacity `error_capacity`) may then receive the reason.
+ */
+typedef int32_t (*yrc_progress_fn)(const yrc_render_progress* progress, const yrc_film_pixel* film,
+                                    uint64_t bad_samples, void* user, char* error, size_t error_capacity);
+
+/* RenderRequest (backend.hpp:33-38). `stop_flag` (optional) is polled between
+ * passes; non-zero cancels like a stop_token. */
+typedef struct yrc_render_request {
+    const yrc_film_pixel* resume_film; /* host, width * height, or NULL */
+    uint64_t resume_bad_samples;
+    int32_t resume_completed_spp;
+    const volatile int32_t* stop_flag;
+    yrc_progress_fn progress;
+    void* user;
+} yrc_render_request;
+
+/* RenderStats (backend.hpp:40-55). */
+typedef struct yrc_render_stats {
+    uint64_t samples_rendered;
+    uint64_t converged_pixels;
+    uint64_t rays_traced;
+    uint64_t shadow_rays;
+    uint64_t occluded_shadow_rays;
+    uint64_t triangle_tests;
+    uint64_t sphere_tests;
+    uint64_t bvh_node_tests;
+    int32_t bvh_nodes;
+    int32_t bvh_max_depth;
+    uint64_t hits;
+    uint64_t misses;
+    uint64_t bad_samples;
+    int32_t threads;
+    double elapsed_seconds;
+    double device_seconds;
+} yrc_render_stats;
+
+/*
+ * Light-table builders for callers that prepare scenes themselves (the same
+ * tables the reference's PrepareLightSampling / BuildEnvironmentDistribution
+ * produce): BuildAliasTable (src/lighting/light_sampling.cpp:148-183) into
+ * caller arrays of `count`; BuildEnvironmentDistribution
+ * (src/lighting/environment.cpp:73-123) for RGBA texels (NULL = black).
+ */
+yrc_status yrc_alias_table_build(const float* weights, int32_t count, float* probability, int32_t* alias,
+                                 float* pmf);
+yrc_status yrc_environment_distribution_build(const float* texels, int32_t width, int32_t height,
+                                              float* texel_weights, float* row_weights, float* row_cdf,
+                                              float* conditional_cdfs, float* total_weight);
+
+typedef struct yrc_render_scene yrc_render_scene;
+
+/* CudaBackend::Prepare (src/runtime/cuda_stub_backend.cpp:20-28): uploads the
+ * scene and its acceleration structure. Fails with YRC_ERR_UNSUPPORTED for
+ * scene features the device does not shade (textures, measured BRDFs). */
+yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene** out);
+void yrc_render_scene_destroy(yrc_render_scene* scene);
+int64_t yrc_render_scene_device_bytes(const yrc_render_scene* scene);
+
+/*
+ * CudaBackend::Render (cuda_stub_backend.cpp:30-37) for the Path integrator:
+ * the pass loop of RenderCpuPathTrace (src/backends/cpu/cpu_path_tracer.cpp:
+ * 39-229) on the device. `film_out` (host, width * height) receives the
+ * film; `bad_samples_out` the film's non-finite sample count. On
+ * cancellation returns YRC_ERR_CANCELLED with the reference's message
+ * ("render cancelled" or the callback's text) and leaves film_out untouched.
+ */
+yrc_status yrc_render(yrc_render_scene* scene, const yrc_render_request* request, yrc_film_pixel* film_out,
+                      uint64_t* bad_samples_out, yrc_render_stats* stats);
+
 /* Wait for all work the library queued on `stream` (NULL = legacy default). */
 yrc_status yrc_stream_synchronize(void* stream);
 

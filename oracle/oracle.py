@@ -386,3 +386,114 @@ def ref_film(width: int, height: int, samples: np.ndarray):
     px = np.zeros(width * height, FILM_PIXEL_DTYPE)
     bad = ref_lib().yrref_film_accumulate(width, height, s.ctypes.data, s.shape[0], px.ctypes.data)
     return px, int(bad)
+
+
+# ------------------------------------------------ reference renders (CPU)
+
+def _bind_jobs(L):
+    if getattr(L, "_jobs_bound", False):
+        return L
+    L.yrref_pbrt_load.restype = P
+    L.yrref_pbrt_load.argtypes = [C.c_char_p]
+    L.yrref_job_destroy.argtypes = [P]
+    L.yrref_job_counts.argtypes = [P, P]
+    L.yrref_job_geometry.argtypes = [P, P, P, P, P, P]
+    L.yrref_job_materials.argtypes = [P, P]
+    L.yrref_job_lights.argtypes = [P, P, P, P, P, P, P]
+    L.yrref_job_from_desc.restype = P
+    L.yrref_job_from_desc.argtypes = [P]
+    L.yrref_job_render.argtypes = [P, C.c_int, C.c_int, P, P, P]
+    L._jobs_bound = True
+    return L
+
+
+class RefJob:
+    """A RenderJob of the reference: loaded from a PBRT file by its own
+    frontend, or assembled from a RenderScene; rendered by its CpuBackend."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    @staticmethod
+    def load_pbrt(path) -> "RefJob":
+        L = _bind_jobs(ref_lib())
+        h = L.yrref_pbrt_load(str(path).encode())
+        if not h:
+            raise RuntimeError(L.yrref_last_error().decode())
+        return RefJob(h)
+
+    @staticmethod
+    def from_scene(scene) -> "RefJob":
+        from yaoray_b200.render import scene_desc
+        L = _bind_jobs(ref_lib())
+        desc, keep = scene_desc(scene)
+        h = L.yrref_job_from_desc(C.addressof(desc))
+        del keep
+        return RefJob(h)
+
+    def __del__(self):
+        try:
+            _bind_jobs(ref_lib()).yrref_job_destroy(self.h)
+        except Exception:
+            pass
+
+    def export(self):
+        """The compiled RenderSceneIR + settings as a yaoray_b200 RenderScene."""
+        from yaoray_b200 import _lib
+        from yaoray_b200.accel import SceneGeometry
+        from yaoray_b200.render import EMISSIVE_DTYPE, MATERIAL_DTYPE, Camera, RenderScene, Settings
+        L = _bind_jobs(ref_lib())
+        c = np.zeros(11, np.int64)
+        L.yrref_job_counts(self.h, c.ctypes.data)
+        nv, ni, npr, ns, nin, nm, ne = (int(x) for x in c[:7])
+        verts = np.zeros((nv, 12), np.float32)
+        idx = np.zeros(ni, np.uint32)
+        prims = np.zeros(npr, _lib.PRIM_DTYPE)
+        sph = np.zeros(ns, _lib.SPHERE_DTYPE)
+        inst = np.zeros(nin, _lib.INSTANCE_DTYPE)
+        L.yrref_job_geometry(self.h, _p(verts), _p(idx), _p(prims), _p(sph), _p(inst))
+        mats = np.zeros(nm, MATERIAL_DTYPE)
+        L.yrref_job_materials(self.h, _p(mats))
+        em = np.zeros(ne, EMISSIVE_DTYPE)
+        na = int(c[10])
+        prob = np.zeros(na, np.float32)
+        alias = np.zeros(na, np.int32)
+        pmf = np.zeros(na, np.float32)
+        cam = Camera()
+        st = Settings()
+        L.yrref_job_lights(self.h, _p(em), _p(prob), _p(alias), _p(pmf), C.addressof(cam), C.addressof(st))
+        geom = SceneGeometry(verts[:, 0:3], idx, prims, sph, inst)
+        camd = {"origin": tuple(cam.origin), "forward": tuple(cam.forward), "right": tuple(cam.right),
+                "up": tuple(cam.up), "fov_y_radians": cam.fov_y_radians}
+        return RenderScene(geom, mats, camd, st.width, st.height, spp=st.spp, max_depth=st.max_depth, seed=st.seed,
+                           sampler=st.sampler, radiance_clamp=st.radiance_clamp,
+                           normals=verts[:, 3:6].copy() if (prims["flags"] & 1).any() else None, emissive=em,
+                           alias=(prob, alias, pmf) if na else None,
+                           adaptive={"enabled": bool(st.adaptive_enabled), "min_spp": st.adaptive_min_spp,
+                                     "relative_error": st.adaptive_relative_error,
+                                     "absolute_error": st.adaptive_absolute_error,
+                                     "confidence": st.adaptive_confidence})
+
+    def render(self, threads: int = 0, spp: int = 0):
+        """CpuBackend render -> (film FILM_PIXEL_DTYPE (H*W), stats dict, seconds)."""
+        L = _bind_jobs(ref_lib())
+        c = np.zeros(11, np.int64)
+        L.yrref_job_counts(self.h, c.ctypes.data)
+        from yaoray_b200.render import Settings
+        cam_dummy = None  # noqa: F841
+        st = Settings()
+        from yaoray_b200.render import Camera
+        cam = Camera()
+        em = np.zeros(max(int(c[6]), 1), np.dtype([("a", "<i4"), ("b", "<f4", 4)]))
+        na = max(int(c[10]), 1)
+        L.yrref_job_lights(self.h, _p(em), _p(np.zeros(na, np.float32)), _p(np.zeros(na, np.int32)),
+                           _p(np.zeros(na, np.float32)), C.addressof(cam), C.addressof(st))
+        film = np.zeros(st.width * st.height, FILM_PIXEL_DTYPE)
+        stats = np.zeros(7, np.uint64)
+        secs = C.c_double()
+        rc = L.yrref_job_render(self.h, threads, spp, film.ctypes.data, stats.ctypes.data, C.byref(secs))
+        if rc != 0:
+            raise RuntimeError(L.yrref_last_error().decode())
+        keys = ["samples_rendered", "rays_traced", "shadow_rays", "occluded_shadow_rays", "hits", "misses",
+                "bad_samples"]
+        return film.reshape(st.height, st.width), dict(zip(keys, map(int, stats))), float(secs.value)

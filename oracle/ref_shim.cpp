@@ -384,3 +384,326 @@ std::uint64_t yrref_film_accumulate(int width, int height, const float* samples,
 }
 
 } // extern "C"
+
+// ============================================================== rendering ==
+// RenderJobs for the CPU backend: loaded from a PBRT file through the
+// reference frontend (LoadPbrtScene + CompilePbrtScene) or assembled from the
+// C-ABI scene description, exported back as arrays, and rendered with
+// CpuBackend::Prepare / Render.
+
+#include "yrcuda.h"
+
+#include <yaoray/lighting/environment.hpp>
+#include <yaoray/lighting/light_sampling.hpp>
+
+namespace {
+
+struct RefJob {
+    yr::RenderSceneIR ir;
+    yr::RenderSettings settings;
+    std::vector<float> alias_prob;
+    std::vector<int> alias_index;
+    std::vector<float> alias_pmf;
+};
+
+void CopyRgb(const yr::Color3f& c, float* out) {
+    out[0] = c.x;
+    out[1] = c.y;
+    out[2] = c.z;
+}
+
+yr::Color3f Rgb(const float* c) { return yr::Color3f{c[0], c[1], c[2]}; }
+
+void PrepareAlias(RefJob& job) {
+    yr::RenderSceneIR copy = job.ir;
+    yr::PrepareLightSampling(copy);
+    job.alias_prob = copy.light_sampling.emissive_power.probability;
+    job.alias_index = copy.light_sampling.emissive_power.alias;
+    job.alias_pmf = copy.light_sampling.emissive_power.pmf;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Returns a job handle, or null with the first error diagnostic in yrref_last_error().
+void* yrref_pbrt_load(const char* path) {
+    yr::PbrtSceneLoadResult loaded = yr::LoadPbrtScene(path);
+    if (!loaded.scene) {
+        g_last_error = loaded.diagnostics.empty() ? "PBRT load failed" : loaded.diagnostics.front().message;
+        return nullptr;
+    }
+    yr::SceneCompileResult compiled = yr::CompilePbrtScene(*loaded.scene);
+    if (!compiled.scene) {
+        g_last_error = compiled.diagnostics.empty() ? "PBRT compile failed" : compiled.diagnostics.front().message;
+        return nullptr;
+    }
+    auto* job = new RefJob();
+    job->ir = std::move(*compiled.scene);
+    job->settings = compiled.settings;
+    PrepareAlias(*job);
+    return job;
+}
+
+void yrref_job_destroy(void* job) { delete static_cast<RefJob*>(job); }
+
+// counts: vertices, indices, primitives, spheres, instances, materials,
+// emissive, analytic, env width, env height, alias count.
+void yrref_job_counts(void* handle, std::int64_t* c) {
+    const RefJob& j = *static_cast<RefJob*>(handle);
+    c[0] = static_cast<std::int64_t>(j.ir.vertices.size());
+    c[1] = static_cast<std::int64_t>(j.ir.indices.size());
+    c[2] = static_cast<std::int64_t>(j.ir.primitives.size());
+    c[3] = static_cast<std::int64_t>(j.ir.spheres.size());
+    c[4] = static_cast<std::int64_t>(j.ir.instances.size());
+    c[5] = static_cast<std::int64_t>(j.ir.materials.size());
+    c[6] = static_cast<std::int64_t>(j.ir.emissive_primitives.size());
+    c[7] = static_cast<std::int64_t>(j.ir.analytic_lights.size());
+    const yr::RenderEnvironment& env = j.ir.environment;
+    const bool tex = env.texture_index >= 0 && static_cast<std::size_t>(env.texture_index) < j.ir.textures.size();
+    c[8] = tex ? j.ir.textures[env.texture_index].width : 0;
+    c[9] = tex ? j.ir.textures[env.texture_index].height : 0;
+    c[10] = static_cast<std::int64_t>(j.alias_pmf.size());
+}
+
+// vertices: 12 floats each (position, normal, uv, tangent, handedness).
+void yrref_job_geometry(void* handle, float* vertices, std::uint32_t* indices, yrc_primitive* prims,
+                        yrc_sphere* spheres, yrc_instance* instances) {
+    const RefJob& j = *static_cast<RefJob*>(handle);
+    for (std::size_t i = 0; i < j.ir.vertices.size(); ++i) {
+        const yr::RenderVertex& v = j.ir.vertices[i];
+        const float row[12] = {v.position.x, v.position.y, v.position.z, v.normal.x, v.normal.y, v.normal.z,
+                               v.uv.x, v.uv.y, v.tangent.x, v.tangent.y, v.tangent.z, v.tangent_handedness};
+        std::copy(row, row + 12, vertices + 12 * i);
+    }
+    std::copy(j.ir.indices.begin(), j.ir.indices.end(), indices);
+    for (std::size_t i = 0; i < j.ir.primitives.size(); ++i) {
+        const yr::RenderPrimitive& p = j.ir.primitives[i];
+        prims[i] = yrc_primitive{p.first_index, p.index_count, p.material_index,
+                                 (p.has_normals ? 1u : 0u) | (p.has_uvs ? 2u : 0u) | (p.has_tangents ? 4u : 0u)};
+    }
+    for (std::size_t i = 0; i < j.ir.spheres.size(); ++i) {
+        const yr::RenderSphere& s = j.ir.spheres[i];
+        spheres[i] = yrc_sphere{{s.center.x, s.center.y, s.center.z}, s.radius, s.material_index, s.area_light_index,
+                                s.flip_normals ? 1 : 0, 0};
+    }
+    for (std::size_t i = 0; i < j.ir.instances.size(); ++i) {
+        instances[i].primitive = j.ir.instances[i].primitive.Value();
+        std::copy(j.ir.instances[i].object_to_world.m.begin(), j.ir.instances[i].object_to_world.m.end(),
+                  instances[i].object_to_world);
+    }
+}
+
+void yrref_job_materials(void* handle, yrc_material* out) {
+    const RefJob& j = *static_cast<RefJob*>(handle);
+    for (std::size_t i = 0; i < j.ir.materials.size(); ++i) {
+        const yr::RenderMaterial& m = j.ir.materials[i];
+        yrc_material& o = out[i];
+        std::memset(&o, 0, sizeof(o));
+        o.kind = static_cast<int32_t>(m.kind);
+        CopyRgb(m.reflectance.value, o.reflectance);
+        CopyRgb(m.eta.value, o.eta);
+        CopyRgb(m.k.value, o.k);
+        o.ior = m.ior;
+        o.uroughness = m.uroughness.value;
+        o.vroughness = m.vroughness.value;
+        o.remap_roughness = m.remap_roughness ? 1 : 0;
+        o.mix_material_a = m.mix_material_a;
+        o.mix_material_b = m.mix_material_b;
+        o.mix_amount = m.mix_amount.value;
+        o.coating_ior = m.coating_ior;
+        o.coating_roughness = m.coating_roughness.value;
+        o.coat_thickness = m.coat_thickness;
+        CopyRgb(m.coat_absorption, o.coat_absorption);
+        o.coat_maxdepth = m.coat_maxdepth;
+        o.coat_nsamples = m.coat_nsamples;
+        CopyRgb(m.sigma_a, o.sigma_a);
+        CopyRgb(m.sigma_s, o.sigma_s);
+        o.bssrdf_eta = m.bssrdf_eta;
+        o.bssrdf_index = m.bssrdf_index;
+        CopyRgb(m.emission, o.emission);
+        o.alpha = m.alpha.value;
+        CopyRgb(m.absorption_color, o.absorption_color);
+        o.absorption_distance = m.absorption_distance;
+        o.reflectance_texture = m.reflectance.texture;
+        o.alpha_texture = m.alpha.texture;
+        o.normal_map = m.normal_map;
+        o.measured_index = m.measured_index;
+    }
+}
+
+// Emissive primitives, the emissive power alias table, camera and settings.
+void yrref_job_lights(void* handle, yrc_emissive_primitive* emissive, float* alias_prob, int32_t* alias_index,
+                      float* alias_pmf, yrc_camera* camera, yrc_render_settings* settings) {
+    const RefJob& j = *static_cast<RefJob*>(handle);
+    for (std::size_t i = 0; i < j.ir.emissive_primitives.size(); ++i) {
+        const yr::EmissivePrimitive& e = j.ir.emissive_primitives[i];
+        emissive[i].primitive_index = e.primitive_index;
+        CopyRgb(e.radiance, emissive[i].radiance);
+        emissive[i].area = e.area;
+    }
+    std::copy(j.alias_prob.begin(), j.alias_prob.end(), alias_prob);
+    std::copy(j.alias_index.begin(), j.alias_index.end(), alias_index);
+    std::copy(j.alias_pmf.begin(), j.alias_pmf.end(), alias_pmf);
+    const yr::RenderCamera& c = j.ir.camera;
+    *camera = yrc_camera{{c.origin.x, c.origin.y, c.origin.z}, {c.forward.x, c.forward.y, c.forward.z},
+                         {c.right.x, c.right.y, c.right.z}, {c.up.x, c.up.y, c.up.z}, c.fov_y_radians};
+    const yr::RenderSettings& s = j.settings;
+    std::memset(settings, 0, sizeof(*settings));
+    settings->width = s.width;
+    settings->height = s.height;
+    settings->spp = s.spp;
+    settings->max_depth = s.max_depth;
+    settings->seed = s.seed;
+    settings->sampler = static_cast<int32_t>(s.sampler);
+    settings->radiance_clamp = s.radiance_clamp;
+    settings->adaptive_enabled = s.adaptive_sampling.enabled ? 1 : 0;
+    settings->adaptive_min_spp = s.adaptive_sampling.min_spp;
+    settings->adaptive_relative_error = s.adaptive_sampling.relative_error;
+    settings->adaptive_absolute_error = s.adaptive_sampling.absolute_error;
+    settings->adaptive_confidence = s.adaptive_sampling.confidence;
+}
+
+// Builds a job from the C-ABI scene description (textures, BSSRDF tables and
+// analytic lights are not carried). The environment texture becomes a
+// bilinear, repeat-wrapped RGBA texture with its distribution rebuilt by
+// BuildEnvironmentDistribution.
+void* yrref_job_from_desc(const yrc_scene_desc* d) {
+    auto* job = new RefJob();
+    yr::RenderSceneIR& ir = job->ir;
+    const yrc_geometry& g = d->geometry;
+    ir.vertices.resize(static_cast<std::size_t>(g.vertex_count));
+    for (std::int64_t v = 0; v < g.vertex_count; ++v) {
+        const float* p = reinterpret_cast<const float*>(reinterpret_cast<const char*>(g.positions) + v * g.vertex_stride);
+        ir.vertices[v].position = yr::Point3f{p[0], p[1], p[2]};
+        if (d->normals) {
+            const float* n = reinterpret_cast<const float*>(reinterpret_cast<const char*>(d->normals) + v * d->normal_stride);
+            ir.vertices[v].normal = yr::Vec3f{n[0], n[1], n[2]};
+        }
+    }
+    ir.indices.assign(g.indices, g.indices + g.index_count);
+    for (int32_t p = 0; p < g.primitive_count; ++p) {
+        const yrc_primitive& s = g.primitives[p];
+        ir.primitives.push_back(yr::RenderPrimitive{s.first_index, s.index_count, s.material_index,
+                                                    (s.flags & 1u) != 0, (s.flags & 2u) != 0, (s.flags & 4u) != 0});
+    }
+    for (int32_t i = 0; i < g.sphere_count; ++i) {
+        const yrc_sphere& s = g.spheres[i];
+        ir.spheres.push_back(yr::RenderSphere{yr::Point3f{s.center[0], s.center[1], s.center[2]}, s.radius,
+                                              s.material_index, s.area_light_index, s.flip_normals != 0});
+    }
+    for (int32_t i = 0; i < g.instance_count; ++i) {
+        yr::RenderInstance inst;
+        inst.primitive = yr::MeshPrimitiveHandle{g.instances[i].primitive};
+        std::copy(g.instances[i].object_to_world, g.instances[i].object_to_world + 16, inst.object_to_world.m.begin());
+        ir.instances.push_back(inst);
+    }
+    for (int32_t i = 0; i < d->material_count; ++i) {
+        const yrc_material& m = d->materials[i];
+        yr::RenderMaterial r;
+        r.kind = static_cast<yr::RenderMaterialKind>(m.kind);
+        r.reflectance.value = Rgb(m.reflectance);
+        r.eta.value = Rgb(m.eta);
+        r.k.value = Rgb(m.k);
+        r.ior = m.ior;
+        r.uroughness.value = m.uroughness;
+        r.vroughness.value = m.vroughness;
+        r.remap_roughness = m.remap_roughness != 0;
+        r.coating_ior = m.coating_ior;
+        r.coating_roughness.value = m.coating_roughness;
+        r.coat_thickness = m.coat_thickness;
+        r.coat_absorption = Rgb(m.coat_absorption);
+        r.coat_maxdepth = m.coat_maxdepth;
+        r.coat_nsamples = m.coat_nsamples;
+        r.sigma_a = Rgb(m.sigma_a);
+        r.sigma_s = Rgb(m.sigma_s);
+        r.bssrdf_eta = m.bssrdf_eta;
+        r.emission = Rgb(m.emission);
+        r.alpha.value = m.alpha;
+        r.absorption_color = Rgb(m.absorption_color);
+        r.absorption_distance = m.absorption_distance;
+        ir.materials.push_back(r);
+    }
+    for (int32_t i = 0; i < d->emissive_count; ++i) {
+        const yrc_emissive_primitive& e = d->emissive[i];
+        ir.emissive_primitives.push_back(yr::EmissivePrimitive{e.primitive_index, Rgb(e.radiance), e.area});
+    }
+    const yrc_environment& env = d->environment;
+    ir.environment.active = env.active != 0;
+    ir.environment.radiance = Rgb(env.radiance);
+    ir.environment.strength = env.strength;
+    ir.environment.rotation_radians = env.rotation_radians;
+    if (env.active && env.texels && env.width > 0 && env.height > 0) {
+        yr::RenderTexture tex;
+        tex.width = env.width;
+        tex.height = env.height;
+        tex.texels.resize(static_cast<std::size_t>(env.width) * env.height);
+        for (std::size_t i = 0; i < tex.texels.size(); ++i) {
+            tex.texels[i] = yr::Color4f{env.texels[4 * i], env.texels[4 * i + 1], env.texels[4 * i + 2], env.texels[4 * i + 3]};
+        }
+        ir.environment_distributions.push_back(yr::BuildEnvironmentDistribution(tex));
+        ir.environment.texture_index = static_cast<int>(ir.textures.size());
+        ir.environment.distribution_index = 0;
+        ir.textures.push_back(std::move(tex));
+    }
+    const yrc_camera& c = d->camera;
+    ir.camera.origin = yr::Point3f{c.origin[0], c.origin[1], c.origin[2]};
+    ir.camera.forward = yr::Vec3f{c.forward[0], c.forward[1], c.forward[2]};
+    ir.camera.right = yr::Vec3f{c.right[0], c.right[1], c.right[2]};
+    ir.camera.up = yr::Vec3f{c.up[0], c.up[1], c.up[2]};
+    ir.camera.fov_y_radians = c.fov_y_radians;
+    const yrc_render_settings& s = d->settings;
+    job->settings.integrator = yr::RenderIntegratorKind::Path;
+    job->settings.sampler = static_cast<yr::RenderSamplerKind>(s.sampler);
+    job->settings.width = s.width;
+    job->settings.height = s.height;
+    job->settings.spp = s.spp;
+    job->settings.max_depth = s.max_depth;
+    job->settings.seed = s.seed;
+    job->settings.radiance_clamp = s.radiance_clamp;
+    job->settings.adaptive_sampling.enabled = s.adaptive_enabled != 0;
+    job->settings.adaptive_sampling.min_spp = s.adaptive_min_spp;
+    job->settings.adaptive_sampling.relative_error = s.adaptive_relative_error;
+    job->settings.adaptive_sampling.absolute_error = s.adaptive_absolute_error;
+    job->settings.adaptive_sampling.confidence = s.adaptive_confidence;
+    PrepareAlias(*job);
+    return job;
+}
+
+// Renders the job with the reference CPU backend. film_out: width*height
+// FilmPixel (56 bytes each). stats: samples, rays_traced, shadow_rays,
+// occluded, hits, misses, bad samples (7 uint64). Returns 0 on success.
+int yrref_job_render(void* handle, int threads, int spp_override, void* film_out, std::uint64_t* stats,
+                     double* seconds) {
+    const RefJob& j = *static_cast<RefJob*>(handle);
+    yr::RenderJob job{j.ir, j.settings};
+    job.settings.requested_backend = yr::RenderBackendKind::Cpu;
+    job.settings.threads = threads;
+    if (spp_override > 0) job.settings.spp = spp_override;
+    yr::CpuBackend backend;
+    yr::BackendPrepareResult prepared = backend.Prepare(std::move(job));
+    if (!prepared.ok) {
+        g_last_error = prepared.error;
+        return 1;
+    }
+    yr::RenderRequest request;
+    yr::RenderResult result = backend.Render(*prepared.scene, request);
+    if (!result.ok || !result.film) {
+        g_last_error = result.error;
+        return 2;
+    }
+    std::memcpy(film_out, result.film->Pixels().data(), result.film->Pixels().size() * sizeof(yr::FilmPixel));
+    if (stats) {
+        stats[0] = result.stats.samples_rendered;
+        stats[1] = result.stats.rays_traced;
+        stats[2] = result.stats.shadow_rays;
+        stats[3] = result.stats.occluded_shadow_rays;
+        stats[4] = result.stats.hits;
+        stats[5] = result.stats.misses;
+        stats[6] = result.film->BadSampleCount();
+    }
+    if (seconds) *seconds = result.stats.elapsed_seconds;
+    return 0;
+}
+
+}  // extern "C"

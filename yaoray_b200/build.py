@@ -25,6 +25,7 @@ OBJ = PKG / "_build"
 LIB = PKG / "libyrcuda.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NO_FMA_UNITS = {"render_kernels.cu": ["-fmad=false"]}
 
 
 def _nvcc() -> str:
@@ -61,6 +62,8 @@ def _compile(src: Path, ptxas_verbose: bool) -> tuple[Path, str]:
     if src.suffix == ".cu":
         cmd += ["-Xptxas", "-v"] if ptxas_verbose else []
         cmd += ["--expt-relaxed-constexpr"]
+        # Shading follows the reference's rounding: no fused multiply-add.
+        cmd += NO_FMA_UNITS.get(src.name, [])
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{res.stdout}\n{res.stderr}")

@@ -1,0 +1,144 @@
+"""Cornell-box scene of the plain-MIS configuration: a 5.56-unit box of five
+wall quads, a short box (1.65 tall, rotated -17 degrees about y) and a tall
+box (3.3 tall, +17 degrees) — 34 triangles — plus a 1.3 x 1.05 quad area
+light (2 more triangles) emitting (17, 12, 4); Lambertian red
+(0.63, 0.065, 0.05), green (0.14, 0.45, 0.09) and white 0.73; pinhole camera
+with a 40 degree vertical fov; 256 x 256, 64 spp Owen-scrambled Sobol (seed
+0), max depth 8 (Russian roulette from depth 3 is built into the path
+integrator).
+
+`pbrt_text()` writes it as a PBRT v4 "trianglemesh" file for the reference's
+own frontend; `scene()` builds the same RenderSceneIR directly (the tests
+check both agree field by field with what the reference compiles).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .accel import SceneGeometry
+from .render import EMISSIVE_DTYPE, OWEN_SOBOL, RenderScene, default_material
+
+SIZE = 5.56
+WHITE = (0.73, 0.73, 0.73)
+RED = (0.63, 0.065, 0.05)
+GREEN = (0.14, 0.45, 0.09)
+LIGHT_L = (17.0, 12.0, 4.0)
+EYE = (2.78, 2.73, -8.0)
+LOOK = (2.78, 2.73, 0.0)
+FOV = 40.0
+
+
+def _box(cx, cz, w, h, d, deg):
+    """Axis box rotated about y by `deg` around its centre: 8 corners, 12
+    triangles wound outward."""
+    a = math.radians(deg)
+    ca, sa = math.cos(a), math.sin(a)
+    pts = []
+    for y in (0.0, h):
+        for (x, z) in ((-w / 2, -d / 2), (w / 2, -d / 2), (w / 2, d / 2), (-w / 2, d / 2)):
+            pts.append((round(cx + ca * x + sa * z, 4), y, round(cz - sa * x + ca * z, 4)))
+    tris = [[0, 2, 1], [0, 3, 2],          # bottom
+            [4, 5, 6], [4, 6, 7],          # top
+            [0, 1, 5], [0, 5, 4],          # front
+            [1, 2, 6], [1, 6, 5],          # right
+            [2, 3, 7], [2, 7, 6],          # back
+            [3, 0, 4], [3, 4, 7]]          # left
+    return pts, tris
+
+
+def shapes():
+    """[(material name, points, triangles, emission or None)] in file order."""
+    s = SIZE
+    quad = [[0, 1, 2], [0, 2, 3]]
+    out = [
+        ("white", [(0, 0, 0), (s, 0, 0), (s, 0, s), (0, 0, s)], quad, None),            # floor
+        ("white", [(0, s, 0), (0, s, s), (s, s, s), (s, s, 0)], quad, None),            # ceiling
+        ("white", [(0, 0, s), (s, 0, s), (s, s, s), (0, s, s)], quad, None),            # back
+        ("red", [(s, 0, 0), (s, s, 0), (s, s, s), (s, 0, s)], quad, None),              # left (image left)
+        ("green", [(0, 0, 0), (0, 0, s), (0, s, s), (0, s, 0)], quad, None),            # right
+    ]
+    p, t = _box(1.85, 1.69, 1.65, 1.65, 1.65, -17.0)
+    out.append(("white", p, t, None))
+    p, t = _box(3.69, 3.51, 1.65, 3.30, 1.65, 17.0)
+    out.append(("white", p, t, None))
+    y = s - 0.005
+    lx0, lx1, lz0, lz1 = 2.13, 3.43, 2.27, 3.32
+    out.append(("white", [(lx0, y, lz0), (lx0, y, lz1), (lx1, y, lz1), (lx1, y, lz0)], quad, LIGHT_L))
+    return out
+
+
+def pbrt_text(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8) -> str:
+    lines = [
+        "# Cornell box: 34 scene triangles + a 2-triangle area light.",
+        f"LookAt {EYE[0]} {EYE[1]} {EYE[2]}  {LOOK[0]} {LOOK[1]} {LOOK[2]}  0 1 0",
+        f'Camera "perspective" "float fov" [{FOV}]',
+        f'Sampler "sobol" "integer pixelsamples" [{spp}]',
+        f'Integrator "path" "integer maxdepth" [{max_depth}]',
+        f'Film "rgb" "integer xresolution" [{width}] "integer yresolution" [{height}] "string filename" ["cornell.exr"]',
+        "WorldBegin",
+    ]
+    for name, rgb in (("white", WHITE), ("red", RED), ("green", GREEN)):
+        lines.append(f'MakeNamedMaterial "{name}" "string type" ["diffuse"] "rgb reflectance" [{rgb[0]} {rgb[1]} {rgb[2]}]')
+    for name, pts, tris, emission in shapes():
+        lines.append("AttributeBegin")
+        if emission is not None:
+            lines.append(f'AreaLightSource "diffuse" "rgb L" [{emission[0]} {emission[1]} {emission[2]}]')
+        lines.append(f'NamedMaterial "{name}"')
+        flat_p = " ".join(f"{c}" for pt in pts for c in pt)
+        flat_i = " ".join(str(i) for tri in tris for i in tri)
+        lines.append(f'Shape "trianglemesh" "point3 P" [{flat_p}] "integer indices" [{flat_i}]')
+        lines.append("AttributeEnd")
+    lines.append("WorldEnd")
+    return "\n".join(lines) + "\n"
+
+
+def camera() -> dict:
+    """The camera basis the reference derives from LookAt + fov (forward,
+    right = forward x up, true up = right x forward)."""
+    eye = np.array(EYE, np.float32)
+    fwd = np.array(LOOK, np.float32) - eye
+    fwd = fwd / np.float32(np.sqrt(np.float32(np.dot(fwd, fwd))))
+    right = np.cross(fwd, np.array([0, 1, 0], np.float32)).astype(np.float32)
+    right = right / np.float32(np.sqrt(np.float32(np.dot(right, right))))
+    up = np.cross(right, fwd).astype(np.float32)
+    return {"origin": tuple(map(float, eye)), "forward": tuple(map(float, fwd)), "right": tuple(map(float, right)),
+            "up": tuple(map(float, up)), "fov_y_radians": float(np.float32(FOV) * np.float32(math.pi) / np.float32(180))}
+
+
+def scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8) -> RenderScene:
+    """The RenderSceneIR the reference compiles from `pbrt_text()`."""
+    # Named materials in the order the reference's compiler emits them.
+    names = {"green": 0, "red": 1, "white": 2}
+    mats = np.stack([default_material(reflectance=GREEN), default_material(reflectance=RED),
+                     default_material(reflectance=WHITE)])
+    meshes, emissive = [], []
+    light_mat = None
+    for k, (name, pts, tris, em) in enumerate(shapes()):
+        meshes.append((np.array(pts, np.float32), np.array(tris, np.uint32)))
+        if em is not None:
+            light_mat = k
+    geom = SceneGeometry.from_meshes(meshes)
+    prims = geom.primitives
+    for k, (name, pts, tris, em) in enumerate(shapes()):
+        prims[k]["material_index"] = names[name]
+    # The emitting shape gets its own material carrying the emission.
+    lm = default_material(reflectance=WHITE, emission=LIGHT_L)
+    mats = np.concatenate([mats, lm[None]])
+    prims[light_mat]["material_index"] = len(mats) - 1
+    p = geom.positions
+    idx = geom.indices.reshape(-1, 3)
+    first = prims[light_mat]["first_index"] // 3
+    count = prims[light_mat]["index_count"] // 3
+    area = np.float32(0)
+    for t in range(first, first + count):
+        a, b, c = p[idx[t, 0]], p[idx[t, 1]], p[idx[t, 2]]
+        cr = np.cross(b - a, c - a).astype(np.float32)
+        area = np.float32(area + np.float32(np.sqrt(np.float32(np.dot(cr, cr)))) * np.float32(0.5))
+    em = np.zeros(1, EMISSIVE_DTYPE)
+    em[0]["primitive_index"] = light_mat
+    em[0]["radiance"] = LIGHT_L
+    em[0]["area"] = area
+    return RenderScene(geom, mats, camera(), width, height, spp=spp, max_depth=max_depth, seed=0,
+                       sampler=OWEN_SOBOL, emissive=em)

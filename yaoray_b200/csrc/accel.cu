@@ -335,6 +335,10 @@ yrc_status LaunchInternal(yrc_accel* a, const yrc_ray* rays, int64_t count, int3
 
 }  // namespace
 
+AccelParams AccelParamsOf(const yrc_accel* a) { return a->params; }
+int TraceShapeOf(const yrc_accel* a, int any_hit) { return a->trace_shape[any_hit ? 1 : 0]; }
+int* AccelErrorWord(yrc_accel* a) { return a->d_error; }
+
 yrc_status CheckDeviceError(yrc_accel* a) {
     int status = 0;
     cudaError_t err = cudaMemcpy(&status, a->d_error, sizeof(int), cudaMemcpyDeviceToHost);

@@ -1,0 +1,676 @@
+// Render scene upload and the device pass loop behind yrc_render_scene_create
+// / yrc_render — the CUDA backend's Prepare and Render.
+//
+// Pass semantics follow RenderCpuPathTrace (src/backends/cpu/cpu_path_tracer.cpp:
+// 39-229): every active pixel takes one sample attempt per pass, its sample
+// index is the film's current sample count, a non-finite sample is dropped
+// and counted, and (with adaptive sampling) converged pixels stop. To fill
+// the GPU, one batch renders several consecutive passes at once: pixel p's
+// j-th path uses sample index count(p) + j, and the film kernel accepts them
+// in order, stopping at the first non-finite sample (whose index the next
+// batch re-uses, as the reference's next pass would) or at convergence.
+// With a progress callback the batch is one pass, so the callback sees the
+// film after every pass exactly as the reference's does.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "render_kernels.hpp"
+#include "render_types.hpp"
+#include "trace_kernels.hpp"
+#include "yrc_internal.hpp"
+
+namespace yrc {
+namespace {
+
+yrc_status CudaError(cudaError_t err, const char* what) {
+    return Fail(err == cudaErrorMemoryAllocation ? YRC_ERR_OUT_OF_MEMORY : YRC_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+// Device allocation bookkeeping for one render scene.
+struct DeviceArena {
+    std::vector<void*> blocks;
+    int64_t bytes = 0;
+    cudaError_t err = cudaSuccess;
+
+    template <typename T>
+    T* Alloc(size_t count) {
+        if (err != cudaSuccess) return nullptr;
+        void* p = nullptr;
+        const size_t n = std::max<size_t>(count, 1) * sizeof(T);
+        err = cudaMalloc(&p, n);
+        if (err != cudaSuccess) return nullptr;
+        blocks.push_back(p);
+        bytes += static_cast<int64_t>(n);
+        return static_cast<T*>(p);
+    }
+    template <typename T>
+    T* Upload(const T* src, size_t count) {
+        T* d = Alloc<T>(count);
+        if (d && count && src) err = cudaMemcpy(d, src, count * sizeof(T), cudaMemcpyHostToDevice);
+        return d;
+    }
+    template <typename T>
+    T* Upload(const std::vector<T>& v) {
+        return Upload(v.data(), v.size());
+    }
+    void Release() {
+        for (void* p : blocks) cudaFree(p);
+        blocks.clear();
+        bytes = 0;
+    }
+};
+
+float HostTriangleArea(const float* a, const float* b, const float* c) {
+    const float e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    const float e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+    const float cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    const float area = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) * 0.5f;
+    return std::isfinite(area) && area > 0.0f ? area : 0.0f;
+}
+
+float HostLuminance(const float* c) { return std::max(0.0f, 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2]); }
+
+constexpr int kMaxBatch = 64;
+
+}  // namespace
+}  // namespace yrc
+
+struct yrc_render_scene {
+    int device = 0;
+    int sm_count = 148;
+    yrc_accel* accel = nullptr;
+    yrc::DevScene dev{};
+    yrc::DeviceArena arena;
+    yrc_render_settings settings{};
+    int bvh_nodes = 0;
+    int bvh_max_depth = 0;
+    // Render resources, allocated on first render.
+    yrc::DeviceArena work;
+    int64_t capacity = 0;
+    yrc::PathState ps{};
+    yrc::Queues q{};
+    float4* transmittance = nullptr;
+    yrc_film_pixel* film = nullptr;
+    int32_t* attempts = nullptr;
+    int32_t* active = nullptr;
+    unsigned long long* scalars = nullptr;  // active count, next count, bad, converged
+    int32_t* batch = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int32_t graph_max_batch = -1;
+    std::mutex mutex;
+};
+
+extern "C" {
+
+void yrc_render_scene_destroy(yrc_render_scene* scene) {
+    if (!scene) return;
+    cudaSetDevice(scene->device);
+    if (scene->graph) cudaGraphExecDestroy(scene->graph);
+    if (scene->stream) cudaStreamDestroy(scene->stream);
+    scene->work.Release();
+    scene->arena.Release();
+    yrc_accel_destroy(scene->accel);
+    delete scene;
+}
+
+int64_t yrc_render_scene_device_bytes(const yrc_render_scene* scene) {
+    return scene ? scene->arena.bytes + scene->work.bytes + yrc_accel_device_bytes(scene->accel) : 0;
+}
+
+yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene** out) {
+    using namespace yrc;
+    if (!desc || !out) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_scene_create: null argument");
+    *out = nullptr;
+    const yrc_geometry& g = desc->geometry;
+    const yrc_render_settings& st = desc->settings;
+    if (st.width <= 0 || st.height <= 0) return Fail(YRC_ERR_INVALID_ARGUMENT, "Film dimensions must be positive");
+    if ((desc->flat == nullptr) == (desc->two_level == nullptr)) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "exactly one of flat / two_level acceleration must be given");
+    }
+    if (desc->material_count < 0 || (desc->material_count > 0 && !desc->materials) || desc->emissive_count < 0 ||
+        (desc->emissive_count > 0 && !desc->emissive)) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "invalid material or light arrays");
+    }
+    if (desc->analytic_count > 0) {
+        return Fail(YRC_ERR_UNSUPPORTED, "analytic (point/spot/distant) lights are not rendered on the device");
+    }
+    for (int32_t i = 0; i < desc->material_count; ++i) {
+        const yrc_material& m = desc->materials[i];
+        if (m.reflectance_texture >= 0 || m.alpha_texture >= 0 || m.normal_map >= 0) {
+            return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": textured materials are not shaded on the device");
+        }
+        if (m.kind == YRC_MAT_MEASURED && m.measured_index >= 0) {
+            return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": measured BRDFs are not shaded on the device");
+        }
+        if (m.kind == YRC_MAT_SUBSURFACE) {
+            return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": subsurface materials are not shaded on the device");
+        }
+        if (m.alpha < 0.5f) {
+            return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": alpha-cut-out surfaces are not traced on the device");
+        }
+    }
+    auto* s = new (std::nothrow) yrc_render_scene();
+    if (!s) return Fail(YRC_ERR_OUT_OF_MEMORY, "host allocation failed");
+    cudaGetDevice(&s->device);
+    cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device);
+    s->settings = st;
+
+    yrc_status status = desc->flat ? yrc_accel_create_flat(&g, desc->flat, &s->accel)
+                                   : yrc_accel_create_two_level(&g, desc->two_level, &s->accel);
+    if (status != YRC_OK) {
+        const std::string msg = yrc_last_error();
+        yrc_render_scene_destroy(s);
+        return Fail(status, msg);
+    }
+    if (desc->flat) {
+        s->bvh_nodes = static_cast<int>(desc->flat->node_count);
+        s->bvh_max_depth = desc->flat->max_depth;
+    } else {
+        int64_t nodes = desc->two_level->tlas_node_count;
+        int blas_depth = 0;
+        for (int32_t b = 0; b < desc->two_level->blas_count; ++b) {
+            nodes += desc->two_level->blases[b].bvh.node_count;
+            blas_depth = std::max(blas_depth, desc->two_level->blases[b].bvh.max_depth);
+        }
+        s->bvh_nodes = static_cast<int>(nodes);
+        s->bvh_max_depth = desc->two_level->tlas_max_depth + blas_depth;
+    }
+
+    DeviceArena& A = s->arena;
+    DevScene& d = s->dev;
+    d.accel = AccelParamsOf(s->accel);
+
+    // Shading geometry: flat triangle -> (primitive, vertex indices).
+    std::vector<int32_t> tri_prim;
+    std::vector<int4> tri_vertices;
+    std::vector<int32_t> prim_first_flat(static_cast<size_t>(g.primitive_count), 0);
+    for (int32_t p = 0; p < g.primitive_count; ++p) {
+        prim_first_flat[static_cast<size_t>(p)] = static_cast<int32_t>(tri_prim.size());
+        const uint32_t tris = g.primitives[p].index_count / 3;
+        for (uint32_t t = 0; t < tris; ++t) {
+            const uint64_t o = static_cast<uint64_t>(g.primitives[p].first_index) + 3ull * t;
+            int4 v = make_int4(0, 0, 0, 0);
+            if (o + 2 < static_cast<uint64_t>(g.index_count)) {
+                v = make_int4(static_cast<int>(g.indices[o]), static_cast<int>(g.indices[o + 1]),
+                              static_cast<int>(g.indices[o + 2]), 0);
+            }
+            tri_prim.push_back(p);
+            tri_vertices.push_back(v);
+        }
+    }
+    std::vector<float4> pos(static_cast<size_t>(g.vertex_count));
+    for (int64_t v = 0; v < g.vertex_count; ++v) {
+        const float* q = VertexPosition(g, static_cast<uint64_t>(v));
+        pos[static_cast<size_t>(v)] = make_float4(q[0], q[1], q[2], 0.0f);
+    }
+    std::vector<float4> nrm;
+    if (desc->normals) {
+        nrm.resize(static_cast<size_t>(g.vertex_count));
+        for (int64_t v = 0; v < g.vertex_count; ++v) {
+            const float* q = reinterpret_cast<const float*>(reinterpret_cast<const char*>(desc->normals) +
+                                                            v * desc->normal_stride);
+            nrm[static_cast<size_t>(v)] = make_float4(q[0], q[1], q[2], 0.0f);
+        }
+    }
+    std::vector<int32_t> prim_material(static_cast<size_t>(g.primitive_count));
+    std::vector<uint32_t> prim_flags(static_cast<size_t>(g.primitive_count));
+    for (int32_t p = 0; p < g.primitive_count; ++p) {
+        const int32_t mi = g.primitives[p].material_index;
+        prim_material[static_cast<size_t>(p)] = (mi >= 0 && mi < desc->material_count) ? mi : -1;
+        prim_flags[static_cast<size_t>(p)] = g.primitives[p].flags;
+    }
+    std::vector<float4> spheres(static_cast<size_t>(g.sphere_count));
+    std::vector<int32_t> sphere_material(static_cast<size_t>(g.sphere_count)), sphere_flip(static_cast<size_t>(g.sphere_count));
+    for (int32_t i = 0; i < g.sphere_count; ++i) {
+        const yrc_sphere& sp = g.spheres[i];
+        spheres[static_cast<size_t>(i)] = make_float4(sp.center[0], sp.center[1], sp.center[2], sp.radius);
+        sphere_material[static_cast<size_t>(i)] =
+            (sp.material_index >= 0 && sp.material_index < desc->material_count) ? sp.material_index : -1;
+        sphere_flip[static_cast<size_t>(i)] = sp.flip_normals ? 1 : 0;
+    }
+    std::vector<float> o2w;
+    if (desc->two_level) {
+        for (int32_t i = 0; i < desc->two_level->instance_count; ++i) {
+            const float* m = desc->two_level->instances[i].object_to_world;
+            o2w.insert(o2w.end(), m, m + 16);
+        }
+    }
+    d.tri_prim = A.Upload(tri_prim);
+    d.tri_vertices = A.Upload(tri_vertices);
+    d.positions = A.Upload(pos);
+    d.normals = nrm.empty() ? nullptr : A.Upload(nrm);
+    d.prim_material = A.Upload(prim_material);
+    d.prim_flags = A.Upload(prim_flags);
+    d.spheres = A.Upload(spheres);
+    d.sphere_material = A.Upload(sphere_material);
+    d.sphere_flip = A.Upload(sphere_flip);
+    d.instance_o2w = A.Upload(o2w);
+    d.primitive_count = g.primitive_count;
+    d.sphere_count = g.sphere_count;
+    d.instance_count = desc->two_level ? desc->two_level->instance_count : 0;
+
+    // Materials.
+    std::vector<DevMaterial> mats(static_cast<size_t>(desc->material_count));
+    bool transparent = false;
+    for (int32_t i = 0; i < desc->material_count; ++i) {
+        const yrc_material& m = desc->materials[i];
+        DevMaterial& dm = mats[static_cast<size_t>(i)];
+        std::memset(&dm, 0, sizeof(dm));
+        dm.kind = m.kind;
+        std::memcpy(dm.reflectance, m.reflectance, sizeof(dm.reflectance));
+        dm.ior = m.ior;
+        dm.uroughness = m.uroughness;
+        dm.vroughness = m.vroughness;
+        dm.coating_ior = m.coating_ior;
+        dm.coat_thickness = m.coat_thickness;
+        std::memcpy(dm.coat_absorption, m.coat_absorption, sizeof(dm.coat_absorption));
+        dm.coat_maxdepth = m.coat_maxdepth;
+        dm.coat_nsamples = m.coat_nsamples;
+        std::memcpy(dm.emission, m.emission, sizeof(dm.emission));
+        std::memcpy(dm.absorption_color, m.absorption_color, sizeof(dm.absorption_color));
+        dm.absorption_distance = m.absorption_distance;
+        std::memcpy(dm.sigma_a, m.sigma_a, sizeof(dm.sigma_a));
+        std::memcpy(dm.sigma_s, m.sigma_s, sizeof(dm.sigma_s));
+        dm.bssrdf_eta = m.bssrdf_eta;
+        dm.bssrdf_index = m.bssrdf_index;
+        if (m.kind == YRC_MAT_DIELECTRIC || m.kind == YRC_MAT_THIN_DIELECTRIC) transparent = true;
+    }
+    d.materials = A.Upload(mats);
+    d.material_count = desc->material_count;
+    d.any_transparent = transparent ? 1 : 0;
+
+    // Emissive lights, alias table, per-light triangle area CDF.
+    const int32_t ne = desc->emissive_count;
+    std::vector<int32_t> e_prim(static_cast<size_t>(ne)), tri_off(static_cast<size_t>(ne)), tri_cnt(static_cast<size_t>(ne));
+    std::vector<float> e_rad(static_cast<size_t>(ne) * 3), e_area(static_cast<size_t>(ne)), e_parea(static_cast<size_t>(ne));
+    std::vector<float> cdf;
+    std::vector<int32_t> cdf_tri;
+    std::vector<int32_t> prim_emissive(static_cast<size_t>(g.primitive_count), -1);
+    float total_power = 0.0f;
+    for (int32_t e = 0; e < ne; ++e) {
+        const yrc_emissive_primitive& ep = desc->emissive[e];
+        e_prim[static_cast<size_t>(e)] = ep.primitive_index;
+        std::memcpy(&e_rad[3 * static_cast<size_t>(e)], ep.radiance, 3 * sizeof(float));
+        e_area[static_cast<size_t>(e)] = ep.area;
+        const float area = std::isfinite(ep.area) && ep.area > 0.0f ? ep.area : 0.0f;
+        total_power += area * HostLuminance(ep.radiance);
+        tri_off[static_cast<size_t>(e)] = static_cast<int32_t>(cdf.size());
+        float cum = 0.0f;
+        if (ep.primitive_index >= 0 && ep.primitive_index < g.primitive_count) {
+            if (prim_emissive[static_cast<size_t>(ep.primitive_index)] < 0) {
+                prim_emissive[static_cast<size_t>(ep.primitive_index)] = e;
+            }
+            const yrc_primitive& pr = g.primitives[ep.primitive_index];
+            const uint32_t tris = pr.index_count / 3;
+            for (uint32_t t = 0; t < tris; ++t) {
+                const uint64_t o = static_cast<uint64_t>(pr.first_index) + 3ull * t;
+                const float a = HostTriangleArea(VertexPosition(g, g.indices[o]), VertexPosition(g, g.indices[o + 1]),
+                                                 VertexPosition(g, g.indices[o + 2]));
+                if (a <= 0.0f) continue;
+                cum += a;
+                cdf.push_back(cum);
+                cdf_tri.push_back(prim_first_flat[static_cast<size_t>(ep.primitive_index)] + static_cast<int32_t>(t));
+            }
+        }
+        tri_cnt[static_cast<size_t>(e)] = static_cast<int32_t>(cdf.size()) - tri_off[static_cast<size_t>(e)];
+        e_parea[static_cast<size_t>(e)] = cum;
+    }
+    d.emissive_count = ne;
+    d.emissive_prim = A.Upload(e_prim);
+    d.emissive_radiance = A.Upload(e_rad);
+    d.emissive_area = A.Upload(e_area);
+    d.emissive_tri_offset = A.Upload(tri_off);
+    d.emissive_tri_count = A.Upload(tri_cnt);
+    d.tri_cdf = A.Upload(cdf);
+    d.tri_local = A.Upload(cdf_tri);
+    d.emissive_prim_area = A.Upload(e_parea);
+    d.prim_emissive = A.Upload(prim_emissive);
+    d.total_emissive_power = total_power;
+    const yrc_alias_table& at = desc->emissive_power;
+    d.alias_count = (at.count == ne && at.probability && at.alias && at.pmf) ? ne : 0;
+    d.alias_prob = d.alias_count ? A.Upload(at.probability, static_cast<size_t>(ne)) : nullptr;
+    d.alias_index = d.alias_count ? A.Upload(at.alias, static_cast<size_t>(ne)) : nullptr;
+    d.alias_pmf = d.alias_count ? A.Upload(at.pmf, static_cast<size_t>(ne)) : nullptr;
+
+    // Environment.
+    const yrc_environment& env = desc->environment;
+    DevEnvironment& de = d.env;
+    std::memset(&de, 0, sizeof(de));
+    de.active = env.active;
+    std::memcpy(de.radiance, env.radiance, sizeof(de.radiance));
+    de.strength = env.strength;
+    de.rotation = env.rotation_radians;
+    if (env.active && env.texels && env.width > 0 && env.height > 0) {
+        const size_t texels = static_cast<size_t>(env.width) * static_cast<size_t>(env.height);
+        de.width = env.width;
+        de.height = env.height;
+        de.texels = A.Upload(env.texels, texels * 4);
+        if (env.texel_weights && env.row_weights && env.row_cdf && env.conditional_cdfs) {
+            de.texel_weights = A.Upload(env.texel_weights, texels);
+            de.row_weights = A.Upload(env.row_weights, static_cast<size_t>(env.height));
+            de.row_cdf = A.Upload(env.row_cdf, static_cast<size_t>(env.height));
+            de.conditional_cdfs = A.Upload(env.conditional_cdfs, texels);
+            de.total_weight = env.total_weight;
+        }
+    }
+
+    // Camera and settings.
+    const yrc_camera& c = desc->camera;
+    std::memcpy(d.cam_origin, c.origin, sizeof(d.cam_origin));
+    std::memcpy(d.cam_forward, c.forward, sizeof(d.cam_forward));
+    std::memcpy(d.cam_right, c.right, sizeof(d.cam_right));
+    std::memcpy(d.cam_up, c.up, sizeof(d.cam_up));
+    d.cam_half_height = std::tan(c.fov_y_radians * 0.5f);
+    d.width = st.width;
+    d.height = st.height;
+    d.spp = std::max(1, st.spp);
+    d.max_depth = std::max(1, st.max_depth);
+    d.sampler = st.sampler;
+    d.seed = st.seed;
+    d.radiance_clamp = st.radiance_clamp;
+
+    if (A.err != cudaSuccess) {
+        const cudaError_t err = A.err;
+        yrc_render_scene_destroy(s);
+        return CudaError(err, "render scene upload");
+    }
+    *out = s;
+    return Ok();
+}
+
+}  // extern "C"
+
+namespace yrc {
+namespace {
+
+// Allocates the path state and queues for `capacity` paths.
+yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
+    const int64_t pixels = static_cast<int64_t>(s->settings.width) * s->settings.height;
+    if (s->capacity >= capacity && s->film) return Ok();
+    if (s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    s->work.Release();
+    DeviceArena& W = s->work;
+    PathState& ps = s->ps;
+    ps.pixel = W.Alloc<int32_t>(capacity);
+    ps.sample = W.Alloc<int32_t>(capacity);
+    ps.throughput = W.Alloc<float4>(capacity);
+    ps.radiance = W.Alloc<float4>(capacity);
+    ps.prev = W.Alloc<float4>(capacity);
+    ps.flags = W.Alloc<uint32_t>(capacity);
+    ps.medium = W.Alloc<float4>(capacity);
+    ps.rng_state = W.Alloc<uint64_t>(capacity);
+    ps.rng_inc = W.Alloc<uint64_t>(capacity);
+    ps.aov_albedo = W.Alloc<float4>(capacity);
+    ps.aov_normal = W.Alloc<float4>(capacity);
+    ps.nee = W.Alloc<float4>(3 * capacity);
+    ps.nee_tp = W.Alloc<float4>(capacity);
+    ps.nee_vis = nullptr;
+    Queues& q = s->q;
+    q.ray_in = W.Alloc<float4>(2 * capacity);
+    q.path_in = W.Alloc<int32_t>(capacity);
+    q.hits = W.Alloc<float4>(capacity);
+    q.inst = W.Alloc<int32_t>(capacity);
+    q.ray_out = W.Alloc<float4>(2 * capacity);
+    q.path_out = W.Alloc<int32_t>(capacity);
+    q.shadow_ray = W.Alloc<float4>(2 * 2 * capacity);
+    q.shadow_slot = W.Alloc<int32_t>(2 * capacity);
+    q.shadow_occluded = W.Alloc<uint8_t>(3 * capacity);
+    q.nee_paths = W.Alloc<int32_t>(capacity);
+    q.counters = W.Alloc<unsigned long long>(kCtrCount);
+    s->transmittance = s->dev.any_transparent ? W.Alloc<float4>(3 * capacity) : nullptr;
+    s->film = W.Alloc<yrc_film_pixel>(static_cast<size_t>(pixels));
+    s->attempts = W.Alloc<int32_t>(static_cast<size_t>(pixels));
+    s->active = W.Alloc<int32_t>(static_cast<size_t>(pixels));
+    s->scalars = W.Alloc<unsigned long long>(4);
+    s->batch = W.Alloc<int32_t>(1);
+    if (W.err == cudaSuccess && !s->stream) W.err = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (W.err != cudaSuccess) {
+        const cudaError_t err = W.err;
+        s->work.Release();
+        s->film = nullptr;
+        s->capacity = 0;
+        return CudaError(err, "render working memory");
+    }
+    if (s->transmittance) cudaMemsetAsync(s->transmittance, 0, sizeof(float4) * 3 * capacity, s->stream);
+    cudaMemsetAsync(q.shadow_occluded, 1, 3 * capacity, s->stream);
+    s->capacity = capacity;
+    return Ok();
+}
+
+// Records one batch (generate, max_depth bounces, film, next active list).
+yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
+    const DevScene& sc = s->dev;
+    const int64_t C = s->capacity;
+    const int64_t pixels = static_cast<int64_t>(sc.width) * sc.height;
+    cudaStream_t st = s->stream;
+    BatchArgs b{s->active, s->scalars + 0, s->scalars + 1, s->batch, s->film};
+    FilmArgs f{s->attempts, s->scalars + 2, s->scalars + 3, s->settings.adaptive_enabled, s->settings.adaptive_min_spp,
+               s->settings.adaptive_relative_error, s->settings.adaptive_absolute_error,
+               s->settings.adaptive_confidence};
+    LaunchGenerate(sc, s->ps, s->q, b, C, s->sm_count, st);
+    Queues q = s->q;
+    for (int depth = 0; depth < sc.max_depth; ++depth) {
+        LaunchResetCounters(q, st);
+        TraceArgs ta{};
+        ta.accel = sc.accel;
+        ta.rays = q.ray_in;
+        ta.count = C;
+        ta.count_ptr = q.counters + kCtrIn;
+        ta.hits = reinterpret_cast<yrc_hit*>(q.hits);
+        ta.instances = q.inst;
+        ta.counter = q.counters + kCtrTrace;
+        ta.error = AccelErrorWord(s->accel);
+        cudaError_t err = LaunchTrace(ta, false, false, TraceShapeOf(s->accel, 0), st, s->sm_count);
+        if (err != cudaSuccess) return CudaError(err, "extend trace");
+        LaunchShade(sc, s->ps, q, depth, C, s->sm_count, st);
+        if (sc.any_transparent) {
+            ShadowArgs sa{};
+            sa.accel = sc.accel;
+            sa.rays = q.shadow_ray;
+            sa.count_ptr = q.counters + kCtrShadow;
+            sa.capacity = 2 * C;
+            sa.out_index = q.shadow_slot;
+            sa.transmittance = s->transmittance;
+            sa.tri_prim = sc.tri_prim;
+            sa.prim_material = sc.prim_material;
+            sa.sphere_material = sc.sphere_material;
+            sa.materials = sc.materials;
+            sa.error = ta.error;
+            err = LaunchShadowTransmittance(sa, st, s->sm_count);
+        } else {
+            TraceArgs sh{};
+            sh.accel = sc.accel;
+            sh.rays = q.shadow_ray;
+            sh.count = 2 * C;
+            sh.count_ptr = q.counters + kCtrShadow;
+            sh.occluded = q.shadow_occluded;
+            sh.out_index = q.shadow_slot;
+            sh.counter = q.counters + kCtrShadowTrace;
+            sh.error = ta.error;
+            err = LaunchTrace(sh, true, false, TraceShapeOf(s->accel, 1), st, s->sm_count);
+        }
+        if (err != cudaSuccess) return CudaError(err, "shadow trace");
+        LaunchNeeResolve(s->ps, q, s->transmittance, C, s->sm_count, st);
+        LaunchAdvanceQueue(q, st);
+        std::swap(q.ray_in, q.ray_out);
+        std::swap(q.path_in, q.path_out);
+    }
+    LaunchFilm(sc, s->ps, b, f, pixels, s->sm_count, st);
+    LaunchActivePixels(sc, b, f, pixels, s->sm_count, st);
+    LaunchFinishActive(s->scalars + 0, s->scalars + 1, s->batch, max_batch, C, st);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return CudaError(err, "batch launch");
+    return Ok();
+}
+
+}  // namespace
+}  // namespace yrc
+
+extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* req, yrc_film_pixel* film_out,
+                                 uint64_t* bad_samples_out, yrc_render_stats* stats) {
+    using namespace yrc;
+    if (!s || !film_out) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render: null argument");
+    std::lock_guard<std::mutex> lock(s->mutex);
+    cudaSetDevice(s->device);
+    const auto start = std::chrono::steady_clock::now();
+    const yrc_render_settings& st = s->settings;
+    const int64_t pixels = static_cast<int64_t>(st.width) * st.height;
+    const int spp = std::max(1, st.spp);
+    yrc_render_request none{};
+    const yrc_render_request& r = req ? *req : none;
+    if (r.resume_completed_spp < 0 || r.resume_completed_spp > spp) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "invalid resume completed spp");
+    }
+    if (r.resume_film) {
+        for (int64_t i = 0; i < pixels; ++i) {
+            const uint32_t count = r.resume_film[i].samples;
+            const bool bad = st.adaptive_enabled ? count > static_cast<uint32_t>(r.resume_completed_spp)
+                                                 : count != static_cast<uint32_t>(r.resume_completed_spp);
+            if (bad) return Fail(YRC_ERR_INVALID_ARGUMENT, "resume film sample counts do not match resume completed spp");
+        }
+    }
+    if (r.stop_flag && *r.stop_flag) return Fail(YRC_ERR_CANCELLED, "render cancelled");
+
+    // Concurrent paths: enough for several passes of a small image at once,
+    // one full pass of a large one.
+    const int64_t capacity = std::min<int64_t>(std::max<int64_t>(pixels, int64_t{1} << 21),
+                                               pixels * std::min(spp, kMaxBatch));
+    yrc_status status = EnsureWork(s, capacity);
+    if (status != YRC_OK) return status;
+    cudaStream_t stream = s->stream;
+    std::vector<yrc_film_pixel> host_film(static_cast<size_t>(pixels));
+    if (r.resume_film) {
+        std::memcpy(host_film.data(), r.resume_film, sizeof(yrc_film_pixel) * static_cast<size_t>(pixels));
+    } else {
+        std::memset(host_film.data(), 0, sizeof(yrc_film_pixel) * static_cast<size_t>(pixels));
+    }
+    std::vector<int32_t> attempts(static_cast<size_t>(pixels), spp - r.resume_completed_spp);
+    cudaMemcpyAsync(s->film, host_film.data(), sizeof(yrc_film_pixel) * pixels, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(s->attempts, attempts.data(), sizeof(int32_t) * pixels, cudaMemcpyHostToDevice, stream);
+    const unsigned long long init_scalars[4] = {0, 0, r.resume_bad_samples, 0};
+    cudaMemcpyAsync(s->scalars, init_scalars, sizeof(init_scalars), cudaMemcpyHostToDevice, stream);
+    cudaMemsetAsync(s->q.counters, 0, sizeof(unsigned long long) * kCtrCount, stream);
+    const int32_t max_batch = r.progress ? 1 : std::min(spp, kMaxBatch);
+    {
+        const DevScene& sc = s->dev;
+        BatchArgs b{s->active, s->scalars + 0, s->scalars + 1, s->batch, s->film};
+        FilmArgs f{s->attempts, s->scalars + 2, s->scalars + 3, st.adaptive_enabled, st.adaptive_min_spp,
+                   st.adaptive_relative_error, st.adaptive_absolute_error, st.adaptive_confidence};
+        LaunchActivePixels(sc, b, f, pixels, s->sm_count, stream);
+        LaunchFinishActive(s->scalars + 0, s->scalars + 1, s->batch, max_batch, s->capacity, stream);
+    }
+    // Capture one batch as a CUDA graph (all sizes are read on the device).
+    if (!s->graph || s->graph_max_batch != max_batch) {
+        if (s->graph) cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        cudaGraph_t graph = nullptr;
+        cudaError_t err = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (err != cudaSuccess) return CudaError(err, "graph capture");
+        status = EnqueueBatch(s, max_batch);
+        err = cudaStreamEndCapture(stream, &graph);
+        if (status != YRC_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return status;
+        }
+        if (err != cudaSuccess) return CudaError(err, "graph capture");
+        err = cudaGraphInstantiate(&s->graph, graph, 0);
+        cudaGraphDestroy(graph);
+        if (err != cudaSuccess) return CudaError(err, "graph instantiate");
+        s->graph_max_batch = max_batch;
+    }
+
+    int completed_passes = r.resume_completed_spp;
+    uint64_t total_samples = 0;
+    for (int64_t i = 0; i < pixels; ++i) total_samples += host_film[static_cast<size_t>(i)].samples;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, stream);
+    unsigned long long sc_host[4] = {0, 0, 0, 0};
+    int32_t batch_host = 0;
+    cudaMemcpyAsync(sc_host, s->scalars, sizeof(sc_host), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(&batch_host, s->batch, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
+    cudaError_t err = cudaStreamSynchronize(stream);
+    if (err != cudaSuccess) return CudaError(err, "render setup");
+    uint64_t converged = sc_host[3];
+    while (sc_host[0] > 0) {
+        if (r.stop_flag && *r.stop_flag) return Fail(YRC_ERR_CANCELLED, "render cancelled");
+        const int32_t this_batch = batch_host;
+        cudaMemsetAsync(s->scalars + 3, 0, sizeof(unsigned long long), stream);  // recounted by the batch
+        err = cudaGraphLaunch(s->graph, stream);
+        if (err != cudaSuccess) return CudaError(err, "batch launch");
+        cudaMemcpyAsync(sc_host, s->scalars, sizeof(sc_host), cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(&batch_host, s->batch, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
+        err = cudaStreamSynchronize(stream);
+        if (err != cudaSuccess) return CudaError(err, "batch");
+        completed_passes += this_batch;
+        converged = sc_host[3];
+        if (r.progress) {
+            cudaMemcpy(host_film.data(), s->film, sizeof(yrc_film_pixel) * pixels, cudaMemcpyDeviceToHost);
+            uint64_t done = 0;
+            for (int64_t i = 0; i < pixels; ++i) done += host_film[static_cast<size_t>(i)].samples;
+            unsigned long long counters[kCtrCount];
+            cudaMemcpy(counters, s->q.counters, sizeof(counters), cudaMemcpyDeviceToHost);
+            yrc_render_progress prog{};
+            prog.completed_spp = std::min(completed_passes, spp);
+            prog.target_spp = spp;
+            prog.completed_samples = done;
+            prog.target_samples = static_cast<uint64_t>(spp) * static_cast<uint64_t>(pixels);
+            prog.active_pixels = sc_host[0];
+            prog.converged_pixels = sc_host[3];
+            prog.rays_traced = counters[kCtrStatsBase + 0];
+            prog.elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+            char msg[512] = {0};
+            if (r.progress(&prog, host_film.data(), sc_host[2], r.user, msg, sizeof(msg))) {
+                return Fail(YRC_ERR_CANCELLED, msg[0] ? msg : "render cancelled by progress callback");
+            }
+        }
+    }
+    cudaEventRecord(e1, stream);
+    err = cudaMemcpyAsync(film_out, s->film, sizeof(yrc_film_pixel) * pixels, cudaMemcpyDeviceToHost, stream);
+    unsigned long long counters[kCtrCount];
+    if (err == cudaSuccess) err = cudaMemcpyAsync(counters, s->q.counters, sizeof(counters), cudaMemcpyDeviceToHost, stream);
+    unsigned long long fin[4];
+    if (err == cudaSuccess) err = cudaMemcpyAsync(fin, s->scalars, sizeof(fin), cudaMemcpyDeviceToHost, stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    if (err != cudaSuccess) return CudaError(err, "render readback");
+    status = CheckDeviceError(s->accel);
+    if (status != YRC_OK) return status;
+    float device_ms = 0.0f;
+    cudaEventElapsedTime(&device_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (bad_samples_out) *bad_samples_out = fin[2];
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        uint64_t done = 0;
+        for (int64_t i = 0; i < pixels; ++i) done += film_out[i].samples;
+        stats->samples_rendered = done;
+        stats->converged_pixels = converged;
+        stats->rays_traced = counters[kCtrStatsBase + 0];
+        stats->shadow_rays = counters[kCtrStatsBase + 1];
+        stats->occluded_shadow_rays = counters[kCtrStatsBase + 2];
+        stats->hits = counters[kCtrStatsBase + 3];
+        stats->misses = counters[kCtrStatsBase + 4];
+        stats->bad_samples = fin[2];
+        stats->bvh_nodes = s->bvh_nodes;
+        stats->bvh_max_depth = s->bvh_max_depth;
+        stats->threads = 1;
+        stats->device_seconds = device_ms / 1e3;
+        stats->elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+    }
+    (void)total_samples;
+    return Ok();
+}

@@ -1,0 +1,756 @@
+// Wavefront path-tracing stages: the bounce loop of IntegratePathSample
+// (src/integrators/path_integrator.cpp:23-197) split into
+//   generate  camera rays + per-path sampler/RNG state   (cpu_path_tracer.cpp:120-150)
+//   extend    closest-hit traversal of the ray queue     (trace_kernels.cu)
+//   shade     surface resolve, emission + MIS, next-event estimation samples,
+//             BSDF sampling, Russian roulette             (path_integrator.cpp:46-192)
+//   shadow    any-hit or transparent-shadow traversal    (path_direct_lighting.cpp:23-113)
+//   resolve   adds the visible next-event contributions  (path_direct_lighting.cpp:170-283)
+//   film      in-order Film::AddSample per pixel          (film.cpp:160-183)
+// The bounce depth is a launch parameter (every path in flight is at the same
+// depth), queue sizes live on the device so a whole batch can be replayed as
+// one CUDA graph.
+#include <cuda_runtime.h>
+
+#include "bsdf.cuh"
+#include "render_kernels.hpp"
+#include "render_types.hpp"
+#include "sampler.cuh"
+#include "shading.cuh"
+
+namespace yrc {
+namespace {
+
+constexpr float kMinShadowBias = 1.0e-4f;
+constexpr float kShadowBiasScale = 1.0e-5f;
+constexpr float kMaxShadowBiasFraction = 1.0e-2f;
+
+__device__ __forceinline__ float MaxAbs(V3 p) { return fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))); }
+
+// SurfaceBias / ShadowBias (src/integrators/path_integrator_common.cpp:129-138).
+__device__ __forceinline__ float SurfaceBias(V3 p) { return fmaxf(kMinShadowBias, MaxAbs(p) * kShadowBiasScale); }
+__device__ __forceinline__ float ShadowBias(V3 o, V3 t, float dist) {
+    const float scaled = fmaxf(MaxAbs(o), MaxAbs(t)) * kShadowBiasScale;
+    return fminf(fmaxf(kMinShadowBias, scaled), dist * kMaxShadowBiasFraction);
+}
+
+__device__ __forceinline__ V3 F4(const float4& v) { return V3{v.x, v.y, v.z}; }
+__device__ __forceinline__ float4 ToF4(V3 v, float w = 0.0f) { return make_float4(v.x, v.y, v.z, w); }
+
+// Warp-aggregated append to a device queue; returns this lane's slot.
+__device__ __forceinline__ unsigned long long QueueAppend(unsigned long long* counter) {
+    const unsigned mask = __activemask();
+    const int leader = __ffs(mask) - 1;
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned long long base = 0;
+    if (static_cast<int>(lane) == leader) base = atomicAdd(counter, static_cast<unsigned long long>(__popc(mask)));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void CountStat(unsigned long long* counters, int which) {
+    const unsigned mask = __activemask();
+    if ((threadIdx.x & 31u) == static_cast<unsigned>(__ffs(mask) - 1)) {
+        atomicAdd(counters + kCtrStatsBase + which, static_cast<unsigned long long>(__popc(mask)));
+    }
+}
+
+enum StatIndex { kStatRays = 0, kStatShadow = 1, kStatOccluded = 2, kStatHits = 3, kStatMisses = 4 };
+
+// PerspectiveDirection (src/scene/camera.cpp:9-16); tan(fov/2) comes from the host.
+__device__ inline V3 CameraDirection(const DevScene& sc, float fx, float fy) {
+    const float w = static_cast<float>(sc.width < 1 ? 1 : sc.width);
+    const float h = static_cast<float>(sc.height < 1 ? 1 : sc.height);
+    const float aspect = w / h;
+    const float sx = (2.0f * fx / w - 1.0f) * aspect * sc.cam_half_height;
+    const float sy = (1.0f - 2.0f * fy / h) * sc.cam_half_height;
+    return Normalize(Ld3(sc.cam_forward) + Ld3(sc.cam_right) * sx + Ld3(sc.cam_up) * sy);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ generate
+
+__global__ void GenerateKernel(DevScene sc, PathState ps, Queues q, BatchArgs b) {
+    const int64_t n_active = static_cast<int64_t>(*b.active_count);
+    const int32_t batch = *b.batch;
+    const int64_t total = n_active * batch;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t p = i % n_active;
+        const int32_t j = static_cast<int32_t>(i / n_active);
+        const int32_t pixel = b.active[p];
+        const int x = pixel % sc.width, y = pixel / sc.width;
+        const int32_t sample = static_cast<int32_t>(b.film[pixel].samples) + j;
+        PixelSampler smp;
+        smp.Init(sc.sampler, sc.seed, x, y, sample, sc.spp);
+        float sx, sy;
+        smp.Sample2D(kDimPixel, 0, sx, sy);
+        const float fx = static_cast<float>(x) + sx;
+        const float fy = static_cast<float>(y) + sy;
+        const V3 d = CameraDirection(sc, fx, fy);
+        Pcg32 rng;
+        rng.Seed(SeedForPixelSample(sc.seed, x, y, sample) ^ kDefaultSeed);
+        ps.pixel[i] = pixel;
+        ps.sample[i] = sample;
+        ps.throughput[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        ps.radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        ps.flags[i] = 0;
+        ps.rng_state[i] = rng.state;
+        ps.rng_inc[i] = rng.inc;
+        ps.aov_albedo[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        ps.aov_normal[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        ps.nee[3 * i] = ps.nee[3 * i + 1] = ps.nee[3 * i + 2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        q.ray_in[2 * i] = make_float4(sc.cam_origin[0], sc.cam_origin[1], sc.cam_origin[2], 1.0e-5f);
+        q.ray_in[2 * i + 1] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
+        q.path_in[i] = static_cast<int32_t>(i);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) q.counters[kCtrIn] = static_cast<unsigned long long>(total);
+}
+
+// Resets the per-bounce queue counters (so the bounce loop can be captured).
+__global__ void ResetCountersKernel(Queues q) {
+    if (threadIdx.x == 0) {
+        q.counters[kCtrOut] = 0;
+        q.counters[kCtrShadow] = 0;
+        q.counters[kCtrNee] = 0;
+        q.counters[kCtrTrace] = 0;
+        q.counters[kCtrShadowTrace] = 0;
+    }
+}
+
+// Makes the next-bounce queue the current one.
+__global__ void AdvanceQueueKernel(Queues q) {
+    if (threadIdx.x == 0) q.counters[kCtrIn] = q.counters[kCtrOut];
+}
+
+// ------------------------------------------------------------------- shade
+
+namespace {
+
+struct Surface {
+    V3 p;        // hit point
+    V3 n;        // shading normal (face-forwarded as the reference does)
+    V3 ng_obj;   // object-space geometric normal of a triangle (emission MIS)
+    int32_t material;
+    int32_t prim;  // mesh primitive, -1 for spheres
+    bool triangle;
+};
+
+__device__ inline V3 VertexPos(const DevScene& sc, int32_t v) { return F4(sc.positions[v]); }
+
+// TransformNormal (src/core/transform.cpp:46-74).
+__device__ inline V3 TransformNormal(const float* m, V3 n) {
+    const float a = m[0], b = m[4], c = m[8], d = m[1], e = m[5], f = m[9], g = m[2], h = m[6], i = m[10];
+    const float det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+    if (fabsf(det) <= 1.0e-12f) {
+        const V3 tv = V3{m[0] * n.x + m[4] * n.y + m[8] * n.z, m[1] * n.x + m[5] * n.y + m[9] * n.z,
+                         m[2] * n.x + m[6] * n.y + m[10] * n.z};
+        const V3 fb = Normalize(tv);
+        return LengthSq(fb) > 0.0f ? fb : Normalize(n);
+    }
+    const float inv = 1.0f / det;
+    return Normalize(V3{((e * i - f * h) * n.x + (f * g - d * i) * n.y + (d * h - e * g) * n.z) * inv,
+                        ((c * h - b * i) * n.x + (a * i - c * g) * n.y + (b * g - a * h) * n.z) * inv,
+                        ((b * f - c * e) * n.x + (c * d - a * f) * n.y + (a * e - b * d) * n.z) * inv});
+}
+
+// ResolveShadingNormal (src/geometry/intersection.cpp:84-106).
+__device__ inline V3 ResolveShadingNormal(const DevScene& sc, int32_t prim, int4 tv, float u, float v, V3 gn) {
+    V3 n = Normalize(gn);
+    if (sc.normals && (sc.prim_flags[prim] & 1u)) {
+        const float w = 1.0f - u - v;
+        const V3 n0 = F4(sc.normals[tv.x]), n1 = F4(sc.normals[tv.y]), n2 = F4(sc.normals[tv.z]);
+        const V3 in = Normalize(V3{n0.x * w + n1.x * u + n2.x * v, n0.y * w + n1.y * u + n2.y * v,
+                                   n0.z * w + n1.z * u + n2.z * v});
+        if (LengthSq(in) > 0.0f) n = in;
+    }
+    if (Dot(n, gn) < 0.0f) n = -n;
+    if (LengthSq(n) == 0.0f) return Normalize(gn);
+    return n;
+}
+
+// TraceVisibleSurface's surface resolve (src/integrators/surface_query.cpp:129-187)
+// and EvaluateMaterialAtSurface (src/shading/material_evaluator.cpp:112-180),
+// untextured. Returns false for a hit on an invalid triangle material.
+__device__ inline bool ResolveSurface(const DevScene& sc, V3 o, V3 d, float4 hit, int32_t inst, Surface& s) {
+    const int32_t id = __float_as_int(hit.y);
+    s.p = o + d * hit.x;
+    if (id <= -2) {
+        const int32_t sphere = -2 - id;
+        const float4 c = sc.spheres[sphere];
+        const V3 gn = Normalize(V3{s.p.x - c.x, s.p.y - c.y, s.p.z - c.z});
+        s.n = sc.sphere_flip[sphere] ? -gn : gn;
+        s.material = sc.sphere_material[sphere];
+        s.prim = -1;
+        s.triangle = false;
+        if (s.material < 0) {  // default RenderMaterial with the default (0, 0, 1) normal
+            s.n = V3{0.0f, 0.0f, 1.0f};
+        }
+        return true;
+    }
+    const int32_t prim = sc.tri_prim[id];
+    const int4 tv = sc.tri_vertices[id];
+    s.prim = prim;
+    s.triangle = true;
+    s.material = sc.prim_material[prim];
+    if (s.material < 0) return false;
+    const V3 p0 = VertexPos(sc, tv.x), p1 = VertexPos(sc, tv.y), p2 = VertexPos(sc, tv.z);
+    const V3 raw = Normalize(Cross(p1 - p0, p2 - p0));
+    s.ng_obj = raw;
+    const float u = hit.z, v = hit.w;
+    const V3 wo = -d;
+    if (inst >= 0) {
+        const float* m = sc.instance_o2w + 16 * inst;
+        const V3 wraw = TransformNormal(m, raw);
+        const V3 gn = Dot(wraw, wo) < 0.0f ? -wraw : wraw;
+        V3 n = TransformNormal(m, ResolveShadingNormal(sc, prim, tv, u, v, raw));
+        if (Dot(n, gn) < 0.0f) n = -n;
+        s.n = Dot(n, wo) < 0.0f ? -n : n;
+    } else {
+        const V3 gn = Dot(raw, wo) < 0.0f ? -raw : raw;
+        const V3 n = ResolveShadingNormal(sc, prim, tv, u, v, gn);
+        s.n = Dot(n, wo) < 0.0f ? -n : n;
+    }
+    return true;
+}
+
+// SampleAliasTable (src/lighting/light_sampling.cpp:185-204).
+__device__ inline int SampleAlias(const float* prob, const int32_t* alias, const float* pmf, int count, float u,
+                                  float& out_pmf, float& remapped) {
+    const float hi = 0.99999994f;
+    const float su = isfinite(u) ? Clampf(u, 0.0f, 1.0f) : 0.0f;
+    const float scaled = fminf(su, hi) * static_cast<float>(count);
+    const int column = min(static_cast<int>(scaled), count - 1);
+    const float frac = scaled - static_cast<float>(column);
+    const float p = prob[column];
+    int index = column;
+    float r = 0.0f;
+    if (frac < p) {
+        r = p > 0.0f ? frac / p : 0.0f;
+    } else {
+        index = alias[column];
+        r = p < 1.0f ? (frac - p) / (1.0f - p) : 0.0f;
+    }
+    out_pmf = pmf[index];
+    remapped = Clampf(r, 0.0f, hi);
+    return index;
+}
+
+__device__ __forceinline__ float EmissiveArea(const DevScene& sc, int e) {
+    const float a = sc.emissive_area[e];
+    return isfinite(a) && a > 0.0f ? a : 0.0f;
+}
+
+__device__ __forceinline__ float Luminance(V3 c) { return fmaxf(0.0f, 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z); }
+
+struct LightSample {
+    V3 point, normal, radiance;
+    float pdf;
+    int32_t emissive;
+    bool valid;
+};
+
+// SampleEmissiveLights / SampleEmissivePrimitive (light_sampling.cpp:275-355).
+__device__ inline LightSample SampleEmissive(const DevScene& sc, float u_select, float tx, float ty) {
+    LightSample out{};
+    out.valid = false;
+    if (sc.emissive_count == 0) return out;
+    int e = -1;
+    float pmf = 0.0f, local = 0.0f;
+    if (sc.alias_count == sc.emissive_count) {
+        e = SampleAlias(sc.alias_prob, sc.alias_index, sc.alias_pmf, sc.alias_count, u_select, pmf, local);
+        if (e < 0 || pmf <= 0.0f) return out;
+    } else {
+        const float total = sc.total_emissive_power;
+        if (!isfinite(total) || total <= 0.0f) return out;
+        const float su = isfinite(u_select) ? Clampf(u_select, 0.0f, 1.0f) : 0.0f;
+        const float target = su * total;
+        float cum = 0.0f;
+        for (int i = 0; i < sc.emissive_count; ++i) {
+            const float power = EmissiveArea(sc, i) * Luminance(Ld3(sc.emissive_radiance + 3 * i));
+            if (power <= 0.0f) continue;
+            const float prev = cum;
+            cum += power;
+            e = i;
+            pmf = power / total;
+            local = 1.0f;
+            if (target < cum) {
+                local = (target - prev) / power;
+                break;
+            }
+        }
+        if (e < 0) return out;
+    }
+    const float area = EmissiveArea(sc, e);
+    if (area <= 0.0f) return out;
+    const int32_t prim = sc.emissive_prim[e];
+    if (prim < 0 || prim >= sc.primitive_count) return out;
+    // SelectTriangleByArea: first triangle whose cumulative area exceeds the
+    // target (zero-area triangles never raise the cumulative sum).
+    const int32_t off = sc.emissive_tri_offset[e], cnt = sc.emissive_tri_count[e];
+    const float parea = sc.emissive_prim_area[e];
+    if (cnt == 0 || !isfinite(parea) || parea <= 0.0f) return out;
+    const float su = isfinite(local) ? Clampf(local, 0.0f, 1.0f) : 0.0f;
+    const float target = su * parea;
+    int lo = 0, hi = cnt;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (sc.tri_cdf[off + mid] <= target) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo == cnt) lo = cnt - 1;  // the last positive-area triangle
+    const int32_t flat = sc.tri_local[off + lo];
+    const int4 tv = sc.tri_vertices[flat];
+    const V3 p0 = VertexPos(sc, tv.x), p1 = VertexPos(sc, tv.y), p2 = VertexPos(sc, tv.z);
+    const float sq = sqrtf(tx);
+    const float u = 1.0f - sq;
+    const float v = ty * sq;
+    out.point = p0 * (1.0f - u - v) + p1 * u + p2 * v;
+    const V3 e1 = p1 - p0, e2 = p2 - p0;
+    const V3 cr = Cross(e1, e2);
+    out.normal = Normalize(cr);
+    const float tri_area = sqrtf(LengthSq(cr)) * 0.5f;
+    if (!(isfinite(tri_area) && tri_area > 0.0f) || LengthSq(out.normal) == 0.0f) return out;
+    out.radiance = Ld3(sc.emissive_radiance + 3 * e);
+    out.pdf = (1.0f / area) * pmf;
+    out.emissive = e;
+    out.valid = true;
+    return out;
+}
+
+// PdfEmissiveLightSolidAngle (light_sampling.cpp:357-396).
+__device__ inline float PdfEmissiveSolidAngle(const DevScene& sc, V3 shading, V3 light, V3 ln, int e) {
+    if (sc.emissive_count == 0) return 0.0f;
+    float area_pdf = 0.0f;
+    if (e >= 0 && e < sc.emissive_count) {
+        const float area = EmissiveArea(sc, e);
+        if (area <= 0.0f) return 0.0f;
+        float pmf = 0.0f;
+        if (sc.alias_count == sc.emissive_count) {
+            pmf = sc.alias_pmf[e];
+        } else {
+            const float total = sc.total_emissive_power;
+            pmf = total > 0.0f ? (area * Luminance(Ld3(sc.emissive_radiance + 3 * e))) / total : 0.0f;
+        }
+        area_pdf = pmf / area;
+    } else {
+        float total_area = 0.0f;
+        for (int i = 0; i < sc.emissive_count; ++i) total_area += EmissiveArea(sc, i);
+        if (!isfinite(total_area) || total_area <= 0.0f) return 0.0f;
+        area_pdf = 1.0f / total_area;
+    }
+    const V3 dir = light - shading;
+    const float dsq = LengthSq(dir);
+    if (dsq <= 0.0f) return 0.0f;
+    const float c = fabsf(Dot(ln, Normalize(shading - light)));
+    if (c <= 0.0f) return 0.0f;
+    return area_pdf * dsq / c;
+}
+
+__device__ __forceinline__ void PushShadow(Queues& q, V3 o, V3 d, float tmax, int32_t slot) {
+    const unsigned long long k = QueueAppend(q.counters + kCtrShadow);
+    q.shadow_ray[2 * k] = make_float4(o.x, o.y, o.z, 1.0e-5f);
+    q.shadow_ray[2 * k + 1] = make_float4(d.x, d.y, d.z, tmax);
+    q.shadow_slot[k] = slot;
+}
+
+}  // namespace
+
+__global__ void ShadeKernel(DevScene sc, PathState ps, Queues q, int depth) {
+    const int64_t count = static_cast<int64_t>(q.counters[kCtrIn]);
+    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < count;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t path = q.path_in[e];
+        const float4 ra = q.ray_in[2 * e], rb = q.ray_in[2 * e + 1];
+        const V3 o = F4(ra), d = F4(rb);
+        const float4 hit = q.hits[e];
+        const int32_t inst = q.inst[e];
+        const int32_t id = __float_as_int(hit.y);
+        V3 tp = F4(ps.throughput[path]);
+        V3 rad = F4(ps.radiance[path]);
+        uint32_t flags = ps.flags[path];
+        const float4 prev = ps.prev[path];
+        CountStat(q.counters, kStatRays);
+
+        // --- miss: environment with the BSDF-sampling MIS weight
+        if (id == -1) {
+            CountStat(q.counters, kStatMisses);
+            float w = 1.0f;
+            if ((flags & kPathPrevValid) && !(flags & kPathPrevDelta)) {
+                w = PowerHeuristic(1, prev.w, 1, PdfEnvironment(sc.env, d));
+            }
+            rad = rad + Mul(tp, EvalEnvironment(sc.env, d)) * w;
+            ps.radiance[path] = ToF4(rad);
+            continue;
+        }
+        CountStat(q.counters, kStatHits);
+
+        // --- medium attenuation (Beer-Lambert inside a thick dielectric)
+        if (flags & kPathMedium) {
+            const float4 md = ps.medium[path];
+            if (hit.x > 0.0f && md.w > 0.0f) {
+                const float inv = 1.0f / md.w;
+                const float c[3] = {Clampf(md.x, 1.0e-6f, 1.0f), Clampf(md.y, 1.0e-6f, 1.0f), Clampf(md.z, 1.0e-6f, 1.0f)};
+                tp = V3{tp.x * expf(logf(c[0]) * hit.x * inv), tp.y * expf(logf(c[1]) * hit.x * inv),
+                        tp.z * expf(logf(c[2]) * hit.x * inv)};
+            }
+        }
+        if (IsBlack(tp)) {
+            ps.throughput[path] = ToF4(tp);
+            continue;
+        }
+
+        Surface s;
+        if (!ResolveSurface(sc, o, d, hit, inst, s)) {
+            rad = rad + Mul(tp, V3{1.0f, 0.0f, 1.0f});  // invalid material marker
+            ps.radiance[path] = ToF4(rad);
+            continue;
+        }
+        Mat m;
+        V3 emission{0.0f, 0.0f, 0.0f};
+        if (s.material >= 0) {
+            const DevMaterial& dm = sc.materials[s.material];
+            m = LoadMat(dm);
+            emission = Ld3(dm.emission);
+        } else {  // default RenderMaterial: diffuse 0.5
+            m = Mat{kDiffuse, {0.5f, 0.5f, 0.5f}, 1.5f, 0.0f, 0.0f, 1.5f, 0.01f, {0, 0, 0}, 10, 1};
+        }
+        const V3 wo = -d;
+        if (depth == 0) {
+            flags |= kPathPrimary;
+            ps.aov_albedo[path] = ToF4(m.reflectance, hit.x);
+            ps.aov_normal[path] = ToF4(s.n);
+        }
+
+        // --- emission with the BSDF-sampling MIS weight (triangle lights only)
+        if (!IsBlack(emission) && s.triangle) {
+            float w = 1.0f;
+            if ((flags & kPathPrevValid) && !(flags & kPathPrevDelta)) {
+                const int32_t ei = sc.prim_emissive[s.prim];
+                const float pl = PdfEmissiveSolidAngle(sc, F4(prev), s.p, s.ng_obj, ei);
+                w = PowerHeuristic(1, prev.w, 1, pl);
+            }
+            rad = rad + Mul(tp, emission) * w;
+        }
+
+        PixelSampler smp;
+        const int32_t pixel = ps.pixel[path];
+        smp.Init(sc.sampler, sc.seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
+        Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
+
+        // --- next-event estimation: samples now, visibility in the shadow stage
+        if (!IsDelta(m)) {
+            bool any = false;
+            const V3 n = s.n;
+            if (sc.emissive_count > 0) {
+                const float us = smp.Sample1D(kDimDirectLightSelect, depth);
+                float tx, ty;
+                smp.Sample2D(kDimDirectLightSurface, depth, tx, ty);
+                const LightSample ls = SampleEmissive(sc, us, tx, ty);
+                if (ls.valid && ls.pdf > 0.0f && !IsBlack(ls.radiance)) {
+                    const V3 to_light = ls.point - s.p;
+                    const float dsq = LengthSq(to_light);
+                    if (dsq > kMinShadowBias * kMinShadowBias) {
+                        const float dist = sqrtf(dsq);
+                        const float sb = ShadowBias(s.p, ls.point, dist);
+                        if (dist > sb) {
+                            const V3 so = s.p + n * sb;
+                            const V3 stl = ls.point - so;
+                            const float sdsq = LengthSq(stl);
+                            if (sdsq > kMinShadowBias * kMinShadowBias) {
+                                const float sd = sqrtf(sdsq);
+                                const V3 wi = stl / sd;
+                                const float cs = fmaxf(0.0f, Dot(n, wi));
+                                if (cs > 0.0f) {
+                                    const float pl = PdfEmissiveSolidAngle(sc, s.p, ls.point, ls.normal, ls.emissive);
+                                    if (pl > 0.0f) {
+                                        CountStat(q.counters, kStatShadow);
+                                        const V3 f = EvalBsdf(m, wo, wi, n, rng);
+                                        if (!IsBlack(f)) {
+                                            const float pb = PdfBsdf(m, wo, wi, n, rng);
+                                            const float mis = PowerHeuristic(1, pl, 1, pb);
+                                            ps.nee[3 * path + 0] = ToF4(Mul(f, ls.radiance) * (cs * mis / pl));
+                                            PushShadow(q, so, wi, sd - sb, 3 * path + 0);
+                                            any = true;
+                                        } else {
+                                            ps.nee[3 * path + 0] = make_float4(0, 0, 0, 0);
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            if (EnvSampleable(sc.env)) {
+                float tx, ty;
+                smp.Sample2D(kDimDirectLightSurface, depth, tx, ty);
+                const EnvSample es = SampleEnvironment(sc.env, tx, ty);
+                if (es.valid && es.pdf > 0.0f && !IsBlack(es.radiance)) {
+                    const float cs = fmaxf(0.0f, Dot(n, es.dir));
+                    if (cs > 0.0f) {
+                        const V3 f = EvalBsdf(m, wo, es.dir, n, rng);
+                        if (!IsBlack(f)) {
+                            CountStat(q.counters, kStatShadow);
+                            const float pb = PdfBsdf(m, wo, es.dir, n, rng);
+                            const float mis = PowerHeuristic(1, es.pdf, 1, pb);
+                            ps.nee[3 * path + 2] = ToF4(Mul(f, es.radiance) * (cs * mis / es.pdf));
+                            PushShadow(q, s.p + n * SurfaceBias(s.p), es.dir, __int_as_float(0x7f800000),
+                                       3 * path + 2);
+                            any = true;
+                        }
+                    }
+                }
+            }
+            if (any) {
+                flags |= kPathNee;
+                ps.nee_tp[path] = ToF4(tp);
+                const unsigned long long k = QueueAppend(q.counters + kCtrNee);
+                q.nee_paths[k] = path;
+            }
+        }
+
+        bool cont = depth + 1 < sc.max_depth;
+        BsdfSample bs = NoSample();
+        if (cont) {
+            float bx, by;
+            smp.Sample2D(kDimBsdf, depth, bx, by);
+            bs = SampleBsdf(m, wo, s.n, bx, by, rng);
+            cont = bs.valid && !IsBlack(bs.weight);
+        }
+        if (cont) {
+            tp = Mul(tp, bs.weight);
+            // SurviveRussianRoulette (path_integrator_common.cpp:185-201)
+            if (depth >= 3) {
+                const float survival = Clampf(MaxComp(tp), 0.05f, 0.95f);
+                if (smp.Sample1D(kDimRussianRoulette, depth) >= survival) {
+                    cont = false;
+                } else {
+                    tp = tp / survival;
+                }
+            }
+        }
+        if (cont) {
+            // UpdateMediumStateAfterBsdf (path_integrator_common.cpp:108-123)
+            if (m.kind == kDielectric && Dot(bs.wi, s.n) < 0.0f) {
+                if (flags & kPathMedium) {
+                    flags &= ~kPathMedium;
+                } else {
+                    flags |= kPathMedium;
+                    const DevMaterial& dm = sc.materials[s.material];
+                    ps.medium[path] = make_float4(dm.absorption_color[0], dm.absorption_color[1],
+                                                  dm.absorption_color[2], dm.absorption_distance);
+                }
+            }
+            flags |= kPathPrevValid;
+            flags = bs.specular ? (flags | kPathPrevDelta) : (flags & ~kPathPrevDelta);
+            ps.prev[path] = ToF4(s.p, bs.pdf);
+            const V3 bn = Dot(bs.wi, s.n) >= 0.0f ? s.n : -s.n;
+            const V3 no = s.p + bn * SurfaceBias(s.p);
+            const unsigned long long k = QueueAppend(q.counters + kCtrOut);
+            q.ray_out[2 * k] = make_float4(no.x, no.y, no.z, 1.0e-5f);
+            q.ray_out[2 * k + 1] = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, __int_as_float(0x7f800000));
+            q.path_out[k] = path;
+        }
+        ps.throughput[path] = ToF4(tp);
+        ps.radiance[path] = ToF4(rad);
+        ps.flags[path] = flags;
+        ps.rng_state[path] = rng.state;
+    }
+}
+
+// Adds each path's visible next-event contributions:
+// radiance += throughput_at_vertex * ((emissive + analytic) + environment).
+template <bool kTransmittance>
+__global__ void NeeResolveKernel(PathState ps, Queues q, const float4* transmittance) {
+    const int64_t count = static_cast<int64_t>(q.counters[kCtrNee]);
+    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < count;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t path = q.nee_paths[e];
+        V3 sum{0.0f, 0.0f, 0.0f};
+        bool occluded_any = false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int32_t slot = 3 * path + k;
+            const V3 c = F4(ps.nee[slot]);
+            V3 vis{0.0f, 0.0f, 0.0f};
+            if (kTransmittance) {
+                vis = F4(transmittance[slot]);
+            } else {
+                vis = q.shadow_occluded[slot] ? V3{0, 0, 0} : V3{1, 1, 1};
+            }
+            sum = sum + Mul(c, vis);
+            ps.nee[slot] = make_float4(0, 0, 0, 0);
+            (void)occluded_any;
+        }
+        const V3 tp = F4(ps.nee_tp[path]);
+        ps.radiance[path] = ToF4(F4(ps.radiance[path]) + Mul(tp, sum));
+        ps.flags[path] &= ~kPathNee;
+    }
+}
+
+// Marks every NEE slot of the queued shadow rays as occluded before the
+// any-hit trace (unused slots then contribute zero as they hold zero).
+__global__ void ClearOcclusionKernel(Queues q, int64_t slots) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < slots;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        q.shadow_occluded[i] = 1;
+    }
+}
+
+// ------------------------------------------------------------------- film
+
+// Film::AddSample in sample order for each active pixel (film.cpp:160-183),
+// with the radiance clamp of IntegratePathSample (path_integrator.cpp:195).
+// A batch rendered `batch` consecutive sample indices per pixel on the
+// assumption that every sample is finite; accepting stops at the first
+// non-finite one (the reference re-uses that sample index on its next pass)
+// or when adaptive sampling declares the pixel converged.
+__global__ void FilmKernel(DevScene sc, PathState ps, BatchArgs b, FilmArgs f) {
+    const int64_t n_active = static_cast<int64_t>(*b.active_count);
+    const int32_t batch = *b.batch;
+    for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < n_active;
+         p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t pixel = b.active[p];
+        yrc_film_pixel px = b.film[pixel];
+        int32_t attempts = f.attempts_left[pixel];
+        for (int32_t j = 0; j < batch && attempts > 0; ++j) {
+            const int64_t slot = j * n_active + p;
+            V3 beauty = F4(ps.radiance[slot]);
+            // ClampMaxComponent (path_integrator_common.cpp:37-46)
+            if (sc.radiance_clamp > 0.0f) {
+                const float mc = MaxComp(beauty);
+                if (!(mc <= sc.radiance_clamp || mc <= 0.0f)) beauty = beauty * (sc.radiance_clamp / mc);
+            }
+            --attempts;
+            if (!(isfinite(beauty.x) && isfinite(beauty.y) && isfinite(beauty.z))) {
+                atomicAdd(f.bad_samples, 1ull);
+                break;
+            }
+            px.sum[0] = px.sum[0] + beauty.x;
+            px.sum[1] = px.sum[1] + beauty.y;
+            px.sum[2] = px.sum[2] + beauty.z;
+            ++px.samples;
+            const float lum = 0.2126f * beauty.x + 0.7152f * beauty.y + 0.0722f * beauty.z;
+            const float delta = lum - px.luminance_mean;
+            px.luminance_mean += delta / static_cast<float>(px.samples);
+            const float delta2 = lum - px.luminance_mean;
+            px.luminance_m2 += delta * delta2;
+            if (ps.flags[slot] & kPathPrimary) {
+                const float4 al = ps.aov_albedo[slot];
+                const float4 nm = ps.aov_normal[slot];
+                const float depth = al.w;
+                if (isfinite(al.x) && isfinite(al.y) && isfinite(al.z) && isfinite(nm.x) && isfinite(nm.y) &&
+                    isfinite(nm.z) && isfinite(depth) && depth >= 0.0f) {
+                    px.albedo_sum[0] = px.albedo_sum[0] + al.x;
+                    px.albedo_sum[1] = px.albedo_sum[1] + al.y;
+                    px.albedo_sum[2] = px.albedo_sum[2] + al.z;
+                    px.normal_sum[0] = px.normal_sum[0] + nm.x;
+                    px.normal_sum[1] = px.normal_sum[1] + nm.y;
+                    px.normal_sum[2] = px.normal_sum[2] + nm.z;
+                    px.depth_sum += depth;
+                    ++px.aov_samples;
+                }
+            }
+            if (px.samples >= static_cast<uint32_t>(sc.spp)) break;
+            if (f.adaptive && px.samples >= static_cast<uint32_t>(max(2, f.min_spp))) {
+                // Film::IsConverged (film.cpp:113-121)
+                const float var = px.samples > 1 ? px.luminance_m2 / static_cast<float>(px.samples - 1) : 0.0f;
+                const float se = px.samples > 1 ? sqrtf(fmaxf(0.0f, var) / static_cast<float>(px.samples))
+                                                : __int_as_float(0x7f800000);
+                const float bound = fmaxf(0.0f, f.confidence) * se;
+                const float tol = fmaxf(0.0f, f.absolute_error) + fmaxf(0.0f, f.relative_error) * fabsf(px.luminance_mean);
+                if (isfinite(bound) && bound <= tol) break;
+            }
+        }
+        b.film[pixel] = px;
+        f.attempts_left[pixel] = attempts;
+    }
+}
+
+// Rebuilds the active-pixel list: pixels with attempts left, fewer than spp
+// samples and (with adaptive sampling) not converged; also counts converged
+// pixels. Order is irrelevant: every pixel's samples are independent.
+__global__ void ActivePixelsKernel(DevScene sc, BatchArgs b, FilmArgs f, int64_t pixels) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < pixels;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const yrc_film_pixel px = b.film[i];
+        bool converged = false;
+        if (f.adaptive && px.samples >= static_cast<uint32_t>(max(2, f.min_spp))) {
+            const float var = px.samples > 1 ? px.luminance_m2 / static_cast<float>(px.samples - 1) : 0.0f;
+            const float se = px.samples > 1 ? sqrtf(fmaxf(0.0f, var) / static_cast<float>(px.samples))
+                                            : __int_as_float(0x7f800000);
+            const float bound = fmaxf(0.0f, f.confidence) * se;
+            const float tol = fmaxf(0.0f, f.absolute_error) + fmaxf(0.0f, f.relative_error) * fabsf(px.luminance_mean);
+            converged = isfinite(bound) && bound <= tol;
+        }
+        if (converged) atomicAdd(f.converged, 1ull);
+        if (!converged && px.samples < static_cast<uint32_t>(sc.spp) && f.attempts_left[i] > 0) {
+            const unsigned long long k = QueueAppend(b.active_count_next);
+            b.active[k] = static_cast<int32_t>(i);
+        }
+    }
+}
+
+// Publishes the rebuilt active list and sizes the next batch: as many sample
+// attempts per active pixel as fit in the path-state capacity (at least 1).
+__global__ void FinishActiveKernel(unsigned long long* active_count, unsigned long long* next, int32_t* batch,
+                                   int32_t max_batch, int64_t capacity) {
+    if (threadIdx.x == 0) {
+        const unsigned long long n = *next;
+        *active_count = n;
+        *next = 0;
+        int64_t b = n > 0 ? capacity / static_cast<int64_t>(n) : 1;
+        if (b > max_batch) b = max_batch;
+        if (b < 1) b = 1;
+        *batch = static_cast<int32_t>(b);
+    }
+}
+
+namespace {
+constexpr int kThreads = 256;
+unsigned Grid(int64_t work, int sm_count, int per_sm = 8) {
+    int64_t blocks = (work + kThreads - 1) / kThreads;
+    const int64_t cap = static_cast<int64_t>(sm_count) * per_sm;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    return static_cast<unsigned>(blocks);
+}
+}  // namespace
+
+void LaunchGenerate(const DevScene& sc, const PathState& ps, const Queues& q, const BatchArgs& b, int64_t capacity,
+                    int sm_count, cudaStream_t st) {
+    GenerateKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, b);
+}
+void LaunchResetCounters(const Queues& q, cudaStream_t st) { ResetCountersKernel<<<1, 32, 0, st>>>(q); }
+void LaunchAdvanceQueue(const Queues& q, cudaStream_t st) { AdvanceQueueKernel<<<1, 32, 0, st>>>(q); }
+void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity, int sm_count,
+                 cudaStream_t st) {
+    ShadeKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
+}
+void LaunchNeeResolve(const PathState& ps, const Queues& q, const float4* transmittance, int64_t capacity,
+                      int sm_count, cudaStream_t st) {
+    if (transmittance) {
+        NeeResolveKernel<true><<<Grid(capacity, sm_count), kThreads, 0, st>>>(ps, q, transmittance);
+    } else {
+        NeeResolveKernel<false><<<Grid(capacity, sm_count), kThreads, 0, st>>>(ps, q, nullptr);
+    }
+}
+void LaunchClearOcclusion(const Queues& q, int64_t slots, int sm_count, cudaStream_t st) {
+    ClearOcclusionKernel<<<Grid(slots, sm_count), kThreads, 0, st>>>(q, slots);
+}
+void LaunchFilm(const DevScene& sc, const PathState& ps, const BatchArgs& b, const FilmArgs& f, int64_t pixels,
+                int sm_count, cudaStream_t st) {
+    FilmKernel<<<Grid(pixels, sm_count), kThreads, 0, st>>>(sc, ps, b, f);
+}
+void LaunchActivePixels(const DevScene& sc, const BatchArgs& b, const FilmArgs& f, int64_t pixels, int sm_count,
+                        cudaStream_t st) {
+    ActivePixelsKernel<<<Grid(pixels, sm_count), kThreads, 0, st>>>(sc, b, f, pixels);
+}
+void LaunchFinishActive(unsigned long long* active_count, unsigned long long* active_count_next, int32_t* batch,
+                        int32_t max_batch, int64_t capacity, cudaStream_t st) {
+    FinishActiveKernel<<<1, 32, 0, st>>>(active_count, active_count_next, batch, max_batch, capacity);
+}
+
+}  // namespace yrc

@@ -1,0 +1,49 @@
+// Launch interface of the wavefront render kernels (render_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "render_types.hpp"
+#include "yrcuda.h"
+
+namespace yrc {
+
+// Per-batch device state shared by generate / film / active-list kernels.
+struct BatchArgs {
+    int32_t* active;                         // active pixel indices
+    const unsigned long long* active_count;  // entries in `active`
+    unsigned long long* active_count_next;   // rebuilt list size
+    const int32_t* batch;                    // sample attempts per active pixel in this batch
+    yrc_film_pixel* film;                    // device film
+};
+
+struct FilmArgs {
+    int32_t* attempts_left;   // per pixel: passes this pixel may still take
+    unsigned long long* bad_samples;
+    unsigned long long* converged;
+    int32_t adaptive;
+    int32_t min_spp;
+    float relative_error;
+    float absolute_error;
+    float confidence;
+};
+
+// Host launchers (grid sizes are multiples of the SM count; every kernel
+// reads its work count from device memory, so the sequence is graph-safe).
+void LaunchGenerate(const DevScene& sc, const PathState& ps, const Queues& q, const BatchArgs& b, int64_t capacity,
+                    int sm_count, cudaStream_t st);
+void LaunchResetCounters(const Queues& q, cudaStream_t st);
+void LaunchAdvanceQueue(const Queues& q, cudaStream_t st);
+void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity, int sm_count,
+                 cudaStream_t st);
+void LaunchNeeResolve(const PathState& ps, const Queues& q, const float4* transmittance, int64_t capacity,
+                      int sm_count, cudaStream_t st);
+void LaunchClearOcclusion(const Queues& q, int64_t slots, int sm_count, cudaStream_t st);
+void LaunchFilm(const DevScene& sc, const PathState& ps, const BatchArgs& b, const FilmArgs& f, int64_t pixels,
+                int sm_count, cudaStream_t st);
+void LaunchActivePixels(const DevScene& sc, const BatchArgs& b, const FilmArgs& f, int64_t pixels, int sm_count,
+                        cudaStream_t st);
+void LaunchFinishActive(unsigned long long* active_count, unsigned long long* active_count_next, int32_t* batch,
+                        int32_t max_batch, int64_t capacity, cudaStream_t st);
+
+}  // namespace yrc

@@ -1,0 +1,183 @@
+// Device-resident render scene and wavefront path state.
+//
+// HBM layout (structure of arrays, one slot per in-flight path):
+//   * geometry for shading: per flat triangle its mesh primitive (int32) and
+//     its three vertex indices (int4); vertex positions and normals as float4;
+//   * materials as a compact 128-byte record per RenderMaterial;
+//   * lights: emissive primitives, their alias table, a per-emissive-primitive
+//     cumulative triangle-area table (the reference scans triangles linearly;
+//     the same float cumulative sums searched by bisection select the same
+//     triangle), and a primitive -> emissive index map;
+//   * path state: ray (2 x float4, the trace kernels' yrc_ray layout),
+//     throughput, radiance, previous-bounce MIS data, medium state, PCG state,
+//     first-hit AOVs, and three pending next-event contributions.
+#pragma once
+
+#include <cstdint>
+
+#include "device_layout.cuh"
+
+namespace yrc {
+
+struct DevEnvironment {
+    int32_t active;
+    float radiance[3];
+    float strength;
+    float rotation;
+    int32_t width, height;
+    const float* texels;  // RGBA
+    const float* texel_weights;
+    const float* row_weights;
+    const float* row_cdf;
+    const float* conditional_cdfs;
+    float total_weight;
+};
+
+struct alignas(16) DevMaterial {
+    int32_t kind;
+    float reflectance[3];
+    float ior;
+    float uroughness;
+    float vroughness;
+    float coating_ior;
+    float coat_thickness;
+    float coat_absorption[3];
+    int32_t coat_maxdepth;
+    int32_t coat_nsamples;
+    float emission[3];
+    float absorption_color[3];
+    float absorption_distance;
+    float sigma_a[3];
+    float sigma_s[3];
+    float bssrdf_eta;
+    int32_t bssrdf_index;
+    int32_t pad[3];
+};
+
+struct DevBssrdf {
+    int32_t rho_count, radius_count;
+    const float* rho;
+    const float* radius;
+    const float* profile;
+    const float* rho_eff;
+    const float* profile_cdf;
+};
+
+struct DevAnalytic {
+    int32_t kind;
+    float position[3];
+    float direction[3];
+    float intensity[3];
+    float cone_angle;
+    float cone_cos_inner;
+};
+
+struct DevScene {
+    AccelParams accel;
+    // shading geometry
+    const int32_t* tri_prim;      // flat triangle -> mesh primitive
+    const int4* tri_vertices;     // flat triangle -> vertex indices (w unused)
+    const float4* positions;      // per vertex
+    const float4* normals;        // per vertex (w unused), may be null
+    const int32_t* prim_material; // per mesh primitive
+    const uint32_t* prim_flags;   // per mesh primitive (bit0 has_normals)
+    const int32_t* sphere_material;
+    const float4* spheres;        // center.xyz, radius
+    const int32_t* sphere_flip;
+    const float* instance_o2w;    // 16 floats per instance (column-major)
+    int32_t primitive_count;
+    int32_t sphere_count;
+    int32_t instance_count;
+    // materials
+    const DevMaterial* materials;
+    int32_t material_count;
+    // emissive lights
+    int32_t emissive_count;
+    const int32_t* emissive_prim;
+    const float* emissive_radiance;  // 3 per emissive
+    const float* emissive_area;
+    const float* alias_prob;
+    const int32_t* alias_index;
+    const float* alias_pmf;
+    int32_t alias_count;            // 0: linear power selection
+    float total_emissive_power;
+    const int32_t* emissive_tri_offset;  // per emissive: first entry in tri_cdf / tri_local
+    const int32_t* emissive_tri_count;
+    const float* tri_cdf;               // cumulative triangle areas
+    const int32_t* tri_local;           // local triangle index of each entry
+    const float* emissive_prim_area;    // sum of triangle areas per emissive primitive
+    const int32_t* prim_emissive;       // mesh primitive -> first emissive index or -1
+    // analytic lights
+    int32_t analytic_count;
+    const DevAnalytic* analytic;
+    const float* analytic_alias_prob;
+    const int32_t* analytic_alias_index;
+    const float* analytic_alias_pmf;
+    // environment
+    DevEnvironment env;
+    // subsurface
+    const DevBssrdf* bssrdf;
+    int32_t bssrdf_count;
+    // camera
+    float cam_origin[3], cam_forward[3], cam_right[3], cam_up[3];
+    float cam_half_height;  // tan(fov_y / 2), computed on the host
+    // settings
+    int32_t width, height, spp, max_depth, sampler;
+    uint64_t seed;
+    float radiance_clamp;
+    int32_t any_transparent;  // scene has Dielectric / ThinDielectric materials
+};
+
+// Path state, structure of arrays over `capacity` slots.
+struct PathState {
+    int32_t* pixel;       // pixel index
+    int32_t* sample;      // sample index (Sobol)
+    float4* throughput;   // xyz, w = unused
+    float4* radiance;     // xyz
+    float4* prev;         // origin xyz, bsdf pdf
+    uint32_t* flags;      // bit0 prev valid, bit1 prev delta, bit2 medium active, bit3 primary hit, bit4 done
+    float4* medium;       // absorption colour xyz, distance
+    uint64_t* rng_state;
+    uint64_t* rng_inc;
+    float4* aov_albedo;   // xyz, w = depth
+    float4* aov_normal;
+    float4* nee;          // 3 per path: contribution xyz (before throughput), w unused
+    float4* nee_tp;       // throughput at the vertex that made the NEE samples
+    float* nee_vis;       // 3 per path: shadow transmittance (1 visible, 0 occluded)
+};
+
+constexpr uint32_t kPathPrevValid = 1u << 0;
+constexpr uint32_t kPathPrevDelta = 1u << 1;
+constexpr uint32_t kPathMedium = 1u << 2;
+constexpr uint32_t kPathPrimary = 1u << 3;
+constexpr uint32_t kPathNee = 1u << 5;  // pending next-event contributions
+
+// Work queues (device counters live in a small array).
+struct Queues {
+    float4* ray_in;       // 2 per entry
+    int32_t* path_in;     // path slot per entry
+    float4* hits;         // closest hit per entry (t, id, u, v)
+    int32_t* inst;        // instance per entry
+    float4* ray_out;      // next bounce rays
+    int32_t* path_out;
+    float4* shadow_ray;   // 2 per shadow entry
+    int32_t* shadow_slot; // path * 3 + light type
+    uint8_t* shadow_occluded;
+    int32_t* nee_paths;   // paths with pending NEE
+    int32_t* class_paths[8];  // per material class: entry index into the extend queue
+    unsigned long long* counters;  // see kCounter*
+};
+
+enum CounterIndex {
+    kCtrIn = 0,
+    kCtrOut = 1,
+    kCtrShadow = 2,
+    kCtrNee = 3,
+    kCtrClass0 = 4,  // 8 class counters
+    kCtrTrace = 12,  // traversal work counter
+    kCtrShadowTrace = 13,
+    kCtrStatsBase = 16,  // rays, shadow rays, occluded, hits, misses, bad
+    kCtrCount = 24,
+};
+
+}  // namespace yrc

@@ -21,6 +21,7 @@
 //    total depth covers the BVH's longest root-to-leaf path;
 //  * nodes and leaf records are read with 128-bit read-only loads.
 #include "device_layout.cuh"
+#include "render_types.hpp"
 #include "trace_kernels.hpp"
 
 #include <cuda_runtime.h>
@@ -43,6 +44,7 @@ struct Traversal {
     int32_t tl_resume;  // TLAS record to resume after the BLAS, -1 = none
     int32_t cur_inst;   // instance being traversed
     uint32_t nodes, tris, spheres;  // BvhTraceStats
+    float wo[3], wd[3];  // world-space ray, restored after a BLAS
 };
 
 __device__ __forceinline__ float4 Ld(const float4* p) { return __ldg(p); }
@@ -67,24 +69,25 @@ struct StackStore {
     }
 };
 
-// Sets the world-space origin/direction of ray i (not t_min / t_max).
-__device__ __forceinline__ void LoadWorldRay(const float4* rays, int64_t i, Traversal& s) {
-    const float4 a = Ld(rays + 2 * i);
-    const float4 b = Ld(rays + 2 * i + 1);
-    s.r.o[0] = a.x;
-    s.r.o[1] = a.y;
-    s.r.o[2] = a.z;
-    s.r.d[0] = b.x;
-    s.r.d[1] = b.y;
-    s.r.d[2] = b.z;
+__device__ __forceinline__ void RestoreWorldRay(Traversal& s) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        s.r.o[k] = s.wo[k];
+        s.r.d[k] = s.wd[k];
+    }
     Precompute(s.r);
 }
 
-// Begins a traversal of ray i over [tmin, tmax]; returns false when the ray
-// already finished at the root (empty BVH or root box missed).
-__device__ __forceinline__ bool Begin(const AccelParams& a, const float4* rays, int64_t i, float tmin, float tmax,
-                                      Traversal& s) {
-    LoadWorldRay(rays, i, s);
+// Begins a traversal of the ray (o, d) over [tmin, tmax]; returns false when
+// the ray already finished at the root (empty BVH or root box missed).
+__device__ __forceinline__ bool BeginRay(const AccelParams& a, const float o[3], const float d[3], float tmin,
+                                         float tmax, Traversal& s) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        s.wo[k] = o[k];
+        s.wd[k] = d[k];
+    }
+    RestoreWorldRay(s);
     s.tmin = tmin;
     s.best.t = tmax;
     s.best.id = -1;
@@ -108,6 +111,16 @@ __device__ __forceinline__ bool Begin(const AccelParams& a, const float4* rays, 
     return true;
 }
 
+// Begin for ray i of a yrc_ray array.
+__device__ __forceinline__ bool Begin(const AccelParams& a, const float4* rays, int64_t i, float tmin, float tmax,
+                                      Traversal& s) {
+    const float4 ra = Ld(rays + 2 * i);
+    const float4 rb = Ld(rays + 2 * i + 1);
+    const float o[3] = {ra.x, ra.y, ra.z};
+    const float d[3] = {rb.x, rb.y, rb.z};
+    return BeginRay(a, o, d, tmin, tmax, s);
+}
+
 // Pops the next live stack entry into s.cur (culled against the nearest t of
 // the current level) and closes finished BLAS traversals. Returns false when
 // the ray's traversal is complete.
@@ -121,7 +134,7 @@ __device__ __forceinline__ bool Pop(const float4* rays, int64_t ray, Traversal& 
                 s.best_inst = s.cur_inst;
             }
             s.level = 0;
-            LoadWorldRay(rays, ray, s);
+            RestoreWorldRay(s);
             if (kAny && s.best.hit) return false;
             if (s.tl_resume >= 0) {
                 s.cur = ~s.tl_resume;
@@ -270,7 +283,7 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
 template <bool kAny, bool kStats>
 __device__ __forceinline__ void WriteResult(const TraceArgs& args, int64_t ray, const Traversal& s) {
     if (kAny) {
-        args.occluded[ray] = s.best.hit ? 1 : 0;
+        args.occluded[args.out_index ? args.out_index[ray] : ray] = s.best.hit ? 1 : 0;
     } else {
         reinterpret_cast<float4*>(args.hits)[ray] =
             make_float4(s.best.t, __int_as_float(s.best.hit ? s.best.id : -1), s.best.u, s.best.v);
@@ -294,6 +307,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args
     int64_t ray = -1;
     bool alive = false;
     bool exhausted = false;
+    const unsigned long long count =
+        args.count_ptr ? *args.count_ptr : static_cast<unsigned long long>(args.count);
 
     for (;;) {
         const unsigned need = __ballot_sync(kFull, !alive && !exhausted);
@@ -306,7 +321,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args
             base = __shfl_sync(kFull, base, leader);
             if (!alive && !exhausted) {
                 const unsigned long long idx = base + __popc(need & lt_mask);
-                if (idx >= static_cast<unsigned long long>(args.count)) {
+                if (idx >= count) {
                     exhausted = true;
                 } else {
                     ray = static_cast<int64_t>(idx);
@@ -374,6 +389,104 @@ __global__ void __launch_bounds__(kTraceBlock) ProbeKernel(ProbeArgs args) {
     }
 }
 
+// TraceShadowVisibility (src/integrators/path_direct_lighting.cpp:23-113):
+// up to 16 closest-hit queries along the shadow segment; Dielectric surfaces
+// toggle a Beer-Lambert medium, ThinDielectric ones multiply by their clamped
+// reflectance, anything else occludes. One thread per shadow ray; writes the
+// RGB transmittance (0 when occluded) to transmittance[out_index[i]].
+template <bool kTwo, int kTotal>
+__global__ void __launch_bounds__(kTraceBlock) ShadowTransmittanceKernel(ShadowArgs args) {
+    __shared__ int2 s_stack[kShortStack * kTraceBlock];
+    int2* col = s_stack + threadIdx.x;
+    StackStore<kTotal> st;
+    Traversal s;
+    const int64_t count = static_cast<int64_t>(*args.count_ptr);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const float4 ra = Ld(args.rays + 2 * i);
+        const float4 rb = Ld(args.rays + 2 * i + 1);
+        float o[3] = {ra.x, ra.y, ra.z};
+        const float d[3] = {rb.x, rb.y, rb.z};
+        float remaining = rb.w;
+        float T[3] = {1.0f, 1.0f, 1.0f};
+        bool medium = false;
+        float mc[3] = {1.0f, 1.0f, 1.0f};
+        float md = 1.0f;
+        bool visible = false;
+        auto beer = [&](float dist) {
+            if (dist <= 0.0f || md <= 0.0f) return;
+            const float inv = 1.0f / md;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float c = fminf(fmaxf(mc[k], 1.0e-6f), 1.0f);
+                T[k] = T[k] * expf(logf(c) * dist * inv);
+            }
+        };
+        auto black = [&]() { return fmaxf(T[0], fmaxf(T[1], T[2])) <= 1.0e-6f; };
+        for (int hitc = 0; hitc < 16; ++hitc) {
+            bool alive = BeginRay(args.accel, o, d, 1.0e-5f, remaining, s);
+            while (alive) alive = Step<false, false, kTwo>(args.accel, args.rays, i, s, st, col, args.error);
+            const bool finite = isfinite(remaining);
+            if (!s.best.hit) {
+                if (medium) {
+                    if (!finite) break;  // occluded
+                    beer(remaining);
+                }
+                visible = !black();
+                break;
+            }
+            const float t = s.best.t;
+            if (medium) {
+                beer(t);
+                if (black()) break;
+            }
+            int32_t material = -1;
+            bool valid_material = true;
+            if (s.best.id >= 0) {
+                const int32_t prim = args.tri_prim[s.best.id];
+                material = args.prim_material[prim];
+                valid_material = material >= 0;
+            } else {
+                material = args.sphere_material[-2 - s.best.id];
+            }
+            if (!valid_material || material < 0) break;  // invalid or default (opaque diffuse) material
+            const DevMaterial& m = args.materials[material];
+            if (m.kind != 2 && m.kind != 3) break;  // only Dielectric / ThinDielectric pass light
+            float hp[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) hp[k] = o[k] + d[k] * t;
+            if (m.kind == 3) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) T[k] = T[k] * fminf(fmaxf(m.reflectance[k], 0.0f), 1.0f);
+                if (black()) break;
+            } else if (medium) {
+                medium = false;
+                mc[0] = mc[1] = mc[2] = 1.0f;
+                md = 1.0f;
+            } else {
+                medium = true;
+                mc[0] = m.absorption_color[0];
+                mc[1] = m.absorption_color[1];
+                mc[2] = m.absorption_color[2];
+                md = m.absorption_distance;
+            }
+            const float bias = fmaxf(1.0e-4f, fmaxf(fabsf(hp[0]), fmaxf(fabsf(hp[1]), fabsf(hp[2]))) * 1.0e-5f);
+            if (finite) {
+                remaining -= t + bias;
+                if (remaining <= 0.0f) {
+                    visible = !black();
+                    break;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) o[k] = hp[k] + d[k] * bias;
+        }
+        const int32_t slot = args.out_index[i];
+        args.transmittance[slot] =
+            visible ? make_float4(T[0], T[1], T[2], 1.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
 template <typename Kernel>
 cudaError_t PersistentGrid(Kernel kernel, int block, int64_t count, int sm_count, int64_t& blocks) {
     int per_sm = 0;
@@ -428,7 +541,26 @@ cudaError_t LaunchProbeOne(const ProbeArgs& args, cudaStream_t stream, int sm_co
     return cudaGetLastError();
 }
 
+template <bool kTwo, int kTotal>
+cudaError_t LaunchShadowOne(const ShadowArgs& args, cudaStream_t stream, int sm_count) {
+    auto kernel = ShadowTransmittanceKernel<kTwo, kTotal>;
+    int64_t blocks = 0;
+    const cudaError_t err = PersistentGrid(kernel, kTraceBlock, args.capacity, sm_count, blocks);
+    if (err != cudaSuccess) return err;
+    kernel<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+cudaError_t LaunchShadowTransmittance(const ShadowArgs& args, cudaStream_t stream, int sm_count) {
+    const bool two = args.accel.two_level != 0;
+    const bool deep = args.accel.stack_limit > 64;
+    if (two) return deep ? LaunchShadowOne<true, kMaxTraceStack>(args, stream, sm_count)
+                         : LaunchShadowOne<true, 64>(args, stream, sm_count);
+    return deep ? LaunchShadowOne<false, kMaxTraceStack>(args, stream, sm_count)
+                : LaunchShadowOne<false, 64>(args, stream, sm_count);
+}
 
 cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, int shape, cudaStream_t stream,
                         int sm_count) {

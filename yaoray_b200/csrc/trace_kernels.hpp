@@ -30,6 +30,8 @@ struct TraceArgs {
     uint32_t* sphere_tests;
     unsigned long long* counter;  // ray work counter, zeroed before the launch
     int* error;                   // device error word
+    const unsigned long long* count_ptr;  // optional: ray count read on the device (count = capacity)
+    const int32_t* out_index;             // optional: any-hit output slot per ray
 };
 
 constexpr int kProbeMaxHits = YRC_PROBE_MAX_HITS;  // BvhProbeHits::MaxHits
@@ -49,6 +51,30 @@ struct ProbeArgs {
 
 // shape: index of the launch shape (block size / refill interval / register
 // budget) for the flat closest- and any-hit kernels, 0 = default.
+struct DevMaterial;
+
+struct ShadowArgs {
+    AccelParams accel;
+    const float4* rays;                   // shadow queue (2 x float4 per ray)
+    const unsigned long long* count_ptr;  // entries in the queue (device)
+    int64_t capacity;                     // grid sizing bound
+    const int32_t* out_index;             // slot per ray
+    float4* transmittance;                // per slot
+    const int32_t* tri_prim;
+    const int32_t* prim_material;
+    const int32_t* sphere_material;
+    const DevMaterial* materials;
+    int* error;
+};
+
+// Accessors of accelerator internals used by the render stages (accel.cu).
+AccelParams AccelParamsOf(const yrc_accel* a);
+int TraceShapeOf(const yrc_accel* a, int any_hit);
+int* AccelErrorWord(yrc_accel* a);
+yrc_status CheckDeviceError(yrc_accel* a);
+
+cudaError_t LaunchShadowTransmittance(const ShadowArgs& args, cudaStream_t stream, int sm_count);
+
 cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, int shape, cudaStream_t stream,
                         int sm_count);
 cudaError_t LaunchProbe(const ProbeArgs& args, cudaStream_t stream, int sm_count);
