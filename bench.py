@@ -305,8 +305,62 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+def run_cornell(args):
+    """--workload cornell: the plain MIS path tracer on the Cornell box
+    (256x256, 64 spp, Owen-Sobol seed 0, max depth 8). One step = one full
+    64-spp render through CudaBackend.render (device-resident scene, film
+    read back to the host); value = samples/s. The CPU baseline renders the
+    same scene with the reference CPU backend at 8 spp on all host threads."""
+    import torch
+    from yaoray_b200 import cornell
+    from yaoray_b200.render import CudaBackend
+
+    scene = cornell.scene()
+    backend = CudaBackend()
+    prepared = backend.prepare(scene)
+    for _ in range(args.warmup):
+        res = backend.render(prepared)
+        assert res.ok, res.error
+    gpu_index = 0
+    times, devs = [], []
+    with ClockSampler(gpu_index) as clocks:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = backend.render(prepared)
+            times.append(time.perf_counter() - t0)
+            devs.append(res.stats["device_seconds"])
+    samples = scene.width * scene.height * scene.spp
+    dt = sum(times) / len(times)
+    ddt = sum(devs) / len(devs)
+    base = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle
+        if oracle.ref_available():
+            job = oracle.RefJob.from_scene(scene)
+            job.render(spp=1)
+            film, st, secs = job.render(spp=8)
+            base = {"value": round(scene.width * scene.height * 8 / secs, 1), "unit": "samples/s",
+                    "cores": os.cpu_count(), "kind": "reference",
+                    "sample": f"reference CpuBackend, same scene at 8 spp ({secs:.2f} s)"}
+    line = {"metric": "samples/s (plain MIS path tracer, Cornell box)", "value": round(samples / ddt, 1),
+            "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ddt * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "cornell-256x256-64spp-depth8", "triangles": scene.geometry.triangle_count,
+                       "path_segments_per_step": int(res.stats["rays_traced"]),
+                       "shadow_rays_per_step": int(res.stats["shadow_rays"])},
+            "e2e": {"value": round(samples / dt, 1), "unit": "samples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": scene.width * scene.height * 56},
+            "path_segments_per_s": round(res.stats["rays_traced"] / ddt, 1),
+            "cpu_baseline": base, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--workload", choices=["traversal", "cornell"], default="traversal")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
@@ -320,6 +374,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "cornell":
+        run_cornell(args)
     else:
         run_gpu(args)
 

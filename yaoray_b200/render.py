@@ -130,7 +130,7 @@ class Progress(C.Structure):
                 ("rays_traced", C.c_uint64), ("elapsed_seconds", C.c_double)]
 
 
-PROGRESS_FN = C.CFUNCTYPE(C.c_int32, C.POINTER(Progress), C.c_void_p, C.c_uint64, C.c_void_p, C.c_char_p,
+PROGRESS_FN = C.CFUNCTYPE(C.c_int32, C.POINTER(Progress), C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                           C.c_size_t)
 
 
@@ -404,8 +404,9 @@ class CudaBackend:
                                      FILM_PIXEL_DTYPE).reshape(sc.height, sc.width).copy()
                 prog = {f[0]: getattr(p.contents, f[0]) for f in Progress._fields_}
                 cancel, msg = req.progress_callback(prog, film)
-                if cancel and msg:
-                    C.memmove(err, msg.encode()[: cap - 1] + b"\0", min(len(msg) + 1, cap))
+                if cancel and msg and err and cap > 0:
+                    data = msg.encode()[: cap - 1] + b"\0"
+                    C.memmove(err, data, len(data))
                 return 1 if cancel else 0
             r.progress = PROGRESS_FN(cb)
             keep.append(r.progress)
