@@ -110,12 +110,14 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per launch of the trace kernel from the committed ncu summary."""
+def profiled_traffic(rays: int):
+    """DRAM bytes (read + write) of one trace launch over `rays` rays: the
+    per-ray figure of the committed ncu capture (a 1M-ray launch of the same
+    workload) scaled by the ray count."""
     if PROFILE_SUMMARY.exists():
-        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", PROFILE_SUMMARY.read_text())
+        m = re.search(r"dram_bytes_per_ray:\s*([0-9.eE+]+)", PROFILE_SUMMARY.read_text())
         if m:
-            return float(m.group(1))
+            return round(float(m.group(1)) * rays)
     return None
 
 
@@ -219,6 +221,9 @@ def run_gpu(args):
     tri_tests = int(st[1].to(torch.int64).sum().item())
     algo_bytes = 32 * node_tests + 48 * tri_tests + (32 + 16) * n
     del st
+    # Device BVH: one 32-byte box+ref per node (stored as 64-byte child pairs)
+    # and one 48-byte record per triangle.
+    bvh_mib = (32 * len(bvh.nodes) + 48 * geom.triangle_count) >> 20
 
     def barrier():
         if ws > 1:
@@ -274,7 +279,7 @@ def run_gpu(args):
 
     peak, peak_kind = measured_peak()
     achieved = algo_bytes / per_launch_s / 1e9
-    traffic = profiled_traffic()
+    traffic = profiled_traffic(n)
     base = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(geom, rays_np, seconds=args.cpu_seconds)
@@ -285,7 +290,8 @@ def run_gpu(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "triangles": geom.triangle_count, "bvh_nodes": int(len(bvh.nodes)),
                        "rays_per_step_per_gpu": n, "ray_set": "incoherent: origin U[0,100]^3, direction uniform",
-                       "l2": "inputs larger than L2 (rays 256 MB + hits 128 MB + BVH), no flush",
+                       "l2": f"inputs larger than L2 (rays {n * 32 >> 20} MiB + hits {n * 16 >> 20} MiB + "
+                             f"BVH {bvh_mib} MiB, L2 126 MB), no flush",
                        "parallelism": f"replicas x{ws}", "launch_shape": tune["shape"],
                        "autotune_ms": tune["times_ms"]},
             "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": n * 32,

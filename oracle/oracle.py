@@ -30,6 +30,8 @@ def build(reference: bool = True) -> None:
     if reference and REFERENCE_SRC.exists():
         jobs = str(min(16, os.cpu_count() or 4))
         subprocess.run(["make", "-s", "-C", str(HERE), f"-j{jobs}", "ref", f"REF={REFERENCE_SRC}"], check=True)
+        # the drop-in driver links the product library, built before this step
+        subprocess.run(["make", "-s", "-C", str(HERE), f"-j{jobs}", "dropin", f"REF={REFERENCE_SRC}"], check=True)
 
 
 def ref_available() -> bool:
