@@ -278,6 +278,41 @@ yrc_status yrc_trace_stats_device(yrc_accel* accel, const yrc_ray* rays, int64_t
                                   uint32_t* node_tests, uint32_t* triangle_tests, uint32_t* sphere_tests,
                                   void* stream);
 
+/* Rays per call accepted by yrc_trace_stats_device_noalloc. */
+#define YRC_NOALLOC_STATS_MAX_RAYS 262144
+
+/*
+ * yrc_trace_stats_device without any device allocation. No counterpart in the
+ * reference: it exists for callers of this library that cannot allocate.
+ *
+ * yrc_trace_stats_device takes a temporary buffer from the stream-ordered
+ * allocator for the hit records that the counting traversal writes and then
+ * discards. Some callers cannot let it: an application that hands all device
+ * memory to its own pool at start-up (a later allocation fails, or takes
+ * memory the pool counts on), or a per-frame loop that must never enter the
+ * CUDA allocator. This variant calls no cudaMalloc, cudaFree or other
+ * allocating routine; it uses a fixed scratch array that the library keeps on
+ * every GPU that loads it, from load until the process exits
+ * (256 + 16 * YRC_NOALLOC_STATS_MAX_RAYS bytes, just over 4 MiB).
+ *
+ * - count above YRC_NOALLOC_STATS_MAX_RAYS returns YRC_ERR_INVALID_ARGUMENT
+ *   before any work is queued; split larger batches.
+ * - The first call on each device looks up the scratch array's device address
+ *   (with that device current) and caches it. Make that first call before any
+ *   stream capture begins.
+ * - All calls on one device share the scratch array, which keeps whatever the
+ *   last call left there. The part that must start at zero (the ray-refill
+ *   counter) is reset on `stream` before each launch; the rest is write-only.
+ *   Calls whose GPU work overlaps (unordered streams, or several accelerators
+ *   or host threads on one device) race on it and return wrong counts: order
+ *   them, e.g. on one stream.
+ * - Outputs are the per-ray counters of yrc_trace_stats_device; arrays may be
+ *   NULL.
+ */
+yrc_status yrc_trace_stats_device_noalloc(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags,
+                                          uint32_t* node_tests, uint32_t* triangle_tests,
+                                          uint32_t* sphere_tests, void* stream);
+
 /*
  * Autotuner: times every compiled launch shape of the flat closest-hit (or,
  * with YRC_TRACE_ANY, any-hit) kernel on `count` device rays (results are

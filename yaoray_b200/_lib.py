@@ -27,6 +27,7 @@ YRC_TRACE_CLOSEST = 0
 YRC_TRACE_ANY = 1
 YRC_TRACE_STATS = 2
 YRC_PROBE_MAX_HITS = 64
+YRC_NOALLOC_STATS_MAX_RAYS = 262144
 
 STATUS_NAMES = {
     0: "ok",
@@ -171,6 +172,7 @@ def lib() -> C.CDLL:
         "yrc_trace_device": (C.c_int, [P, P, I64, I32, P, P, P, P]),
         "yrc_trace_host": (C.c_int, [P, P, I64, I32, P, P, P, P]),
         "yrc_trace_stats_device": (C.c_int, [P, P, I64, I32, P, P, P, P]),
+        "yrc_trace_stats_device_noalloc": (C.c_int, [P, P, I64, I32, P, P, P, P]),
         "yrc_probe_device": (C.c_int, [P, P, P, I64, P, P, P, P, P]),
         "yrc_accel_check": (C.c_int, [P]),
         "yrc_accel_autotune": (C.c_int, [P, P, I64, I32, P, P]),

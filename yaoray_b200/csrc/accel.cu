@@ -353,6 +353,45 @@ yrc_status CheckDeviceError(yrc_accel* a) {
 
 }  // namespace yrc
 
+// Fixed scratch of yrc_trace_stats_device_noalloc, resident on every GPU that
+// loads this library until the process exits. Bytes [0, 256) hold the
+// persistent-warp ray-refill counter, which must be zero when a launch starts
+// (reset with cudaMemsetAsync on the caller's stream before every launch);
+// from byte 256 on, the hit records (16 B per ray) or occlusion bytes (1 B per
+// ray) that the stats traversal writes and nobody reads — they need no
+// clearing. Host code sees this name only as a host-side stand-in: the device
+// address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char yrc_noalloc_stats_scratch[256 + 16 * YRC_NOALLOC_STATS_MAX_RAYS];
+
+namespace yrc {
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_scratch[kNoAllocMaxDevices] = {};
+
+// Device address of yrc_noalloc_stats_scratch on `device`, which must be the
+// current device. Looked up on the first call per device and cached.
+yrc_status NoAllocScratch(int device, unsigned char** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) {
+        return Fail(YRC_ERR_UNSUPPORTED, "yrc_trace_stats_device_noalloc: device index " + std::to_string(device) +
+                                             " is beyond the " + std::to_string(kNoAllocMaxDevices) +
+                                             " devices this entry point keeps scratch addresses for");
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_scratch[device]) {
+        void* p = nullptr;
+        const cudaError_t err = cudaGetSymbolAddress(&p, yrc_noalloc_stats_scratch);
+        if (err != cudaSuccess) return CudaFail(err, "yrc_trace_stats_device_noalloc: scratch address lookup");
+        g_noalloc_scratch[device] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_scratch[device];
+    return Ok();
+}
+
+}  // namespace
+}  // namespace yrc
+
 extern "C" {
 
 yrc_status yrc_accel_create_flat(const yrc_geometry* geometry, const yrc_bvh_view* bvh, yrc_accel** out) {
@@ -485,6 +524,34 @@ yrc_status yrc_trace_stats_device(yrc_accel* accel, const yrc_ray* rays, int64_t
                                   sphere_tests, accel->d_counter, static_cast<cudaStream_t>(stream));
     cudaFreeAsync(scratch, static_cast<cudaStream_t>(stream));
     return s;
+}
+
+yrc_status yrc_trace_stats_device_noalloc(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags,
+                                          uint32_t* node_tests, uint32_t* triangle_tests, uint32_t* sphere_tests,
+                                          void* stream) {
+    using namespace yrc;
+    if (!accel || count < 0 || (count > 0 && !rays)) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_trace_stats_device_noalloc: bad argument");
+    }
+    if (count > YRC_NOALLOC_STATS_MAX_RAYS) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT,
+                    "yrc_trace_stats_device_noalloc: " + std::to_string(count) + " rays exceed the fixed maximum of " +
+                        std::to_string(YRC_NOALLOC_STATS_MAX_RAYS) +
+                        " per call (the size of its preallocated scratch); split the batch or use "
+                        "yrc_trace_stats_device");
+    }
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    cudaSetDevice(accel->device);
+    unsigned char* scratch = nullptr;
+    const yrc_status set_up = NoAllocScratch(accel->device, &scratch);
+    if (set_up != YRC_OK) return set_up;
+    const bool any = (flags & YRC_TRACE_ANY) != 0;
+    // LaunchInternal zeroes the counter (cudaMemsetAsync) before the launch.
+    auto* counter = reinterpret_cast<unsigned long long*>(scratch);
+    unsigned char* discard = scratch + 256;
+    return LaunchInternal(accel, rays, count, flags | YRC_TRACE_STATS, any ? nullptr : reinterpret_cast<yrc_hit*>(discard),
+                          nullptr, any ? discard : nullptr, node_tests, triangle_tests, sphere_tests, counter,
+                          static_cast<cudaStream_t>(stream));
 }
 
 yrc_status yrc_trace_host(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags, yrc_hit* hits,
