@@ -277,6 +277,39 @@ def run_gpu(args):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = ws * n * e_steps / float(te.item()) / 1e6
 
+    # The workload's other two query sets, timed the same way (device-resident,
+    # CUDA events, max over ranks): coherent primary rays (closest hit) and
+    # shadow queries (any hit, t_max = distance to a uniform random point).
+    del host_rays, host_hits
+    other_sets = {}
+    for key, make, any_hit in (("coherent_closest_hit", lambda: scenes.coherent_rays(), False),
+                               ("incoherent_any_hit_shadow", lambda: scenes.shadow_rays(seed=3 + 1000 * rank), True)):
+        set_rays = torch.from_numpy(make()).to(dev)
+        m = set_rays.shape[0]
+        if any_hit:
+            out = torch.empty(m, dtype=torch.uint8, device=dev)
+        else:
+            out = hits[:m] if m <= n else torch.empty((m, 4), dtype=torch.float32, device=dev)
+        acc.autotune(set_rays[: min(m, 1 << 21)], any_hit=any_hit, stream=stream)
+        for _ in range(args.warmup):
+            acc.intersect(set_rays, any_hit=any_hit, hits=None if any_hit else out,
+                          occluded=out if any_hit else None, stream=stream)
+        barrier()
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(args.steps):
+            acc.intersect(set_rays, any_hit=any_hit, hits=None if any_hit else out,
+                          occluded=out if any_hit else None, stream=stream)
+        end.record(stream)
+        end.synchronize()
+        acc.check()
+        ts = torch.tensor([start.elapsed_time(end)], dtype=torch.float64, device=dev)
+        if ws > 1:
+            dist.all_reduce(ts, op=dist.ReduceOp.MAX)
+        other_sets[key] = {"rays_per_step_per_gpu": m,
+                           "mrays_s": round(ws * m * args.steps / (float(ts.item()) / 1e3) / 1e6, 2)}
+        del set_rays, out
+
     peak, peak_kind = measured_peak()
     achieved = algo_bytes / per_launch_s / 1e9
     traffic = profiled_traffic(n)
@@ -302,6 +335,7 @@ def run_gpu(args):
                          "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": algo_bytes,
                          "node_tests_per_ray": round(node_tests / n, 2),
                          "triangle_tests_per_ray": round(tri_tests / n, 2)},
+            "other_ray_sets": other_sets,
             "cpu_baseline": base,
             "clocks": clocks.summary(),
         }
@@ -311,19 +345,42 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
-def run_cornell(args):
+RENDER_WORKLOADS = {
+    "cornell": ("samples/s (plain MIS path tracer, Cornell box)", "cornell-256x256-64spp-depth8"),
+    "instanced": ("samples/s (plain wavefront path tracer, instanced scene)",
+                  "instanced-256inst-31M-tris-1920x1080-depth16"),
+}
+
+
+def render_scene(workload: str, spp: int):
+    if workload == "cornell":
+        from yaoray_b200 import cornell
+        return cornell.scene()
+    from yaoray_b200 import instanced
+    return instanced.scene(spp=spp)
+
+
+def run_render(args):
     """--workload cornell: the plain MIS path tracer on the Cornell box
-    (256x256, 64 spp, Owen-Sobol seed 0, max depth 8). One step = one full
-    64-spp render through CudaBackend.render (device-resident scene, film
-    read back to the host); value = samples/s. The CPU baseline renders the
-    same scene with the reference CPU backend at 8 spp on all host threads."""
+    (256x256, 64 spp, Owen-Sobol seed 0, max depth 8); one step = one full
+    64-spp render.
+    --workload instanced: the instanced scene (256 affine instances of four
+    procedural meshes, 31.4M instanced triangles, HDRI + 64 emissive
+    triangles, 1920x1080, max depth 16); one step = one render of
+    --render-spp samples per pixel (the full 256 spp is 256/--render-spp
+    steps).
+    Both go through CudaBackend.render (device-resident scene, film read back
+    to the host); value = samples/s from the device time of the render,
+    e2e from the host wall clock around the call. The CPU baseline renders the
+    same scene with the reference CPU backend on all host threads at a few spp."""
     import torch
-    from yaoray_b200 import cornell
     from yaoray_b200.render import CudaBackend
 
-    scene = cornell.scene()
+    scene = render_scene(args.workload, args.render_spp)
     backend = CudaBackend()
+    t0 = time.perf_counter()
     prepared = backend.prepare(scene)
+    prepare_s = time.perf_counter() - t0
     for _ in range(args.warmup):
         res = backend.render(prepared)
         assert res.ok, res.error
@@ -346,17 +403,26 @@ def run_cornell(args):
         if oracle.ref_available():
             job = oracle.RefJob.from_scene(scene)
             job.render(spp=1)
-            film, st, secs = job.render(spp=8)
-            base = {"value": round(scene.width * scene.height * 8 / secs, 1), "unit": "samples/s",
+            base_spp = 8 if args.workload == "cornell" else 1
+            film, st, secs = job.render(spp=base_spp)
+            base = {"value": round(scene.width * scene.height * base_spp / secs, 1), "unit": "samples/s",
                     "cores": os.cpu_count(), "kind": "reference",
-                    "sample": f"reference CpuBackend, same scene at 8 spp ({secs:.2f} s)"}
-    line = {"metric": "samples/s (plain MIS path tracer, Cornell box)", "value": round(samples / ddt, 1),
+                    "sample": f"reference CpuBackend, same scene at {base_spp} spp ({secs:.2f} s)"}
+    metric, workload = RENDER_WORKLOADS[args.workload]
+    config = {"workload": workload, "triangles": scene.geometry.triangle_count,
+              "width": scene.width, "height": scene.height, "spp_per_step": scene.spp,
+              "max_depth": scene.max_depth,
+              "path_segments_per_step": int(res.stats["rays_traced"]),
+              "shadow_rays_per_step": int(res.stats["shadow_rays"])}
+    if args.workload == "instanced":
+        from yaoray_b200 import instanced
+        config.update(instances=int(instanced.INSTANCES), instanced_triangles=instanced.instanced_triangles(scene),
+                      hdri="2048x1024 RGBA32F", emissive_triangles=int(scene.emissive.size),
+                      prepare_seconds=round(prepare_s, 2))
+    line = {"metric": metric, "value": round(samples / ddt, 1),
             "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ddt * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "cornell-256x256-64spp-depth8", "triangles": scene.geometry.triangle_count,
-                       "path_segments_per_step": int(res.stats["rays_traced"]),
-                       "shadow_rays_per_step": int(res.stats["shadow_rays"])},
+            "dtype": "f32", "data": "synthetic", "config": config,
             "e2e": {"value": round(samples / dt, 1), "unit": "samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": scene.width * scene.height * 56},
             "path_segments_per_s": round(res.stats["rays_traced"] / ddt, 1),
@@ -366,7 +432,8 @@ def run_cornell(args):
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--workload", choices=["traversal", "cornell"], default="traversal")
+    ap.add_argument("--workload", choices=["traversal", "cornell", "instanced"], default="traversal")
+    ap.add_argument("--render-spp", type=int, default=16, help="spp per step of --workload instanced")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
@@ -380,8 +447,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "cornell":
-        run_cornell(args)
+    elif args.workload in RENDER_WORKLOADS:
+        run_render(args)
     else:
         run_gpu(args)
 

@@ -85,3 +85,36 @@ def test_environment_distribution_builder():
     env = EnvironmentMap(active=True, texels=np.zeros((4, 4, 4), np.float32))
     env.build_distribution()
     assert env.total_weight == 16 and np.all(env.texel_weights == 1)
+
+
+def test_instanced_config_shape():
+    from yaoray_b200 import instanced
+    s = instanced.scene(width=32, height=16, spp=1, mesh_scale=0.01, instances=40, env_width=64)
+    g = s.geometry
+    assert g.instances.size == 40 + 1 + 64  # instances, then identity instances of ground + emitters
+    assert (g.instances["primitive"][:40] < instanced.OBJECTS).all()
+    assert np.array_equal(g.instances["primitive"][40:], np.arange(instanced.OBJECTS, instanced.OBJECTS + 65))
+    assert s.emissive.size == 64 and (s.emissive["area"] > 0).all()
+    kinds = s.materials["kind"][: instanced.OBJECTS]
+    assert [int((kinds == k).sum()) for k in (0, 1, 2, 4)] == [13, 8, 6, 5]
+    # every object primitive owns its index range
+    p = g.primitives
+    assert (p["first_index"][1:] == p["first_index"][:-1] + p["index_count"][:-1]).all()
+    assert s.environment.texels.shape == (32, 64, 4) and s.environment.total_weight > 0
+    # the sun: at full resolution texels inside the 0.5 degree disk carry
+    # 1e4; at any resolution the disk's power (radiance x solid angle) is kept
+    import math
+    sun_power = instanced.SUN_RADIANCE * 2 * math.pi * (1 - math.cos(math.radians(instanced.SUN_DIAMETER_DEG / 2)))
+    for w in (256, 2048):
+        t = instanced.hdri(w, w // 2)[..., 0]
+        th = (np.arange(w // 2) + 0.5) * np.pi / (w // 2)
+        solid = (np.pi / (w // 2)) * (2 * np.pi / w) * np.sin(th)[:, None]
+        power = float((np.where(t > 2, t - 1, 0) * solid).sum())
+        assert abs(power / sun_power - 1) < 0.05, (w, power, sun_power)
+    assert instanced.hdri(2048, 1024)[..., 0].max() == instanced.SUN_RADIANCE
+
+
+def test_instanced_full_size_counts():
+    from yaoray_b200 import instanced
+    ms = instanced.meshes()
+    assert [t.shape[0] for _, t, _ in ms] == [50000, 75000, 100000, 249218]
