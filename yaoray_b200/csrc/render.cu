@@ -98,6 +98,7 @@ struct yrc_render_scene {
     yrc::PathState ps{};
     yrc::Queues q{};
     float4* transmittance = nullptr;
+    int32_t* shadow_pending = nullptr;  // shadow rays (2 per path) left for the transmittance pass
     yrc_film_pixel* film = nullptr;
     int32_t* attempts = nullptr;
     int32_t* active = nullptr;
@@ -287,6 +288,22 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
     d.materials = A.Upload(mats);
     d.material_count = desc->material_count;
     d.any_transparent = transparent ? 1 : 0;
+    if (transparent) {
+        // Surfaces a shadow ray may pass (TraceShadowVisibility continues only
+        // through Dielectric and ThinDielectric hits).
+        auto clear = [&](int32_t mi) {
+            return static_cast<uint8_t>(mi >= 0 && (mats[static_cast<size_t>(mi)].kind == YRC_MAT_DIELECTRIC ||
+                                                    mats[static_cast<size_t>(mi)].kind == YRC_MAT_THIN_DIELECTRIC));
+        };
+        std::vector<uint8_t> tri_clear(tri_prim.size()), sphere_clear(sphere_material.size());
+        for (size_t t = 0; t < tri_prim.size(); ++t) {
+            const int32_t p = tri_prim[t];
+            tri_clear[t] = p >= 0 ? clear(prim_material[static_cast<size_t>(p)]) : 0;
+        }
+        for (size_t i = 0; i < sphere_material.size(); ++i) sphere_clear[i] = clear(sphere_material[i]);
+        d.tri_clear = A.Upload(tri_clear);
+        d.sphere_clear = A.Upload(sphere_clear);
+    }
 
     // Emissive lights, alias table, per-light triangle area CDF.
     const int32_t ne = desc->emissive_count;
@@ -428,8 +445,11 @@ yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     q.shadow_slot = W.Alloc<int32_t>(2 * capacity);
     q.shadow_occluded = W.Alloc<uint8_t>(3 * capacity);
     q.nee_paths = W.Alloc<int32_t>(capacity);
+    q.order = W.Alloc<int32_t>(capacity);
+    q.shade_class = W.Alloc<uint8_t>(capacity);
     q.counters = W.Alloc<unsigned long long>(kCtrCount);
     s->transmittance = s->dev.any_transparent ? W.Alloc<float4>(3 * capacity) : nullptr;
+    s->shadow_pending = s->dev.any_transparent ? W.Alloc<int32_t>(2 * capacity) : nullptr;
     s->film = W.Alloc<yrc_film_pixel>(static_cast<size_t>(pixels));
     s->attempts = W.Alloc<int32_t>(static_cast<size_t>(pixels));
     s->active = W.Alloc<int32_t>(static_cast<size_t>(pixels));
@@ -487,6 +507,11 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
             sa.prim_material = sc.prim_material;
             sa.sphere_material = sc.sphere_material;
             sa.materials = sc.materials;
+            sa.tri_clear = sc.tri_clear;
+            sa.sphere_clear = sc.sphere_clear;
+            sa.pending = s->shadow_pending;
+            sa.pending_count = q.counters + kCtrPending;
+            sa.counter = q.counters + kCtrShadowTrace;
             sa.error = ta.error;
             err = LaunchShadowTransmittance(sa, st, s->sm_count);
         } else {

@@ -116,12 +116,95 @@ __global__ void ResetCountersKernel(Queues q) {
         q.counters[kCtrNee] = 0;
         q.counters[kCtrTrace] = 0;
         q.counters[kCtrShadowTrace] = 0;
+        q.counters[kCtrPending] = 0;
+        for (int c = 0; c < kShadeClasses; ++c) {
+            q.counters[kCtrClass0 + c] = 0;
+            q.counters[kCtrCursor0 + c] = 0;
+        }
     }
 }
 
 // Makes the next-bounce queue the current one.
 __global__ void AdvanceQueueKernel(Queues q) {
     if (threadIdx.x == 0) q.counters[kCtrIn] = q.counters[kCtrOut];
+}
+
+// ------------------------------------------------------------ class sort
+
+// Shading class of one extend-queue entry (its hit's material kind).
+__device__ inline int ShadeClassOf(const DevScene& sc, float4 hit) {
+    const int32_t id = __float_as_int(hit.y);
+    if (id == -1) return kClassMiss;
+    int32_t material;
+    if (id <= -2) {
+        material = sc.sphere_material[-2 - id];
+        if (material < 0) return kClassDiffuse;  // default RenderMaterial
+    } else {
+        material = sc.prim_material[sc.tri_prim[id]];
+        if (material < 0) return kClassGeneric;  // invalid material marker
+    }
+    switch (sc.materials[material].kind) {
+        case kDiffuse: return kClassDiffuse;
+        case kConductor: return kClassConductor;
+        case kDielectric: return kClassDielectric;
+        case kCoatedDiffuse: return kClassCoatedDiffuse;
+        default: return kClassGeneric;
+    }
+}
+
+// Per-entry class plus per-class counts (block-aggregated in shared memory).
+__global__ void ClassifyKernel(DevScene sc, Queues q) {
+    __shared__ unsigned int s_count[kShadeClasses];
+    if (threadIdx.x < kShadeClasses) s_count[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t count = static_cast<int64_t>(q.counters[kCtrIn]);
+    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < count;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int c = ShadeClassOf(sc, q.hits[e]);
+        q.shade_class[e] = static_cast<uint8_t>(c);
+        atomicAdd(&s_count[c], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < kShadeClasses && s_count[threadIdx.x] > 0) {
+        atomicAdd(q.counters + kCtrClass0 + threadIdx.x, static_cast<unsigned long long>(s_count[threadIdx.x]));
+    }
+}
+
+// Writes the entries into `order` grouped by class (class c occupies
+// [sum of the counts of classes < c, + count of c)); order within a class is
+// unspecified, which changes no result: every path's state is indexed by path.
+__global__ void ScatterByClassKernel(Queues q) {
+    __shared__ unsigned long long s_begin[kShadeClasses];
+    __shared__ unsigned int s_count[kShadeClasses];
+    __shared__ unsigned long long s_base[kShadeClasses];
+    if (threadIdx.x == 0) {
+        unsigned long long b = 0;
+        for (int c = 0; c < kShadeClasses; ++c) {
+            s_begin[c] = b;
+            b += q.counters[kCtrClass0 + c];
+        }
+    }
+    const int64_t count = static_cast<int64_t>(q.counters[kCtrIn]);
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t base = blockIdx.x * static_cast<int64_t>(blockDim.x); base < count; base += stride) {
+        if (threadIdx.x < kShadeClasses) s_count[threadIdx.x] = 0;
+        __syncthreads();
+        const int64_t e = base + threadIdx.x;
+        int c = -1;
+        unsigned int local = 0;
+        if (e < count) {
+            c = q.shade_class[e];
+            local = atomicAdd(&s_count[c], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x < kShadeClasses && s_count[threadIdx.x] > 0) {
+            s_base[threadIdx.x] = atomicAdd(q.counters + kCtrCursor0 + threadIdx.x,
+                                            static_cast<unsigned long long>(s_count[threadIdx.x]));
+        }
+        __syncthreads();
+        if (c >= 0) q.order[s_begin[c] + s_base[c] + local] = static_cast<int32_t>(e);
+        __syncthreads();
+    }
 }
 
 // ------------------------------------------------------------------- shade
@@ -357,10 +440,26 @@ __device__ __forceinline__ void PushShadow(Queues& q, V3 o, V3 d, float tmax, in
 
 }  // namespace
 
-__global__ void ShadeKernel(DevScene sc, PathState ps, Queues q, int depth) {
-    const int64_t count = static_cast<int64_t>(q.counters[kCtrIn]);
-    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < count;
-         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+// The material kind a shading class folds to (-1: any kind).
+template <int kClass>
+__device__ constexpr int32_t ClassKind() {
+    return kClass == kClassDiffuse ? kDiffuse
+         : kClass == kClassConductor ? kConductor
+         : kClass == kClassDielectric ? kDielectric
+         : kClass == kClassCoatedDiffuse ? kCoatedDiffuse : -1;
+}
+
+// IntegratePathSample's per-bounce body (src/integrators/path_integrator.cpp:23-197)
+// for the entries of one shading class.
+template <int kClass>
+__global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps, Queues q, int depth) {
+    unsigned long long begin = 0;
+#pragma unroll
+    for (int c = 0; c < kClass; ++c) begin += q.counters[kCtrClass0 + c];
+    const int64_t count = static_cast<int64_t>(q.counters[kCtrClass0 + kClass]);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t e = q.order[begin + i];
         const int32_t path = q.path_in[e];
         const float4 ra = q.ray_in[2 * e], rb = q.ray_in[2 * e + 1];
         const V3 o = F4(ra), d = F4(rb);
@@ -374,7 +473,7 @@ __global__ void ShadeKernel(DevScene sc, PathState ps, Queues q, int depth) {
         CountStat(q.counters, kStatRays);
 
         // --- miss: environment with the BSDF-sampling MIS weight
-        if (id == -1) {
+        if (kClass == kClassMiss || id == -1) {
             CountStat(q.counters, kStatMisses);
             float w = 1.0f;
             if ((flags & kPathPrevValid) && !(flags & kPathPrevDelta)) {
@@ -416,6 +515,7 @@ __global__ void ShadeKernel(DevScene sc, PathState ps, Queues q, int depth) {
         } else {  // default RenderMaterial: diffuse 0.5
             m = Mat{kDiffuse, {0.5f, 0.5f, 0.5f}, 1.5f, 0.0f, 0.0f, 1.5f, 0.01f, {0, 0, 0}, 10, 1};
         }
+        if constexpr (ClassKind<kClass>() >= 0) m.kind = ClassKind<kClass>();  // the class fixes the kind
         const V3 wo = -d;
         if (depth == 0) {
             flags |= kPathPrimary;
@@ -727,7 +827,14 @@ void LaunchResetCounters(const Queues& q, cudaStream_t st) { ResetCountersKernel
 void LaunchAdvanceQueue(const Queues& q, cudaStream_t st) { AdvanceQueueKernel<<<1, 32, 0, st>>>(q); }
 void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity, int sm_count,
                  cudaStream_t st) {
-    ShadeKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
+    ClassifyKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, q);
+    ScatterByClassKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(q);
+    ShadeKernel<kClassMiss><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
+    ShadeKernel<kClassDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
+    ShadeKernel<kClassConductor><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
+    ShadeKernel<kClassDielectric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
+    ShadeKernel<kClassCoatedDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
+    ShadeKernel<kClassGeneric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
 }
 void LaunchNeeResolve(const PathState& ps, const Queues& q, const float4* transmittance, int64_t capacity,
                       int sm_count, cudaStream_t st) {

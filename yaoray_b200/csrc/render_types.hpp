@@ -85,6 +85,8 @@ struct DevScene {
     const float4* spheres;        // center.xyz, radius
     const int32_t* sphere_flip;
     const float* instance_o2w;    // 16 floats per instance (column-major)
+    const uint8_t* tri_clear;     // per flat triangle: 1 if its material passes light (Dielectric / ThinDielectric)
+    const uint8_t* sphere_clear;  // per sphere, likewise
     int32_t primitive_count;
     int32_t sphere_count;
     int32_t instance_count;
@@ -164,7 +166,8 @@ struct Queues {
     int32_t* shadow_slot; // path * 3 + light type
     uint8_t* shadow_occluded;
     int32_t* nee_paths;   // paths with pending NEE
-    int32_t* class_paths[8];  // per material class: entry index into the extend queue
+    int32_t* order;       // extend-queue entries sorted by shading class
+    uint8_t* shade_class; // shading class per extend-queue entry
     unsigned long long* counters;  // see kCounter*
 };
 
@@ -173,11 +176,26 @@ enum CounterIndex {
     kCtrOut = 1,
     kCtrShadow = 2,
     kCtrNee = 3,
-    kCtrClass0 = 4,  // 8 class counters
+    kCtrClass0 = 4,  // entries per shading class (kShadeClasses of them)
     kCtrTrace = 12,  // traversal work counter
     kCtrShadowTrace = 13,
+    kCtrPending = 14,  // shadow rays left for the transmittance pass
     kCtrStatsBase = 16,  // rays, shadow rays, occluded, hits, misses, bad
-    kCtrCount = 24,
+    kCtrCursor0 = 24,  // scatter cursors per shading class
+    kCtrCount = 32,
+};
+
+// Shading classes: the extend queue is sorted by class before shading and
+// each class is shaded by its own kernel instance, whose BSDF dispatch folds
+// to the class's one material kind (coherent warps, fewer registers).
+enum ShadeClass {
+    kClassMiss = 0,
+    kClassDiffuse = 1,       // Diffuse and the default material
+    kClassConductor = 2,
+    kClassDielectric = 3,
+    kClassCoatedDiffuse = 4,
+    kClassGeneric = 5,       // every other kind, and invalid materials
+    kShadeClasses = 6,
 };
 
 }  // namespace yrc

@@ -45,6 +45,7 @@ struct Traversal {
     int32_t cur_inst;   // instance being traversed
     uint32_t nodes, tris, spheres;  // BvhTraceStats
     float wo[3], wd[3];  // world-space ray, restored after a BLAS
+    bool saw;            // filtered any-hit: a surface that passes light was skipped
 };
 
 __device__ __forceinline__ float4 Ld(const float4* p) { return __ldg(p); }
@@ -100,6 +101,7 @@ __device__ __forceinline__ bool BeginRay(const AccelParams& a, const float o[3],
     s.level = 0;
     s.tl_resume = -1;
     s.nodes = s.tris = s.spheres = 0;
+    s.saw = false;
     if (a.root_ref == kAbsentRef) return false;
     s.nodes = 1;
     float entry;
@@ -154,9 +156,14 @@ __device__ __forceinline__ bool Pop(const float4* rays, int64_t ray, Traversal& 
 
 // One traversal step: an interior node (test both children) or a leaf (test
 // its records). Returns false when the ray's traversal is complete.
-template <bool kAny, bool kStats, bool kTwo, typename Stack>
+//
+// kFilter (any-hit only): candidates on surfaces flagged in `tri_clear` /
+// `sphere_clear` are not accepted; the traversal records that it skipped one
+// (s.saw) and goes on, so it ends at the first hit on any other surface.
+template <bool kAny, bool kStats, bool kTwo, typename Stack, bool kFilter = false>
 __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, int64_t ray, Traversal& s, Stack& st,
-                                     int2* col, int* error) {
+                                     int2* col, int* error, const uint8_t* tri_clear = nullptr,
+                                     const uint8_t* sphere_clear = nullptr) {
     const bool in_blas = kTwo && s.level == 1;
     if (s.cur >= 0) {
         const float4* p = reinterpret_cast<const float4*>(a.pairs + s.cur);
@@ -207,29 +214,57 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
             const float4 v2 = Ld(q + 2);
             if (kStats) ++s.tris;
             if (in_blas) {
+                const Nearest keep = s.local;
                 const bool acc = TriangleTest(s.r, v0, v1, v2, s.tmin, s.local);
                 if (kAny && acc && s.local.t < s.best.t) {
-                    s.best = s.local;
-                    s.best_inst = s.cur_inst;
-                    return false;
+                    if (kFilter && tri_clear[s.local.id]) {
+                        s.saw = true;
+                        s.local = keep;
+                    } else {
+                        s.best = s.local;
+                        s.best_inst = s.cur_inst;
+                        return false;
+                    }
                 }
             } else {
+                const Nearest keep = s.best;
                 const bool acc = TriangleTest(s.r, v0, v1, v2, s.tmin, s.best);
-                if (kAny && acc) return false;
+                if (kAny && acc) {
+                    if (kFilter && tri_clear[s.best.id]) {
+                        s.saw = true;
+                        s.best = keep;
+                    } else {
+                        return false;
+                    }
+                }
             }
         } else if (kind == kRecSphere) {
             if (kStats) ++s.spheres;
             if (in_blas) {
+                const Nearest keep = s.local;
                 const bool acc = SphereTest(s.r, v0, v1, s.tmin, s.local);
                 if (kAny && acc && s.local.t < s.best.t) {
-                    s.best = s.local;
-                    s.best_inst = s.cur_inst;
-                    return false;
+                    if (kFilter && sphere_clear[-2 - s.local.id]) {
+                        s.saw = true;
+                        s.local = keep;
+                    } else {
+                        s.best = s.local;
+                        s.best_inst = s.cur_inst;
+                        return false;
+                    }
                 }
             } else {
+                const Nearest keep = s.best;
                 const bool acc = SphereTest(s.r, v0, v1, s.tmin, s.best);
                 if (acc) s.best_inst = -1;
-                if (kAny && acc) return false;
+                if (kAny && acc) {
+                    if (kFilter && sphere_clear[-2 - s.best.id]) {
+                        s.saw = true;
+                        s.best = keep;
+                    } else {
+                        return false;
+                    }
+                }
             }
         } else if (kTwo && kind == kRecInstance) {
             // Descend into the instance's BLAS with the ray in object space
@@ -389,20 +424,88 @@ __global__ void __launch_bounds__(kTraceBlock) ProbeKernel(ProbeArgs args) {
     }
 }
 
+// First pass of TraceShadowVisibility for every shadow ray: an any-hit
+// traversal that does not accept surfaces which pass light. Whatever the
+// order of the surfaces along the segment, the reference's loop ends occluded
+// (zero) as soon as an opaque surface lies on it, and returns full visibility
+// when its first query finds nothing; so a ray that hits an opaque surface
+// gets 0, a ray that met no surface at all gets 1, and only the rest (clear
+// surfaces and no opaque one) go to the pending list for the exact loop.
+// Persistent warps with per-lane refill, like TraceKernel.
+template <bool kTwo, int kTotal>
+__global__ void __launch_bounds__(kTraceBlock) ShadowFilterKernel(ShadowArgs args) {
+    __shared__ int2 s_stack[kShortStack * kTraceBlock];
+    int2* col = s_stack + threadIdx.x;
+    StackStore<kTotal> st;
+    Traversal s;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    int64_t ray = -1;
+    bool alive = false;
+    bool exhausted = false;
+    const unsigned long long count = *args.count_ptr;
+    auto finish = [&]() {
+        const int32_t slot = args.out_index[ray];
+        if (s.best.hit) {
+            args.transmittance[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        } else if (!s.saw) {
+            args.transmittance[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        } else {
+            const unsigned long long k = atomicAdd(args.pending_count, 1ull);
+            args.pending[k] = static_cast<int32_t>(ray);
+        }
+    };
+    for (;;) {
+        const unsigned need = __ballot_sync(kFull, !alive && !exhausted);
+        if (need) {
+            unsigned long long base = 0;
+            const int leader = __ffs(need) - 1;
+            if (static_cast<int>(lane) == leader) {
+                base = atomicAdd(args.counter, static_cast<unsigned long long>(__popc(need)));
+            }
+            base = __shfl_sync(kFull, base, leader);
+            if (!alive && !exhausted) {
+                const unsigned long long idx = base + __popc(need & lt_mask);
+                if (idx >= count) {
+                    exhausted = true;
+                } else {
+                    ray = static_cast<int64_t>(idx);
+                    const float4 b = Ld(args.rays + 2 * ray + 1);
+                    const float tmin = Ld(args.rays + 2 * ray).w;
+                    alive = Begin(args.accel, args.rays, ray, tmin, b.w, s);
+                    if (!alive) finish();
+                }
+            }
+        }
+        if (!__any_sync(kFull, alive)) {
+            if (__all_sync(kFull, exhausted)) break;
+            continue;
+        }
+#pragma unroll 1
+        for (int k = 0; k < 8 && alive; ++k) {
+            alive = Step<true, false, kTwo, StackStore<kTotal>, true>(args.accel, args.rays, ray, s, st, col,
+                                                                     args.error, args.tri_clear, args.sphere_clear);
+            if (!alive) finish();
+        }
+    }
+}
+
 // TraceShadowVisibility (src/integrators/path_direct_lighting.cpp:23-113):
 // up to 16 closest-hit queries along the shadow segment; Dielectric surfaces
 // toggle a Beer-Lambert medium, ThinDielectric ones multiply by their clamped
-// reflectance, anything else occludes. One thread per shadow ray; writes the
-// RGB transmittance (0 when occluded) to transmittance[out_index[i]].
+// reflectance, anything else occludes. One thread per shadow ray of the
+// pending list (the rays ShadowFilterKernel could not settle); writes the RGB
+// transmittance (0 when occluded) to transmittance[out_index[i]].
 template <bool kTwo, int kTotal>
 __global__ void __launch_bounds__(kTraceBlock) ShadowTransmittanceKernel(ShadowArgs args) {
     __shared__ int2 s_stack[kShortStack * kTraceBlock];
     int2* col = s_stack + threadIdx.x;
     StackStore<kTotal> st;
     Traversal s;
-    const int64_t count = static_cast<int64_t>(*args.count_ptr);
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t count = static_cast<int64_t>(*args.pending_count);
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < count;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t i = args.pending[k];
         const float4 ra = Ld(args.rays + 2 * i);
         const float4 rb = Ld(args.rays + 2 * i + 1);
         float o[3] = {ra.x, ra.y, ra.z};
@@ -543,11 +646,15 @@ cudaError_t LaunchProbeOne(const ProbeArgs& args, cudaStream_t stream, int sm_co
 
 template <bool kTwo, int kTotal>
 cudaError_t LaunchShadowOne(const ShadowArgs& args, cudaStream_t stream, int sm_count) {
-    auto kernel = ShadowTransmittanceKernel<kTwo, kTotal>;
+    auto filter = ShadowFilterKernel<kTwo, kTotal>;
     int64_t blocks = 0;
-    const cudaError_t err = PersistentGrid(kernel, kTraceBlock, args.capacity, sm_count, blocks);
+    cudaError_t err = PersistentGrid(filter, kTraceBlock, args.capacity, sm_count, blocks);
     if (err != cudaSuccess) return err;
-    kernel<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
+    filter<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
+    auto exact = ShadowTransmittanceKernel<kTwo, kTotal>;
+    err = PersistentGrid(exact, kTraceBlock, args.capacity, sm_count, blocks);
+    if (err != cudaSuccess) return err;
+    exact<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
     return cudaGetLastError();
 }
 

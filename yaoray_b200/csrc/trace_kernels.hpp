@@ -64,6 +64,11 @@ struct ShadowArgs {
     const int32_t* prim_material;
     const int32_t* sphere_material;
     const DevMaterial* materials;
+    const uint8_t* tri_clear;             // per flat triangle: passes light (1) or occludes (0)
+    const uint8_t* sphere_clear;          // per sphere
+    int32_t* pending;                     // capacity entries: rays left for the transmittance pass
+    unsigned long long* pending_count;    // zeroed before the launch
+    unsigned long long* counter;          // ray work counter of the filtered any-hit pass, zeroed before
     int* error;
 };
 
