@@ -65,8 +65,10 @@ def test_cornell_matches_reference_cpu(cuda, cornell_job):
     for k in ("albedo_sum", "normal_sum", "depth_sum"):
         assert res.film[k].tobytes() == cpu_film[k].tobytes(), k
     assert res.bad_samples == 0
-    # same path-segment accounting within sampling divergence
+    # same path-segment and shadow-ray accounting within sampling divergence
     assert abs(res.stats["rays_traced"] / cpu_stats["rays_traced"] - 1) < 0.02
+    assert abs(res.stats["shadow_rays"] / cpu_stats["shadow_rays"] - 1) < 0.02
+    assert abs(res.stats["occluded_shadow_rays"] / cpu_stats["occluded_shadow_rays"] - 1) < 0.03
 
 
 def test_depth_one_stats_contract(cuda, cornell_job):
@@ -168,3 +170,5 @@ def test_instanced_scene_matches_reference_cpu(cuda, ref):
         assert res.film[k].tobytes() == cpu_film[k].tobytes(), k
     assert res.bad_samples == 0
     assert abs(res.stats["rays_traced"] / cpu_stats["rays_traced"] - 1) < 0.02
+    assert abs(res.stats["shadow_rays"] / cpu_stats["shadow_rays"] - 1) < 0.02
+    assert abs(res.stats["occluded_shadow_rays"] / cpu_stats["occluded_shadow_rays"] - 1) < 0.03

@@ -512,6 +512,8 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
             sa.pending = s->shadow_pending;
             sa.pending_count = q.counters + kCtrPending;
             sa.counter = q.counters + kCtrShadowTrace;
+            sa.exact_counter = q.counters + kCtrExact;
+            sa.occluded_count = q.counters + kCtrStatsBase + 2;
             sa.error = ta.error;
             err = LaunchShadowTransmittance(sa, st, s->sm_count);
         } else {
@@ -523,6 +525,7 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
             sh.occluded = q.shadow_occluded;
             sh.out_index = q.shadow_slot;
             sh.counter = q.counters + kCtrShadowTrace;
+            sh.occluded_count = q.counters + kCtrStatsBase + 2;
             sh.error = ta.error;
             err = LaunchTrace(sh, true, false, TraceShapeOf(s->accel, 1), st, s->sm_count);
         }

@@ -117,6 +117,7 @@ __global__ void ResetCountersKernel(Queues q) {
         q.counters[kCtrTrace] = 0;
         q.counters[kCtrShadowTrace] = 0;
         q.counters[kCtrPending] = 0;
+        q.counters[kCtrExact] = 0;
         for (int c = 0; c < kShadeClasses; ++c) {
             q.counters[kCtrClass0 + c] = 0;
             q.counters[kCtrCursor0 + c] = 0;

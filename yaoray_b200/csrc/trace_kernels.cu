@@ -50,6 +50,14 @@ struct Traversal {
 
 __device__ __forceinline__ float4 Ld(const float4* p) { return __ldg(p); }
 
+// Warp-aggregated increment of a statistics counter by the calling lanes.
+__device__ __forceinline__ void CountLanes(unsigned long long* counter) {
+    const unsigned mask = __activemask();
+    if ((threadIdx.x & 31u) == static_cast<unsigned>(__ffs(mask) - 1)) {
+        atomicAdd(counter, static_cast<unsigned long long>(__popc(mask)));
+    }
+}
+
 // Traversal stack of kTotal entries per thread: the first kShortStack in the
 // block's shared memory (column `col`, stride kBlock), the rest local.
 template <int kTotal, int kBlock = kTraceBlock>
@@ -319,6 +327,7 @@ template <bool kAny, bool kStats>
 __device__ __forceinline__ void WriteResult(const TraceArgs& args, int64_t ray, const Traversal& s) {
     if (kAny) {
         args.occluded[args.out_index ? args.out_index[ray] : ray] = s.best.hit ? 1 : 0;
+        if (args.occluded_count && s.best.hit) CountLanes(args.occluded_count);
     } else {
         reinterpret_cast<float4*>(args.hits)[ray] =
             make_float4(s.best.t, __int_as_float(s.best.hit ? s.best.id : -1), s.best.u, s.best.v);
@@ -448,6 +457,7 @@ __global__ void __launch_bounds__(kTraceBlock) ShadowFilterKernel(ShadowArgs arg
         const int32_t slot = args.out_index[ray];
         if (s.best.hit) {
             args.transmittance[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            CountLanes(args.occluded_count);
         } else if (!s.saw) {
             args.transmittance[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
         } else {
@@ -502,66 +512,79 @@ __global__ void __launch_bounds__(kTraceBlock) ShadowTransmittanceKernel(ShadowA
     int2* col = s_stack + threadIdx.x;
     StackStore<kTotal> st;
     Traversal s;
-    const int64_t count = static_cast<int64_t>(*args.pending_count);
-    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < count;
-         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t i = args.pending[k];
-        const float4 ra = Ld(args.rays + 2 * i);
-        const float4 rb = Ld(args.rays + 2 * i + 1);
-        float o[3] = {ra.x, ra.y, ra.z};
-        const float d[3] = {rb.x, rb.y, rb.z};
-        float remaining = rb.w;
-        float T[3] = {1.0f, 1.0f, 1.0f};
-        bool medium = false;
-        float mc[3] = {1.0f, 1.0f, 1.0f};
-        float md = 1.0f;
-        bool visible = false;
-        auto beer = [&](float dist) {
-            if (dist <= 0.0f || md <= 0.0f) return;
-            const float inv = 1.0f / md;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const unsigned long long count = *args.pending_count;
+    // Per-lane loop state of the reference's query loop; a lane that finishes
+    // its ray takes the next pending one (persistent warps, per-lane refill).
+    int64_t i = -1;
+    float o[3], d[3], remaining = 0.0f, T[3], mc[3], md = 1.0f;
+    bool medium = false;
+    int hitc = 0;
+    bool active = false, alive = false, exhausted = false;
+    auto black = [&]() { return fmaxf(T[0], fmaxf(T[1], T[2])) <= 1.0e-6f; };
+    auto beer = [&](float dist) {
+        if (dist <= 0.0f || md <= 0.0f) return;
+        const float inv = 1.0f / md;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const float c = fminf(fmaxf(mc[k], 1.0e-6f), 1.0f);
-                T[k] = T[k] * expf(logf(c) * dist * inv);
-            }
-        };
-        auto black = [&]() { return fmaxf(T[0], fmaxf(T[1], T[2])) <= 1.0e-6f; };
-        for (int hitc = 0; hitc < 16; ++hitc) {
-            bool alive = BeginRay(args.accel, o, d, 1.0e-5f, remaining, s);
-            while (alive) alive = Step<false, false, kTwo>(args.accel, args.rays, i, s, st, col, args.error);
+        for (int k = 0; k < 3; ++k) {
+            const float c = fminf(fmaxf(mc[k], 1.0e-6f), 1.0f);
+            T[k] = T[k] * expf(logf(c) * dist * inv);
+        }
+    };
+    auto write = [&](bool visible) {
+        args.transmittance[args.out_index[i]] =
+            visible ? make_float4(T[0], T[1], T[2], 1.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (!visible) CountLanes(args.occluded_count);
+        active = false;
+    };
+    // The loop body after one closest-hit query; returns true when the next
+    // query's traversal started, false when the ray's result was written.
+    auto resolve = [&]() -> bool {
+        for (;;) {
             const bool finite = isfinite(remaining);
             if (!s.best.hit) {
                 if (medium) {
-                    if (!finite) break;  // occluded
+                    if (!finite) {  // occluded
+                        write(false);
+                        return false;
+                    }
                     beer(remaining);
                 }
-                visible = !black();
-                break;
+                write(!black());
+                return false;
             }
             const float t = s.best.t;
             if (medium) {
                 beer(t);
-                if (black()) break;
+                if (black()) {
+                    write(false);
+                    return false;
+                }
             }
             int32_t material = -1;
-            bool valid_material = true;
             if (s.best.id >= 0) {
-                const int32_t prim = args.tri_prim[s.best.id];
-                material = args.prim_material[prim];
-                valid_material = material >= 0;
+                material = args.prim_material[args.tri_prim[s.best.id]];
             } else {
                 material = args.sphere_material[-2 - s.best.id];
             }
-            if (!valid_material || material < 0) break;  // invalid or default (opaque diffuse) material
+            // Invalid or default (opaque diffuse) material, or a kind other
+            // than Dielectric / ThinDielectric: occluded.
+            if (material < 0 || (args.materials[material].kind != 2 && args.materials[material].kind != 3)) {
+                write(false);
+                return false;
+            }
             const DevMaterial& m = args.materials[material];
-            if (m.kind != 2 && m.kind != 3) break;  // only Dielectric / ThinDielectric pass light
             float hp[3];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) hp[k] = o[k] + d[k] * t;
+            for (int k = 0; k < 3; ++k) hp[k] = __fadd_rn(o[k], __fmul_rn(d[k], t));
             if (m.kind == 3) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) T[k] = T[k] * fminf(fmaxf(m.reflectance[k], 0.0f), 1.0f);
-                if (black()) break;
+                if (black()) {
+                    write(false);
+                    return false;
+                }
             } else if (medium) {
                 medium = false;
                 mc[0] = mc[1] = mc[2] = 1.0f;
@@ -575,18 +598,61 @@ __global__ void __launch_bounds__(kTraceBlock) ShadowTransmittanceKernel(ShadowA
             }
             const float bias = fmaxf(1.0e-4f, fmaxf(fabsf(hp[0]), fmaxf(fabsf(hp[1]), fabsf(hp[2]))) * 1.0e-5f);
             if (finite) {
-                remaining -= t + bias;
+                remaining = __fsub_rn(remaining, __fadd_rn(t, bias));
                 if (remaining <= 0.0f) {
-                    visible = !black();
-                    break;
+                    write(!black());
+                    return false;
                 }
             }
 #pragma unroll
-            for (int k = 0; k < 3; ++k) o[k] = hp[k] + d[k] * bias;
+            for (int k = 0; k < 3; ++k) o[k] = __fadd_rn(hp[k], __fmul_rn(d[k], bias));
+            if (++hitc >= 16) {  // the reference gives up after 16 queries: occluded
+                write(false);
+                return false;
+            }
+            if (BeginRay(args.accel, o, d, 1.0e-5f, remaining, s)) return true;
         }
-        const int32_t slot = args.out_index[i];
-        args.transmittance[slot] =
-            visible ? make_float4(T[0], T[1], T[2], 1.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    };
+    for (;;) {
+        const unsigned need = __ballot_sync(kFull, !active && !exhausted);
+        if (need) {
+            unsigned long long base = 0;
+            const int leader = __ffs(need) - 1;
+            if (static_cast<int>(lane) == leader) {
+                base = atomicAdd(args.exact_counter, static_cast<unsigned long long>(__popc(need)));
+            }
+            base = __shfl_sync(kFull, base, leader);
+            if (!active && !exhausted) {
+                const unsigned long long idx = base + __popc(need & lt_mask);
+                if (idx >= count) {
+                    exhausted = true;
+                } else {
+                    i = args.pending[idx];
+                    const float4 ra = Ld(args.rays + 2 * i);
+                    const float4 rb = Ld(args.rays + 2 * i + 1);
+                    o[0] = ra.x, o[1] = ra.y, o[2] = ra.z;
+                    d[0] = rb.x, d[1] = rb.y, d[2] = rb.z;
+                    remaining = rb.w;
+                    T[0] = T[1] = T[2] = 1.0f;
+                    mc[0] = mc[1] = mc[2] = 1.0f;
+                    md = 1.0f;
+                    medium = false;
+                    hitc = 0;
+                    active = true;
+                    alive = BeginRay(args.accel, o, d, 1.0e-5f, remaining, s);
+                    if (!alive) alive = resolve();
+                }
+            }
+        }
+        if (!__any_sync(kFull, alive)) {
+            if (__all_sync(kFull, exhausted)) break;
+            continue;
+        }
+#pragma unroll 1
+        for (int k = 0; k < 8 && alive; ++k) {
+            alive = Step<false, false, kTwo>(args.accel, args.rays, i, s, st, col, args.error);
+            if (!alive) alive = resolve();
+        }
     }
 }
 

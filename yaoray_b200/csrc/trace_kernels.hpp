@@ -32,6 +32,7 @@ struct TraceArgs {
     int* error;                   // device error word
     const unsigned long long* count_ptr;  // optional: ray count read on the device (count = capacity)
     const int32_t* out_index;             // optional: any-hit output slot per ray
+    unsigned long long* occluded_count;   // optional: any-hit rays that hit something (RenderStats)
 };
 
 constexpr int kProbeMaxHits = YRC_PROBE_MAX_HITS;  // BvhProbeHits::MaxHits
@@ -69,6 +70,8 @@ struct ShadowArgs {
     int32_t* pending;                     // capacity entries: rays left for the transmittance pass
     unsigned long long* pending_count;    // zeroed before the launch
     unsigned long long* counter;          // ray work counter of the filtered any-hit pass, zeroed before
+    unsigned long long* exact_counter;    // ray work counter of the transmittance pass, zeroed before
+    unsigned long long* occluded_count;   // shadow rays found not visible (RenderStats::occluded_shadow_rays)
     int* error;
 };
 
