@@ -614,6 +614,53 @@ yrc_status yrc_render(yrc_render_scene* scene, const yrc_render_request* request
 /* Wait for all work the library queued on `stream` (NULL = legacy default). */
 yrc_status yrc_stream_synchronize(void* stream);
 
+/* ------------------------------------------------------------------------
+ * Neural radiance cache. No counterpart in the reference (its renderer has
+ * no learned component): a multiresolution hash grid over the scene box
+ * (16 levels x 2 fp16 features, 2^19 entries per level, resolutions 16 to
+ * 2048) plus degree-0..3 spherical harmonics of the view direction and the
+ * surface attributes, into a 64-wide MLP (5 hidden ReLU layers, exp RGB
+ * output) run on the tensor cores in bf16 with fp32 accumulation, trained
+ * with a relative-L2 loss and Adam (lr 1e-2, betas 0.9 / 0.99).
+ *
+ * A query is 16 floats: position[3], roughness, direction[3] (unit, away
+ * from the surface towards the viewer of the cached radiance), normal[3],
+ * diffuse albedo[3], specular albedo[3]. Targets and outputs are float4 RGB
+ * (w unused). Query, target and output arrays are device memory.
+ * ---------------------------------------------------------------------- */
+typedef struct yrc_nrc yrc_nrc;
+
+#define YRC_NRC_QUERY_FLOATS 16
+#define YRC_NRC_WEIGHT_COUNT (6 * 64 * 64) /* 6 matrices [out][in]; output rows 3..63 zero */
+#define YRC_NRC_GRID_COUNT (16 * 524288 * 2)
+
+/* Creates a cache on the current device for positions in the cube
+ * [box_lo, box_lo + box_extent]^3; weights and grid from `seed`. */
+yrc_status yrc_nrc_create(const float box_lo[3], float box_extent, uint64_t seed, yrc_nrc** out);
+void yrc_nrc_destroy(yrc_nrc* cache);
+
+/* Host copies of the fp32 master parameters (either pointer may be NULL). */
+yrc_status yrc_nrc_set_params(yrc_nrc* cache, const float* weights, const float* grid);
+yrc_status yrc_nrc_get_params(yrc_nrc* cache, float* weights_out, float* grid_out);
+
+/* rgb[i] = cache(queries[i]) for n queries, asynchronous on `stream`. */
+yrc_status yrc_nrc_infer(yrc_nrc* cache, const float* queries, int64_t n, float* rgb, void* stream);
+
+/* One optimiser step on n (query, target) pairs, asynchronous on `stream`;
+ * `loss_out` (device float, optional) receives the sum of per-sample losses
+ * (divide by 3n for the mean). */
+yrc_status yrc_nrc_train_step(yrc_nrc* cache, const float* queries, const float* targets, int64_t n,
+                              float* loss_out, void* stream);
+
+/* Gradients of the mean loss over n pairs without an optimiser step
+ * (synchronous; host outputs, each optional): YRC_NRC_WEIGHT_COUNT and
+ * YRC_NRC_GRID_COUNT floats, and the mean loss. */
+yrc_status yrc_nrc_gradients(yrc_nrc* cache, const float* queries, const float* targets, int64_t n,
+                             float* weight_grads, float* grid_grads, float* loss);
+
+/* Synchronises and reports a tensor-core wait that timed out. */
+yrc_status yrc_nrc_check(yrc_nrc* cache);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -28,6 +28,9 @@ YRC_TRACE_ANY = 1
 YRC_TRACE_STATS = 2
 YRC_PROBE_MAX_HITS = 64
 YRC_NOALLOC_STATS_MAX_RAYS = 262144
+YRC_NRC_QUERY_FLOATS = 16
+YRC_NRC_WEIGHT_COUNT = 6 * 64 * 64
+YRC_NRC_GRID_COUNT = 16 * 524288 * 2
 
 STATUS_NAMES = {
     0: "ok",
@@ -179,6 +182,14 @@ def lib() -> C.CDLL:
         "yrc_accel_set_trace_shape": (C.c_int, [P, I32, I32]),
         "yrc_accel_get_trace_shape": (I32, [P, I32]),
         "yrc_stream_synchronize": (C.c_int, [P]),
+        "yrc_nrc_create": (C.c_int, [P, C.c_float, C.c_uint64, P]),
+        "yrc_nrc_destroy": (None, [P]),
+        "yrc_nrc_set_params": (C.c_int, [P, P, P]),
+        "yrc_nrc_get_params": (C.c_int, [P, P, P]),
+        "yrc_nrc_infer": (C.c_int, [P, P, I64, P, P]),
+        "yrc_nrc_train_step": (C.c_int, [P, P, P, I64, P, P]),
+        "yrc_nrc_gradients": (C.c_int, [P, P, P, I64, P, P, P]),
+        "yrc_nrc_check": (C.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
