@@ -430,9 +430,110 @@ def run_render(args):
     print(json.dumps(line), flush=True)
 
 
+def run_nrc(args):
+    """--workload nrc: equal-relMSE time of the neural-cached path tracer
+    against the plain one on the instanced scene (960x540, max depth 16,
+    radiance clamp 20 for every render so that the reference's rare
+    numerically extreme samples do not dominate the error).
+
+    Reference: `--ref-spp` samples per pixel of the plain tracer, accumulated
+    in FP64 over renders of different seeds. Plain curve: renders of 1..64
+    spp. Cached renders: a fresh cache trained online by 8 renders of 2 spp
+    (4 optimiser steps per batch; its time is reported separately), then
+    renders of 1, 4 and 16 spp that keep training (1 step per batch). Every
+    timing is the device time of the second render of a prepared scene (the
+    first captures the batch graph). For each cached render, the time the
+    plain tracer needs for the same relMSE is interpolated on its log-log
+    time/error curve; value = that time / the cached render's time at 16 spp."""
+    import torch
+    from yaoray_b200 import instanced
+    from yaoray_b200.nrc import RadianceCache
+    from yaoray_b200.render import CudaBackend
+
+    W, H, CLAMP, C_SPREAD = args.nrc_width, args.nrc_height, 20.0, 0.001
+
+    def scene(spp, seed):
+        s = instanced.scene(width=W, height=H, spp=spp)
+        s.radiance_clamp = CLAMP
+        s.seed = seed
+        return s
+
+    def relmse(img, ref):
+        return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    backend = CudaBackend()
+    base = scene(1, 0)
+    lo = base.geometry.positions.min(0)
+    extent = float((base.geometry.positions.max(0) - lo).max())
+    ref = np.zeros((H, W, 3), np.float64)
+    per = 128
+    for k in range(max(1, args.ref_spp // per)):
+        p = backend.prepare(scene(per, 1000 + k))
+        ref += backend.render(p).linear()
+        p.close()
+    ref /= max(1, args.ref_spp // per)
+
+    def timed(prep):
+        backend.render(prep)  # graph capture
+        torch.cuda.synchronize()
+        r = backend.render(prep)
+        return r.linear(), r.stats
+
+    plain = []
+    for spp in (1, 2, 4, 8, 16, 32, 64):
+        p = backend.prepare(scene(spp, 7))
+        img, st = timed(p)
+        plain.append((spp, relmse(img, ref), st["device_seconds"]))
+        p.close()
+    cache = RadianceCache(lo, extent, seed=1)
+    warm = backend.prepare(scene(2, 99))
+    warm.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=4)
+    warm_s = sum(backend.render(warm).stats["device_seconds"] for _ in range(8))
+    warm.close()
+    cached = []
+    with ClockSampler(0) as clocks:
+        for spp in (1, 4, 16):
+            p = backend.prepare(scene(spp, 7))
+            p.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=1)
+            img, st = timed(p)
+            cached.append((spp, relmse(img, ref), st["device_seconds"], st["cache_queries"], st["rays_traced"]))
+            p.close()
+    cache.check()
+    cache.close()
+
+    def plain_time_for(err):
+        pts = sorted(plain, key=lambda x: -x[1])  # decreasing error
+        for (s0, e0, t0), (s1, e1, t1) in zip(pts, pts[1:]):
+            if e1 <= err <= e0:
+                f = (np.log(err) - np.log(e0)) / (np.log(e1) - np.log(e0))
+                return float(np.exp(np.log(t0) + f * (np.log(t1) - np.log(t0))))
+        # beyond the curve: extrapolate with relMSE ~ 1/time from the last point
+        s1, e1, t1 = pts[-1]
+        return float(t1 * e1 / err)
+
+    ratios = {spp: plain_time_for(e) / t for spp, e, t, _, _ in cached}
+    line = {"metric": "equal-relMSE time ratio, plain / neural-cached (instanced scene)",
+            "value": round(ratios[16], 3), "unit": "x", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": round(cached[-1][2] * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 render, bf16 MLP", "data": "synthetic",
+            "config": {"workload": f"instanced-{W}x{H}-depth16-clamp20", "reference_spp": args.ref_spp,
+                       "reference_accumulation": "fp64", "spread_threshold": C_SPREAD,
+                       "cache": "16x2^19x2 hash grid + SH4, 64x5 MLP, bf16 tcgen05, Adam 1e-2",
+                       "cache_warmup_ms": round(warm_s * 1e3, 2)},
+            "plain": [{"spp": s_, "relmse": round(e, 5), "ms": round(t * 1e3, 3)} for s_, e, t in plain],
+            "cached": [{"spp": s_, "relmse": round(e, 5), "ms": round(t * 1e3, 3), "cache_queries": q,
+                        "path_segments": n, "equal_relmse_ratio": round(ratios[s_], 3)}
+                       for s_, e, t, q, n in cached],
+            "e2e": None, "cpu_baseline": None, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--workload", choices=["traversal", "cornell", "instanced"], default="traversal")
+    ap.add_argument("--workload", choices=["traversal", "cornell", "instanced", "nrc"], default="traversal")
+    ap.add_argument("--nrc-width", type=int, default=960)
+    ap.add_argument("--nrc-height", type=int, default=540)
+    ap.add_argument("--ref-spp", type=int, default=512)
     ap.add_argument("--render-spp", type=int, default=16, help="spp per step of --workload instanced")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -449,6 +550,8 @@ def main():
         run_reference(args)
     elif args.workload in RENDER_WORKLOADS:
         run_render(args)
+    elif args.workload == "nrc":
+        run_nrc(args)
     else:
         run_gpu(args)
 

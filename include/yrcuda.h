@@ -576,6 +576,8 @@ typedef struct yrc_render_stats {
     int32_t threads;
     double elapsed_seconds;
     double device_seconds;
+    uint64_t cache_queries;    /* paths ended at the radiance cache (0 without one) */
+    uint64_t cache_records;    /* training records fed to the cache */
 } yrc_render_stats;
 
 /*
@@ -660,6 +662,22 @@ yrc_status yrc_nrc_gradients(yrc_nrc* cache, const float* queries, const float* 
 
 /* Synchronises and reports a tensor-core wait that timed out. */
 yrc_status yrc_nrc_check(yrc_nrc* cache);
+
+/* How the path tracer uses an attached radiance cache. */
+typedef struct yrc_cache_settings {
+    float spread_threshold; /* end a path once its spread exceeds this x its primary footprint (0.01) */
+    int32_t train_one_in;   /* 1 in this many paths runs unbiased and trains the cache (16) */
+    int32_t train_records;  /* training records per batch (65536) */
+    int32_t train;          /* 0 freezes the cache (inference only) */
+    int32_t train_steps;    /* optimiser steps per batch on that batch's records (1) */
+} yrc_cache_settings;
+
+/* Attaches `cache` (NULL detaches) to a prepared scene: subsequent
+ * yrc_render calls end paths at the cache when the footprint heuristic fires
+ * and, unless frozen, train it on the unbiased training paths once per
+ * batch. No counterpart in the reference. The cache must outlive the
+ * attachment. */
+yrc_status yrc_render_scene_set_cache(yrc_render_scene* scene, yrc_nrc* cache, const yrc_cache_settings* settings);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -252,8 +252,11 @@ __device__ __forceinline__ float ExpOut(float o) { return expf(fminf(o, kOClamp)
 // ----------------------------------------------------------- inference
 
 __global__ void __launch_bounds__(kThreads) CacheInferKernel(GridArgs g, const __nv_bfloat16* weights,
-                                                            const float* queries, int64_t n, float4* out,
+                                                            const float* queries, int64_t n_max,
+                                                            const unsigned long long* n_ptr, float4* out,
                                                             int* error) {
+    // The query count: n_max, or min(*n_ptr, n_max) when it lives on the device.
+    const int64_t n = n_ptr ? static_cast<int64_t>(min(*n_ptr, static_cast<unsigned long long>(n_max))) : n_max;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sw = smem + kOffW;
     uint8_t* sa = smem + kOffA;
@@ -317,8 +320,10 @@ __global__ void __launch_bounds__(kThreads) CacheInferKernel(GridArgs g, const _
 
 __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const __nv_bfloat16* weights,
                                                             float* weight_grad, const float* queries,
-                                                            const float4* targets, int64_t n, float* loss_sum,
+                                                            const float4* targets, int64_t n_max,
+                                                            const unsigned long long* n_ptr, float* loss_sum,
                                                             int* error) {
+    const int64_t n = n_ptr ? static_cast<int64_t>(min(*n_ptr, static_cast<unsigned long long>(n_max))) : n_max;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sw = smem + kOffW;
     uint8_t* sa = smem + kOffA;  // a_0 .. a_5
@@ -340,7 +345,7 @@ __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const _
     uint32_t phase = 0;
     const int r = threadIdx.x;
     const int64_t tiles = (n + kTile - 1) / kTile;
-    const float inv3n = 1.0f / (3.0f * static_cast<float>(n));
+    const float inv3n = n > 0 ? 1.0f / (3.0f * static_cast<float>(n)) : 0.0f;
     float my_loss = 0.0f;
     bool first = true, ok = true;
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
@@ -477,11 +482,14 @@ __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const _
 
 // ---------------------------------------------------------------- Adam
 
-// One Adam step with bias correction (c1 = 1 - beta1^t, c2 = 1 - beta2^t),
-// in the operation order of the oracle; `half_out` / `bf16_out` receive the
+// One Adam step with bias correction (c1 = 1 - beta1^t, c2 = 1 - beta2^t,
+// t read from the device so that a captured graph replays correctly), in
+// the operation order of the oracle; `half_out` / `bf16_out` receive the
 // rounded copy read by the kernels.
-__global__ void AdamKernel(float* p, float* m, float* v, const float* grad, int64_t count, float c1, float c2,
+__global__ void AdamKernel(float* p, float* m, float* v, const float* grad, int64_t count, const int64_t* step,
                            __half* half_out, __nv_bfloat16* bf16_out) {
+    const float c1 = static_cast<float>(1.0 - pow(kBeta1, static_cast<double>(*step)));
+    const float c2 = static_cast<float>(1.0 - pow(kBeta2, static_cast<double>(*step)));
     const float b1 = static_cast<float>(kBeta1), b2 = static_cast<float>(kBeta2);
     const float nb1 = static_cast<float>(1.0 - kBeta1), nb2 = static_cast<float>(1.0 - kBeta2);
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
@@ -500,6 +508,8 @@ __global__ void AdamKernel(float* p, float* m, float* v, const float* grad, int6
         if (bf16_out) bf16_out[i] = __float2bfloat16_rn(pi);
     }
 }
+
+__global__ void StepKernel(int64_t* step) { ++*step; }
 
 __global__ void RoundKernel(const float* p, int64_t count, __half* half_out, __nv_bfloat16* bf16_out) {
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
@@ -543,7 +553,7 @@ struct yrc_nrc {
     float* w_grad = nullptr;
     float* loss = nullptr;  // device scalar (sum of per-sample losses)
     int* error = nullptr;
-    int64_t step = 0;
+    int64_t* step = nullptr;  // device: optimiser steps taken
     std::mutex mutex;
 };
 
@@ -565,11 +575,13 @@ unsigned Blocks(int64_t count, int sm_count) {
 
 void FreeAll(yrc_nrc* c) {
     void* ptrs[] = {c->table, c->table_master, c->table_m, c->table_v, c->table_grad, c->w, c->w_master,
-                    c->w_m,   c->w_v,          c->w_grad,  c->loss,    c->error};
+                    c->w_m,   c->w_v,          c->w_grad,  c->loss,    c->error, c->step};
     for (void* p : ptrs) cudaFree(p);
 }
 
-yrc_status LaunchTrain(yrc_nrc* c, const float* queries, const float* targets, int64_t n, cudaStream_t st) {
+// Gradients of n pairs (n_ptr: the count on the device, at most n).
+yrc_status LaunchTrain(yrc_nrc* c, const float* queries, const float* targets, int64_t n,
+                       const unsigned long long* n_ptr, cudaStream_t st) {
     cudaError_t err = cudaMemsetAsync(c->table_grad, 0, sizeof(float) * kGridParams, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(c->w_grad, 0, sizeof(float) * kWeightCount, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(c->loss, 0, sizeof(float), st);
@@ -580,20 +592,18 @@ yrc_status LaunchTrain(yrc_nrc* c, const float* queries, const float* targets, i
     const int64_t tiles = (n + kTile - 1) / kTile;
     const int64_t blocks = tiles < c->sm_count ? tiles : c->sm_count;  // one CTA per SM (TMEM, smem)
     CacheTrainKernel<<<static_cast<unsigned>(blocks), kThreads, kTrainSmem, st>>>(
-        g, c->w, c->w_grad, queries, reinterpret_cast<const float4*>(targets), n, c->loss, c->error);
+        g, c->w, c->w_grad, queries, reinterpret_cast<const float4*>(targets), n, n_ptr, c->loss, c->error);
     err = cudaGetLastError();
     if (err != cudaSuccess) return CudaFailN(err, "training launch");
     return Ok();
 }
 
 yrc_status LaunchAdam(yrc_nrc* c, cudaStream_t st) {
-    ++c->step;
-    const float c1 = static_cast<float>(1.0 - std::pow(kBeta1, static_cast<double>(c->step)));
-    const float c2 = static_cast<float>(1.0 - std::pow(kBeta2, static_cast<double>(c->step)));
+    StepKernel<<<1, 1, 0, st>>>(c->step);
     AdamKernel<<<Blocks(kWeightCount, c->sm_count), 256, 0, st>>>(c->w_master, c->w_m, c->w_v, c->w_grad,
-                                                                  kWeightCount, c1, c2, nullptr, c->w);
+                                                                  kWeightCount, c->step, nullptr, c->w);
     AdamKernel<<<Blocks(kGridParams, c->sm_count), 256, 0, st>>>(c->table_master, c->table_m, c->table_v,
-                                                                 c->table_grad, kGridParams, c1, c2, c->table,
+                                                                 c->table_grad, kGridParams, c->step, c->table,
                                                                  nullptr);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return CudaFailN(err, "optimiser launch");
@@ -613,7 +623,8 @@ yrc_status CheckError(yrc_nrc* c) {
 
 }  // namespace
 
-yrc_status Infer(yrc_nrc* c, const float* queries, int64_t n, float* rgb, cudaStream_t st) {
+yrc_status Infer(yrc_nrc* c, const float* queries, int64_t n, const unsigned long long* n_ptr, float* rgb,
+                 cudaStream_t st) {
     if (n <= 0) return Ok();
     const int64_t tiles = (n + kTile - 1) / kTile;
     int per_sm = 0;
@@ -623,14 +634,15 @@ yrc_status Infer(yrc_nrc* c, const float* queries, int64_t n, float* rgb, cudaSt
     const int64_t cap = static_cast<int64_t>(per_sm) * c->sm_count;
     const int64_t blocks = tiles < cap ? tiles : cap;
     CacheInferKernel<<<static_cast<unsigned>(blocks), kThreads, kInferSmem, st>>>(
-        c->grid, c->w, queries, n, reinterpret_cast<float4*>(rgb), c->error);
+        c->grid, c->w, queries, n, n_ptr, reinterpret_cast<float4*>(rgb), c->error);
     err = cudaGetLastError();
     if (err != cudaSuccess) return CudaFailN(err, "inference launch");
     return Ok();
 }
 
-yrc_status TrainStep(yrc_nrc* c, const float* queries, const float* targets, int64_t n, cudaStream_t st) {
-    yrc_status s = LaunchTrain(c, queries, targets, n, st);
+yrc_status TrainStep(yrc_nrc* c, const float* queries, const float* targets, int64_t n,
+                     const unsigned long long* n_ptr, cudaStream_t st) {
+    yrc_status s = LaunchTrain(c, queries, targets, n, n_ptr, st);
     if (s != YRC_OK) return s;
     return LaunchAdam(c, st);
 }
@@ -676,6 +688,7 @@ yrc_status yrc_nrc_create(const float box_lo[3], float box_extent, uint64_t seed
     alloc(&c->w_grad, sizeof(float) * kWeightCount);
     alloc(&c->loss, sizeof(float));
     alloc(&c->error, sizeof(int));
+    alloc(&c->step, sizeof(int64_t));
     if (err == cudaSuccess) err = cudaFuncSetAttribute(CacheTrainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        kTrainSmem);
     if (err == cudaSuccess) err = cudaFuncSetAttribute(CacheInferKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -703,6 +716,7 @@ yrc_status yrc_nrc_create(const float box_lo[3], float box_extent, uint64_t seed
     if (err == cudaSuccess) err = cudaMemset(c->table_m, 0, sizeof(float) * kGridParams);
     if (err == cudaSuccess) err = cudaMemset(c->table_v, 0, sizeof(float) * kGridParams);
     if (err == cudaSuccess) err = cudaMemset(c->error, 0, sizeof(int));
+    if (err == cudaSuccess) err = cudaMemset(c->step, 0, sizeof(int64_t));
     if (err == cudaSuccess) {
         InitGridKernel<<<Blocks(kGridParams, c->sm_count), 256>>>(c->table_master, kGridParams, seed);
         RoundKernel<<<Blocks(kGridParams, c->sm_count), 256>>>(c->table_master, kGridParams, c->table, nullptr);
@@ -771,7 +785,7 @@ yrc_status yrc_nrc_infer(yrc_nrc* c, const float* queries, int64_t n, float* rgb
     if (!c || n < 0 || (n > 0 && (!queries || !rgb))) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_nrc_infer: bad argument");
     std::lock_guard<std::mutex> lock(c->mutex);
     cudaSetDevice(c->device);
-    return nrc::Infer(c, queries, n, rgb, static_cast<cudaStream_t>(stream));
+    return nrc::Infer(c, queries, n, nullptr, rgb, static_cast<cudaStream_t>(stream));
 }
 
 yrc_status yrc_nrc_gradients(yrc_nrc* c, const float* queries, const float* targets, int64_t n, float* weight_grads,
@@ -783,7 +797,7 @@ yrc_status yrc_nrc_gradients(yrc_nrc* c, const float* queries, const float* targ
     }
     std::lock_guard<std::mutex> lock(c->mutex);
     cudaSetDevice(c->device);
-    yrc_status s = LaunchTrain(c, queries, targets, n, nullptr);
+    yrc_status s = LaunchTrain(c, queries, targets, n, nullptr, nullptr);
     if (s != YRC_OK) return s;
     cudaError_t err = cudaDeviceSynchronize();
     if (err != cudaSuccess) return CudaFailN(err, "gradients");
@@ -812,7 +826,7 @@ yrc_status yrc_nrc_train_step(yrc_nrc* c, const float* queries, const float* tar
     std::lock_guard<std::mutex> lock(c->mutex);
     cudaSetDevice(c->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    yrc_status s = TrainStep(c, queries, targets, n, st);
+    yrc_status s = TrainStep(c, queries, targets, n, nullptr, st);
     if (s != YRC_OK) return s;
     if (loss_out) {
         const cudaError_t err = cudaMemcpyAsync(loss_out, c->loss, sizeof(float), cudaMemcpyDeviceToDevice, st);

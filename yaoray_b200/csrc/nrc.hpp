@@ -11,10 +11,13 @@
 namespace yrc {
 namespace nrc {
 
-// rgb[i] (float4, w unused) = cache(queries[i]) for n queries of 16 floats.
-yrc_status Infer(yrc_nrc* cache, const float* queries, int64_t n, float* rgb, cudaStream_t stream);
-// One optimiser step on n (query, target float4) pairs.
-yrc_status TrainStep(yrc_nrc* cache, const float* queries, const float* targets, int64_t n, cudaStream_t stream);
+// rgb[i] (float4, w unused) = cache(queries[i]) for n queries of 16 floats;
+// with n_ptr, the count is min(*n_ptr, n) read on the device (graph-safe).
+yrc_status Infer(yrc_nrc* cache, const float* queries, int64_t n, const unsigned long long* n_ptr, float* rgb,
+                 cudaStream_t stream);
+// One optimiser step on n (query, target float4) pairs (n_ptr as above).
+yrc_status TrainStep(yrc_nrc* cache, const float* queries, const float* targets, int64_t n,
+                     const unsigned long long* n_ptr, cudaStream_t stream);
 
 }  // namespace nrc
 }  // namespace yrc

@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "nrc.hpp"
 #include "render_kernels.hpp"
 #include "render_types.hpp"
 #include "trace_kernels.hpp"
@@ -107,6 +108,12 @@ struct yrc_render_scene {
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int32_t graph_max_batch = -1;
+    // Radiance cache (optional).
+    yrc_nrc* cache = nullptr;
+    yrc_cache_settings cache_settings{};
+    yrc::DeviceArena cache_work;
+    int64_t cache_capacity = 0;
+    yrc::CacheArgs cargs{};
     std::mutex mutex;
 };
 
@@ -117,10 +124,35 @@ void yrc_render_scene_destroy(yrc_render_scene* scene) {
     cudaSetDevice(scene->device);
     if (scene->graph) cudaGraphExecDestroy(scene->graph);
     if (scene->stream) cudaStreamDestroy(scene->stream);
+    scene->cache_work.Release();
     scene->work.Release();
     scene->arena.Release();
     yrc_accel_destroy(scene->accel);
     delete scene;
+}
+
+yrc_status yrc_render_scene_set_cache(yrc_render_scene* scene, yrc_nrc* cache, const yrc_cache_settings* settings) {
+    using namespace yrc;
+    if (!scene) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_scene_set_cache: null scene");
+    yrc_cache_settings cs{0.01f, 16, 65536, 1, 1};
+    if (settings) cs = *settings;
+    if (cache && (!(cs.spread_threshold > 0.0f) || cs.train_one_in < 1 || cs.train_records < 0 ||
+                  cs.train_steps < 0 || cs.train_steps > 64)) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_scene_set_cache: bad settings");
+    }
+    std::lock_guard<std::mutex> lock(scene->mutex);
+    cudaSetDevice(scene->device);
+    if (scene->stream) cudaStreamSynchronize(scene->stream);
+    if (scene->graph) {
+        cudaGraphExecDestroy(scene->graph);
+        scene->graph = nullptr;
+    }
+    scene->cache_work.Release();
+    scene->cargs = CacheArgs{};
+    scene->cache_capacity = 0;
+    scene->cache = cache;
+    scene->cache_settings = cs;
+    return Ok();
 }
 
 int64_t yrc_render_scene_device_bytes(const yrc_render_scene* scene) {
@@ -433,6 +465,7 @@ yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     ps.aov_normal = W.Alloc<float4>(capacity);
     ps.nee = W.Alloc<float4>(3 * capacity);
     ps.nee_tp = W.Alloc<float4>(capacity);
+    ps.spread = W.Alloc<float2>(capacity);
     ps.nee_vis = nullptr;
     Queues& q = s->q;
     q.ray_in = W.Alloc<float4>(2 * capacity);
@@ -469,6 +502,57 @@ yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     return Ok();
 }
 
+// Allocates the radiance-cache queues for `capacity` paths (or releases
+// them when no cache is attached).
+yrc_status EnsureCache(yrc_render_scene* s) {
+    if (!s->cache) {
+        s->cargs = CacheArgs{};
+        return Ok();
+    }
+    if (s->cache_capacity == s->capacity && s->cargs.enabled) return Ok();
+    if (s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    s->cache_work.Release();
+    DeviceArena& W = s->cache_work;
+    const yrc_cache_settings& cs = s->cache_settings;
+    const int64_t cap = s->capacity;
+    CacheArgs c{};
+    c.enabled = 1;
+    c.spread_c = cs.spread_threshold;
+    c.train_one_in = std::max(1, cs.train_one_in);
+    c.train_records = cs.train ? std::max(128, cs.train_records) : 0;
+    c.train_paths = cs.train ? static_cast<int32_t>(std::min<int64_t>(cap, c.train_records)) : 0;
+    c.max_depth = s->dev.max_depth;
+    // The film's radiance clamp when set, else the brightest emitter the
+    // instanced scenes carry (a 1e4 sun).
+    c.target_max = s->dev.radiance_clamp > 0.0f ? s->dev.radiance_clamp : 1.0e4f;
+    c.queries = W.Alloc<float>(16 * cap);
+    c.query_path = W.Alloc<int32_t>(cap);
+    c.query_tp = W.Alloc<float4>(cap);
+    c.query_rgb = W.Alloc<float4>(cap);
+    c.train_slot = W.Alloc<int32_t>(cap);
+    const int64_t tp = std::max<int32_t>(c.train_paths, 1);
+    c.slot_path = W.Alloc<int32_t>(tp);
+    c.slot_len = W.Alloc<int32_t>(tp);
+    c.slot_q = W.Alloc<float>(16 * tp * std::max(1, c.max_depth));
+    c.slot_lt = W.Alloc<float4>(2 * tp * std::max(1, c.max_depth));
+    c.rec_q = W.Alloc<float>(16 * static_cast<int64_t>(std::max(c.train_records, 1)));
+    c.rec_t = W.Alloc<float4>(std::max(c.train_records, 1));
+    c.counters = W.Alloc<unsigned long long>(4);
+    if (W.err != cudaSuccess) {
+        const cudaError_t err = W.err;
+        s->cache_work.Release();
+        s->cargs = CacheArgs{};
+        s->cache_capacity = 0;
+        return CudaError(err, "radiance cache working memory");
+    }
+    s->cargs = c;
+    s->cache_capacity = cap;
+    return Ok();
+}
+
 // Records one batch (generate, max_depth bounces, film, next active list).
 yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
     const DevScene& sc = s->dev;
@@ -479,7 +563,12 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
     FilmArgs f{s->attempts, s->scalars + 2, s->scalars + 3, s->settings.adaptive_enabled, s->settings.adaptive_min_spp,
                s->settings.adaptive_relative_error, s->settings.adaptive_absolute_error,
                s->settings.adaptive_confidence};
-    LaunchGenerate(sc, s->ps, s->q, b, C, s->sm_count, st);
+    const CacheArgs& cache = s->cargs;
+    if (cache.enabled) {
+        const cudaError_t err = cudaMemsetAsync(cache.counters, 0, 4 * sizeof(unsigned long long), st);
+        if (err != cudaSuccess) return CudaError(err, "cache counters");
+    }
+    LaunchGenerate(sc, s->ps, s->q, b, cache, C, s->sm_count, st);
     Queues q = s->q;
     for (int depth = 0; depth < sc.max_depth; ++depth) {
         LaunchResetCounters(q, st);
@@ -494,7 +583,7 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
         ta.error = AccelErrorWord(s->accel);
         cudaError_t err = LaunchTrace(ta, false, false, TraceShapeOf(s->accel, 0), st, s->sm_count);
         if (err != cudaSuccess) return CudaError(err, "extend trace");
-        LaunchShade(sc, s->ps, q, depth, C, s->sm_count, st);
+        LaunchShade(sc, s->ps, q, cache, depth, C, s->sm_count, st);
         if (sc.any_transparent) {
             ShadowArgs sa{};
             sa.accel = sc.accel;
@@ -534,6 +623,21 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
         LaunchAdvanceQueue(q, st);
         std::swap(q.ray_in, q.ray_out);
         std::swap(q.path_in, q.path_out);
+    }
+    if (cache.enabled) {
+        // Paths that ended at the cache get its radiance; then one training
+        // step on the unbiased training paths of this batch.
+        yrc_status cs = nrc::Infer(s->cache, cache.queries, C, cache.counters + 0, reinterpret_cast<float*>(cache.query_rgb), st);
+        if (cs != YRC_OK) return cs;
+        LaunchCacheResolve(s->ps, cache, C, s->sm_count, st);
+        if (cache.train_records > 0) {
+            LaunchCacheTargets(s->ps, cache, s->sm_count, st);
+            for (int k = 0; k < std::max(1, s->cache_settings.train_steps); ++k) {
+                cs = nrc::TrainStep(s->cache, cache.rec_q, reinterpret_cast<const float*>(cache.rec_t),
+                                    cache.train_records, cache.counters + 2, st);
+                if (cs != YRC_OK) return cs;
+            }
+        }
     }
     LaunchFilm(sc, s->ps, b, f, pixels, s->sm_count, st);
     LaunchActivePixels(sc, b, f, pixels, s->sm_count, st);
@@ -576,6 +680,7 @@ extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* 
     const int64_t capacity = std::min<int64_t>(std::max<int64_t>(pixels, int64_t{1} << 21),
                                                pixels * std::min(spp, kMaxBatch));
     yrc_status status = EnsureWork(s, capacity);
+    if (status == YRC_OK) status = EnsureCache(s);
     if (status != YRC_OK) return status;
     cudaStream_t stream = s->stream;
     std::vector<yrc_film_pixel> host_film(static_cast<size_t>(pixels));
@@ -633,6 +738,7 @@ extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* 
     cudaError_t err = cudaStreamSynchronize(stream);
     if (err != cudaSuccess) return CudaError(err, "render setup");
     uint64_t converged = sc_host[3];
+    uint64_t cache_queries = 0, cache_records = 0;
     while (sc_host[0] > 0) {
         if (r.stop_flag && *r.stop_flag) return Fail(YRC_ERR_CANCELLED, "render cancelled");
         const int32_t this_batch = batch_host;
@@ -641,8 +747,15 @@ extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* 
         if (err != cudaSuccess) return CudaError(err, "batch launch");
         cudaMemcpyAsync(sc_host, s->scalars, sizeof(sc_host), cudaMemcpyDeviceToHost, stream);
         cudaMemcpyAsync(&batch_host, s->batch, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
+        unsigned long long cache_host[4] = {0, 0, 0, 0};
+        if (s->cargs.enabled) {
+            cudaMemcpyAsync(cache_host, s->cargs.counters, sizeof(cache_host), cudaMemcpyDeviceToHost, stream);
+        }
         err = cudaStreamSynchronize(stream);
         if (err != cudaSuccess) return CudaError(err, "batch");
+        cache_queries += cache_host[0];
+        cache_records += std::min<unsigned long long>(cache_host[2], static_cast<unsigned long long>(
+                                                                        std::max(s->cargs.train_records, 0)));
         completed_passes += this_batch;
         converged = sc_host[3];
         if (r.progress) {
@@ -692,6 +805,8 @@ extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* 
         stats->occluded_shadow_rays = counters[kCtrStatsBase + 2];
         stats->hits = counters[kCtrStatsBase + 3];
         stats->misses = counters[kCtrStatsBase + 4];
+        stats->cache_queries = cache_queries;
+        stats->cache_records = cache_records;
         stats->bad_samples = fin[2];
         stats->bvh_nodes = s->bvh_nodes;
         stats->bvh_max_depth = s->bvh_max_depth;

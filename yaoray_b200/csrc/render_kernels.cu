@@ -71,7 +71,17 @@ __device__ inline V3 CameraDirection(const DevScene& sc, float fx, float fy) {
 
 // ------------------------------------------------------------------ generate
 
-__global__ void GenerateKernel(DevScene sc, PathState ps, Queues q, BatchArgs b) {
+// Radiance cache: 1 in `train_one_in` paths (by a hash of pixel and sample)
+// takes a training slot while slots last; the others may end at the cache.
+__device__ __forceinline__ uint32_t CacheHash(uint32_t a, uint32_t b) {
+    uint32_t h = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u) * 0x85EBCA77u;
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    return h;
+}
+
+__global__ void GenerateKernel(DevScene sc, PathState ps, Queues q, BatchArgs b, CacheArgs cache) {
     const int64_t n_active = static_cast<int64_t>(*b.active_count);
     const int32_t batch = *b.batch;
     const int64_t total = n_active * batch;
@@ -104,6 +114,20 @@ __global__ void GenerateKernel(DevScene sc, PathState ps, Queues q, BatchArgs b)
         q.ray_in[2 * i] = make_float4(sc.cam_origin[0], sc.cam_origin[1], sc.cam_origin[2], 1.0e-5f);
         q.ray_in[2 * i + 1] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
         q.path_in[i] = static_cast<int32_t>(i);
+        if (cache.enabled) {
+            int32_t slot = -1;
+            if (CacheHash(static_cast<uint32_t>(pixel), static_cast<uint32_t>(sample)) %
+                    static_cast<uint32_t>(cache.train_one_in) == 0) {
+                const unsigned long long k = atomicAdd(cache.counters + 1, 1ull);
+                if (k < static_cast<unsigned long long>(cache.train_paths)) {
+                    slot = static_cast<int32_t>(k);
+                    cache.slot_path[slot] = static_cast<int32_t>(i);
+                    cache.slot_len[slot] = 0;
+                }
+            }
+            cache.train_slot[i] = slot;
+            ps.spread[i] = make_float2(0.0f, 0.0f);
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) q.counters[kCtrIn] = static_cast<unsigned long long>(total);
 }
@@ -441,6 +465,21 @@ __device__ __forceinline__ void PushShadow(Queues& q, V3 o, V3 d, float tmax, in
 
 }  // namespace
 
+// Radiance-cache query of a surface vertex (the 16-float layout of
+// yrc_nrc_infer): position, roughness, direction towards the viewer,
+// shading normal, diffuse and specular albedo.
+__device__ __forceinline__ void WriteCacheQuery(float* out, V3 p, V3 wo, V3 n, const Mat& m) {
+    const bool diffuse_like = m.kind == kDiffuse || m.kind == kCoatedDiffuse || m.kind == kDiffuseTransmission;
+    const bool specular_like = m.kind != kDiffuse && m.kind != kDiffuseTransmission;
+    const V3 kd = diffuse_like ? m.reflectance : V3{0.0f, 0.0f, 0.0f};
+    const float ks = specular_like ? 1.0f : 0.0f;
+    float4* o = reinterpret_cast<float4*>(out);
+    o[0] = make_float4(p.x, p.y, p.z, m.ur);
+    o[1] = make_float4(wo.x, wo.y, wo.z, n.x);
+    o[2] = make_float4(n.y, n.z, kd.x, kd.y);
+    o[3] = make_float4(kd.z, ks, ks, ks);
+}
+
 // The material kind a shading class folds to (-1: any kind).
 template <int kClass>
 __device__ constexpr int32_t ClassKind() {
@@ -453,7 +492,8 @@ __device__ constexpr int32_t ClassKind() {
 // IntegratePathSample's per-bounce body (src/integrators/path_integrator.cpp:23-197)
 // for the entries of one shading class.
 template <int kClass>
-__global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps, Queues q, int depth) {
+__global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps, Queues q, int depth,
+                                                       CacheArgs cache) {
     unsigned long long begin = 0;
 #pragma unroll
     for (int c = 0; c < kClass; ++c) begin += q.counters[kCtrClass0 + c];
@@ -533,6 +573,40 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
                 w = PowerHeuristic(1, prev.w, 1, pl);
             }
             rad = rad + Mul(tp, emission) * w;
+        }
+
+        // --- radiance cache: path spread (footprint heuristic), training
+        // records, early termination into the cache
+        if (cache.enabled) {
+            const float cv = fmaxf(fabsf(Dot(d, s.n)), 1.0e-4f);
+            float2 sp = ps.spread[path];
+            if (depth == 0) {
+                sp.x = hit.x * hit.x / (4.0f * kPi * cv);
+                sp.y = 0.0f;
+            } else if (!(flags & kPathPrevDelta)) {
+                sp.y += sqrtf(hit.x * hit.x / (fmaxf(prev.w, 1.0e-12f) * cv));
+            }
+            ps.spread[path] = sp;
+            const int32_t slot = cache.train_slot[path];
+            if (slot >= 0) {
+                const int32_t k = cache.slot_len[slot];
+                if (k < cache.max_depth) {
+                    const int64_t v = static_cast<int64_t>(slot) * cache.max_depth + k;
+                    WriteCacheQuery(cache.slot_q + 16 * v, s.p, wo, s.n, m);
+                    cache.slot_lt[2 * v] = ToF4(rad);
+                    cache.slot_lt[2 * v + 1] = ToF4(tp);
+                    cache.slot_len[slot] = k + 1;
+                }
+            } else if (depth >= 1 && !IsDelta(m) && sp.y * sp.y > cache.spread_c * sp.x) {
+                const unsigned long long k = QueueAppend(cache.counters + 0);
+                WriteCacheQuery(cache.queries + 16 * k, s.p, wo, s.n, m);
+                cache.query_path[k] = path;
+                cache.query_tp[k] = ToF4(tp);
+                ps.throughput[path] = ToF4(tp);
+                ps.radiance[path] = ToF4(rad);
+                ps.flags[path] = flags;
+                continue;
+            }
         }
 
         PixelSampler smp;
@@ -700,6 +774,57 @@ __global__ void ClearOcclusionKernel(Queues q, int64_t slots) {
     }
 }
 
+// ------------------------------------------------------- radiance cache
+
+// Adds throughput x cached radiance to every path that ended at the cache.
+__global__ void CacheResolveKernel(PathState ps, CacheArgs cache) {
+    const int64_t n = static_cast<int64_t>(cache.counters[0]);
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t path = cache.query_path[k];
+        const V3 c = F4(cache.query_rgb[k]);
+        if (!(isfinite(c.x) && isfinite(c.y) && isfinite(c.z))) continue;
+        ps.radiance[path] = ToF4(F4(ps.radiance[path]) + Mul(F4(cache.query_tp[k]), c));
+    }
+}
+
+// Training records of the unbiased training paths: for each recorded vertex,
+// target = (final path radiance - radiance before the vertex's reflected
+// light) / throughput at the vertex, i.e. a one-sample estimate of the
+// radiance the vertex reflects towards the previous one.
+__global__ void CacheTargetsKernel(PathState ps, CacheArgs cache) {
+    const int64_t slots = static_cast<int64_t>(
+        min(cache.counters[1], static_cast<unsigned long long>(cache.train_paths)));
+    for (int64_t slot = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; slot < slots;
+         slot += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t path = cache.slot_path[slot];
+        const V3 L = F4(ps.radiance[path]);
+        const int32_t len = cache.slot_len[slot];
+        for (int32_t k = 0; k < len; ++k) {
+            const int64_t v = slot * cache.max_depth + k;
+            const V3 lb = F4(cache.slot_lt[2 * v]);
+            const V3 t = F4(cache.slot_lt[2 * v + 1]);
+            V3 target{t.x > 1.0e-8f ? fmaxf(L.x - lb.x, 0.0f) / t.x : 0.0f,
+                      t.y > 1.0e-8f ? fmaxf(L.y - lb.y, 0.0f) / t.y : 0.0f,
+                      t.z > 1.0e-8f ? fmaxf(L.z - lb.z, 0.0f) / t.z : 0.0f};
+            // Rare numerically extreme samples would dominate the optimiser's
+            // moment estimates: bound each target's largest component.
+            const float mc = MaxComp(target);
+            if (mc > cache.target_max) target = target * (cache.target_max / mc);
+            if (!(isfinite(target.x) && isfinite(target.y) && isfinite(target.z))) continue;
+            const unsigned long long r = atomicAdd(cache.counters + 2, 1ull);
+            if (r >= static_cast<unsigned long long>(cache.train_records)) break;
+            const float4* src = reinterpret_cast<const float4*>(cache.slot_q + 16 * v);
+            float4* dst = reinterpret_cast<float4*>(cache.rec_q + 16 * r);
+            dst[0] = src[0];
+            dst[1] = src[1];
+            dst[2] = src[2];
+            dst[3] = src[3];
+            cache.rec_t[r] = ToF4(target);
+        }
+    }
+}
+
 // ------------------------------------------------------------------- film
 
 // Film::AddSample in sample order for each active pixel (film.cpp:160-183),
@@ -820,22 +945,29 @@ unsigned Grid(int64_t work, int sm_count, int per_sm = 8) {
 }
 }  // namespace
 
-void LaunchGenerate(const DevScene& sc, const PathState& ps, const Queues& q, const BatchArgs& b, int64_t capacity,
-                    int sm_count, cudaStream_t st) {
-    GenerateKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, b);
+void LaunchGenerate(const DevScene& sc, const PathState& ps, const Queues& q, const BatchArgs& b,
+                    const CacheArgs& cache, int64_t capacity, int sm_count, cudaStream_t st) {
+    GenerateKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, b, cache);
 }
 void LaunchResetCounters(const Queues& q, cudaStream_t st) { ResetCountersKernel<<<1, 32, 0, st>>>(q); }
 void LaunchAdvanceQueue(const Queues& q, cudaStream_t st) { AdvanceQueueKernel<<<1, 32, 0, st>>>(q); }
-void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity, int sm_count,
-                 cudaStream_t st) {
+void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, const CacheArgs& cache, int depth,
+                 int64_t capacity, int sm_count, cudaStream_t st) {
     ClassifyKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, q);
     ScatterByClassKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(q);
-    ShadeKernel<kClassMiss><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
-    ShadeKernel<kClassDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
-    ShadeKernel<kClassConductor><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
-    ShadeKernel<kClassDielectric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
-    ShadeKernel<kClassCoatedDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
-    ShadeKernel<kClassGeneric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
+    ShadeKernel<kClassMiss><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    ShadeKernel<kClassDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    ShadeKernel<kClassConductor><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    ShadeKernel<kClassDielectric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    ShadeKernel<kClassCoatedDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    ShadeKernel<kClassGeneric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
+}
+void LaunchCacheResolve(const PathState& ps, const CacheArgs& cache, int64_t capacity, int sm_count,
+                        cudaStream_t st) {
+    CacheResolveKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(ps, cache);
+}
+void LaunchCacheTargets(const PathState& ps, const CacheArgs& cache, int sm_count, cudaStream_t st) {
+    CacheTargetsKernel<<<Grid(cache.train_paths, sm_count), kThreads, 0, st>>>(ps, cache);
 }
 void LaunchNeeResolve(const PathState& ps, const Queues& q, const float4* transmittance, int64_t capacity,
                       int sm_count, cudaStream_t st) {

@@ -30,12 +30,17 @@ struct FilmArgs {
 
 // Host launchers (grid sizes are multiples of the SM count; every kernel
 // reads its work count from device memory, so the sequence is graph-safe).
-void LaunchGenerate(const DevScene& sc, const PathState& ps, const Queues& q, const BatchArgs& b, int64_t capacity,
-                    int sm_count, cudaStream_t st);
+void LaunchGenerate(const DevScene& sc, const PathState& ps, const Queues& q, const BatchArgs& b,
+                    const CacheArgs& cache, int64_t capacity, int sm_count, cudaStream_t st);
 void LaunchResetCounters(const Queues& q, cudaStream_t st);
 void LaunchAdvanceQueue(const Queues& q, cudaStream_t st);
-void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity, int sm_count,
-                 cudaStream_t st);
+void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, const CacheArgs& cache, int depth,
+                 int64_t capacity, int sm_count, cudaStream_t st);
+// Radiance cache: add cached radiance to the paths that ended at the cache;
+// build the training records of the training paths.
+void LaunchCacheResolve(const PathState& ps, const CacheArgs& cache, int64_t capacity, int sm_count,
+                        cudaStream_t st);
+void LaunchCacheTargets(const PathState& ps, const CacheArgs& cache, int sm_count, cudaStream_t st);
 void LaunchNeeResolve(const PathState& ps, const Queues& q, const float4* transmittance, int64_t capacity,
                       int sm_count, cudaStream_t st);
 void LaunchClearOcclusion(const Queues& q, int64_t slots, int sm_count, cudaStream_t st);

@@ -146,6 +146,31 @@ struct PathState {
     float4* nee;          // 3 per path: contribution xyz (before throughput), w unused
     float4* nee_tp;       // throughput at the vertex that made the NEE samples
     float* nee_vis;       // 3 per path: shadow transmittance (1 visible, 0 occluded)
+    float2* spread;       // radiance cache: primary footprint a0, running spread sum
+};
+
+// Radiance-cache stage of the path tracer (device pointers; all counts live
+// in `counters`: [0] cache queries, [1] training paths, [2] training records).
+struct CacheArgs {
+    int32_t enabled;
+    float spread_c;        // terminate when spread^2 > spread_c * a0
+    int32_t train_one_in;  // 1 in train_one_in paths traces unbiased for training
+    int32_t train_paths;   // capacity of the training-path slots
+    int32_t train_records; // capacity of the training records
+    int32_t max_depth;
+    float target_max;      // bound on a training target's largest component
+    float* queries;        // per terminated path: 16-float query
+    int32_t* query_path;
+    float4* query_tp;      // throughput at the query vertex
+    float4* query_rgb;     // cache output
+    int32_t* train_slot;   // per path: training slot or -1
+    int32_t* slot_path;    // per training slot: path
+    int32_t* slot_len;     // per training slot: recorded vertices
+    float* slot_q;         // train_paths * max_depth queries
+    float4* slot_lt;       // train_paths * max_depth * 2: radiance before the vertex, throughput
+    float* rec_q;          // training records: queries
+    float4* rec_t;         //                   targets
+    unsigned long long* counters;
 };
 
 constexpr uint32_t kPathPrevValid = 1u << 0;

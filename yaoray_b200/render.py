@@ -146,7 +146,13 @@ class Stats(C.Structure):
                 ("sphere_tests", C.c_uint64), ("bvh_node_tests", C.c_uint64), ("bvh_nodes", C.c_int32),
                 ("bvh_max_depth", C.c_int32), ("hits", C.c_uint64), ("misses", C.c_uint64),
                 ("bad_samples", C.c_uint64), ("threads", C.c_int32), ("elapsed_seconds", C.c_double),
-                ("device_seconds", C.c_double)]
+                ("device_seconds", C.c_double), ("cache_queries", C.c_uint64), ("cache_records", C.c_uint64)]
+
+
+class CacheSettings(C.Structure):
+    """yrc_cache_settings: how the path tracer uses an attached radiance cache."""
+    _fields_ = [("spread_threshold", C.c_float), ("train_one_in", C.c_int32), ("train_records", C.c_int32),
+                ("train", C.c_int32), ("train_steps", C.c_int32)]
 
 
 def _bind():
@@ -159,6 +165,7 @@ def _bind():
         ("yrc_render_scene_destroy", None, [P]),
         ("yrc_render_scene_device_bytes", C.c_int64, [P]),
         ("yrc_render", C.c_int, [P, P, P, P, P]),
+        ("yrc_render_scene_set_cache", C.c_int, [P, P, P]),
         ("yrc_alias_table_build", C.c_int, [P, C.c_int32, P, P, P]),
         ("yrc_environment_distribution_build", C.c_int, [P, C.c_int32, C.c_int32, P, P, P, P, P]),
     ]:
@@ -344,6 +351,17 @@ class PreparedScene:
     @property
     def device_bytes(self) -> int:
         return int(_bind().yrc_render_scene_device_bytes(self._handle))
+
+    def set_radiance_cache(self, cache, spread_threshold: float = 0.01, train_one_in: int = 16,
+                           train_records: int = 65536, train: bool = True, train_steps: int = 1) -> None:
+        """Attaches a yaoray_b200.nrc.RadianceCache (None detaches): paths end
+        at the cache when their footprint heuristic fires, and the cache
+        takes `train_steps` optimiser steps per batch on the records of 1 in
+        `train_one_in` unbiased paths."""
+        st = CacheSettings(spread_threshold, train_one_in, train_records, 1 if train else 0, train_steps)
+        self._cache = cache
+        check(_bind().yrc_render_scene_set_cache(self._handle, cache._handle if cache is not None else None,
+                                                 C.byref(st)))
 
     def close(self):
         if getattr(self, "_handle", None) and self._handle.value:
