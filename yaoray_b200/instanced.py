@@ -4,7 +4,9 @@
 ≈30M instanced triangles — over a ground plane.
 
 Materials are drawn per instanced object: 40 % Lambertian (albedo
-U[0.1, 0.8]), 25 % GGX conductor (alpha U[0.05, 0.5], gold-like RGB eta/k),
+U[0.1, 0.8]), 25 % GGX conductor (alpha U[0.05, 0.5], gold-like RGB eta/k,
+carried as reflectance = ConductorF0(eta, k) because the reference's plain
+conductor is Schlick on `reflectance`),
 20 % rough dielectric (eta 1.5), 15 % coated diffuse (dielectric coat,
 thickness 0.01, Beer–Lambert absorption U[0, 0.5]). Lights: a procedural
 2048 x 1024 FP32 HDRI (sky gradient plus a 0.5 degree sun disk of radiance
@@ -42,6 +44,17 @@ EMITTERS = 64
 # Gold, RGB approximation of its complex index of refraction.
 GOLD_ETA = (0.143, 0.374, 1.442)
 GOLD_K = (3.983, 2.385, 1.603)
+
+
+def conductor_f0(eta: float, k: float) -> float:
+    """ConductorF0 (scene_compiler_conductor_materials.cpp:116-120), in float32."""
+    e, kk = np.float32(eta), np.float32(k)
+    num = (e - np.float32(1)) * (e - np.float32(1)) + kk * kk
+    den = (e + np.float32(1)) * (e + np.float32(1)) + kk * kk
+    return float(num / den) if den > 0 else 1.0
+
+
+GOLD_F0 = tuple(conductor_f0(e, k) for e, k in zip(GOLD_ETA, GOLD_K))
 SUN_RADIANCE = 1.0e4
 SUN_DIAMETER_DEG = 0.5
 EYE = (0.0, 55.0, -150.0)
@@ -151,9 +164,13 @@ def materials(rng: np.random.Generator) -> np.ndarray:
         if kind == DIFFUSE:
             out.append(default_material(reflectance=rng.uniform(0.1, 0.8, 3)))
         elif kind == CONDUCTOR:
+            # The reference's plain conductor shades with Schlick on
+            # `reflectance` and ignores eta/k, so the gold colour is carried
+            # as ConductorF0(eta, k) per channel
+            # (src/frontend/pbrt/scene_compiler_conductor_materials.cpp:116-120).
             alpha = rng.uniform(0.05, 0.5)
-            out.append(default_material(kind=CONDUCTOR, eta=GOLD_ETA, k=GOLD_K, uroughness=alpha,
-                                        vroughness=alpha, remap_roughness=0))
+            out.append(default_material(kind=CONDUCTOR, eta=GOLD_ETA, k=GOLD_K, reflectance=GOLD_F0,
+                                        uroughness=alpha, vroughness=alpha, remap_roughness=0))
         elif kind == DIELECTRIC:
             alpha = rng.uniform(0.05, 0.3)
             out.append(default_material(kind=DIELECTRIC, ior=1.5, uroughness=alpha, vroughness=alpha,
