@@ -461,6 +461,15 @@ typedef struct yrc_bssrdf_table {
     const float* profile_cdf;    /* rho_count * radius_count */
 } yrc_bssrdf_table;
 
+/*
+ * ComputeBeamDiffusionBSSRDF (src/shading/bssrdf.cpp:124-151): fills a
+ * rho_count x radius_count photon-beam-diffusion profile table for phase
+ * asymmetry g and relative index eta (the reference uses 100 x 64 and g = 0
+ * for every subsurface material). Bit-identical to the reference's table.
+ */
+yrc_status yrc_bssrdf_table_build(float g, float eta, int32_t rho_count, int32_t radius_count, float* rho_samples,
+                                  float* radius_samples, float* profile, float* rho_eff, float* profile_cdf);
+
 /* RenderCamera (include/yaoray/scene/camera.hpp:7-13). */
 typedef struct yrc_camera {
     float origin[3];

@@ -363,6 +363,18 @@ def ref_sampler(kind: int, seed: int, spp: int, queries: np.ndarray, two_d: bool
     return out.reshape(-1, 2) if two_d else out
 
 
+def ref_bssrdf_table(g: float, eta: float, rho_count: int = 100, radius_count: int = 64) -> dict:
+    """The reference's ComputeBeamDiffusionBSSRDF table."""
+    L = ref_lib()
+    t = {"rho_samples": np.zeros(rho_count, np.float32), "radius_samples": np.zeros(radius_count, np.float32),
+         "profile": np.zeros(rho_count * radius_count, np.float32), "rho_eff": np.zeros(rho_count, np.float32),
+         "profile_cdf": np.zeros(rho_count * radius_count, np.float32)}
+    L.yrref_bssrdf_table.argtypes = [C.c_float, C.c_float, C.c_int, C.c_int, P, P, P, P, P]
+    L.yrref_bssrdf_table(g, eta, rho_count, radius_count, _p(t["rho_samples"]), _p(t["radius_samples"]),
+                         _p(t["profile"]), _p(t["rho_eff"]), _p(t["profile_cdf"]))
+    return t
+
+
 def ref_rng(seed: int, count: int) -> np.ndarray:
     out = np.empty(count, np.float32)
     ref_lib().yrref_rng_floats(seed, count, out.ctypes.data)

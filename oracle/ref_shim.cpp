@@ -395,6 +395,7 @@ std::uint64_t yrref_film_accumulate(int width, int height, const float* samples,
 
 #include <yaoray/lighting/environment.hpp>
 #include <yaoray/lighting/light_sampling.hpp>
+#include <yaoray/shading/bssrdf.hpp>
 
 namespace {
 
@@ -618,6 +619,7 @@ void* yrref_job_from_desc(const yrc_scene_desc* d) {
         r.sigma_a = Rgb(m.sigma_a);
         r.sigma_s = Rgb(m.sigma_s);
         r.bssrdf_eta = m.bssrdf_eta;
+        r.bssrdf_index = m.bssrdf_index;
         r.emission = Rgb(m.emission);
         r.alpha.value = m.alpha;
         r.absorption_color = Rgb(m.absorption_color);
@@ -629,6 +631,17 @@ void* yrref_job_from_desc(const yrc_scene_desc* d) {
         ir.emissive_primitives.push_back(yr::EmissivePrimitive{e.primitive_index, Rgb(e.radiance), e.area});
     }
     const yrc_environment& env = d->environment;
+    for (int32_t i = 0; d->bssrdf_tables && i < d->bssrdf_count; ++i) {
+        const yrc_bssrdf_table& t = d->bssrdf_tables[i];
+        auto table = std::make_shared<yr::BSSRDFTable>(t.rho_count, t.radius_count);
+        const std::size_t cells = static_cast<std::size_t>(t.rho_count) * t.radius_count;
+        std::copy(t.rho_samples, t.rho_samples + t.rho_count, table->rho_samples.begin());
+        std::copy(t.radius_samples, t.radius_samples + t.radius_count, table->radius_samples.begin());
+        std::copy(t.profile, t.profile + cells, table->profile.begin());
+        std::copy(t.rho_eff, t.rho_eff + t.rho_count, table->rho_eff.begin());
+        std::copy(t.profile_cdf, t.profile_cdf + cells, table->profile_cdf.begin());
+        ir.bssrdf_tables.push_back(std::move(table));
+    }
     ir.environment.active = env.active != 0;
     ir.environment.radiance = Rgb(env.radiance);
     ir.environment.strength = env.strength;
@@ -704,6 +717,38 @@ int yrref_job_render(void* handle, int threads, int spp_override, void* film_out
     }
     if (seconds) *seconds = result.stats.elapsed_seconds;
     return 0;
+}
+
+// ComputeBeamDiffusionBSSRDF of the reference, for checking the product's
+// table builder.
+void yrref_bssrdf_table(float g, float eta, int rho_count, int radius_count, float* rho, float* radius,
+                        float* profile, float* rho_eff, float* cdf) {
+    yr::BSSRDFTable t(rho_count, radius_count);
+    yr::ComputeBeamDiffusionBSSRDF(g, eta, t);
+    std::copy(t.rho_samples.begin(), t.rho_samples.end(), rho);
+    std::copy(t.radius_samples.begin(), t.radius_samples.end(), radius);
+    std::copy(t.profile.begin(), t.profile.end(), profile);
+    std::copy(t.rho_eff.begin(), t.rho_eff.end(), rho_eff);
+    std::copy(t.profile_cdf.begin(), t.profile_cdf.end(), cdf);
+}
+
+// The reference's TabulatedBSSRDF evaluated at n points (for checking the
+// device restatement): sample_r[i] = Sample_Sr(ch[i], u[i]),
+// pdf[i] = Pdf_Sr(ch[i], r[i]), sr[3 i..] = Sr(r[i]).
+void yrref_bssrdf_eval(const float* sigma_a, const float* sigma_s, float eta, float g, int n, const int* ch,
+                       const float* u, const float* r, float* sample_r, float* pdf, float* sr) {
+    yr::BSSRDFTable t(100, 64);
+    yr::ComputeBeamDiffusionBSSRDF(g, eta, t);
+    const yr::TabulatedBSSRDF b(yr::Color3f{sigma_a[0], sigma_a[1], sigma_a[2]},
+                                yr::Color3f{sigma_s[0], sigma_s[1], sigma_s[2]}, eta, t);
+    for (int i = 0; i < n; ++i) {
+        sample_r[i] = b.Sample_Sr(ch[i], u[i]);
+        pdf[i] = b.Pdf_Sr(ch[i], r[i]);
+        const yr::Color3f c = b.Sr(r[i]);
+        sr[3 * i] = c.x;
+        sr[3 * i + 1] = c.y;
+        sr[3 * i + 2] = c.z;
+    }
 }
 
 }  // extern "C"

@@ -18,7 +18,7 @@ import math
 import numpy as np
 
 from .accel import SceneGeometry
-from .render import EMISSIVE_DTYPE, OWEN_SOBOL, RenderScene, default_material
+from .render import EMISSIVE_DTYPE, OWEN_SOBOL, SUBSURFACE, RenderScene, build_bssrdf_table, default_material
 
 SIZE = 5.56
 WHITE = (0.73, 0.73, 0.73)
@@ -142,3 +142,26 @@ def scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8
     em[0]["area"] = area
     return RenderScene(geom, mats, camera(), width, height, spp=spp, max_depth=max_depth, seed=0,
                        sampler=OWEN_SOBOL, emissive=em)
+
+
+# The reference compiler's "Skin1" subsurface preset, per scene unit
+# (src/frontend/pbrt/scene_compiler_special_materials.cpp:33-35).
+SKIN1_SIGMA_A = (0.032, 0.17, 0.48)
+SKIN1_SIGMA_S = (0.74, 0.88, 1.01)
+
+
+def subsurface_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8,
+                     scale: float = 1.0, eta: float = 1.33) -> RenderScene:
+    """The Cornell box with the tall box made of a subsurface material (the
+    Skin1 coefficients times `scale`, relative index `eta`) and its
+    100 x 64 beam-diffusion profile table, as the reference's compiler would
+    build it from `Material "subsurface"`."""
+    s = scene(width, height, spp, max_depth)
+    m = default_material(kind=SUBSURFACE, sigma_a=np.float32(scale) * np.array(SKIN1_SIGMA_A, np.float32),
+                         sigma_s=np.float32(scale) * np.array(SKIN1_SIGMA_S, np.float32), bssrdf_eta=eta,
+                         bssrdf_index=0)
+    s.materials = np.concatenate([s.materials, m[None]])
+    tall_box = 6  # shapes(): five walls, short box, tall box, light
+    s.geometry.primitives[tall_box]["material_index"] = len(s.materials) - 1
+    s.bssrdf_tables = [build_bssrdf_table(eta)]
+    return s

@@ -185,7 +185,15 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
             return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": measured BRDFs are not shaded on the device");
         }
         if (m.kind == YRC_MAT_SUBSURFACE) {
-            return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": subsurface materials are not shaded on the device");
+            if (m.bssrdf_index < 0 || m.bssrdf_index >= desc->bssrdf_count || !desc->bssrdf_tables) {
+                return Fail(YRC_ERR_UNSUPPORTED,
+                            "material " + std::to_string(i) + ": subsurface material without a BSSRDF table");
+            }
+            const yrc_bssrdf_table& t = desc->bssrdf_tables[m.bssrdf_index];
+            if (t.rho_count < 4 || t.radius_count < 4 || !t.rho_samples || !t.radius_samples || !t.profile ||
+                !t.rho_eff || !t.profile_cdf) {
+                return Fail(YRC_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + ": malformed BSSRDF table");
+            }
         }
         if (m.alpha < 0.5f) {
             return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": alpha-cut-out surfaces are not traced on the device");
@@ -412,6 +420,28 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
         }
     }
 
+    // BSSRDF tables (ComputeBeamDiffusionBSSRDF output, consumed as given).
+    if (desc->bssrdf_count > 0 && desc->bssrdf_tables) {
+        std::vector<DevBssrdf> tables(static_cast<size_t>(desc->bssrdf_count));
+        for (int32_t i = 0; i < desc->bssrdf_count; ++i) {
+            const yrc_bssrdf_table& t = desc->bssrdf_tables[i];
+            DevBssrdf& b = tables[static_cast<size_t>(i)];
+            const size_t cells = static_cast<size_t>(t.rho_count) * static_cast<size_t>(t.radius_count);
+            b.rho_count = t.rho_count;
+            b.radius_count = t.radius_count;
+            b.rho = A.Upload(t.rho_samples, static_cast<size_t>(t.rho_count));
+            b.radius = A.Upload(t.radius_samples, static_cast<size_t>(t.radius_count));
+            b.profile = A.Upload(t.profile, cells);
+            b.rho_eff = A.Upload(t.rho_eff, static_cast<size_t>(t.rho_count));
+            b.profile_cdf = A.Upload(t.profile_cdf, cells);
+        }
+        d.bssrdf = A.Upload(tables);
+        d.bssrdf_count = desc->bssrdf_count;
+    }
+    for (int32_t i = 0; i < desc->material_count; ++i) {
+        if (desc->materials[i].kind == YRC_MAT_SUBSURFACE) d.any_subsurface = 1;
+    }
+
     // Camera and settings.
     const yrc_camera& c = desc->camera;
     std::memcpy(d.cam_origin, c.origin, sizeof(d.cam_origin));
@@ -483,6 +513,13 @@ yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     q.counters = W.Alloc<unsigned long long>(kCtrCount);
     s->transmittance = s->dev.any_transparent ? W.Alloc<float4>(3 * capacity) : nullptr;
     s->shadow_pending = s->dev.any_transparent ? W.Alloc<int32_t>(2 * capacity) : nullptr;
+    if (s->dev.any_subsurface) {
+        q.probe_ray = W.Alloc<float4>(2 * capacity);
+        q.probe_target = W.Alloc<int4>(capacity);
+        q.probe_entry = W.Alloc<float4>(2 * capacity);
+        q.probe_hit = W.Alloc<float4>(capacity);
+        q.probe_count = W.Alloc<int32_t>(capacity);
+    }
     s->film = W.Alloc<yrc_film_pixel>(static_cast<size_t>(pixels));
     s->attempts = W.Alloc<int32_t>(static_cast<size_t>(pixels));
     s->active = W.Alloc<int32_t>(static_cast<size_t>(pixels));
@@ -584,6 +621,21 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
         cudaError_t err = LaunchTrace(ta, false, false, TraceShapeOf(s->accel, 0), st, s->sm_count);
         if (err != cudaSuccess) return CudaError(err, "extend trace");
         LaunchShade(sc, s->ps, q, cache, depth, C, s->sm_count, st);
+        if (sc.any_subsurface) {
+            RenderProbeArgs pa{};
+            pa.accel = sc.accel;
+            pa.rays = q.probe_ray;
+            pa.targets = q.probe_target;
+            pa.selection = q.probe_entry;
+            pa.count_ptr = q.counters + kCtrProbe;
+            pa.capacity = C;
+            pa.hit = q.probe_hit;
+            pa.hits = q.probe_count;
+            pa.error = AccelErrorWord(s->accel);
+            const cudaError_t perr = LaunchRenderProbe(pa, st, s->sm_count);
+            if (perr != cudaSuccess) return CudaError(perr, "subsurface probe");
+            LaunchSubsurfaceExit(sc, s->ps, q, depth, C, s->sm_count, st);
+        }
         if (sc.any_transparent) {
             ShadowArgs sa{};
             sa.accel = sc.accel;

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "bsdf.cuh"
+#include "bssrdf.cuh"
 #include "render_kernels.hpp"
 #include "render_types.hpp"
 #include "sampler.cuh"
@@ -142,6 +143,7 @@ __global__ void ResetCountersKernel(Queues q) {
         q.counters[kCtrShadowTrace] = 0;
         q.counters[kCtrPending] = 0;
         q.counters[kCtrExact] = 0;
+        q.counters[kCtrProbe] = 0;
         for (int c = 0; c < kShadeClasses; ++c) {
             q.counters[kCtrClass0 + c] = 0;
             q.counters[kCtrCursor0 + c] = 0;
@@ -465,6 +467,82 @@ __device__ __forceinline__ void PushShadow(Queues& q, V3 o, V3 d, float tmax, in
 
 }  // namespace
 
+// EstimateDirectLight (src/integrators/path_direct_lighting.cpp:170-283) with
+// visibility deferred: draws the light samples of vertex p (normal n, towards
+// the viewer wo), stores each contribution without visibility in the path's
+// NEE slots and queues the shadow rays; the shadow stage and NeeResolveKernel
+// finish the estimate.
+__device__ inline void NextEvent(const DevScene& sc, PathState& ps, Queues& q, int32_t path, PixelSampler& smp,
+                                 Pcg32& rng, int depth, const Mat& m, V3 p, V3 n, V3 wo, V3 tp, uint32_t& flags) {
+    bool any = false;
+    if (sc.emissive_count > 0) {
+        const float us = smp.Sample1D(kDimDirectLightSelect, depth);
+        float tx, ty;
+        smp.Sample2D(kDimDirectLightSurface, depth, tx, ty);
+        const LightSample ls = SampleEmissive(sc, us, tx, ty);
+        if (ls.valid && ls.pdf > 0.0f && !IsBlack(ls.radiance)) {
+            const V3 to_light = ls.point - p;
+            const float dsq = LengthSq(to_light);
+            if (dsq > kMinShadowBias * kMinShadowBias) {
+                const float dist = sqrtf(dsq);
+                const float sb = ShadowBias(p, ls.point, dist);
+                if (dist > sb) {
+                    const V3 so = p + n * sb;
+                    const V3 stl = ls.point - so;
+                    const float sdsq = LengthSq(stl);
+                    if (sdsq > kMinShadowBias * kMinShadowBias) {
+                        const float sd = sqrtf(sdsq);
+                        const V3 wi = stl / sd;
+                        const float cs = fmaxf(0.0f, Dot(n, wi));
+                        if (cs > 0.0f) {
+                            const float pl = PdfEmissiveSolidAngle(sc, p, ls.point, ls.normal, ls.emissive);
+                            if (pl > 0.0f) {
+                                CountStat(q.counters, kStatShadow);
+                                const V3 f = EvalBsdf(m, wo, wi, n, rng);
+                                if (!IsBlack(f)) {
+                                    const float pb = PdfBsdf(m, wo, wi, n, rng);
+                                    const float mis = PowerHeuristic(1, pl, 1, pb);
+                                    ps.nee[3 * path + 0] = ToF4(Mul(f, ls.radiance) * (cs * mis / pl));
+                                    PushShadow(q, so, wi, sd - sb, 3 * path + 0);
+                                    any = true;
+                                } else {
+                                    ps.nee[3 * path + 0] = make_float4(0, 0, 0, 0);
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (EnvSampleable(sc.env)) {
+        float tx, ty;
+        smp.Sample2D(kDimDirectLightSurface, depth, tx, ty);
+        const EnvSample es = SampleEnvironment(sc.env, tx, ty);
+        if (es.valid && es.pdf > 0.0f && !IsBlack(es.radiance)) {
+            const float cs = fmaxf(0.0f, Dot(n, es.dir));
+            if (cs > 0.0f) {
+                const V3 f = EvalBsdf(m, wo, es.dir, n, rng);
+                if (!IsBlack(f)) {
+                    CountStat(q.counters, kStatShadow);
+                    const float pb = PdfBsdf(m, wo, es.dir, n, rng);
+                    const float mis = PowerHeuristic(1, es.pdf, 1, pb);
+                    ps.nee[3 * path + 2] = ToF4(Mul(f, es.radiance) * (cs * mis / es.pdf));
+                    PushShadow(q, p + n * SurfaceBias(p), es.dir, __int_as_float(0x7f800000),
+                               3 * path + 2);
+                    any = true;
+                }
+            }
+        }
+    }
+    if (any) {
+        flags |= kPathNee;
+        ps.nee_tp[path] = ToF4(tp);
+        const unsigned long long k = QueueAppend(q.counters + kCtrNee);
+        q.nee_paths[k] = path;
+    }
+}
+
 // Radiance-cache query of a surface vertex (the 16-float layout of
 // yrc_nrc_infer): position, roughness, direction towards the viewer,
 // shading normal, diffuse and specular albedo.
@@ -615,75 +693,78 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
         Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
 
         // --- next-event estimation: samples now, visibility in the shadow stage
-        if (!IsDelta(m)) {
-            bool any = false;
-            const V3 n = s.n;
-            if (sc.emissive_count > 0) {
-                const float us = smp.Sample1D(kDimDirectLightSelect, depth);
-                float tx, ty;
-                smp.Sample2D(kDimDirectLightSurface, depth, tx, ty);
-                const LightSample ls = SampleEmissive(sc, us, tx, ty);
-                if (ls.valid && ls.pdf > 0.0f && !IsBlack(ls.radiance)) {
-                    const V3 to_light = ls.point - s.p;
-                    const float dsq = LengthSq(to_light);
-                    if (dsq > kMinShadowBias * kMinShadowBias) {
-                        const float dist = sqrtf(dsq);
-                        const float sb = ShadowBias(s.p, ls.point, dist);
-                        if (dist > sb) {
-                            const V3 so = s.p + n * sb;
-                            const V3 stl = ls.point - so;
-                            const float sdsq = LengthSq(stl);
-                            if (sdsq > kMinShadowBias * kMinShadowBias) {
-                                const float sd = sqrtf(sdsq);
-                                const V3 wi = stl / sd;
-                                const float cs = fmaxf(0.0f, Dot(n, wi));
-                                if (cs > 0.0f) {
-                                    const float pl = PdfEmissiveSolidAngle(sc, s.p, ls.point, ls.normal, ls.emissive);
-                                    if (pl > 0.0f) {
-                                        CountStat(q.counters, kStatShadow);
-                                        const V3 f = EvalBsdf(m, wo, wi, n, rng);
-                                        if (!IsBlack(f)) {
-                                            const float pb = PdfBsdf(m, wo, wi, n, rng);
-                                            const float mis = PowerHeuristic(1, pl, 1, pb);
-                                            ps.nee[3 * path + 0] = ToF4(Mul(f, ls.radiance) * (cs * mis / pl));
-                                            PushShadow(q, so, wi, sd - sb, 3 * path + 0);
-                                            any = true;
-                                        } else {
-                                            ps.nee[3 * path + 0] = make_float4(0, 0, 0, 0);
-                                        }
-                                    }
-                                }
-                            }
+        if (!IsDelta(m)) NextEvent(sc, ps, q, path, smp, rng, depth, m, s.p, s.n, wo, tp, flags);
+
+        // --- subsurface entry (path_integrator.cpp:103-135): Fresnel split at
+        // the interface; the transmitted part becomes a probe ray that the
+        // subsurface stage traces and closes (SubsurfaceExitKernel).
+        if (kClass == kClassGeneric && m.kind == kSubsurface && s.material >= 0 &&
+            sc.materials[s.material].bssrdf_index >= 0 && sc.materials[s.material].bssrdf_index < sc.bssrdf_count) {
+            if (depth + 1 < sc.max_depth) {
+                const DevMaterial& dm = sc.materials[s.material];
+                const V3 ns = s.n;
+                V3 ss, ts;
+                BssrdfFrame(ns, ss, ts);
+                const float fr = FrDielectric(fabsf(Dot(wo, ns)), dm.bssrdf_eta);
+                if (smp.Sample1D(kDimBssrdfReflect, depth) < fr) {
+                    // Specular reflection (the selection probability cancels Fresnel).
+                    const V3 wr = ns * (2.0f * Dot(wo, ns)) - wo;
+                    flags |= kPathPrevValid | kPathPrevDelta;
+                    ps.prev[path] = ToF4(s.p, 1.0f);
+                    const V3 bn = Dot(wr, ns) >= 0.0f ? ns : -ns;
+                    const V3 no = s.p + bn * SurfaceBias(s.p);
+                    const unsigned long long k = QueueAppend(q.counters + kCtrOut);
+                    q.ray_out[2 * k] = make_float4(no.x, no.y, no.z, 1.0e-5f);
+                    q.ray_out[2 * k + 1] = make_float4(wr.x, wr.y, wr.z, __int_as_float(0x7f800000));
+                    q.path_out[k] = path;
+                } else {
+                    // SampleBssrdfProbe (src/integrators/bssrdf_probe.cpp:17-60): projection
+                    // axis, colour channel, radius, and the probe segment through the disk.
+                    const TabBssrdf tab = MakeTabBssrdf(dm, sc.bssrdf[dm.bssrdf_index]);
+                    float u1 = smp.Sample1D(kDimBssrdfAxis, depth);
+                    float ux, uy;
+                    smp.Sample2D(kDimBssrdfDisk, depth, ux, uy);
+                    V3 vx, vy, vz;
+                    if (u1 < 0.5f) {
+                        vx = ss, vy = ts, vz = ns;
+                        u1 *= 2.0f;
+                    } else if (u1 < 0.75f) {
+                        vx = ts, vy = ns, vz = ss;
+                        u1 = (u1 - 0.5f) * 4.0f;
+                    } else {
+                        vx = ns, vy = ss, vz = ts;
+                        u1 = (u1 - 0.75f) * 4.0f;
+                    }
+                    const int channel = min(max(static_cast<int>(u1 * 3.0f), 0), 2);
+                    u1 = u1 * 3.0f - static_cast<float>(channel);
+                    const float radius = BssrdfSampleSr(tab, channel, ux);
+                    if (radius >= 0.0f) {
+                        const float phi = 2.0f * kPi * uy;
+                        const float max_radius = BssrdfSampleSr(tab, channel, 0.999f);
+                        if (radius < max_radius) {
+                            const float length = 2.0f * sqrtf(fmaxf(0.0f, max_radius * max_radius - radius * radius));
+                            // cos/sin rounded from double precision: the correctly rounded
+                            // float values, as the host libm's float cos/sin return them.
+                            const float cphi = static_cast<float>(cos(static_cast<double>(phi)));
+                            const float sphi = static_cast<float>(sin(static_cast<double>(phi)));
+                            const V3 disk = vx * (radius * cphi) + vy * (radius * sphi);
+                            const V3 base = s.p + disk - vz * (length * 0.5f);
+                            const unsigned long long k = QueueAppend(q.counters + kCtrProbe);
+                            q.probe_ray[2 * k] = make_float4(base.x, base.y, base.z, 1.0e-5f);
+                            q.probe_ray[2 * k + 1] = make_float4(vz.x, vz.y, vz.z, length);
+                            q.probe_target[k] = make_int4(s.triangle ? s.prim : -1, s.triangle ? inst : -1,
+                                                          s.triangle ? -1 : -2 - id, path);
+                            q.probe_entry[2 * k] = ToF4(s.p, u1);
+                            q.probe_entry[2 * k + 1] = ToF4(ns, __int_as_float(s.material));
                         }
                     }
                 }
             }
-            if (EnvSampleable(sc.env)) {
-                float tx, ty;
-                smp.Sample2D(kDimDirectLightSurface, depth, tx, ty);
-                const EnvSample es = SampleEnvironment(sc.env, tx, ty);
-                if (es.valid && es.pdf > 0.0f && !IsBlack(es.radiance)) {
-                    const float cs = fmaxf(0.0f, Dot(n, es.dir));
-                    if (cs > 0.0f) {
-                        const V3 f = EvalBsdf(m, wo, es.dir, n, rng);
-                        if (!IsBlack(f)) {
-                            CountStat(q.counters, kStatShadow);
-                            const float pb = PdfBsdf(m, wo, es.dir, n, rng);
-                            const float mis = PowerHeuristic(1, es.pdf, 1, pb);
-                            ps.nee[3 * path + 2] = ToF4(Mul(f, es.radiance) * (cs * mis / es.pdf));
-                            PushShadow(q, s.p + n * SurfaceBias(s.p), es.dir, __int_as_float(0x7f800000),
-                                       3 * path + 2);
-                            any = true;
-                        }
-                    }
-                }
-            }
-            if (any) {
-                flags |= kPathNee;
-                ps.nee_tp[path] = ToF4(tp);
-                const unsigned long long k = QueueAppend(q.counters + kCtrNee);
-                q.nee_paths[k] = path;
-            }
+            ps.throughput[path] = ToF4(tp);
+            ps.radiance[path] = ToF4(rad);
+            ps.flags[path] = flags;
+            ps.rng_state[path] = rng.state;
+            continue;
         }
 
         bool cont = depth + 1 < sc.max_depth;
@@ -771,6 +852,88 @@ __global__ void ClearOcclusionKernel(Queues q, int64_t slots) {
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < slots;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         q.shadow_occluded[i] = 1;
+    }
+}
+
+// ---------------------------------------------------------- subsurface
+
+// The exit half of the subsurface branch (path_integrator.cpp:136-170,
+// bssrdf_probe.cpp:61-90): for each probe, the exit point among the target
+// hits the probe stage selected, Sp / pdf, next-event estimation at the exit
+// through the normalised Fresnel-weighted cosine lobe (Sw), and the
+// continuation sampled from that lobe.
+__global__ void SubsurfaceExitKernel(DevScene sc, PathState ps, Queues q, int depth) {
+    const int64_t n = static_cast<int64_t>(q.counters[kCtrProbe]);
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t hits = q.probe_count[k];
+        if (hits <= 0) continue;  // no exit: the path ends
+        const int32_t path = q.probe_target[k].w;
+        const float4 h = q.probe_hit[k];
+        const int32_t id = __float_as_int(h.y);
+        const V3 base = F4(q.probe_ray[2 * k]), vz = F4(q.probe_ray[2 * k + 1]);
+        const V3 pi = base + vz * h.x;
+        V3 ni;
+        if (id >= 0) {  // GeometricNormal of the triangle, object space (intersection.cpp:75-82)
+            const int4 tv = sc.tri_vertices[id];
+            const V3 p0 = VertexPos(sc, tv.x), p1 = VertexPos(sc, tv.y), p2 = VertexPos(sc, tv.z);
+            ni = Normalize(Cross(p1 - p0, p2 - p0));
+        } else {  // SphereNormal (intersection.cpp:136-143)
+            const float4 c = sc.spheres[-2 - id];
+            ni = Normalize(V3{pi.x - c.x, pi.y - c.y, pi.z - c.z});
+        }
+        const float4 e0 = q.probe_entry[2 * k], e1 = q.probe_entry[2 * k + 1];
+        const V3 po = F4(e0), ns = F4(e1);
+        const DevMaterial& dm = sc.materials[__float_as_int(e1.w)];
+        V3 ss, ts;
+        BssrdfFrame(ns, ss, ts);
+        const TabBssrdf tab = MakeTabBssrdf(dm, sc.bssrdf[dm.bssrdf_index]);
+        const V3 sp = BssrdfSr(tab, sqrtf(LengthSq(po - pi)));
+        const float pdf = BssrdfPdfSp(tab, po, ss, ts, ns, pi, ni) / static_cast<float>(hits);
+        if (!(pdf > 0.0f)) continue;
+        V3 tp = F4(ps.throughput[path]);
+        tp = Mul(tp, V3{sp.x / pdf, sp.y / pdf, sp.z / pdf});
+        if (IsBlack(tp)) {
+            ps.throughput[path] = ToF4(tp);
+            continue;
+        }
+        Mat mx{};
+        mx.kind = kSubsurfaceExit;
+        mx.ior = dm.bssrdf_eta;
+        uint32_t flags = ps.flags[path];
+        PixelSampler smp;
+        const int32_t pixel = ps.pixel[path];
+        smp.Init(sc.sampler, sc.seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
+        Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
+        NextEvent(sc, ps, q, path, smp, rng, depth, mx, pi, ni, ni, tp, flags);
+        float bx, by;
+        smp.Sample2D(kDimBssrdfExitBsdf, depth, bx, by);
+        const BsdfSample bs = SampleBsdf(mx, ni, ni, bx, by, rng);
+        bool cont = bs.valid && !IsBlack(bs.weight);
+        if (cont) {
+            tp = Mul(tp, bs.weight);
+            if (depth >= 3) {  // SurviveRussianRoulette
+                const float survival = Clampf(MaxComp(tp), 0.05f, 0.95f);
+                if (smp.Sample1D(kDimRussianRoulette, depth) >= survival) {
+                    cont = false;
+                } else {
+                    tp = tp / survival;
+                }
+            }
+        }
+        if (cont) {
+            flags = (flags | kPathPrevValid) & ~kPathPrevDelta;
+            ps.prev[path] = ToF4(pi, bs.pdf);
+            const V3 bn = Dot(bs.wi, ni) >= 0.0f ? ni : -ni;
+            const V3 no = pi + bn * SurfaceBias(pi);
+            const unsigned long long o = QueueAppend(q.counters + kCtrOut);
+            q.ray_out[2 * o] = make_float4(no.x, no.y, no.z, 1.0e-5f);
+            q.ray_out[2 * o + 1] = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, __int_as_float(0x7f800000));
+            q.path_out[o] = path;
+        }
+        ps.throughput[path] = ToF4(tp);
+        ps.flags[path] = flags;
+        ps.rng_state[path] = rng.state;
     }
 }
 
@@ -961,6 +1124,10 @@ void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, const
     ShadeKernel<kClassDielectric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
     ShadeKernel<kClassCoatedDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
     ShadeKernel<kClassGeneric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
+}
+void LaunchSubsurfaceExit(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
+                          int sm_count, cudaStream_t st) {
+    SubsurfaceExitKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
 }
 void LaunchCacheResolve(const PathState& ps, const CacheArgs& cache, int64_t capacity, int sm_count,
                         cudaStream_t st) {

@@ -36,6 +36,10 @@ void LaunchResetCounters(const Queues& q, cudaStream_t st);
 void LaunchAdvanceQueue(const Queues& q, cudaStream_t st);
 void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, const CacheArgs& cache, int depth,
                  int64_t capacity, int sm_count, cudaStream_t st);
+// Subsurface: close the probes traced by LaunchRenderProbe (exit point,
+// Sp / pdf, NEE at the exit, continuation).
+void LaunchSubsurfaceExit(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
+                          int sm_count, cudaStream_t st);
 // Radiance cache: add cached radiance to the paths that ended at the cache;
 // build the training records of the training paths.
 void LaunchCacheResolve(const PathState& ps, const CacheArgs& cache, int64_t capacity, int sm_count,

@@ -128,6 +128,7 @@ struct DevScene {
     uint64_t seed;
     float radiance_clamp;
     int32_t any_transparent;  // scene has Dielectric / ThinDielectric materials
+    int32_t any_subsurface;   // scene has Subsurface materials (probe stage needed)
 };
 
 // Path state, structure of arrays over `capacity` slots.
@@ -191,6 +192,17 @@ struct Queues {
     int32_t* shadow_slot; // path * 3 + light type
     uint8_t* shadow_occluded;
     int32_t* nee_paths;   // paths with pending NEE
+    // Subsurface probes (BSSRDF entry -> probe traversal -> exit), one per
+    // path at most: probe_ray 2 per entry (base.xyz + t_min, direction.xyz +
+    // length: the yrc_ray layout), target (mesh primitive, instance, sphere,
+    // path), probe_entry 2 per entry (entry point.xyz + selection sample,
+    // entry normal.xyz + material index bits); the probe stage writes the
+    // selected target hit (t, id, u, v) and the number of target hits.
+    float4* probe_ray;
+    int4* probe_target;
+    float4* probe_entry;
+    float4* probe_hit;
+    int32_t* probe_count;
     int32_t* order;       // extend-queue entries sorted by shading class
     uint8_t* shade_class; // shading class per extend-queue entry
     unsigned long long* counters;  // see kCounter*
@@ -202,6 +214,7 @@ enum CounterIndex {
     kCtrShadow = 2,
     kCtrNee = 3,
     kCtrClass0 = 4,  // entries per shading class (kShadeClasses of them)
+    kCtrProbe = 10,  // subsurface probes queued at this depth
     kCtrTrace = 12,  // traversal work counter
     kCtrShadowTrace = 13,
     kCtrPending = 14,  // shadow rays left for the transmittance pass

@@ -433,6 +433,63 @@ __global__ void __launch_bounds__(kTraceBlock) ProbeKernel(ProbeArgs args) {
     }
 }
 
+// SampleBssrdfProbe's probe (src/integrators/bssrdf_probe.cpp:51-66) for the
+// render path: IntersectAccelerationProbe's loop (closest-hit queries with an
+// advancing cursor, target hits kept in t order, at most kProbeMaxHits)
+// run twice per probe, first to count the target hits, then to return the
+// one the selection sample picks (floor(u * count), clamped), so no per-probe
+// hit list is stored.
+template <bool kTwo, int kTotal>
+__global__ void __launch_bounds__(kTraceBlock) RenderProbeKernel(RenderProbeArgs args) {
+    __shared__ int2 s_stack[kShortStack * kTraceBlock];
+    int2* col = s_stack + threadIdx.x;
+    StackStore<kTotal> st;
+    Traversal s;
+    const int64_t n = static_cast<int64_t>(*args.count_ptr);
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int4 target = args.targets[k];
+        const float t_min = Ld(args.rays + 2 * k).w;
+        const float t_max = Ld(args.rays + 2 * k + 1).w;
+        // pass == 0 counts; pass == 1 stops at the selected target hit
+        int32_t count = 0;
+        int32_t selected = -1;
+        float4 chosen = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1) {
+                if (count == 0) break;
+                const float u = args.selection[2 * k].w;
+                selected = min(max(static_cast<int32_t>(u * static_cast<float>(count)), 0), count - 1);
+            }
+            int32_t seen = 0;
+            float cursor = t_min;
+            for (int iter = 0; iter < kProbeMaxIterations; ++iter) {
+                bool alive = Begin(args.accel, args.rays, k, cursor, t_max, s);
+                while (alive) alive = Step<false, false, kTwo>(args.accel, args.rays, k, s, st, col, args.error);
+                if (!s.best.hit) break;
+                const bool inst_ok = !kTwo || target.y < 0 || s.best_inst == target.y;
+                const bool is_target = (target.x >= 0 && s.best.id >= 0 && s.best.prim == target.x && inst_ok) ||
+                                       (target.z >= 0 && s.best.id == -2 - target.z);
+                if (is_target) {
+                    if (seen >= kProbeMaxHits) break;
+                    if (pass == 1 && seen == selected) {
+                        chosen = make_float4(s.best.t, __int_as_float(s.best.id), s.best.u, s.best.v);
+                        break;
+                    }
+                    ++seen;
+                }
+                float next = __fadd_rn(s.best.t, __fmul_rn(1.0e-4f, __fadd_rn(1.0f, fabsf(s.best.t))));
+                if (!(next > cursor)) next = __fadd_rn(cursor, 1.0e-4f);
+                cursor = next;
+                if (cursor >= t_max) break;
+            }
+            if (pass == 0) count = seen;
+        }
+        args.hits[k] = count;
+        args.hit[k] = chosen;
+    }
+}
+
 // First pass of TraceShadowVisibility for every shadow ray: an any-hit
 // traversal that does not accept surfaces which pass light. Whatever the
 // order of the surfaces along the segment, the reference's loop ends occluded
@@ -725,6 +782,25 @@ cudaError_t LaunchShadowOne(const ShadowArgs& args, cudaStream_t stream, int sm_
 }
 
 }  // namespace
+
+template <bool kTwo, int kTotal>
+cudaError_t LaunchRenderProbeOne(const RenderProbeArgs& args, cudaStream_t stream, int sm_count) {
+    auto kernel = RenderProbeKernel<kTwo, kTotal>;
+    int64_t blocks = 0;
+    const cudaError_t err = PersistentGrid(kernel, kTraceBlock, args.capacity, sm_count, blocks);
+    if (err != cudaSuccess) return err;
+    kernel<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchRenderProbe(const RenderProbeArgs& args, cudaStream_t stream, int sm_count) {
+    const bool two = args.accel.two_level != 0;
+    const bool deep = args.accel.stack_limit > 64;
+    if (two) return deep ? LaunchRenderProbeOne<true, kMaxTraceStack>(args, stream, sm_count)
+                         : LaunchRenderProbeOne<true, 64>(args, stream, sm_count);
+    return deep ? LaunchRenderProbeOne<false, kMaxTraceStack>(args, stream, sm_count)
+                : LaunchRenderProbeOne<false, 64>(args, stream, sm_count);
+}
 
 cudaError_t LaunchShadowTransmittance(const ShadowArgs& args, cudaStream_t stream, int sm_count) {
     const bool two = args.accel.two_level != 0;

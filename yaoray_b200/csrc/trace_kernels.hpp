@@ -75,6 +75,24 @@ struct ShadowArgs {
     int* error;
 };
 
+// Subsurface probes of the render path: rays in the yrc_ray layout (t_min,
+// t_max = probe length), targets (mesh primitive, instance, sphere, path),
+// per probe a selection sample in selection[2 * k].w; outputs the selected
+// target hit and the number of target hits (<= kProbeMaxHits).
+struct RenderProbeArgs {
+    AccelParams accel;
+    const float4* rays;
+    const int4* targets;
+    const float4* selection;
+    const unsigned long long* count_ptr;
+    int64_t capacity;
+    float4* hit;
+    int32_t* hits;
+    int* error;
+};
+
+cudaError_t LaunchRenderProbe(const RenderProbeArgs& args, cudaStream_t stream, int sm_count);
+
 // Accessors of accelerator internals used by the render stages (accel.cu).
 AccelParams AccelParamsOf(const yrc_accel* a);
 int TraceShapeOf(const yrc_accel* a, int any_hit);

@@ -102,6 +102,12 @@ class Environment(C.Structure):
                 ("row_cdf", C.c_void_p), ("conditional_cdfs", C.c_void_p), ("total_weight", C.c_float)]
 
 
+class BssrdfTable(C.Structure):
+    _fields_ = [("rho_count", C.c_int32), ("radius_count", C.c_int32), ("rho_samples", C.c_void_p),
+                ("radius_samples", C.c_void_p), ("profile", C.c_void_p), ("rho_eff", C.c_void_p),
+                ("profile_cdf", C.c_void_p)]
+
+
 class Camera(C.Structure):
     _fields_ = [("origin", C.c_float * 3), ("forward", C.c_float * 3), ("right", C.c_float * 3),
                 ("up", C.c_float * 3), ("fov_y_radians", C.c_float)]
@@ -166,6 +172,7 @@ def _bind():
         ("yrc_render_scene_device_bytes", C.c_int64, [P]),
         ("yrc_render", C.c_int, [P, P, P, P, P]),
         ("yrc_render_scene_set_cache", C.c_int, [P, P, P]),
+        ("yrc_bssrdf_table_build", C.c_int, [C.c_float, C.c_float, C.c_int32, C.c_int32, P, P, P, P, P]),
         ("yrc_alias_table_build", C.c_int, [P, C.c_int32, P, P, P]),
         ("yrc_environment_distribution_build", C.c_int, [P, C.c_int32, C.c_int32, P, P, P, P, P]),
     ]:
@@ -209,6 +216,19 @@ class EnvironmentMap:
         self.total_weight = float(tot.value)
 
 
+def build_bssrdf_table(eta: float, g: float = 0.0, rho_count: int = 100, radius_count: int = 64) -> dict:
+    """ComputeBeamDiffusionBSSRDF (src/shading/bssrdf.cpp:124-151): the
+    profile table a subsurface material with relative index `eta` uses (the
+    reference's compiler builds 100 x 64 with g = 0)."""
+    t = {"rho_samples": np.zeros(rho_count, np.float32), "radius_samples": np.zeros(radius_count, np.float32),
+         "profile": np.zeros(rho_count * radius_count, np.float32), "rho_eff": np.zeros(rho_count, np.float32),
+         "profile_cdf": np.zeros(rho_count * radius_count, np.float32)}
+    check(_bind().yrc_bssrdf_table_build(g, eta, rho_count, radius_count, ptr(t["rho_samples"]),
+                                         ptr(t["radius_samples"]), ptr(t["profile"]), ptr(t["rho_eff"]),
+                                         ptr(t["profile_cdf"])))
+    return t
+
+
 def build_alias_table(weights: np.ndarray):
     """BuildAliasTable (src/lighting/light_sampling.cpp:148-183)."""
     w = np.ascontiguousarray(weights, np.float32)
@@ -238,6 +258,7 @@ class RenderScene:
     emissive: np.ndarray = field(default_factory=lambda: np.zeros(0, EMISSIVE_DTYPE))
     alias: tuple | None = None                 # (probability, alias, pmf) over emissive power
     environment: EnvironmentMap = field(default_factory=EnvironmentMap)
+    bssrdf_tables: list = field(default_factory=list)  # build_bssrdf_table() dicts, by bssrdf_index
     adaptive: dict | None = None               # enabled/min_spp/relative_error/absolute_error/confidence
 
     def emissive_power_alias(self):
@@ -329,6 +350,17 @@ class PreparedScene:
             e.conditional_cdfs = ptr(env.conditional_cdfs)
             e.total_weight = env.total_weight
         d.environment = e
+        if scene.bssrdf_tables:
+            tabs = (BssrdfTable * len(scene.bssrdf_tables))()
+            for i, t in enumerate(scene.bssrdf_tables):
+                arrays = {k: np.ascontiguousarray(v, np.float32) for k, v in t.items()}
+                self._keep.append(arrays)
+                tabs[i] = BssrdfTable(arrays["rho_samples"].size, arrays["radius_samples"].size,
+                                      ptr(arrays["rho_samples"]), ptr(arrays["radius_samples"]),
+                                      ptr(arrays["profile"]), ptr(arrays["rho_eff"]), ptr(arrays["profile_cdf"]))
+            self._keep.append(tabs)
+            d.bssrdf_tables = C.addressof(tabs)
+            d.bssrdf_count = len(scene.bssrdf_tables)
         cam = scene.camera
         d.camera = Camera((C.c_float * 3)(*cam["origin"]), (C.c_float * 3)(*cam["forward"]),
                           (C.c_float * 3)(*cam["right"]), (C.c_float * 3)(*cam["up"]), cam["fov_y_radians"])
