@@ -528,12 +528,78 @@ def run_nrc(args):
     print(json.dumps(line), flush=True)
 
 
+def run_jobs(args):
+    """--workload jobs: 48 uneven render jobs (resolutions 128^2..1024^2, spp
+    16..1024 scaled by --spp-scale, 10K-2M-triangle sphere-mesh scenes with
+    the instanced material mix plus subsurface, half with a radiance cache),
+    rendered once untimed (allocation and graph capture), then one at a time
+    and concurrently (device-memory admission, --concurrency workers). value = aggregate samples/s of the concurrent
+    run; the line also carries per-job latency p50/p99 of both runs."""
+    import torch
+    from yaoray_b200 import batch
+
+    t0 = time.perf_counter()
+    jobs = batch.job_set(48, seed=7, spp_scale=args.spp_scale)
+    runner = batch.JobRunner()
+    runner.prepare(jobs)
+    prepare_s = time.perf_counter() - t0
+    runner.run_sequential(jobs)  # warm-up: allocates and captures every job's batch graph
+    seq = runner.run_sequential(jobs)
+    seq_lat = seq.latency_quantiles()
+    seq_sps = seq.samples_per_s
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clocks:
+        conc = runner.run_concurrent(jobs, concurrency=args.concurrency)
+    conc_lat = conc.latency_quantiles()
+    failed = [j.name for j in jobs if not j.ok]
+    runner.close(jobs)
+    tris = [j.scene.geometry.triangle_count for j in jobs]
+    film_bytes = sum(j.scene.width * j.scene.height * 56 for j in jobs)
+    base = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle
+        if oracle.ref_available():
+            # The plain subset (jobs without a cache), one after another at 32 spp.
+            plain = [j for j in jobs if not j.use_cache][:8]
+            n, secs = 0, 0.0
+            for j in plain:
+                film, st, dt = oracle.RefJob.from_scene(j.scene).render(spp=32)
+                n += j.scene.width * j.scene.height * 32
+                secs += dt
+            base = {"value": round(n / secs, 1), "unit": "samples/s", "cores": os.cpu_count(), "kind": "reference",
+                    "sample": f"reference CpuBackend, the first {len(plain)} jobs without a cache, 32 spp each, "
+                              f"one after another ({secs:.2f} s)"}
+    line = {"metric": "samples/s (48 batched uneven render jobs)", "value": round(conc.samples_per_s, 1),
+            "unit": "samples/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": round(conc.wall_s * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "jobs48-128..1024px-16..1024spp-10K..2M-tris", "jobs": len(jobs),
+                       "spp_scale": args.spp_scale, "concurrency": args.concurrency,
+                       "triangles_min_max": [min(tris), max(tris)], "with_radiance_cache": sum(j.use_cache for j in jobs),
+                       "samples_total": conc.samples, "prepare_seconds": round(prepare_s, 2),
+                       "admission_budget_gb": round(conc.extra.get("budget_bytes", 0) / 2**30, 1),
+                       "peak_concurrent_jobs": conc.peak_concurrency},
+            "one_at_a_time": {"samples_per_s": round(seq_sps, 1), "wall_s": round(seq.wall_s, 3),
+                              "latency_p50_s": seq_lat["p50"], "latency_p99_s": seq_lat["p99"]},
+            "concurrent": {"samples_per_s": round(conc.samples_per_s, 1), "wall_s": round(conc.wall_s, 3),
+                           "latency_p50_s": conc_lat["p50"], "latency_p99_s": conc_lat["p99"]},
+            "failed_jobs": failed,
+            "e2e": {"value": round(conc.samples_per_s, 1), "unit": "samples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": film_bytes,
+                    "note": "value is already host wall clock around the CudaBackend.render calls, films read back"},
+            "cpu_baseline": base, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--workload", choices=["traversal", "cornell", "instanced", "nrc"], default="traversal")
+    ap.add_argument("--workload", choices=["traversal", "cornell", "instanced", "nrc", "jobs"], default="traversal")
     ap.add_argument("--nrc-width", type=int, default=960)
     ap.add_argument("--nrc-height", type=int, default=540)
     ap.add_argument("--ref-spp", type=int, default=512)
+    ap.add_argument("--spp-scale", type=float, default=1.0, help="spp scale of --workload jobs")
+    ap.add_argument("--concurrency", type=int, default=8, help="concurrent jobs of --workload jobs")
     ap.add_argument("--render-spp", type=int, default=16, help="spp per step of --workload instanced")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -552,6 +618,8 @@ def main():
         run_render(args)
     elif args.workload == "nrc":
         run_nrc(args)
+    elif args.workload == "jobs":
+        run_jobs(args)
     else:
         run_gpu(args)
 

@@ -1,0 +1,71 @@
+"""Batched uneven render jobs: the workload generator and the admission
+scheduler (host logic, no GPU: renders are replaced by a timed stub)."""
+import threading
+import time
+
+import numpy as np
+
+from yaoray_b200 import batch
+
+
+def test_job_set_shapes():
+    jobs = batch.job_set(8, seed=3, spp_scale=1 / 16, max_triangles=200_000)
+    assert len(jobs) == 8
+    for j in jobs:
+        s = j.scene
+        assert s.width in batch.RESOLUTIONS and s.height == s.width
+        assert 1 <= s.spp <= 1024 // 16
+        assert 10_000 <= s.geometry.triangle_count <= 200_000 + 4096
+        assert s.materials.size >= 5 and s.bssrdf_tables and s.radiance_clamp == 20.0
+        mi = s.geometry.primitives["material_index"]
+        assert mi.min() >= 0 and mi.max() < s.materials.size
+    assert [j.use_cache for j in jobs] == [False, True] * 4
+    again = batch.job_set(8, seed=3, spp_scale=1 / 16, max_triangles=200_000)
+    assert [j.name for j in again] == [j.name for j in jobs]
+    assert np.array_equal(again[5].scene.geometry.positions, jobs[5].scene.geometry.positions)
+
+
+class _StubRunner(batch.JobRunner):
+    """Renders by sleeping in proportion to the job's samples and records
+    the summed working set of the jobs running at once."""
+
+    def __init__(self):
+        super().__init__()
+        self.lock = threading.Lock()
+        self.live = 0
+        self.max_live = 0
+
+    def _render(self, job):
+        need = batch._working_set(job)
+        with self.lock:
+            self.live += need
+            self.max_live = max(self.max_live, self.live)
+        time.sleep(0.002 + 1e-9 * job.scene.width * job.scene.height * job.scene.spp)
+        with self.lock:
+            self.live -= need
+        job.ok, job.samples, job.latency_s = True, job.scene.width * job.scene.height * job.scene.spp, 0.01
+
+
+def test_admission_respects_budget():
+    jobs = batch.job_set(12, seed=5, spp_scale=1 / 64, max_triangles=50_000)
+    need = sorted(batch._working_set(j) for j in jobs)
+    budget = need[-1] + need[-2] // 2  # the two largest never run together
+    r = _StubRunner()
+    res = r.run_concurrent(jobs, concurrency=6, budget_bytes=budget)
+    assert all(j.ok for j in jobs)
+    assert r.max_live <= budget
+    assert res.samples == sum(j.samples for j in jobs)
+    assert 1 <= res.peak_concurrency <= 6
+    # With a budget that fits everything, the pool runs several jobs at once.
+    r2 = _StubRunner()
+    res2 = r2.run_concurrent(jobs, concurrency=6, budget_bytes=sum(need))
+    assert res2.peak_concurrency > 1
+    q = res2.latency_quantiles()
+    assert q["p50"] == 0.01 and q["p99"] == 0.01
+
+
+def test_oversized_job_runs_alone():
+    jobs = batch.job_set(4, seed=9, spp_scale=1 / 64, max_triangles=50_000)
+    r = _StubRunner()
+    res = r.run_concurrent(jobs, concurrency=4, budget_bytes=1)
+    assert all(j.ok for j in jobs) and res.peak_concurrency == 1
