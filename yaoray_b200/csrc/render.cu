@@ -99,7 +99,6 @@ struct yrc_render_scene {
     yrc::PathState ps{};
     yrc::Queues q{};
     float4* transmittance = nullptr;
-    int32_t* shadow_pending = nullptr;  // shadow rays (2 per path) left for the transmittance pass
     yrc_film_pixel* film = nullptr;
     int32_t* attempts = nullptr;
     int32_t* active = nullptr;
@@ -512,7 +511,6 @@ yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     q.shade_class = W.Alloc<uint8_t>(capacity);
     q.counters = W.Alloc<unsigned long long>(kCtrCount);
     s->transmittance = s->dev.any_transparent ? W.Alloc<float4>(3 * capacity) : nullptr;
-    s->shadow_pending = s->dev.any_transparent ? W.Alloc<int32_t>(2 * capacity) : nullptr;
     if (s->dev.any_subsurface) {
         q.probe_ray = W.Alloc<float4>(2 * capacity);
         q.probe_target = W.Alloc<int4>(capacity);
@@ -650,10 +648,7 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
             sa.materials = sc.materials;
             sa.tri_clear = sc.tri_clear;
             sa.sphere_clear = sc.sphere_clear;
-            sa.pending = s->shadow_pending;
-            sa.pending_count = q.counters + kCtrPending;
             sa.counter = q.counters + kCtrShadowTrace;
-            sa.exact_counter = q.counters + kCtrExact;
             sa.occluded_count = q.counters + kCtrStatsBase + 2;
             sa.error = ta.error;
             err = LaunchShadowTransmittance(sa, st, s->sm_count);

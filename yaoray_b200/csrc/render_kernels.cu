@@ -141,8 +141,6 @@ __global__ void ResetCountersKernel(Queues q) {
         q.counters[kCtrNee] = 0;
         q.counters[kCtrTrace] = 0;
         q.counters[kCtrShadowTrace] = 0;
-        q.counters[kCtrPending] = 0;
-        q.counters[kCtrExact] = 0;
         q.counters[kCtrProbe] = 0;
         for (int c = 0; c < kShadeClasses; ++c) {
             q.counters[kCtrClass0 + c] = 0;

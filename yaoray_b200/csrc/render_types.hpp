@@ -217,8 +217,6 @@ enum CounterIndex {
     kCtrProbe = 10,  // subsurface probes queued at this depth
     kCtrTrace = 12,  // traversal work counter
     kCtrShadowTrace = 13,
-    kCtrPending = 14,  // shadow rays left for the transmittance pass
-    kCtrExact = 15,    // work counter of the transmittance pass
     kCtrStatsBase = 16,  // rays, shadow rays, occluded, hits, misses, bad
     kCtrCursor0 = 24,  // scatter cursors per shading class
     kCtrCount = 32,

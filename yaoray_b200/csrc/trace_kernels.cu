@@ -162,16 +162,54 @@ __device__ __forceinline__ bool Pop(const float4* rays, int64_t ray, Traversal& 
     }
 }
 
+// The clear surfaces (those that pass light) a filtered any-hit traversal
+// skipped: the lane's kClearHits nearest as (t, surface id) pairs, ordered by
+// t then id, in the block's shared memory laid out [entry][thread]. More than
+// kClearHits of them never matter: the reference's shadow loop gives up after
+// that many queries.
+constexpr int kClearHits = 16;  // MaxTransparentShadowHits
+
+struct ClearHits {
+    float* t;     // the lane's column, stride kTraceBlock
+    int32_t* id;
+    int n;        // entries held (<= kClearHits)
+    bool dropped; // a farther clear surface did not fit
+
+    __device__ __forceinline__ void Add(float tv, int32_t idv) {
+        int j = n;  // slot the new entry would take; kClearHits = past the end
+        while (j > 0) {
+            const float tp = t[(j - 1) * kTraceBlock];
+            const int32_t ip = id[(j - 1) * kTraceBlock];
+            if (tp < tv || (tp == tv && ip < idv)) break;
+            if (j < kClearHits) {
+                t[j * kTraceBlock] = tp;
+                id[j * kTraceBlock] = ip;
+            } else {
+                dropped = true;
+            }
+            --j;
+        }
+        if (j < kClearHits) {
+            t[j * kTraceBlock] = tv;
+            id[j * kTraceBlock] = idv;
+        } else {
+            dropped = true;
+        }
+        if (n < kClearHits) ++n;
+    }
+};
+
 // One traversal step: an interior node (test both children) or a leaf (test
 // its records). Returns false when the ray's traversal is complete.
 //
 // kFilter (any-hit only): candidates on surfaces flagged in `tri_clear` /
 // `sphere_clear` are not accepted; the traversal records that it skipped one
-// (s.saw) and goes on, so it ends at the first hit on any other surface.
+// (s.saw), adds it to `clear` and goes on, so it ends at the first hit on any
+// other surface.
 template <bool kAny, bool kStats, bool kTwo, typename Stack, bool kFilter = false>
 __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, int64_t ray, Traversal& s, Stack& st,
                                      int2* col, int* error, const uint8_t* tri_clear = nullptr,
-                                     const uint8_t* sphere_clear = nullptr) {
+                                     const uint8_t* sphere_clear = nullptr, ClearHits* clear = nullptr) {
     const bool in_blas = kTwo && s.level == 1;
     if (s.cur >= 0) {
         const float4* p = reinterpret_cast<const float4*>(a.pairs + s.cur);
@@ -227,6 +265,7 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
                 if (kAny && acc && s.local.t < s.best.t) {
                     if (kFilter && tri_clear[s.local.id]) {
                         s.saw = true;
+                        clear->Add(s.local.t, s.local.id);
                         s.local = keep;
                     } else {
                         s.best = s.local;
@@ -240,6 +279,7 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
                 if (kAny && acc) {
                     if (kFilter && tri_clear[s.best.id]) {
                         s.saw = true;
+                        clear->Add(s.best.t, s.best.id);
                         s.best = keep;
                     } else {
                         return false;
@@ -254,6 +294,7 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
                 if (kAny && acc && s.local.t < s.best.t) {
                     if (kFilter && sphere_clear[-2 - s.local.id]) {
                         s.saw = true;
+                        clear->Add(s.local.t, s.local.id);
                         s.local = keep;
                     } else {
                         s.best = s.local;
@@ -268,6 +309,7 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
                 if (kAny && acc) {
                     if (kFilter && sphere_clear[-2 - s.best.id]) {
                         s.saw = true;
+                        clear->Add(s.best.t, s.best.id);
                         s.best = keep;
                     } else {
                         return false;
@@ -490,37 +532,136 @@ __global__ void __launch_bounds__(kTraceBlock) RenderProbeKernel(RenderProbeArgs
     }
 }
 
-// First pass of TraceShadowVisibility for every shadow ray: an any-hit
-// traversal that does not accept surfaces which pass light. Whatever the
-// order of the surfaces along the segment, the reference's loop ends occluded
-// (zero) as soon as an opaque surface lies on it, and returns full visibility
-// when its first query finds nothing; so a ray that hits an opaque surface
-// gets 0, a ray that met no surface at all gets 1, and only the rest (clear
-// surfaces and no opaque one) go to the pending list for the exact loop.
-// Persistent warps with per-lane refill, like TraceKernel.
+// TraceShadowVisibility (src/integrators/path_direct_lighting.cpp:23-113)
+// for every shadow ray in one traversal. The reference runs up to 16
+// closest-hit queries along the segment, each from just past the previous
+// hit: an opaque surface occludes, a Dielectric toggles a Beer-Lambert
+// medium, a ThinDielectric multiplies by its clamped reflectance. Here one
+// any-hit traversal over the whole segment skips the surfaces that pass light
+// and keeps the nearest 16 of them (ClearHits); it stops at the first opaque
+// surface, which gives 0 whatever lies before it (the loop reaches it or
+// turns black, or gives up at 16 queries — all occluded). With no surface at
+// all the ray is fully visible. Otherwise the reference's loop is replayed
+// over the kept list in t order: each query returns the first kept surface
+// beyond the query's origin plus t_min (1e-5), t measured from that origin,
+// with the same bias, remaining-distance and 16-query rules. What differs
+// from re-tracing is rounding: t is the traversal's t from the ray origin
+// less the distance already advanced, not a new intersection from the
+// re-spawned origin. Persistent warps with per-lane refill, like TraceKernel.
 template <bool kTwo, int kTotal>
-__global__ void __launch_bounds__(kTraceBlock) ShadowFilterKernel(ShadowArgs args) {
+__global__ void __launch_bounds__(kTraceBlock) ShadowTransmittanceKernel(ShadowArgs args) {
     __shared__ int2 s_stack[kShortStack * kTraceBlock];
+    __shared__ float s_clear_t[kClearHits * kTraceBlock];
+    __shared__ int32_t s_clear_id[kClearHits * kTraceBlock];
     int2* col = s_stack + threadIdx.x;
     StackStore<kTotal> st;
     Traversal s;
+    ClearHits clear{s_clear_t + threadIdx.x, s_clear_id + threadIdx.x, 0, false};
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
     int64_t ray = -1;
     bool alive = false;
     bool exhausted = false;
     const unsigned long long count = *args.count_ptr;
+
+    // The reference loop over the kept clear surfaces; returns the RGB
+    // transmittance, w = 1 when visible, all 0 when occluded.
+    auto replay = [&]() -> float4 {
+        const float4 ra = Ld(args.rays + 2 * ray);
+        const float4 rb = Ld(args.rays + 2 * ray + 1);
+        float o[3] = {ra.x, ra.y, ra.z};
+        const float d[3] = {rb.x, rb.y, rb.z};
+        float remaining = rb.w;
+        float T[3] = {1.0f, 1.0f, 1.0f}, mc[3] = {1.0f, 1.0f, 1.0f}, md = 1.0f;
+        bool medium = false;
+        float qmin = ra.w;   // t_min of the current query
+        float off = 0.0f;    // distance from the ray origin to the current query's origin
+        const float4 occluded = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        auto black = [&]() { return fmaxf(T[0], fmaxf(T[1], T[2])) <= 1.0e-6f; };
+        auto beer = [&](float dist) {
+            if (dist <= 0.0f || md <= 0.0f) return;
+            const float inv = 1.0f / md;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float c = fminf(fmaxf(mc[k], 1.0e-6f), 1.0f);
+                T[k] = T[k] * expf(logf(c) * dist * inv);
+            }
+        };
+        int k = 0;
+        for (int query = 0; query < kClearHits; ++query) {
+            const bool finite = isfinite(remaining);
+            float t = 0.0f;
+            int32_t id = 0;
+            bool found = false;
+            for (; k < clear.n; ++k) {
+                t = __fsub_rn(clear.t[k * kTraceBlock], off);
+                if (t > qmin && t <= remaining) {
+                    id = clear.id[k * kTraceBlock];
+                    found = true;
+                    ++k;
+                    break;
+                }
+            }
+            if (!found) {
+                // A surface beyond the kept ones would be this query's answer.
+                if (clear.dropped) return occluded;
+                if (medium) {
+                    if (!finite) return occluded;
+                    beer(remaining);
+                }
+                return black() ? occluded : make_float4(T[0], T[1], T[2], 1.0f);
+            }
+            if (medium) {
+                beer(t);
+                if (black()) return occluded;
+            }
+            const int32_t material = id >= 0 ? args.prim_material[args.tri_prim[id]] : args.sphere_material[-2 - id];
+            if (material < 0 || (args.materials[material].kind != 2 && args.materials[material].kind != 3)) {
+                return occluded;
+            }
+            const DevMaterial& m = args.materials[material];
+            float hp[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) hp[c] = __fadd_rn(o[c], __fmul_rn(d[c], t));
+            if (m.kind == 3) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) T[c] = T[c] * fminf(fmaxf(m.reflectance[c], 0.0f), 1.0f);
+                if (black()) return occluded;
+            } else if (medium) {
+                medium = false;
+                mc[0] = mc[1] = mc[2] = 1.0f;
+                md = 1.0f;
+            } else {
+                medium = true;
+                mc[0] = m.absorption_color[0];
+                mc[1] = m.absorption_color[1];
+                mc[2] = m.absorption_color[2];
+                md = m.absorption_distance;
+            }
+            const float bias = fmaxf(1.0e-4f, fmaxf(fabsf(hp[0]), fmaxf(fabsf(hp[1]), fabsf(hp[2]))) * 1.0e-5f);
+            if (finite) {
+                remaining = __fsub_rn(remaining, __fadd_rn(t, bias));
+                if (remaining <= 0.0f) return black() ? occluded : make_float4(T[0], T[1], T[2], 1.0f);
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) o[c] = __fadd_rn(hp[c], __fmul_rn(d[c], bias));
+            off = __fadd_rn(off, __fadd_rn(t, bias));
+            qmin = 1.0e-5f;
+        }
+        return occluded;  // the reference gives up after 16 queries
+    };
     auto finish = [&]() {
         const int32_t slot = args.out_index[ray];
+        float4 tr;
         if (s.best.hit) {
-            args.transmittance[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            CountLanes(args.occluded_count);
+            tr = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         } else if (!s.saw) {
-            args.transmittance[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+            tr = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
         } else {
-            const unsigned long long k = atomicAdd(args.pending_count, 1ull);
-            args.pending[k] = static_cast<int32_t>(ray);
+            tr = replay();
         }
+        args.transmittance[slot] = tr;
+        if (tr.w == 0.0f) CountLanes(args.occluded_count);
     };
     for (;;) {
         const unsigned need = __ballot_sync(kFull, !alive && !exhausted);
@@ -539,6 +680,8 @@ __global__ void __launch_bounds__(kTraceBlock) ShadowFilterKernel(ShadowArgs arg
                     ray = static_cast<int64_t>(idx);
                     const float4 b = Ld(args.rays + 2 * ray + 1);
                     const float tmin = Ld(args.rays + 2 * ray).w;
+                    clear.n = 0;
+                    clear.dropped = false;
                     alive = Begin(args.accel, args.rays, ray, tmin, b.w, s);
                     if (!alive) finish();
                 }
@@ -550,165 +693,9 @@ __global__ void __launch_bounds__(kTraceBlock) ShadowFilterKernel(ShadowArgs arg
         }
 #pragma unroll 1
         for (int k = 0; k < 8 && alive; ++k) {
-            alive = Step<true, false, kTwo, StackStore<kTotal>, true>(args.accel, args.rays, ray, s, st, col,
-                                                                     args.error, args.tri_clear, args.sphere_clear);
+            alive = Step<true, false, kTwo, StackStore<kTotal>, true>(
+                args.accel, args.rays, ray, s, st, col, args.error, args.tri_clear, args.sphere_clear, &clear);
             if (!alive) finish();
-        }
-    }
-}
-
-// TraceShadowVisibility (src/integrators/path_direct_lighting.cpp:23-113):
-// up to 16 closest-hit queries along the shadow segment; Dielectric surfaces
-// toggle a Beer-Lambert medium, ThinDielectric ones multiply by their clamped
-// reflectance, anything else occludes. One thread per shadow ray of the
-// pending list (the rays ShadowFilterKernel could not settle); writes the RGB
-// transmittance (0 when occluded) to transmittance[out_index[i]].
-template <bool kTwo, int kTotal>
-__global__ void __launch_bounds__(kTraceBlock) ShadowTransmittanceKernel(ShadowArgs args) {
-    __shared__ int2 s_stack[kShortStack * kTraceBlock];
-    int2* col = s_stack + threadIdx.x;
-    StackStore<kTotal> st;
-    Traversal s;
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned lt_mask = (1u << lane) - 1u;
-    const unsigned long long count = *args.pending_count;
-    // Per-lane loop state of the reference's query loop; a lane that finishes
-    // its ray takes the next pending one (persistent warps, per-lane refill).
-    int64_t i = -1;
-    float o[3], d[3], remaining = 0.0f, T[3], mc[3], md = 1.0f;
-    bool medium = false;
-    int hitc = 0;
-    bool active = false, alive = false, exhausted = false;
-    auto black = [&]() { return fmaxf(T[0], fmaxf(T[1], T[2])) <= 1.0e-6f; };
-    auto beer = [&](float dist) {
-        if (dist <= 0.0f || md <= 0.0f) return;
-        const float inv = 1.0f / md;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float c = fminf(fmaxf(mc[k], 1.0e-6f), 1.0f);
-            T[k] = T[k] * expf(logf(c) * dist * inv);
-        }
-    };
-    auto write = [&](bool visible) {
-        args.transmittance[args.out_index[i]] =
-            visible ? make_float4(T[0], T[1], T[2], 1.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (!visible) CountLanes(args.occluded_count);
-        active = false;
-    };
-    // The loop body after one closest-hit query; returns true when the next
-    // query's traversal started, false when the ray's result was written.
-    auto resolve = [&]() -> bool {
-        for (;;) {
-            const bool finite = isfinite(remaining);
-            if (!s.best.hit) {
-                if (medium) {
-                    if (!finite) {  // occluded
-                        write(false);
-                        return false;
-                    }
-                    beer(remaining);
-                }
-                write(!black());
-                return false;
-            }
-            const float t = s.best.t;
-            if (medium) {
-                beer(t);
-                if (black()) {
-                    write(false);
-                    return false;
-                }
-            }
-            int32_t material = -1;
-            if (s.best.id >= 0) {
-                material = args.prim_material[args.tri_prim[s.best.id]];
-            } else {
-                material = args.sphere_material[-2 - s.best.id];
-            }
-            // Invalid or default (opaque diffuse) material, or a kind other
-            // than Dielectric / ThinDielectric: occluded.
-            if (material < 0 || (args.materials[material].kind != 2 && args.materials[material].kind != 3)) {
-                write(false);
-                return false;
-            }
-            const DevMaterial& m = args.materials[material];
-            float hp[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) hp[k] = __fadd_rn(o[k], __fmul_rn(d[k], t));
-            if (m.kind == 3) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) T[k] = T[k] * fminf(fmaxf(m.reflectance[k], 0.0f), 1.0f);
-                if (black()) {
-                    write(false);
-                    return false;
-                }
-            } else if (medium) {
-                medium = false;
-                mc[0] = mc[1] = mc[2] = 1.0f;
-                md = 1.0f;
-            } else {
-                medium = true;
-                mc[0] = m.absorption_color[0];
-                mc[1] = m.absorption_color[1];
-                mc[2] = m.absorption_color[2];
-                md = m.absorption_distance;
-            }
-            const float bias = fmaxf(1.0e-4f, fmaxf(fabsf(hp[0]), fmaxf(fabsf(hp[1]), fabsf(hp[2]))) * 1.0e-5f);
-            if (finite) {
-                remaining = __fsub_rn(remaining, __fadd_rn(t, bias));
-                if (remaining <= 0.0f) {
-                    write(!black());
-                    return false;
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) o[k] = __fadd_rn(hp[k], __fmul_rn(d[k], bias));
-            if (++hitc >= 16) {  // the reference gives up after 16 queries: occluded
-                write(false);
-                return false;
-            }
-            if (BeginRay(args.accel, o, d, 1.0e-5f, remaining, s)) return true;
-        }
-    };
-    for (;;) {
-        const unsigned need = __ballot_sync(kFull, !active && !exhausted);
-        if (need) {
-            unsigned long long base = 0;
-            const int leader = __ffs(need) - 1;
-            if (static_cast<int>(lane) == leader) {
-                base = atomicAdd(args.exact_counter, static_cast<unsigned long long>(__popc(need)));
-            }
-            base = __shfl_sync(kFull, base, leader);
-            if (!active && !exhausted) {
-                const unsigned long long idx = base + __popc(need & lt_mask);
-                if (idx >= count) {
-                    exhausted = true;
-                } else {
-                    i = args.pending[idx];
-                    const float4 ra = Ld(args.rays + 2 * i);
-                    const float4 rb = Ld(args.rays + 2 * i + 1);
-                    o[0] = ra.x, o[1] = ra.y, o[2] = ra.z;
-                    d[0] = rb.x, d[1] = rb.y, d[2] = rb.z;
-                    remaining = rb.w;
-                    T[0] = T[1] = T[2] = 1.0f;
-                    mc[0] = mc[1] = mc[2] = 1.0f;
-                    md = 1.0f;
-                    medium = false;
-                    hitc = 0;
-                    active = true;
-                    alive = BeginRay(args.accel, o, d, 1.0e-5f, remaining, s);
-                    if (!alive) alive = resolve();
-                }
-            }
-        }
-        if (!__any_sync(kFull, alive)) {
-            if (__all_sync(kFull, exhausted)) break;
-            continue;
-        }
-#pragma unroll 1
-        for (int k = 0; k < 8 && alive; ++k) {
-            alive = Step<false, false, kTwo>(args.accel, args.rays, i, s, st, col, args.error);
-            if (!alive) alive = resolve();
         }
     }
 }
@@ -769,15 +756,11 @@ cudaError_t LaunchProbeOne(const ProbeArgs& args, cudaStream_t stream, int sm_co
 
 template <bool kTwo, int kTotal>
 cudaError_t LaunchShadowOne(const ShadowArgs& args, cudaStream_t stream, int sm_count) {
-    auto filter = ShadowFilterKernel<kTwo, kTotal>;
+    auto kernel = ShadowTransmittanceKernel<kTwo, kTotal>;
     int64_t blocks = 0;
-    cudaError_t err = PersistentGrid(filter, kTraceBlock, args.capacity, sm_count, blocks);
+    const cudaError_t err = PersistentGrid(kernel, kTraceBlock, args.capacity, sm_count, blocks);
     if (err != cudaSuccess) return err;
-    filter<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
-    auto exact = ShadowTransmittanceKernel<kTwo, kTotal>;
-    err = PersistentGrid(exact, kTraceBlock, args.capacity, sm_count, blocks);
-    if (err != cudaSuccess) return err;
-    exact<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
+    kernel<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
     return cudaGetLastError();
 }
 

@@ -67,10 +67,7 @@ struct ShadowArgs {
     const DevMaterial* materials;
     const uint8_t* tri_clear;             // per flat triangle: passes light (1) or occludes (0)
     const uint8_t* sphere_clear;          // per sphere
-    int32_t* pending;                     // capacity entries: rays left for the transmittance pass
-    unsigned long long* pending_count;    // zeroed before the launch
-    unsigned long long* counter;          // ray work counter of the filtered any-hit pass, zeroed before
-    unsigned long long* exact_counter;    // ray work counter of the transmittance pass, zeroed before
+    unsigned long long* counter;          // ray work counter, zeroed before the launch
     unsigned long long* occluded_count;   // shadow rays found not visible (RenderStats::occluded_shadow_rays)
     int* error;
 };
