@@ -438,37 +438,41 @@ def run_nrc(args):
 
     Reference: `--ref-spp` samples per pixel of the plain tracer, accumulated
     in FP64 over renders of different seeds. Plain curve: renders of 1..64
-    spp. Cached renders: a fresh cache trained online by 8 renders of 2 spp
-    (4 optimiser steps per batch; its time is reported separately), then
-    renders of 1, 4 and 16 spp that keep training (1 step per batch). Every
-    timing is the device time of the second render of a prepared scene (the
+    spp. Cached: a fresh cache trained online by 32 warm-up frames of 2 spp
+    (a new sampler seed per frame, 4 optimiser steps per batch; their time is
+    reported separately), then renders of 1, 4 and 16 spp that keep training
+    (1 step per batch) and query the moving average of the cache's
+    parameters. Every relMSE is the mean over three sampler seeds, every
+    time the mean device time of the second render of a prepared scene (the
     first captures the batch graph). For each cached render, the time the
     plain tracer needs for the same relMSE is interpolated on its log-log
     time/error curve; value = that time / the cached render's time at 16 spp."""
+    import dataclasses
+
     import torch
     from yaoray_b200 import instanced
     from yaoray_b200.nrc import RadianceCache
-    from yaoray_b200.render import CudaBackend
+    from yaoray_b200.render import CudaBackend, build_two_level_bvh
 
-    W, H, CLAMP, C_SPREAD = args.nrc_width, args.nrc_height, 20.0, 0.001
+    W, H, CLAMP, C_SPREAD, DECAY, WARM = args.nrc_width, args.nrc_height, 20.0, 1.0e-4, 0.995, 32
+    SEEDS = (7, 8, 9)
+    base = instanced.scene(width=W, height=H, spp=1)
+    base.radiance_clamp = CLAMP
+    accel = build_two_level_bvh(base.geometry)
 
     def scene(spp, seed):
-        s = instanced.scene(width=W, height=H, spp=spp)
-        s.radiance_clamp = CLAMP
-        s.seed = seed
-        return s
+        return dataclasses.replace(base, spp=spp, seed=seed)
 
     def relmse(img, ref):
         return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
 
     backend = CudaBackend()
-    base = scene(1, 0)
     lo = base.geometry.positions.min(0)
     extent = float((base.geometry.positions.max(0) - lo).max())
     ref = np.zeros((H, W, 3), np.float64)
     per = 128
     for k in range(max(1, args.ref_spp // per)):
-        p = backend.prepare(scene(per, 1000 + k))
+        p = backend.prepare(scene(per, 1000 + k), accel)
         ref += backend.render(p).linear()
         p.close()
     ref /= max(1, args.ref_spp // per)
@@ -481,23 +485,37 @@ def run_nrc(args):
 
     plain = []
     for spp in (1, 2, 4, 8, 16, 32, 64):
-        p = backend.prepare(scene(spp, 7))
-        img, st = timed(p)
-        plain.append((spp, relmse(img, ref), st["device_seconds"]))
-        p.close()
+        errs, secs = [], []
+        for seed in SEEDS:
+            p = backend.prepare(scene(spp, seed), accel)
+            img, st = timed(p)
+            errs.append(relmse(img, ref))
+            secs.append(st["device_seconds"])
+            p.close()
+        plain.append((spp, float(np.mean(errs)), float(np.mean(secs))))
     cache = RadianceCache(lo, extent, seed=1)
-    warm = backend.prepare(scene(2, 99))
-    warm.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=4)
-    warm_s = sum(backend.render(warm).stats["device_seconds"] for _ in range(8))
-    warm.close()
+    cache.set_average_decay(DECAY)
+    warm_s = 0.0
+    for k in range(WARM):
+        w = backend.prepare(scene(2, 100 + k), accel)
+        w.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=4, averaged=True)
+        warm_s += backend.render(w).stats["device_seconds"]
+        w.close()
     cached = []
     with ClockSampler(0) as clocks:
         for spp in (1, 4, 16):
-            p = backend.prepare(scene(spp, 7))
-            p.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=1)
-            img, st = timed(p)
-            cached.append((spp, relmse(img, ref), st["device_seconds"], st["cache_queries"], st["rays_traced"]))
-            p.close()
+            errs, secs, queries, segs = [], [], [], []
+            for seed in SEEDS:
+                p = backend.prepare(scene(spp, seed), accel)
+                p.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=1, averaged=True)
+                img, st = timed(p)
+                errs.append(relmse(img, ref))
+                secs.append(st["device_seconds"])
+                queries.append(st["cache_queries"])
+                segs.append(st["rays_traced"])
+                p.close()
+            cached.append((spp, float(np.mean(errs)), float(np.mean(secs)), int(np.mean(queries)),
+                           int(np.mean(segs))))
     cache.check()
     cache.close()
 
@@ -518,7 +536,9 @@ def run_nrc(args):
             "vs_baseline": None, "dtype": "f32 render, bf16 MLP", "data": "synthetic",
             "config": {"workload": f"instanced-{W}x{H}-depth16-clamp20", "reference_spp": args.ref_spp,
                        "reference_accumulation": "fp64", "spread_threshold": C_SPREAD,
-                       "cache": "16x2^19x2 hash grid + SH4, 64x5 MLP, bf16 tcgen05, Adam 1e-2",
+                       "seeds_per_point": len(SEEDS), "warmup_frames": WARM,
+                       "cache": "16x2^19x2 hash grid + SH4, 64x5 MLP, bf16 tcgen05, Adam 1e-2, "
+                                f"parameter moving average {DECAY}",
                        "cache_warmup_ms": round(warm_s * 1e3, 2)},
             "plain": [{"spp": s_, "relmse": round(e, 5), "ms": round(t * 1e3, 3)} for s_, e, t in plain],
             "cached": [{"spp": s_, "relmse": round(e, 5), "ms": round(t * 1e3, 3), "cache_queries": q,

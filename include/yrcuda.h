@@ -654,6 +654,18 @@ void yrc_nrc_destroy(yrc_nrc* cache);
 yrc_status yrc_nrc_set_params(yrc_nrc* cache, const float* weights, const float* grid);
 yrc_status yrc_nrc_get_params(yrc_nrc* cache, float* weights_out, float* grid_out);
 
+/* The exponential moving average of the parameters that every optimiser
+ * step updates (decay min(d, (1 + t) / (10 + t)) at step t, d = 0.99 unless
+ * set by yrc_nrc_set_average_decay, restarted at
+ * the parameters by yrc_nrc_create / yrc_nrc_set_params), same layout as
+ * yrc_nrc_get_params. No counterpart in the reference. */
+yrc_status yrc_nrc_get_averaged_params(yrc_nrc* cache, float* weights_out, float* grid_out);
+
+/* Sets the largest decay of that moving average (default 0.99; [0, 1)).
+ * Optimiser steps already captured in a prepared scene's batch graph keep
+ * the decay they were captured with: set it before attaching the cache. */
+yrc_status yrc_nrc_set_average_decay(yrc_nrc* cache, float decay);
+
 /* rgb[i] = cache(queries[i]) for n queries, asynchronous on `stream`. */
 yrc_status yrc_nrc_infer(yrc_nrc* cache, const float* queries, int64_t n, float* rgb, void* stream);
 
@@ -679,6 +691,8 @@ typedef struct yrc_cache_settings {
     int32_t train_records;  /* training records per batch (65536) */
     int32_t train;          /* 0 freezes the cache (inference only) */
     int32_t train_steps;    /* optimiser steps per batch on that batch's records (1) */
+    int32_t delta_vertices; /* 1: paths may also end at specular (delta) vertices (0) */
+    int32_t averaged;       /* 1: query the moving average of the parameters (0: the raw ones) */
 } yrc_cache_settings;
 
 /* Attaches `cache` (NULL detaches) to a prepared scene: subsequent

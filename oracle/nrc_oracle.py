@@ -210,6 +210,15 @@ def adam(param: np.ndarray, grad: np.ndarray, m: np.ndarray, v: np.ndarray, step
     param -= np.float32(LR) * mhat / (np.sqrt(vhat) + np.float32(EPS))
 
 
+def average(avg: np.ndarray, param: np.ndarray, step: int, decay_max: float = 0.99):
+    """Moving average of the parameters after optimiser step `step` (counted
+    from 1), in place: decay = min(decay_max, (1 + t) / (10 + t)) rounded to
+    fp32, avg = decay * avg + (1 - decay) * param in fp32."""
+    decay = np.float32(min(float(np.float32(decay_max)), (1.0 + step) / (10.0 + step)))
+    keep = np.float32(1.0 - float(decay))
+    avg[...] = (decay * avg).astype(np.float32) + (keep * param).astype(np.float32)
+
+
 def init_weights(seed: int) -> list[np.ndarray]:
     """Xavier-uniform weights rounded to bf16; output rows 3..15 zero."""
     rng = np.random.default_rng(seed)

@@ -123,6 +123,31 @@ def test_adam_step_matches_oracle(cuda, cache):
     assert (diff > 1e-5).mean() < 1e-3, (diff > 1e-5).mean()
 
 
+def test_parameter_average_matches_oracle(cuda):
+    import torch
+    w, grid = params(17)
+    c = RadianceCache(LO, EXTENT, seed=3)
+    c.set_average_decay(0.9)
+    c.set_params(w, grid)
+    aw, ag = c.get_averaged_params()
+    assert np.array_equal(aw, w) and np.array_equal(ag, grid)  # restarted at the parameters
+    q, flat = queries(1024, 5)
+    qt = torch.from_numpy(flat).to(cuda)
+    tt = torch.from_numpy(np.full((1024, 4), 0.3, np.float32)).to(cuda)
+    avg_w, avg_g = w.copy(), grid.copy()
+    for step in range(1, 5):
+        c.train_step(qt, tt)
+        pw, pg = c.get_params()
+        N.average(avg_w, pw, step, 0.9)
+        N.average(avg_g, pg, step, 0.9)
+    c.check()
+    aw, ag = c.get_averaged_params()
+    c.close()
+    assert np.array_equal(aw, avg_w)
+    assert np.array_equal(ag, avg_g)
+    assert not np.array_equal(aw, pw)
+
+
 def test_training_learns_a_radiance_function(cuda):
     import torch
     c = RadianceCache(LO, EXTENT, seed=4)

@@ -186,6 +186,8 @@ def lib() -> C.CDLL:
         "yrc_nrc_destroy": (None, [P]),
         "yrc_nrc_set_params": (C.c_int, [P, P, P]),
         "yrc_nrc_get_params": (C.c_int, [P, P, P]),
+        "yrc_nrc_get_averaged_params": (C.c_int, [P, P, P]),
+        "yrc_nrc_set_average_decay": (C.c_int, [P, C.c_float]),
         "yrc_nrc_infer": (C.c_int, [P, P, I64, P, P]),
         "yrc_nrc_train_step": (C.c_int, [P, P, P, I64, P, P]),
         "yrc_nrc_gradients": (C.c_int, [P, P, P, I64, P, P, P]),

@@ -160,7 +160,8 @@ class JobRunner:
                 p = job.scene.geometry.positions
                 lo = p.min(0)
                 job.cache = RadianceCache(lo, float((p.max(0) - lo).max()) + 1e-3, seed=1)
-                job.prepared.set_radiance_cache(job.cache, spread_threshold=0.001, train_steps=2)
+                job.cache.set_average_decay(0.995)
+                job.prepared.set_radiance_cache(job.cache, spread_threshold=1e-4, train_steps=2, averaged=True)
             job.prepare_s = time.perf_counter() - t0
 
     def _render(self, job: Job) -> None:

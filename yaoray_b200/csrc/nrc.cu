@@ -49,6 +49,7 @@ constexpr float kOClamp = 15.0f;
 constexpr float kLossEps = 0.01f;
 constexpr float kLr = 1.0e-2f;
 constexpr double kBeta1 = 0.9, kBeta2 = 0.99;
+constexpr float kAvgDecay = 0.99f;  // default decay of the parameter moving average
 constexpr float kAdamEps = 1.0e-15f;
 constexpr uint32_t kPrimeY = 2654435761u, kPrimeZ = 805459861u;
 
@@ -485,11 +486,17 @@ __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const _
 // One Adam step with bias correction (c1 = 1 - beta1^t, c2 = 1 - beta2^t,
 // t read from the device so that a captured graph replays correctly), in
 // the operation order of the oracle; `half_out` / `bf16_out` receive the
-// rounded copy read by the kernels.
+// rounded copy read by the kernels. The same pass updates the exponential
+// moving average of the parameters (Polyak averaging, decay
+// min(avg_decay, (1 + t) / (10 + t))) and its rounded copy.
 __global__ void AdamKernel(float* p, float* m, float* v, const float* grad, int64_t count, const int64_t* step,
-                           __half* half_out, __nv_bfloat16* bf16_out) {
-    const float c1 = static_cast<float>(1.0 - pow(kBeta1, static_cast<double>(*step)));
-    const float c2 = static_cast<float>(1.0 - pow(kBeta2, static_cast<double>(*step)));
+                           __half* half_out, __nv_bfloat16* bf16_out, float* avg, __half* avg_half,
+                           __nv_bfloat16* avg_bf16, float avg_decay) {
+    const double t = static_cast<double>(*step);
+    const float c1 = static_cast<float>(1.0 - pow(kBeta1, t));
+    const float c2 = static_cast<float>(1.0 - pow(kBeta2, t));
+    const float decay = static_cast<float>(fmin(static_cast<double>(avg_decay), (1.0 + t) / (10.0 + t)));
+    const float keep = static_cast<float>(1.0 - static_cast<double>(decay));
     const float b1 = static_cast<float>(kBeta1), b2 = static_cast<float>(kBeta2);
     const float nb1 = static_cast<float>(1.0 - kBeta1), nb2 = static_cast<float>(1.0 - kBeta2);
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
@@ -506,6 +513,10 @@ __global__ void AdamKernel(float* p, float* m, float* v, const float* grad, int6
         p[i] = pi;
         if (half_out) half_out[i] = __float2half_rn(pi);
         if (bf16_out) bf16_out[i] = __float2bfloat16_rn(pi);
+        const float ai = __fadd_rn(__fmul_rn(decay, avg[i]), __fmul_rn(keep, pi));
+        avg[i] = ai;
+        if (avg_half) avg_half[i] = __float2half_rn(ai);
+        if (avg_bf16) avg_bf16[i] = __float2bfloat16_rn(ai);
     }
 }
 
@@ -551,6 +562,13 @@ struct yrc_nrc {
     float* w_m = nullptr;
     float* w_v = nullptr;
     float* w_grad = nullptr;
+    // Exponential moving average of the parameters (fp32) and its rounded
+    // copies, which the path tracer may query instead of the raw ones.
+    float* table_avg_master = nullptr;
+    __half* table_avg = nullptr;
+    float* w_avg_master = nullptr;
+    __nv_bfloat16* w_avg = nullptr;
+    float avg_decay = yrc::nrc::kAvgDecay;
     float* loss = nullptr;  // device scalar (sum of per-sample losses)
     int* error = nullptr;
     int64_t* step = nullptr;  // device: optimiser steps taken
@@ -574,8 +592,10 @@ unsigned Blocks(int64_t count, int sm_count) {
 }
 
 void FreeAll(yrc_nrc* c) {
-    void* ptrs[] = {c->table, c->table_master, c->table_m, c->table_v, c->table_grad, c->w, c->w_master,
-                    c->w_m,   c->w_v,          c->w_grad,  c->loss,    c->error, c->step};
+    void* ptrs[] = {c->table,  c->table_master,     c->table_m,   c->table_v,      c->table_grad,
+                    c->w,      c->w_master,         c->w_m,       c->w_v,          c->w_grad,
+                    c->table_avg_master, c->table_avg, c->w_avg_master, c->w_avg, c->loss,
+                    c->error,  c->step};
     for (void* p : ptrs) cudaFree(p);
 }
 
@@ -601,10 +621,12 @@ yrc_status LaunchTrain(yrc_nrc* c, const float* queries, const float* targets, i
 yrc_status LaunchAdam(yrc_nrc* c, cudaStream_t st) {
     StepKernel<<<1, 1, 0, st>>>(c->step);
     AdamKernel<<<Blocks(kWeightCount, c->sm_count), 256, 0, st>>>(c->w_master, c->w_m, c->w_v, c->w_grad,
-                                                                  kWeightCount, c->step, nullptr, c->w);
+                                                                  kWeightCount, c->step, nullptr, c->w,
+                                                                  c->w_avg_master, nullptr, c->w_avg, c->avg_decay);
     AdamKernel<<<Blocks(kGridParams, c->sm_count), 256, 0, st>>>(c->table_master, c->table_m, c->table_v,
                                                                  c->table_grad, kGridParams, c->step, c->table,
-                                                                 nullptr);
+                                                                 nullptr, c->table_avg_master, c->table_avg,
+                                                                 nullptr, c->avg_decay);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return CudaFailN(err, "optimiser launch");
     return Ok();
@@ -621,10 +643,29 @@ yrc_status CheckError(yrc_nrc* c) {
     return Ok();
 }
 
+// Rounded copies of the master parameters, and the moving average restarted
+// at them (weights and/or grid).
+cudaError_t ResetAverage(yrc_nrc* c, bool weights, bool grid) {
+    cudaError_t err = cudaSuccess;
+    if (weights) {
+        RoundKernel<<<Blocks(kWeightCount, c->sm_count), 256>>>(c->w_master, kWeightCount, nullptr, c->w);
+        err = cudaMemcpy(c->w_avg_master, c->w_master, sizeof(float) * kWeightCount, cudaMemcpyDeviceToDevice);
+        RoundKernel<<<Blocks(kWeightCount, c->sm_count), 256>>>(c->w_master, kWeightCount, nullptr, c->w_avg);
+    }
+    if (grid && err == cudaSuccess) {
+        RoundKernel<<<Blocks(kGridParams, c->sm_count), 256>>>(c->table_master, kGridParams, c->table, nullptr);
+        err = cudaMemcpy(c->table_avg_master, c->table_master, sizeof(float) * kGridParams,
+                         cudaMemcpyDeviceToDevice);
+        RoundKernel<<<Blocks(kGridParams, c->sm_count), 256>>>(c->table_master, kGridParams, c->table_avg, nullptr);
+    }
+    if (err == cudaSuccess) err = cudaDeviceSynchronize();
+    return err;
+}
+
 }  // namespace
 
 yrc_status Infer(yrc_nrc* c, const float* queries, int64_t n, const unsigned long long* n_ptr, float* rgb,
-                 cudaStream_t st) {
+                 cudaStream_t st, bool averaged) {
     if (n <= 0) return Ok();
     const int64_t tiles = (n + kTile - 1) / kTile;
     int per_sm = 0;
@@ -633,8 +674,10 @@ yrc_status Infer(yrc_nrc* c, const float* queries, int64_t n, const unsigned lon
     if (per_sm < 1) per_sm = 1;
     const int64_t cap = static_cast<int64_t>(per_sm) * c->sm_count;
     const int64_t blocks = tiles < cap ? tiles : cap;
+    GridArgs g = c->grid;
+    if (averaged) g.table = reinterpret_cast<const __half2*>(c->table_avg);
     CacheInferKernel<<<static_cast<unsigned>(blocks), kThreads, kInferSmem, st>>>(
-        c->grid, c->w, queries, n, n_ptr, reinterpret_cast<float4*>(rgb), c->error);
+        g, averaged ? c->w_avg : c->w, queries, n, n_ptr, reinterpret_cast<float4*>(rgb), c->error);
     err = cudaGetLastError();
     if (err != cudaSuccess) return CudaFailN(err, "inference launch");
     return Ok();
@@ -686,6 +729,10 @@ yrc_status yrc_nrc_create(const float box_lo[3], float box_extent, uint64_t seed
     alloc(&c->w_m, sizeof(float) * kWeightCount);
     alloc(&c->w_v, sizeof(float) * kWeightCount);
     alloc(&c->w_grad, sizeof(float) * kWeightCount);
+    alloc(&c->table_avg_master, sizeof(float) * kGridParams);
+    alloc(&c->table_avg, sizeof(__half) * kGridParams);
+    alloc(&c->w_avg_master, sizeof(float) * kWeightCount);
+    alloc(&c->w_avg, sizeof(__nv_bfloat16) * kWeightCount);
     alloc(&c->loss, sizeof(float));
     alloc(&c->error, sizeof(int));
     alloc(&c->step, sizeof(int64_t));
@@ -719,9 +766,7 @@ yrc_status yrc_nrc_create(const float box_lo[3], float box_extent, uint64_t seed
     if (err == cudaSuccess) err = cudaMemset(c->step, 0, sizeof(int64_t));
     if (err == cudaSuccess) {
         InitGridKernel<<<Blocks(kGridParams, c->sm_count), 256>>>(c->table_master, kGridParams, seed);
-        RoundKernel<<<Blocks(kGridParams, c->sm_count), 256>>>(c->table_master, kGridParams, c->table, nullptr);
-        RoundKernel<<<Blocks(kWeightCount, c->sm_count), 256>>>(c->w_master, kWeightCount, nullptr, c->w);
-        err = cudaDeviceSynchronize();
+        err = ResetAverage(c, true, true);
     }
     if (err != cudaSuccess) {
         FreeAll(c);
@@ -746,38 +791,50 @@ yrc_status yrc_nrc_set_params(yrc_nrc* c, const float* weights, const float* gri
     std::lock_guard<std::mutex> lock(c->mutex);
     cudaSetDevice(c->device);
     cudaError_t err = cudaSuccess;
-    if (weights) {
-        err = cudaMemcpy(c->w_master, weights, sizeof(float) * kWeightCount, cudaMemcpyHostToDevice);
-        if (err == cudaSuccess) {
-            RoundKernel<<<Blocks(kWeightCount, c->sm_count), 256>>>(c->w_master, kWeightCount, nullptr, c->w);
-        }
-    }
+    if (weights) err = cudaMemcpy(c->w_master, weights, sizeof(float) * kWeightCount, cudaMemcpyHostToDevice);
     if (grid && err == cudaSuccess) {
         err = cudaMemcpy(c->table_master, grid, sizeof(float) * kGridParams, cudaMemcpyHostToDevice);
-        if (err == cudaSuccess) {
-            RoundKernel<<<Blocks(kGridParams, c->sm_count), 256>>>(c->table_master, kGridParams, c->table, nullptr);
-        }
     }
-    if (err == cudaSuccess) err = cudaDeviceSynchronize();
+    if (err == cudaSuccess) err = ResetAverage(c, weights != nullptr, grid != nullptr);
     if (err != cudaSuccess) return CudaFailN(err, "setting parameters");
     return Ok();
 }
 
-yrc_status yrc_nrc_get_params(yrc_nrc* c, float* weights, float* grid) {
+namespace {
+yrc_status GetParams(yrc_nrc* c, const float* w_src, const float* grid_src, float* weights, float* grid) {
     using namespace yrc;
     using namespace yrc::nrc;
-    if (!c) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_nrc_get_params: null cache");
     std::lock_guard<std::mutex> lock(c->mutex);
     cudaSetDevice(c->device);
     cudaError_t err = cudaDeviceSynchronize();
     if (weights && err == cudaSuccess) {
-        err = cudaMemcpy(weights, c->w_master, sizeof(float) * kWeightCount, cudaMemcpyDeviceToHost);
+        err = cudaMemcpy(weights, w_src, sizeof(float) * kWeightCount, cudaMemcpyDeviceToHost);
     }
     if (grid && err == cudaSuccess) {
-        err = cudaMemcpy(grid, c->table_master, sizeof(float) * kGridParams, cudaMemcpyDeviceToHost);
+        err = cudaMemcpy(grid, grid_src, sizeof(float) * kGridParams, cudaMemcpyDeviceToHost);
     }
     if (err != cudaSuccess) return CudaFailN(err, "reading parameters");
     return Ok();
+}
+}  // namespace
+
+yrc_status yrc_nrc_get_params(yrc_nrc* c, float* weights, float* grid) {
+    if (!c) return yrc::Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_nrc_get_params: null cache");
+    return GetParams(c, c->w_master, c->table_master, weights, grid);
+}
+
+yrc_status yrc_nrc_set_average_decay(yrc_nrc* c, float decay) {
+    if (!c || !(decay >= 0.0f && decay < 1.0f)) {
+        return yrc::Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_nrc_set_average_decay: bad argument");
+    }
+    std::lock_guard<std::mutex> lock(c->mutex);
+    c->avg_decay = decay;
+    return yrc::Ok();
+}
+
+yrc_status yrc_nrc_get_averaged_params(yrc_nrc* c, float* weights, float* grid) {
+    if (!c) return yrc::Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_nrc_get_averaged_params: null cache");
+    return GetParams(c, c->w_avg_master, c->table_avg_master, weights, grid);
 }
 
 yrc_status yrc_nrc_infer(yrc_nrc* c, const float* queries, int64_t n, float* rgb, void* stream) {
@@ -785,7 +842,7 @@ yrc_status yrc_nrc_infer(yrc_nrc* c, const float* queries, int64_t n, float* rgb
     if (!c || n < 0 || (n > 0 && (!queries || !rgb))) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_nrc_infer: bad argument");
     std::lock_guard<std::mutex> lock(c->mutex);
     cudaSetDevice(c->device);
-    return nrc::Infer(c, queries, n, nullptr, rgb, static_cast<cudaStream_t>(stream));
+    return nrc::Infer(c, queries, n, nullptr, rgb, static_cast<cudaStream_t>(stream), false);
 }
 
 yrc_status yrc_nrc_gradients(yrc_nrc* c, const float* queries, const float* targets, int64_t n, float* weight_grads,

@@ -557,6 +557,7 @@ yrc_status EnsureCache(yrc_render_scene* s) {
     c.enabled = 1;
     c.spread_c = cs.spread_threshold;
     c.train_one_in = std::max(1, cs.train_one_in);
+    c.delta_vertices = cs.delta_vertices != 0;
     c.train_records = cs.train ? std::max(128, cs.train_records) : 0;
     c.train_paths = cs.train ? static_cast<int32_t>(std::min<int64_t>(cap, c.train_records)) : 0;
     c.max_depth = s->dev.max_depth;
@@ -566,6 +567,7 @@ yrc_status EnsureCache(yrc_render_scene* s) {
     c.queries = W.Alloc<float>(16 * cap);
     c.query_path = W.Alloc<int32_t>(cap);
     c.query_tp = W.Alloc<float4>(cap);
+    c.query_base = W.Alloc<float4>(cap);
     c.query_rgb = W.Alloc<float4>(cap);
     c.train_slot = W.Alloc<int32_t>(cap);
     const int64_t tp = std::max<int32_t>(c.train_paths, 1);
@@ -672,13 +674,16 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
         std::swap(q.path_in, q.path_out);
     }
     if (cache.enabled) {
-        // Paths that ended at the cache get its radiance; then one training
-        // step on the unbiased training paths of this batch.
-        yrc_status cs = nrc::Infer(s->cache, cache.queries, C, cache.counters + 0, reinterpret_cast<float*>(cache.query_rgb), st);
+        // Training targets from the unbiased training paths' full radiance;
+        // then every path that ended at the cache (training paths at their
+        // first terminal vertex too) gets its image estimate; then the
+        // training steps.
+        yrc_status cs = nrc::Infer(s->cache, cache.queries, C, cache.counters + 0,
+                                   reinterpret_cast<float*>(cache.query_rgb), st, s->cache_settings.averaged != 0);
         if (cs != YRC_OK) return cs;
+        if (cache.train_records > 0) LaunchCacheTargets(s->ps, cache, s->sm_count, st);
         LaunchCacheResolve(s->ps, cache, C, s->sm_count, st);
         if (cache.train_records > 0) {
-            LaunchCacheTargets(s->ps, cache, s->sm_count, st);
             for (int k = 0; k < std::max(1, s->cache_settings.train_steps); ++k) {
                 cs = nrc::TrainStep(s->cache, cache.rec_q, reinterpret_cast<const float*>(cache.rec_t),
                                     cache.train_records, cache.counters + 2, st);

@@ -673,15 +673,25 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
                     cache.slot_lt[2 * v + 1] = ToF4(tp);
                     cache.slot_len[slot] = k + 1;
                 }
-            } else if (depth >= 1 && !IsDelta(m) && sp.y * sp.y > cache.spread_c * sp.x) {
+            }
+            const bool fires = depth >= 1 && !(flags & kPathCacheQueued) && (cache.delta_vertices || !IsDelta(m)) &&
+                               sp.y * sp.y > cache.spread_c * sp.x;
+            if (fires) {
+                // The image estimate of the path ends here: radiance so far
+                // plus throughput x cache. A training path goes on as an
+                // unbiased suffix whose radiance only trains the cache.
                 const unsigned long long k = QueueAppend(cache.counters + 0);
                 WriteCacheQuery(cache.queries + 16 * k, s.p, wo, s.n, m);
                 cache.query_path[k] = path;
                 cache.query_tp[k] = ToF4(tp);
-                ps.throughput[path] = ToF4(tp);
-                ps.radiance[path] = ToF4(rad);
-                ps.flags[path] = flags;
-                continue;
+                cache.query_base[k] = ToF4(rad);
+                if (slot < 0) {
+                    ps.throughput[path] = ToF4(tp);
+                    ps.radiance[path] = ToF4(rad);
+                    ps.flags[path] = flags;
+                    continue;
+                }
+                flags |= kPathCacheQueued;
             }
         }
 
@@ -937,15 +947,17 @@ __global__ void SubsurfaceExitKernel(DevScene sc, PathState ps, Queues q, int de
 
 // ------------------------------------------------------- radiance cache
 
-// Adds throughput x cached radiance to every path that ended at the cache.
+// The image estimate of every path that ended at the cache: its radiance up
+// to the query vertex plus throughput x cached radiance. Runs after the
+// training targets were taken from the training paths' full radiance.
 __global__ void CacheResolveKernel(PathState ps, CacheArgs cache) {
     const int64_t n = static_cast<int64_t>(cache.counters[0]);
     for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
          k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int32_t path = cache.query_path[k];
-        const V3 c = F4(cache.query_rgb[k]);
-        if (!(isfinite(c.x) && isfinite(c.y) && isfinite(c.z))) continue;
-        ps.radiance[path] = ToF4(F4(ps.radiance[path]) + Mul(F4(cache.query_tp[k]), c));
+        V3 c = F4(cache.query_rgb[k]);
+        if (!(isfinite(c.x) && isfinite(c.y) && isfinite(c.z))) c = V3{0.0f, 0.0f, 0.0f};
+        ps.radiance[path] = ToF4(F4(cache.query_base[k]) + Mul(F4(cache.query_tp[k]), c));
     }
 }
 

@@ -156,6 +156,7 @@ struct CacheArgs {
     int32_t enabled;
     float spread_c;        // terminate when spread^2 > spread_c * a0
     int32_t train_one_in;  // 1 in train_one_in paths traces unbiased for training
+    int32_t delta_vertices;  // paths may also end at delta vertices
     int32_t train_paths;   // capacity of the training-path slots
     int32_t train_records; // capacity of the training records
     int32_t max_depth;
@@ -163,6 +164,7 @@ struct CacheArgs {
     float* queries;        // per terminated path: 16-float query
     int32_t* query_path;
     float4* query_tp;      // throughput at the query vertex
+    float4* query_base;    // path radiance up to and including the query vertex's emission
     float4* query_rgb;     // cache output
     int32_t* train_slot;   // per path: training slot or -1
     int32_t* slot_path;    // per training slot: path
@@ -179,6 +181,7 @@ constexpr uint32_t kPathPrevDelta = 1u << 1;
 constexpr uint32_t kPathMedium = 1u << 2;
 constexpr uint32_t kPathPrimary = 1u << 3;
 constexpr uint32_t kPathNee = 1u << 5;  // pending next-event contributions
+constexpr uint32_t kPathCacheQueued = 1u << 6;  // the path's image estimate already ended at the cache
 
 // Work queues (device counters live in a small array).
 struct Queues {

@@ -55,6 +55,19 @@ class RadianceCache:
         check(lib().yrc_nrc_get_params(self._handle, ptr(w), ptr(g)))
         return w, g
 
+    def set_average_decay(self, decay: float) -> None:
+        """Largest decay of the parameter moving average (default 0.99); set
+        it before attaching the cache to a scene."""
+        check(lib().yrc_nrc_set_average_decay(self._handle, float(decay)))
+
+    def get_averaged_params(self):
+        """The moving average of the parameters (decay min(0.99, (1+t)/(10+t))
+        at optimiser step t), which a render may query instead."""
+        w = np.empty((6, WIDTH, WIDTH), np.float32)
+        g = np.empty((LEVELS, TABLE, 2), np.float32)
+        check(lib().yrc_nrc_get_averaged_params(self._handle, ptr(w), ptr(g)))
+        return w, g
+
     def infer(self, queries, out=None, stream=None):
         torch = _torch()
         n = queries.shape[0]

@@ -158,7 +158,8 @@ class Stats(C.Structure):
 class CacheSettings(C.Structure):
     """yrc_cache_settings: how the path tracer uses an attached radiance cache."""
     _fields_ = [("spread_threshold", C.c_float), ("train_one_in", C.c_int32), ("train_records", C.c_int32),
-                ("train", C.c_int32), ("train_steps", C.c_int32)]
+                ("train", C.c_int32), ("train_steps", C.c_int32), ("delta_vertices", C.c_int32),
+                ("averaged", C.c_int32)]
 
 
 def _bind():
@@ -385,12 +386,17 @@ class PreparedScene:
         return int(_bind().yrc_render_scene_device_bytes(self._handle))
 
     def set_radiance_cache(self, cache, spread_threshold: float = 0.01, train_one_in: int = 16,
-                           train_records: int = 65536, train: bool = True, train_steps: int = 1) -> None:
+                           train_records: int = 65536, train: bool = True, train_steps: int = 1,
+                           delta_vertices: bool = False, averaged: bool = False) -> None:
         """Attaches a yaoray_b200.nrc.RadianceCache (None detaches): paths end
         at the cache when their footprint heuristic fires, and the cache
         takes `train_steps` optimiser steps per batch on the records of 1 in
-        `train_one_in` unbiased paths."""
-        st = CacheSettings(spread_threshold, train_one_in, train_records, 1 if train else 0, train_steps)
+        `train_one_in` unbiased paths. With `delta_vertices` a path may also
+        end at a specular (delta) vertex once its spread is large; with
+        `averaged` the paths query the moving average of the cache's
+        parameters instead of the latest ones."""
+        st = CacheSettings(spread_threshold, train_one_in, train_records, 1 if train else 0, train_steps,
+                           1 if delta_vertices else 0, 1 if averaged else 0)
         self._cache = cache
         check(_bind().yrc_render_scene_set_cache(self._handle, cache._handle if cache is not None else None,
                                                  C.byref(st)))
