@@ -381,6 +381,11 @@ def run_render(args):
     t0 = time.perf_counter()
     prepared = backend.prepare(scene)
     prepare_s = time.perf_counter() - t0
+    tuning = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        tuning = prepared.autotune()
+        tuning["seconds"] = round(time.perf_counter() - t0, 2)
     for _ in range(args.warmup):
         res = backend.render(prepared)
         assert res.ok, res.error
@@ -413,7 +418,8 @@ def run_render(args):
               "width": scene.width, "height": scene.height, "spp_per_step": scene.spp,
               "max_depth": scene.max_depth,
               "path_segments_per_step": int(res.stats["rays_traced"]),
-              "shadow_rays_per_step": int(res.stats["shadow_rays"])}
+              "shadow_rays_per_step": int(res.stats["shadow_rays"]),
+              "queue_capacity": prepared.capacity, "autotune": tuning}
     if args.workload == "instanced":
         from yaoray_b200 import instanced
         config.update(instances=int(instanced.INSTANCES), instanced_triangles=instanced.instanced_triangles(scene),
@@ -561,7 +567,7 @@ def run_jobs(args):
     t0 = time.perf_counter()
     jobs = batch.job_set(48, seed=7, spp_scale=args.spp_scale)
     runner = batch.JobRunner()
-    runner.prepare(jobs)
+    runner.prepare(jobs, autotune=not args.no_autotune)
     prepare_s = time.perf_counter() - t0
     runner.run_sequential(jobs)  # warm-up: allocates and captures every job's batch graph
     seq = runner.run_sequential(jobs)
@@ -598,6 +604,8 @@ def run_jobs(args):
                        "spp_scale": args.spp_scale, "concurrency": args.concurrency,
                        "triangles_min_max": [min(tris), max(tris)], "with_radiance_cache": sum(j.use_cache for j in jobs),
                        "samples_total": conc.samples, "prepare_seconds": round(prepare_s, 2),
+                       "autotune_seconds": round(sum(j.tune_s for j in jobs), 2),
+                       "capacities": sorted({j.tuning["capacity"] for j in jobs if j.tuning}),
                        "admission_budget_gb": round(conc.extra.get("budget_bytes", 0) / 2**30, 1),
                        "peak_concurrent_jobs": conc.peak_concurrency},
             "one_at_a_time": {"samples_per_s": round(seq_sps, 1), "wall_s": round(seq.wall_s, 3),
@@ -620,6 +628,7 @@ def main():
     ap.add_argument("--ref-spp", type=int, default=512)
     ap.add_argument("--spp-scale", type=float, default=1.0, help="spp scale of --workload jobs")
     ap.add_argument("--concurrency", type=int, default=8, help="concurrent jobs of --workload jobs")
+    ap.add_argument("--no-autotune", action="store_true", help="render workloads: keep the default queue capacity")
     ap.add_argument("--render-spp", type=int, default=16, help="spp per step of --workload instanced")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)

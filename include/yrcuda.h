@@ -611,6 +611,38 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
 void yrc_render_scene_destroy(yrc_render_scene* scene);
 int64_t yrc_render_scene_device_bytes(const yrc_render_scene* scene);
 
+/* Queue capacity of the wavefront (paths in flight per batch). By default
+ * max(pixels, 2^21), bounded to whole passes of the image: at least one
+ * pass, at most min(spp, 64). set_capacity(0) restores the default; any
+ * other value is bounded the same way. The film does not depend on it: a
+ * batch renders whole passes and the film adds samples in pass order.
+ * No counterpart in the reference. */
+yrc_status yrc_render_scene_set_capacity(yrc_render_scene* scene, int64_t capacity);
+int64_t yrc_render_scene_capacity(const yrc_render_scene* scene);
+
+/* Render autotuner: times short probe renders of this scene (sample indices
+ * 0..P-1 of every pixel, P = two batches of the largest candidate) for each
+ * candidate queue capacity (whole passes of the image between 2^17 and 2^23
+ * paths) and, for single-level accelerators, each closest-hit traversal
+ * launch shape of the extend stage at the best capacity; keeps the fastest
+ * for later yrc_render calls. The traversal stack depth is not a candidate:
+ * it follows the BVH's measured depth (64 or 256 entries). Probes run
+ * without an attached radiance cache (they do not train it). Synchronous.
+ * No counterpart in the reference. */
+#define YRC_TUNE_CAPACITY 1
+#define YRC_TUNE_TRACE_SHAPE 2
+typedef struct yrc_render_tuning {
+    int64_t capacity;          /* chosen queue capacity */
+    int32_t trace_shape;       /* chosen closest-hit launch shape */
+    int32_t candidates;        /* configurations timed */
+    double seconds_per_sample; /* device time per sample of the chosen configuration */
+} yrc_render_tuning;
+yrc_status yrc_render_autotune(yrc_render_scene* scene, int32_t flags, yrc_render_tuning* result);
+/* Applies a tuning (capacity and closest-hit launch shape; the other fields
+ * are ignored), e.g. one found by yrc_render_autotune on a scene of the same
+ * image size and spp. */
+yrc_status yrc_render_scene_set_tuning(yrc_render_scene* scene, const yrc_render_tuning* tuning);
+
 /*
  * CudaBackend::Render (cuda_stub_backend.cpp:30-37) for the Path integrator:
  * the pass loop of RenderCpuPathTrace (src/backends/cpu/cpu_path_tracer.cpp:

@@ -47,6 +47,9 @@ class Job:
     prepared: object = None
     cache: object = None
     prepare_s: float = 0.0
+    tuning: dict | None = None
+    tune_s: float = 0.0
+    resident: bool = False  # rendered once: its working memory stays allocated
     latency_s: float = 0.0
     device_s: float = 0.0
     samples: int = 0
@@ -115,11 +118,15 @@ def _free_device_bytes() -> int:
 
 
 def _working_set(job: Job) -> int:
-    """Device bytes a job's first render allocates: the path state and queues
-    for max(2^21, pixels) paths (~400 B each, ~700 B with a cache) plus the
-    film and, with a cache, its grid (~300 MB)."""
+    """Device bytes a job's render still has to allocate: none once it has
+    rendered (its working memory stays allocated), else the path state and queues
+    for its queue capacity (the prepared scene's, else max(2^21, pixels))
+    at ~400 B per path (~700 B with a cache), plus the film and, with a
+    cache, its grid (~300 MB)."""
+    if job.resident:
+        return 0
     pixels = job.scene.width * job.scene.height
-    paths = max(1 << 21, pixels)
+    paths = job.prepared.capacity if job.prepared is not None else max(1 << 21, pixels)
     per = 700 if job.use_cache else 400
     return paths * per + pixels * 80 + (300 << 20 if job.use_cache else 0)
 
@@ -151,11 +158,26 @@ class JobRunner:
         self.reserve = reserve_bytes
         self.keep_films = keep_films
 
-    def prepare(self, jobs: list[Job]) -> None:
+    def prepare(self, jobs: list[Job], autotune: bool = False) -> None:
+        """Builds and uploads every job's scene, attaches the radiance caches
+        and, with `autotune`, runs the render autotuner (queue capacity and
+        traversal launch shape, probes without the cache) once per class of
+        jobs with the same pixel count and batch bound min(spp, 64); the
+        other jobs of a class take its result."""
         from .nrc import RadianceCache
+        tuned: dict = {}
         for job in jobs:
             t0 = time.perf_counter()
             job.prepared = self.backend.prepare(job.scene)
+            if autotune:
+                key = (job.scene.width * job.scene.height, min(job.scene.spp, 64))
+                t1 = time.perf_counter()
+                if key in tuned:
+                    job.tuning = tuned[key]
+                    job.prepared.set_tuning(job.tuning)
+                else:
+                    job.tuning = tuned[key] = job.prepared.autotune()
+                job.tune_s = time.perf_counter() - t1
             if job.use_cache:
                 p = job.scene.geometry.positions
                 lo = p.min(0)
@@ -169,6 +191,7 @@ class JobRunner:
         res = self.backend.render(job.prepared)
         job.latency_s = time.perf_counter() - t0
         job.ok, job.error = res.ok, res.error
+        job.resident = job.resident or res.ok
         job.device_s = res.stats.get("device_seconds", 0.0)
         job.samples = int(res.stats.get("samples_rendered", 0))
         job.film = res.film if self.keep_films else None
@@ -182,9 +205,10 @@ class JobRunner:
 
     def run_concurrent(self, jobs: list[Job], concurrency: int = 8, budget_bytes: int | None = None) -> BatchResult:
         """Renders up to `concurrency` jobs at once, admitting a job only while
-        the summed working sets of running jobs fit the admission budget
-        (`budget_bytes`, by default free device memory at the start minus the
-        reserve); a job larger than the whole budget runs alone. Jobs are
+        the working memory that running jobs still have to allocate fits the
+        admission budget (`budget_bytes`, by default free device memory at
+        the start minus the reserve); a job larger than the whole budget runs
+        alone. Jobs that rendered before hold their memory already. Jobs are
         taken largest-first so small jobs fill the gaps at the end."""
         budget = budget_bytes if budget_bytes is not None else max(_free_device_bytes() - self.reserve, 0)
         lock = threading.Condition()

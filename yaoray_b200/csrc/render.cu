@@ -107,6 +107,7 @@ struct yrc_render_scene {
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int32_t graph_max_batch = -1;
+    int64_t capacity_choice = 0;  // queue capacity chosen by the autotuner or the caller (0: from the image)
     // Radiance cache (optional).
     yrc_nrc* cache = nullptr;
     yrc_cache_settings cache_settings{};
@@ -470,10 +471,21 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
 namespace yrc {
 namespace {
 
+// Concurrent paths of a render: the autotuned (or caller's) choice, else
+// enough for several passes of a small image at once and one full pass of a
+// large one; always at least one pass of every pixel (a batch renders whole
+// passes) and at most kMaxBatch passes.
+int64_t RenderCapacity(const yrc_render_scene* s) {
+    const int64_t pixels = static_cast<int64_t>(s->settings.width) * s->settings.height;
+    const int64_t most = pixels * std::min(std::max(1, s->settings.spp), kMaxBatch);
+    const int64_t c = s->capacity_choice > 0 ? s->capacity_choice : std::max<int64_t>(pixels, int64_t{1} << 21);
+    return std::min(std::max(c, pixels), most);
+}
+
 // Allocates the path state and queues for `capacity` paths.
 yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     const int64_t pixels = static_cast<int64_t>(s->settings.width) * s->settings.height;
-    if (s->capacity >= capacity && s->film) return Ok();
+    if (s->capacity == capacity && s->film) return Ok();
     if (s->graph) {
         cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
@@ -699,6 +711,83 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
     return Ok();
 }
 
+// Captures one batch as a CUDA graph (all sizes are read on the device),
+// unless the scene holds one for this batch bound.
+yrc_status EnsureGraph(yrc_render_scene* s, int32_t max_batch) {
+    if (s->graph && s->graph_max_batch == max_batch) return Ok();
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaError_t err = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+    if (err != cudaSuccess) return CudaError(err, "graph capture");
+    const yrc_status status = EnqueueBatch(s, max_batch);
+    err = cudaStreamEndCapture(s->stream, &graph);
+    if (status != YRC_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return status;
+    }
+    if (err != cudaSuccess) return CudaError(err, "graph capture");
+    err = cudaGraphInstantiate(&s->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) return CudaError(err, "graph instantiate");
+    s->graph_max_batch = max_batch;
+    return Ok();
+}
+
+void DropGraph(yrc_render_scene* s) {
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+}
+
+// Renders sample indices 0..passes-1 of every pixel into the device film
+// with the scene's current capacity and launch shapes (no resume, no
+// progress, no readback); returns the device time of the batches.
+yrc_status ProbeRender(yrc_render_scene* s, int32_t passes, double* seconds) {
+    const int64_t pixels = static_cast<int64_t>(s->settings.width) * s->settings.height;
+    const int spp = std::max(1, s->settings.spp);
+    yrc_status status = EnsureWork(s, RenderCapacity(s));
+    if (status == YRC_OK) status = EnsureCache(s);
+    if (status != YRC_OK) return status;
+    cudaStream_t stream = s->stream;
+    const std::vector<int32_t> attempts(static_cast<size_t>(pixels), passes);
+    cudaMemsetAsync(s->film, 0, sizeof(yrc_film_pixel) * pixels, stream);
+    cudaMemcpyAsync(s->attempts, attempts.data(), sizeof(int32_t) * pixels, cudaMemcpyHostToDevice, stream);
+    cudaMemsetAsync(s->scalars, 0, 4 * sizeof(unsigned long long), stream);
+    cudaMemsetAsync(s->q.counters, 0, sizeof(unsigned long long) * kCtrCount, stream);
+    const int32_t max_batch = std::min(spp, kMaxBatch);
+    {
+        BatchArgs b{s->active, s->scalars + 0, s->scalars + 1, s->batch, s->film};
+        FilmArgs f{s->attempts, s->scalars + 2, s->scalars + 3, 0, 0, 0.0f, 0.0f, 0.0f};
+        LaunchActivePixels(s->dev, b, f, pixels, s->sm_count, stream);
+        LaunchFinishActive(s->scalars + 0, s->scalars + 1, s->batch, max_batch, s->capacity, stream);
+    }
+    status = EnsureGraph(s, max_batch);
+    if (status != YRC_OK) return status;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, stream);
+    unsigned long long active = 0;
+    cudaMemcpyAsync(&active, s->scalars, sizeof(active), cudaMemcpyDeviceToHost, stream);
+    cudaError_t err = cudaStreamSynchronize(stream);
+    for (int guard = 0; err == cudaSuccess && active > 0 && guard <= passes; ++guard) {
+        err = cudaGraphLaunch(s->graph, stream);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(&active, s->scalars, sizeof(active), cudaMemcpyDeviceToHost, stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    }
+    cudaEventRecord(e1, stream);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (err != cudaSuccess) return CudaError(err, "autotune probe");
+    status = CheckDeviceError(s->accel);
+    if (status != YRC_OK) return status;
+    *seconds = ms / 1e3;
+    return Ok();
+}
+
 }  // namespace
 }  // namespace yrc
 
@@ -727,11 +816,7 @@ extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* 
     }
     if (r.stop_flag && *r.stop_flag) return Fail(YRC_ERR_CANCELLED, "render cancelled");
 
-    // Concurrent paths: enough for several passes of a small image at once,
-    // one full pass of a large one.
-    const int64_t capacity = std::min<int64_t>(std::max<int64_t>(pixels, int64_t{1} << 21),
-                                               pixels * std::min(spp, kMaxBatch));
-    yrc_status status = EnsureWork(s, capacity);
+    yrc_status status = EnsureWork(s, RenderCapacity(s));
     if (status == YRC_OK) status = EnsureCache(s);
     if (status != YRC_OK) return status;
     cudaStream_t stream = s->stream;
@@ -756,25 +841,8 @@ extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* 
         LaunchActivePixels(sc, b, f, pixels, s->sm_count, stream);
         LaunchFinishActive(s->scalars + 0, s->scalars + 1, s->batch, max_batch, s->capacity, stream);
     }
-    // Capture one batch as a CUDA graph (all sizes are read on the device).
-    if (!s->graph || s->graph_max_batch != max_batch) {
-        if (s->graph) cudaGraphExecDestroy(s->graph);
-        s->graph = nullptr;
-        cudaGraph_t graph = nullptr;
-        cudaError_t err = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
-        if (err != cudaSuccess) return CudaError(err, "graph capture");
-        status = EnqueueBatch(s, max_batch);
-        err = cudaStreamEndCapture(stream, &graph);
-        if (status != YRC_OK) {
-            if (graph) cudaGraphDestroy(graph);
-            return status;
-        }
-        if (err != cudaSuccess) return CudaError(err, "graph capture");
-        err = cudaGraphInstantiate(&s->graph, graph, 0);
-        cudaGraphDestroy(graph);
-        if (err != cudaSuccess) return CudaError(err, "graph instantiate");
-        s->graph_max_batch = max_batch;
-    }
+    status = EnsureGraph(s, max_batch);
+    if (status != YRC_OK) return status;
 
     int completed_passes = r.resume_completed_spp;
     uint64_t total_samples = 0;
@@ -867,5 +935,117 @@ extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* 
         stats->elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
     }
     (void)total_samples;
+    return Ok();
+}
+
+extern "C" yrc_status yrc_render_scene_set_capacity(yrc_render_scene* s, int64_t capacity) {
+    using namespace yrc;
+    if (!s || capacity < 0) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_scene_set_capacity: bad argument");
+    std::lock_guard<std::mutex> lock(s->mutex);
+    s->capacity_choice = capacity;
+    return Ok();
+}
+
+extern "C" int64_t yrc_render_scene_capacity(const yrc_render_scene* s) {
+    return s ? yrc::RenderCapacity(s) : 0;
+}
+
+extern "C" yrc_status yrc_render_autotune(yrc_render_scene* s, int32_t flags, yrc_render_tuning* result) {
+    using namespace yrc;
+    if (!s || (flags & ~(YRC_TUNE_CAPACITY | YRC_TUNE_TRACE_SHAPE)) != 0) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_autotune: bad argument");
+    }
+    std::lock_guard<std::mutex> lock(s->mutex);
+    cudaSetDevice(s->device);
+    const int64_t pixels = static_cast<int64_t>(s->settings.width) * s->settings.height;
+    const int spp = std::max(1, s->settings.spp);
+    const int most_passes = std::min(spp, kMaxBatch);
+    // Candidate capacities: whole passes of the image, 2^17 .. 2^23 paths
+    // (the smallest and largest whole-pass counts always included).
+    std::vector<int64_t> caps;
+    for (int k = 1; k <= most_passes; k *= 2) {
+        const int64_t c = pixels * k;
+        if ((c >= (int64_t{1} << 17) || k * 2 > most_passes) && (c <= (int64_t{1} << 23) || k == 1)) caps.push_back(c);
+    }
+    if (caps.empty()) caps.push_back(pixels);
+    // Every probe renders the same passes: two batches of the largest candidate.
+    const int32_t passes =
+        static_cast<int32_t>(std::min<int64_t>(spp, std::max<int64_t>(1, 2 * caps.back() / pixels)));
+    // Probes run without the radiance cache, so that they do not train it.
+    yrc_nrc* cache = s->cache;
+    s->cache = nullptr;
+    DropGraph(s);
+    EnsureCache(s);
+    const int64_t saved_choice = s->capacity_choice;
+    const int saved_shape = yrc_accel_get_trace_shape(s->accel, 0);
+    int tried = 0;
+    double best = 0.0;
+    int64_t best_cap = RenderCapacity(s);
+    int best_shape = saved_shape;
+    yrc_status status = YRC_OK;
+    auto time_config = [&](int64_t cap, int shape, double* sec) -> yrc_status {
+        s->capacity_choice = cap;
+        yrc_accel_set_trace_shape(s->accel, 0, shape);
+        DropGraph(s);
+        double first = 0.0;
+        yrc_status st = ProbeRender(s, passes, &first);  // allocation, graph capture, warm-up
+        if (st == YRC_OK) st = ProbeRender(s, passes, sec);
+        ++tried;
+        return st;
+    };
+    if (flags & YRC_TUNE_CAPACITY) {
+        for (const int64_t cap : caps) {
+            double sec = 0.0;
+            status = time_config(cap, saved_shape, &sec);
+            if (status != YRC_OK) break;
+            if (best == 0.0 || sec < best) {
+                best = sec;
+                best_cap = cap;
+            }
+        }
+    }
+    // Traversal launch shapes (single-level accelerators; the two-level
+    // kernel has one shape).
+    const bool two_level = AccelParamsOf(s->accel).two_level != 0;
+    if (status == YRC_OK && (flags & YRC_TUNE_TRACE_SHAPE) && !two_level) {
+        for (int shape = 0; shape < YRC_TRACE_SHAPES; ++shape) {
+            double sec = 0.0;
+            status = time_config(best_cap, shape, &sec);
+            if (status != YRC_OK) break;
+            if (best == 0.0 || sec < best) {
+                best = sec;
+                best_shape = shape;
+            }
+        }
+    }
+    if (status == YRC_OK && best == 0.0) {  // nothing tuned: time the current configuration
+        status = time_config(best_cap, best_shape, &best);
+    }
+    s->capacity_choice = status == YRC_OK ? best_cap : saved_choice;
+    yrc_accel_set_trace_shape(s->accel, 0, status == YRC_OK ? best_shape : saved_shape);
+    DropGraph(s);
+    s->cache = cache;
+    s->cache_capacity = 0;  // re-allocated for the chosen capacity on the next render
+    if (status != YRC_OK) return status;
+    if (result) {
+        result->capacity = best_cap;
+        result->trace_shape = best_shape;
+        result->candidates = tried;
+        result->seconds_per_sample = best / (static_cast<double>(pixels) * passes);
+    }
+    return Ok();
+}
+
+extern "C" yrc_status yrc_render_scene_set_tuning(yrc_render_scene* s, const yrc_render_tuning* tuning) {
+    using namespace yrc;
+    if (!s || !tuning || tuning->capacity < 0 || tuning->trace_shape < 0 || tuning->trace_shape >= YRC_TRACE_SHAPES) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_scene_set_tuning: bad argument");
+    }
+    std::lock_guard<std::mutex> lock(s->mutex);
+    cudaSetDevice(s->device);
+    s->capacity_choice = tuning->capacity;
+    const yrc_status st = yrc_accel_set_trace_shape(s->accel, 0, tuning->trace_shape);
+    if (st != YRC_OK) return st;
+    DropGraph(s);
     return Ok();
 }

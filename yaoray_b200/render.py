@@ -155,6 +155,16 @@ class Stats(C.Structure):
                 ("device_seconds", C.c_double), ("cache_queries", C.c_uint64), ("cache_records", C.c_uint64)]
 
 
+class RenderTuning(C.Structure):
+    """yrc_render_tuning: the configuration the render autotuner chose."""
+    _fields_ = [("capacity", C.c_int64), ("trace_shape", C.c_int32), ("candidates", C.c_int32),
+                ("seconds_per_sample", C.c_double)]
+
+
+TUNE_CAPACITY = 1
+TUNE_TRACE_SHAPE = 2
+
+
 class CacheSettings(C.Structure):
     """yrc_cache_settings: how the path tracer uses an attached radiance cache."""
     _fields_ = [("spread_threshold", C.c_float), ("train_one_in", C.c_int32), ("train_records", C.c_int32),
@@ -173,6 +183,10 @@ def _bind():
         ("yrc_render_scene_device_bytes", C.c_int64, [P]),
         ("yrc_render", C.c_int, [P, P, P, P, P]),
         ("yrc_render_scene_set_cache", C.c_int, [P, P, P]),
+        ("yrc_render_scene_set_capacity", C.c_int, [P, C.c_int64]),
+        ("yrc_render_scene_capacity", C.c_int64, [P]),
+        ("yrc_render_autotune", C.c_int, [P, C.c_int32, P]),
+        ("yrc_render_scene_set_tuning", C.c_int, [P, P]),
         ("yrc_bssrdf_table_build", C.c_int, [C.c_float, C.c_float, C.c_int32, C.c_int32, P, P, P, P, P]),
         ("yrc_alias_table_build", C.c_int, [P, C.c_int32, P, P, P]),
         ("yrc_environment_distribution_build", C.c_int, [P, C.c_int32, C.c_int32, P, P, P, P, P]),
@@ -384,6 +398,31 @@ class PreparedScene:
     @property
     def device_bytes(self) -> int:
         return int(_bind().yrc_render_scene_device_bytes(self._handle))
+
+    @property
+    def capacity(self) -> int:
+        """Paths in flight per batch (queue capacity) of the next render."""
+        return int(_bind().yrc_render_scene_capacity(self._handle))
+
+    def set_capacity(self, capacity: int) -> None:
+        """Sets the queue capacity (0 restores the default); bounded to whole
+        passes of the image. The film does not depend on it."""
+        check(_bind().yrc_render_scene_set_capacity(self._handle, int(capacity)))
+
+    def autotune(self, capacity: bool = True, trace_shape: bool = True) -> dict:
+        """Times probe renders of this scene for each candidate queue
+        capacity and traversal launch shape and keeps the fastest."""
+        t = RenderTuning()
+        flags = (TUNE_CAPACITY if capacity else 0) | (TUNE_TRACE_SHAPE if trace_shape else 0)
+        check(_bind().yrc_render_autotune(self._handle, flags, C.byref(t)))
+        return {"capacity": int(t.capacity), "trace_shape": int(t.trace_shape), "candidates": int(t.candidates),
+                "seconds_per_sample": float(t.seconds_per_sample)}
+
+    def set_tuning(self, tuning: dict) -> None:
+        """Applies an autotune() result (capacity and traversal launch shape),
+        e.g. one found on a scene of the same image size and spp."""
+        t = RenderTuning(int(tuning["capacity"]), int(tuning["trace_shape"]), 0, 0.0)
+        check(_bind().yrc_render_scene_set_tuning(self._handle, C.byref(t)))
 
     def set_radiance_cache(self, cache, spread_threshold: float = 0.01, train_one_in: int = 16,
                            train_records: int = 65536, train: bool = True, train_steps: int = 1,
