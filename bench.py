@@ -489,11 +489,26 @@ def run_nrc(args):
         r = backend.render(prep)
         return r.linear(), r.stats
 
+    # The render autotuner's queue capacity and launch shape per spp level,
+    # found on the plain tracer and used by both tracers.
+    tunings = {}
+    if not args.no_autotune:
+        for spp in (1, 2, 4, 8, 16, 32, 64):
+            p = backend.prepare(scene(spp, SEEDS[0]), accel)
+            tunings[spp] = p.autotune()
+            p.close()
+
+    def prepare(spp, seed):
+        p = backend.prepare(scene(spp, seed), accel)
+        if spp in tunings:
+            p.set_tuning(tunings[spp])
+        return p
+
     plain = []
     for spp in (1, 2, 4, 8, 16, 32, 64):
         errs, secs = [], []
         for seed in SEEDS:
-            p = backend.prepare(scene(spp, seed), accel)
+            p = prepare(spp, seed)
             img, st = timed(p)
             errs.append(relmse(img, ref))
             secs.append(st["device_seconds"])
@@ -512,7 +527,7 @@ def run_nrc(args):
         for spp in (1, 4, 16):
             errs, secs, queries, segs = [], [], [], []
             for seed in SEEDS:
-                p = backend.prepare(scene(spp, seed), accel)
+                p = prepare(spp, seed)
                 p.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=1, averaged=True)
                 img, st = timed(p)
                 errs.append(relmse(img, ref))
@@ -543,6 +558,7 @@ def run_nrc(args):
             "config": {"workload": f"instanced-{W}x{H}-depth16-clamp20", "reference_spp": args.ref_spp,
                        "reference_accumulation": "fp64", "spread_threshold": C_SPREAD,
                        "seeds_per_point": len(SEEDS), "warmup_frames": WARM,
+                       "queue_capacity_per_spp": {s_: t["capacity"] for s_, t in tunings.items()},
                        "cache": "16x2^19x2 hash grid + SH4, 64x5 MLP, bf16 tcgen05, Adam 1e-2, "
                                 f"parameter moving average {DECAY}",
                        "cache_warmup_ms": round(warm_s * 1e3, 2)},
