@@ -870,7 +870,7 @@ __global__ void ClearOcclusionKernel(Queues q, int64_t slots) {
 // hits the probe stage selected, Sp / pdf, next-event estimation at the exit
 // through the normalised Fresnel-weighted cosine lobe (Sw), and the
 // continuation sampled from that lobe.
-__global__ void SubsurfaceExitKernel(DevScene sc, PathState ps, Queues q, int depth) {
+__global__ void __launch_bounds__(256, 2) SubsurfaceExitKernel(DevScene sc, PathState ps, Queues q, int depth) {
     const int64_t n = static_cast<int64_t>(q.counters[kCtrProbe]);
     for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
          k += static_cast<int64_t>(gridDim.x) * blockDim.x) {

@@ -60,21 +60,21 @@ __device__ __forceinline__ void CountLanes(unsigned long long* counter) {
 
 // Traversal stack of kTotal entries per thread: the first kShortStack in the
 // block's shared memory (column `col`, stride kBlock), the rest local.
-template <int kTotal, int kBlock = kTraceBlock>
+template <int kTotal, int kBlock = kTraceBlock, int kShort = kShortStack>
 struct StackStore {
     static constexpr int kTotalEntries = kTotal;
-    static constexpr int kLocal = kTotal > kShortStack ? kTotal - kShortStack : 1;
+    static constexpr int kLocal = kTotal > kShort ? kTotal - kShort : 1;
     int2 local[kLocal];
 
     __device__ __forceinline__ void Put(int2* col, int sp, int2 e) {
-        if (sp < kShortStack) {
+        if (sp < kShort) {
             col[sp * kBlock] = e;
         } else {
-            local[sp - kShortStack] = e;
+            local[sp - kShort] = e;
         }
     }
     __device__ __forceinline__ int2 Get(const int2* col, int sp) const {
-        return sp < kShortStack ? col[sp * kBlock] : local[sp - kShortStack];
+        return sp < kShort ? col[sp * kBlock] : local[sp - kShort];
     }
 };
 
@@ -168,6 +168,10 @@ __device__ __forceinline__ bool Pop(const float4* rays, int64_t ray, Traversal& 
 // kClearHits of them never matter: the reference's shadow loop gives up after
 // that many queries.
 constexpr int kClearHits = 16;  // MaxTransparentShadowHits
+// The shadow kernel keeps 11 stack entries in shared memory (the clear list
+// takes the rest) so that 8 blocks of 128 threads fit an SM.
+constexpr int kShadowShortStack = 11;
+constexpr int kShadowBlocksPerSm = 8;
 
 struct ClearHits {
     float* t;     // the lane's column, stride kTraceBlock
@@ -549,12 +553,12 @@ __global__ void __launch_bounds__(kTraceBlock) RenderProbeKernel(RenderProbeArgs
 // less the distance already advanced, not a new intersection from the
 // re-spawned origin. Persistent warps with per-lane refill, like TraceKernel.
 template <bool kTwo, int kTotal>
-__global__ void __launch_bounds__(kTraceBlock) ShadowTransmittanceKernel(ShadowArgs args) {
-    __shared__ int2 s_stack[kShortStack * kTraceBlock];
+__global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmittanceKernel(ShadowArgs args) {
+    __shared__ int2 s_stack[kShadowShortStack * kTraceBlock];
     __shared__ float s_clear_t[kClearHits * kTraceBlock];
     __shared__ int32_t s_clear_id[kClearHits * kTraceBlock];
     int2* col = s_stack + threadIdx.x;
-    StackStore<kTotal> st;
+    StackStore<kTotal, kTraceBlock, kShadowShortStack> st;
     Traversal s;
     ClearHits clear{s_clear_t + threadIdx.x, s_clear_id + threadIdx.x, 0, false};
     const unsigned lane = threadIdx.x & 31u;
@@ -693,7 +697,7 @@ __global__ void __launch_bounds__(kTraceBlock) ShadowTransmittanceKernel(ShadowA
         }
 #pragma unroll 1
         for (int k = 0; k < 8 && alive; ++k) {
-            alive = Step<true, false, kTwo, StackStore<kTotal>, true>(
+            alive = Step<true, false, kTwo, StackStore<kTotal, kTraceBlock, kShadowShortStack>, true>(
                 args.accel, args.rays, ray, s, st, col, args.error, args.tri_clear, args.sphere_clear, &clear);
             if (!alive) finish();
         }
