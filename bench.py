@@ -205,7 +205,14 @@ def run_gpu(args):
     from yaoray_b200 import accel, scenes
 
     geom = scenes.traversal_scene()
-    bvh = accel.build_bvh(geom)
+    t0 = time.perf_counter()
+    bvh, on_device = accel.build_bvh_device(geom)  # the reference's bytes, built on the GPU
+    build_device_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    host_bvh = accel.build_bvh(geom)  # the same build on the host's threads, for comparison
+    build_host_s = time.perf_counter() - t0
+    assert on_device and host_bvh.nodes.tobytes() == bvh.nodes.tobytes()
+    del host_bvh
     acc = accel.DeviceAccelerator(geom, bvh)
     rays_np = scenes.incoherent_rays(args.rays, seed=2 + 1000 * rank)
     n = rays_np.shape[0]
@@ -326,7 +333,9 @@ def run_gpu(args):
                        "l2": f"inputs larger than L2 (rays {n * 32 >> 20} MiB + hits {n * 16 >> 20} MiB + "
                              f"BVH {bvh_mib} MiB, L2 126 MB), no flush",
                        "parallelism": f"replicas x{ws}", "launch_shape": tune["shape"],
-                       "autotune_ms": tune["times_ms"]},
+                       "autotune_ms": tune["times_ms"],
+                       "bvh_build_s": {"device": round(build_device_s, 3), "host": round(build_host_s, 3),
+                                       "host_threads": os.cpu_count()}},
             "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": n * 32,
                     "d2h_bytes_per_step": n * 16},
             "gpu_launches": args.steps,

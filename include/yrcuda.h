@@ -142,6 +142,17 @@ void yrc_bvh_options_default(yrc_bvh_options* options);
  * YRC_ERR_BUILD with the reference's error string for invalid geometry.
  */
 yrc_status yrc_bvh_build(const yrc_geometry* geometry, const yrc_bvh_options* options, yrc_bvh** out);
+/*
+ * The same build with the hierarchy built on the current CUDA device: the
+ * same nodes, primitive_indices and primitives, byte for byte. Ranges the
+ * reference splits at the median (std::nth_element, used only when every
+ * centroid extent of a range is below 1e-8 or its box has no area) and
+ * median-split options are built by the host builder instead;
+ * *built_on_device (optional) is 1 when the device built the hierarchy.
+ * Synchronous. No counterpart in the reference (its builder is CPU-only).
+ */
+yrc_status yrc_bvh_build_device(const yrc_geometry* geometry, const yrc_bvh_options* options, yrc_bvh** out,
+                                int32_t* built_on_device);
 /* View of a built BVH; valid until yrc_bvh_destroy. */
 yrc_status yrc_bvh_get_view(const yrc_bvh* bvh, yrc_bvh_view* view);
 void yrc_bvh_destroy(yrc_bvh* bvh);
@@ -194,6 +205,12 @@ typedef struct yrc_two_level yrc_two_level; /* host-side built two-level BVH */
 
 /* BuildTwoLevelBvh (src/accel/two_level_bvh.cpp:257-331) on the host. */
 yrc_status yrc_two_level_build(const yrc_geometry* geometry, const yrc_bvh_options* options, yrc_two_level** out);
+/* The same build with every BLAS built by yrc_bvh_build_device's device
+ * path (byte-identical); the TLAS over the instances stays on the host.
+ * *device_blases (optional) counts the BLASes the device built. No
+ * counterpart in the reference. */
+yrc_status yrc_two_level_build_device(const yrc_geometry* geometry, const yrc_bvh_options* options,
+                                      yrc_two_level** out, int32_t* device_blases);
 yrc_status yrc_two_level_get_view(const yrc_two_level* two_level, yrc_two_level_view* view);
 void yrc_two_level_destroy(yrc_two_level* two_level);
 

@@ -163,6 +163,8 @@ def lib() -> C.CDLL:
         "yrc_device_available": (C.c_int, []),
         "yrc_bvh_options_default": (None, [P]),
         "yrc_bvh_build": (C.c_int, [P, P, P]),
+        "yrc_bvh_build_device": (C.c_int, [P, P, P, P]),
+        "yrc_two_level_build_device": (C.c_int, [P, P, P, P]),
         "yrc_bvh_get_view": (C.c_int, [P, P]),
         "yrc_bvh_destroy": (None, [P]),
         "yrc_two_level_build": (C.c_int, [P, P, P]),

@@ -204,14 +204,38 @@ def build_bvh(geometry: SceneGeometry, split_method: str = "sah", max_leaf_trian
         L.yrc_bvh_destroy(h)
 
 
+def build_bvh_device(geometry: SceneGeometry, split_method: str = "sah", max_leaf_triangles: int = 4):
+    """BuildBvh with the hierarchy built on the current CUDA device (byte-identical
+    to build_bvh). Returns (bvh, built_on_device): ranges the reference splits
+    at the median (std::nth_element) make the host builder build it."""
+    L = lib()
+    g = geometry.c_struct()
+    o = _options(split_method, max_leaf_triangles, 0, 1024)
+    h = C.c_void_p()
+    flag = C.c_int32(0)
+    check(L.yrc_bvh_build_device(C.byref(g), C.byref(o), C.byref(h), C.byref(flag)))
+    try:
+        v = _lib.BvhView()
+        check(L.yrc_bvh_get_view(h, C.byref(v)))
+        return _copy_bvh(v), bool(flag.value)
+    finally:
+        L.yrc_bvh_destroy(h)
+
+
 def build_two_level_bvh(geometry: SceneGeometry, split_method: str = "sah", max_leaf_triangles: int = 4,
-                        thread_count: int = 0, parallel_min_subtree_size: int = 1024) -> TwoLevelBvh:
-    """BuildTwoLevelBvh: one BLAS per mesh primitive + TLAS over instances."""
+                        thread_count: int = 0, parallel_min_subtree_size: int = 1024,
+                        device: bool = False) -> TwoLevelBvh:
+    """BuildTwoLevelBvh: one BLAS per mesh primitive + TLAS over instances;
+    with `device` the BLASes are built on the current CUDA device
+    (byte-identical)."""
     L = lib()
     g = geometry.c_struct()
     o = _options(split_method, max_leaf_triangles, thread_count, parallel_min_subtree_size)
     h = C.c_void_p()
-    check(L.yrc_two_level_build(C.byref(g), C.byref(o), C.byref(h)))
+    if device:
+        check(L.yrc_two_level_build_device(C.byref(g), C.byref(o), C.byref(h), None))
+    else:
+        check(L.yrc_two_level_build(C.byref(g), C.byref(o), C.byref(h)))
     try:
         v = _lib.TwoLevelView()
         check(L.yrc_two_level_get_view(h, C.byref(v)))

@@ -334,7 +334,26 @@ bool BuildHierarchy(std::vector<BuildRef>& refs, const yrc_bvh_options& options,
 }
 
 bool BuildFlatBvh(const yrc_geometry& g, const yrc_bvh_options& options, HostBvh& bvh,
-                  std::string& error) {
+                  std::string& error, bool device, bool* on_device) {
+    if (on_device) *on_device = false;
+    if (device) {
+        if (!ValidOptions(options, error)) {
+            bvh = HostBvh{};
+            return false;
+        }
+        bvh = HostBvh{};
+        const int r = BuildFlatDevice(g, options, bvh, error);
+        if (r < 0) {
+            bvh = HostBvh{};
+            return false;
+        }
+        if (r > 0) {
+            if (on_device) *on_device = true;
+            return true;
+        }
+        bvh = HostBvh{};
+        error.clear();
+    }
     bvh = HostBvh{};
     std::vector<BuildRef> refs;
     refs.reserve(static_cast<size_t>(g.index_count / 3 + g.sphere_count));
@@ -461,6 +480,32 @@ yrc_status yrc_bvh_build(const yrc_geometry* geometry, const yrc_bvh_options* op
         delete holder;
         return yrc::Fail(YRC_ERR_OUT_OF_MEMORY, std::string("yrc_bvh_build: ") + e.what());
     }
+    *out = holder;
+    return yrc::Ok();
+}
+
+yrc_status yrc_bvh_build_device(const yrc_geometry* geometry, const yrc_bvh_options* options, yrc_bvh** out,
+                                int32_t* built_on_device) {
+    if (!geometry || !out) return yrc::Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_bvh_build_device: null argument");
+    *out = nullptr;
+    if (built_on_device) *built_on_device = 0;
+    yrc_bvh_options opts;
+    yrc_bvh_options_default(&opts);
+    if (options) opts = *options;
+    auto holder = new (std::nothrow) yrc_bvh();
+    if (!holder) return yrc::Fail(YRC_ERR_OUT_OF_MEMORY, "yrc_bvh_build_device: host allocation failed");
+    std::string error;
+    bool on_device = false;
+    try {
+        if (!yrc::BuildFlatBvh(*geometry, opts, holder->bvh, error, true, &on_device)) {
+            delete holder;
+            return yrc::Fail(error.rfind("device BVH build", 0) == 0 ? YRC_ERR_CUDA : YRC_ERR_BUILD, error);
+        }
+    } catch (const std::exception& e) {
+        delete holder;
+        return yrc::Fail(YRC_ERR_OUT_OF_MEMORY, std::string("yrc_bvh_build_device: ") + e.what());
+    }
+    if (built_on_device) *built_on_device = on_device ? 1 : 0;
     *out = holder;
     return yrc::Ok();
 }

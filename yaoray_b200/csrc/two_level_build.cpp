@@ -104,7 +104,8 @@ bool BuildTlas(const yrc_geometry& g, const yrc_bvh_options& options, HostTwoLev
     return BuildHierarchy(refs, options, tl.tlas, error);
 }
 
-bool BuildTwoLevel(const yrc_geometry& g, const yrc_bvh_options& options, HostTwoLevel& tl, std::string& error) {
+bool BuildTwoLevel(const yrc_geometry& g, const yrc_bvh_options& options, HostTwoLevel& tl, std::string& error,
+                   bool device = false, int32_t* device_blases = nullptr) {
     int32_t flat_offset = 0;
     for (int32_t i = 0; i < g.primitive_count; ++i) {
         yrc_geometry one = g;
@@ -115,7 +116,9 @@ bool BuildTwoLevel(const yrc_geometry& g, const yrc_bvh_options& options, HostTw
         one.instances = nullptr;
         one.instance_count = 0;
         HostTwoLevel::Blas blas;
-        if (!BuildFlatBvh(one, options, blas.bvh, error)) return false;
+        bool on_device = false;
+        if (!BuildFlatBvh(one, options, blas.bvh, error, device, &on_device)) return false;
+        if (on_device && device_blases) ++*device_blases;
         if (blas.bvh.nodes.empty()) {
             error = "BLAS build encountered an empty mesh primitive";
             return false;
@@ -192,6 +195,30 @@ yrc_status yrc_two_level_build(const yrc_geometry* geometry, const yrc_bvh_optio
     } catch (const std::exception& e) {
         delete holder;
         return yrc::Fail(YRC_ERR_OUT_OF_MEMORY, std::string("yrc_two_level_build: ") + e.what());
+    }
+    *out = holder;
+    return yrc::Ok();
+}
+
+yrc_status yrc_two_level_build_device(const yrc_geometry* geometry, const yrc_bvh_options* options,
+                                      yrc_two_level** out, int32_t* device_blases) {
+    if (!geometry || !out) return yrc::Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_two_level_build_device: null argument");
+    *out = nullptr;
+    if (device_blases) *device_blases = 0;
+    yrc_bvh_options opts;
+    yrc_bvh_options_default(&opts);
+    if (options) opts = *options;
+    auto holder = new (std::nothrow) yrc_two_level();
+    if (!holder) return yrc::Fail(YRC_ERR_OUT_OF_MEMORY, "yrc_two_level_build_device: host allocation failed");
+    std::string error;
+    try {
+        if (!yrc::BuildTwoLevel(*geometry, opts, holder->tl, error, true, device_blases)) {
+            delete holder;
+            return yrc::Fail(error.rfind("device BVH build", 0) == 0 ? YRC_ERR_CUDA : YRC_ERR_BUILD, error);
+        }
+    } catch (const std::exception& e) {
+        delete holder;
+        return yrc::Fail(YRC_ERR_OUT_OF_MEMORY, std::string("yrc_two_level_build_device: ") + e.what());
     }
     *out = holder;
     return yrc::Ok();

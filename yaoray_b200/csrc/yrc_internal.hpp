@@ -58,8 +58,24 @@ bool BuildHierarchy(std::vector<BuildRef>& refs, const yrc_bvh_options& options,
                     std::string& error);
 
 // Builds a flat BVH (primitives + hierarchy) over a geometry's triangles and
-// spheres, as BuildBvh does.
+// spheres, as BuildBvh does; with `device`, the hierarchy is built on the
+// current CUDA device (BuildHierarchyDevice) unless that reports a range it
+// leaves to the host, and *on_device (optional) tells which happened.
 bool BuildFlatBvh(const yrc_geometry& geometry, const yrc_bvh_options& options, HostBvh& bvh,
-                  std::string& error);
+                  std::string& error, bool device = false, bool* on_device = nullptr);
+
+// The hierarchy of BuildHierarchy built on the current CUDA device, byte for
+// byte the same. Returns 1 when built, 0 when a range needs the median split
+// (std::nth_element) or the options ask for median splits — the caller then
+// builds on the host — and -1 on a device error (`error` set). `refs` are
+// not reordered.
+int BuildHierarchyDevice(std::vector<BuildRef>& refs, const yrc_bvh_options& options, HostBvh& bvh,
+                         std::string& error);
+
+// The whole flat build on the current CUDA device: refs and primitives from
+// the geometry (uploaded), then the hierarchy; same return convention (0 for
+// median splits and for invalid geometry, which the host build reports).
+int BuildFlatDevice(const yrc_geometry& geometry, const yrc_bvh_options& options, HostBvh& bvh,
+                    std::string& error);
 
 }  // namespace yrc

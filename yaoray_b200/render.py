@@ -19,7 +19,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import YrcError, check, lib, ptr
-from .accel import SceneGeometry, build_bvh, build_two_level_bvh
+from .accel import SceneGeometry, build_bvh, build_bvh_device, build_two_level_bvh
 
 # --------------------------------------------------------------- C mirrors
 
@@ -474,9 +474,13 @@ class CudaBackend:
                 "supports_offline_progress": True, "supports_texture_materials": False}
 
     def prepare(self, scene: RenderScene, accel=None) -> PreparedScene:
-        """Builds the reference-layout BVH on the host (unless given) and uploads."""
+        """Builds the reference-layout BVH on the device (unless given; the
+        reference's bytes, see accel.build_bvh_device) and uploads."""
         if accel is None:
-            accel = build_two_level_bvh(scene.geometry) if scene.geometry.instances.size else build_bvh(scene.geometry)
+            if scene.geometry.instances.size:
+                accel = build_two_level_bvh(scene.geometry, device=True)
+            else:
+                accel = build_bvh_device(scene.geometry)[0]
         return PreparedScene(scene, accel)
 
     def render(self, prepared: PreparedScene, request: RenderRequestPy | None = None) -> RenderResult:
