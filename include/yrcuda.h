@@ -671,6 +671,21 @@ yrc_status yrc_render_scene_set_tuning(yrc_render_scene* scene, const yrc_render
 yrc_status yrc_render(yrc_render_scene* scene, const yrc_render_request* request, yrc_film_pixel* film_out,
                       uint64_t* bad_samples_out, yrc_render_stats* stats);
 
+/*
+ * Renders `count` prepared scenes together: after each scene's setup (as in
+ * yrc_render), every step launches ONE CUDA graph that holds the batch graph
+ * of every scene still rendering, so uneven jobs share each launch and one
+ * host synchronisation; a scene that finishes leaves the combined graph.
+ * Per scene the results equal yrc_render's (films byte for byte). requests
+ * (optional, per scene) may resume and stop, not report progress; scenes
+ * must differ, share one device, and not share a radiance cache.
+ * stats[i].device_seconds and *device_seconds (optional) are the device time
+ * of the whole call. No counterpart in the reference.
+ */
+yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t count, const yrc_render_request* requests,
+                           yrc_film_pixel* const* films_out, uint64_t* bad_samples_out, yrc_render_stats* stats,
+                           double* device_seconds);
+
 /* Wait for all work the library queued on `stream` (NULL = legacy default). */
 yrc_status yrc_stream_synchronize(void* stream);
 

@@ -31,3 +31,23 @@ def test_concurrent_matches_sequential():
             assert f["sum"].mean() > 0
     finally:
         runner.close(jobs)
+
+
+def test_shared_launch_matches_single_renders():
+    """yrc_render_many: one graph launch per step for all unfinished jobs;
+    films equal one-at-a-time renders for the jobs without a cache."""
+    jobs = batch.job_set(6, seed=13, spp_scale=1 / 64, max_triangles=100_000)
+    runner = batch.JobRunner(keep_films=True)
+    try:
+        runner.prepare(jobs)
+        runner.run_sequential(jobs)
+        films = {j.name: j.film.copy() for j in jobs}
+        res = runner.run_shared_launch(jobs, concurrency=6)
+        assert all(j.ok for j in jobs), [j.error for j in jobs if not j.ok]
+        assert res.peak_concurrency > 1
+        for j in jobs:
+            assert (j.film["samples"] == j.scene.spp).all()
+            if not j.use_cache:
+                assert j.film.tobytes() == films[j.name].tobytes(), j.name
+    finally:
+        runner.close(jobs)

@@ -239,6 +239,38 @@ class JobRunner:
         wall = time.perf_counter() - t0
         return BatchResult(list(jobs), wall, sum(j.samples for j in jobs), peak[0], {"budget_bytes": budget})
 
+    def run_shared_launch(self, jobs: list[Job], concurrency: int = 8, budget_bytes: int | None = None) -> BatchResult:
+        """Renders the jobs in groups of up to `concurrency` (largest first,
+        admitted against the budget like run_concurrent), each group with
+        one yrc_render_many call: every step of a group is ONE graph launch
+        holding all of its unfinished jobs. A job's latency is its group's
+        call."""
+        budget = budget_bytes if budget_bytes is not None else max(_free_device_bytes() - self.reserve, 0)
+        order = sorted(jobs, key=lambda j: -j.scene.width * j.scene.height * j.scene.spp)
+        peak = 0
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(order):
+            group, used = [order[i]], _working_set(order[i])
+            i += 1
+            while i < len(order) and len(group) < concurrency and used + _working_set(order[i]) <= budget:
+                used += _working_set(order[i])
+                group.append(order[i])
+                i += 1
+            peak = max(peak, len(group))
+            g0 = time.perf_counter()
+            results = self.backend.render_many([j.prepared for j in group])
+            dt = time.perf_counter() - g0
+            for job, res in zip(group, results):
+                job.latency_s = dt
+                job.ok, job.error = res.ok, res.error
+                job.resident = job.resident or res.ok
+                job.device_s = res.stats.get("device_seconds", 0.0)
+                job.samples = int(res.stats.get("samples_rendered", 0))
+                job.film = res.film if self.keep_films else None
+        wall = time.perf_counter() - t0
+        return BatchResult(list(jobs), wall, sum(j.samples for j in jobs), peak, {"budget_bytes": budget})
+
     def close(self, jobs: list[Job]) -> None:
         for job in jobs:
             if job.prepared is not None:

@@ -106,6 +106,7 @@ struct yrc_render_scene {
     int32_t* batch = nullptr;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
+    cudaGraph_t graph_template = nullptr;  // the captured batch, kept for multi-scene launches
     int32_t graph_max_batch = -1;
     int64_t capacity_choice = 0;  // queue capacity chosen by the autotuner or the caller (0: from the image)
     // Radiance cache (optional).
@@ -117,12 +118,24 @@ struct yrc_render_scene {
     std::mutex mutex;
 };
 
+namespace yrc {
+namespace {
+// Releases the scene's captured batch (executable and template).
+void DropGraph(yrc_render_scene* s) {
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    if (s->graph_template) cudaGraphDestroy(s->graph_template);
+    s->graph = nullptr;
+    s->graph_template = nullptr;
+}
+}  // namespace
+}  // namespace yrc
+
 extern "C" {
 
 void yrc_render_scene_destroy(yrc_render_scene* scene) {
     if (!scene) return;
     cudaSetDevice(scene->device);
-    if (scene->graph) cudaGraphExecDestroy(scene->graph);
+    yrc::DropGraph(scene);
     if (scene->stream) cudaStreamDestroy(scene->stream);
     scene->cache_work.Release();
     scene->work.Release();
@@ -143,10 +156,7 @@ yrc_status yrc_render_scene_set_cache(yrc_render_scene* scene, yrc_nrc* cache, c
     std::lock_guard<std::mutex> lock(scene->mutex);
     cudaSetDevice(scene->device);
     if (scene->stream) cudaStreamSynchronize(scene->stream);
-    if (scene->graph) {
-        cudaGraphExecDestroy(scene->graph);
-        scene->graph = nullptr;
-    }
+    yrc::DropGraph(scene);
     scene->cache_work.Release();
     scene->cargs = CacheArgs{};
     scene->cache_capacity = 0;
@@ -486,10 +496,7 @@ int64_t RenderCapacity(const yrc_render_scene* s) {
 yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     const int64_t pixels = static_cast<int64_t>(s->settings.width) * s->settings.height;
     if (s->capacity == capacity && s->film) return Ok();
-    if (s->graph) {
-        cudaGraphExecDestroy(s->graph);
-        s->graph = nullptr;
-    }
+    DropGraph(s);
     s->work.Release();
     DeviceArena& W = s->work;
     PathState& ps = s->ps;
@@ -557,10 +564,7 @@ yrc_status EnsureCache(yrc_render_scene* s) {
         return Ok();
     }
     if (s->cache_capacity == s->capacity && s->cargs.enabled) return Ok();
-    if (s->graph) {
-        cudaGraphExecDestroy(s->graph);
-        s->graph = nullptr;
-    }
+    DropGraph(s);
     s->cache_work.Release();
     DeviceArena& W = s->cache_work;
     const yrc_cache_settings& cs = s->cache_settings;
@@ -715,8 +719,7 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
 // unless the scene holds one for this batch bound.
 yrc_status EnsureGraph(yrc_render_scene* s, int32_t max_batch) {
     if (s->graph && s->graph_max_batch == max_batch) return Ok();
-    if (s->graph) cudaGraphExecDestroy(s->graph);
-    s->graph = nullptr;
+    DropGraph(s);
     cudaGraph_t graph = nullptr;
     cudaError_t err = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
     if (err != cudaSuccess) return CudaError(err, "graph capture");
@@ -728,15 +731,13 @@ yrc_status EnsureGraph(yrc_render_scene* s, int32_t max_batch) {
     }
     if (err != cudaSuccess) return CudaError(err, "graph capture");
     err = cudaGraphInstantiate(&s->graph, graph, 0);
-    cudaGraphDestroy(graph);
-    if (err != cudaSuccess) return CudaError(err, "graph instantiate");
+    if (err != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return CudaError(err, "graph instantiate");
+    }
+    s->graph_template = graph;
     s->graph_max_batch = max_batch;
     return Ok();
-}
-
-void DropGraph(yrc_render_scene* s) {
-    if (s->graph) cudaGraphExecDestroy(s->graph);
-    s->graph = nullptr;
 }
 
 // Renders sample indices 0..passes-1 of every pixel into the device film
@@ -791,23 +792,45 @@ yrc_status ProbeRender(yrc_render_scene* s, int32_t passes, double* seconds) {
 }  // namespace
 }  // namespace yrc
 
-extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* req, yrc_film_pixel* film_out,
-                                 uint64_t* bad_samples_out, yrc_render_stats* stats) {
-    using namespace yrc;
-    if (!s || !film_out) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render: null argument");
-    std::lock_guard<std::mutex> lock(s->mutex);
+namespace yrc {
+namespace {
+
+// One render call on one prepared scene, split into the steps that a
+// multi-scene call interleaves: Begin (checks, uploads, active list, batch
+// graph), per batch Queue / Collect, Finish (film and statistics).
+struct RenderRun {
+    yrc_render_scene* s = nullptr;
+    yrc_render_request r{};
+    yrc_film_pixel* film_out = nullptr;
+    uint64_t* bad_out = nullptr;
+    yrc_render_stats* stats = nullptr;
+    std::chrono::steady_clock::time_point start;
+    std::vector<yrc_film_pixel> host_film;
+    int64_t pixels = 0;
+    int spp = 1;
+    int completed_passes = 0;
+    unsigned long long sc_host[4] = {0, 0, 0, 0};  // active, next, bad, converged
+    unsigned long long cache_host[4] = {0, 0, 0, 0};
+    int32_t batch_host = 0;
+    int32_t this_batch = 0;
+    uint64_t converged = 0;
+    uint64_t cache_queries = 0, cache_records = 0;
+    bool active() const { return sc_host[0] > 0; }
+};
+
+yrc_status BeginRender(RenderRun& run) {
+    yrc_render_scene* s = run.s;
     cudaSetDevice(s->device);
-    const auto start = std::chrono::steady_clock::now();
+    run.start = std::chrono::steady_clock::now();
     const yrc_render_settings& st = s->settings;
-    const int64_t pixels = static_cast<int64_t>(st.width) * st.height;
-    const int spp = std::max(1, st.spp);
-    yrc_render_request none{};
-    const yrc_render_request& r = req ? *req : none;
-    if (r.resume_completed_spp < 0 || r.resume_completed_spp > spp) {
+    run.pixels = static_cast<int64_t>(st.width) * st.height;
+    run.spp = std::max(1, st.spp);
+    const yrc_render_request& r = run.r;
+    if (r.resume_completed_spp < 0 || r.resume_completed_spp > run.spp) {
         return Fail(YRC_ERR_INVALID_ARGUMENT, "invalid resume completed spp");
     }
     if (r.resume_film) {
-        for (int64_t i = 0; i < pixels; ++i) {
+        for (int64_t i = 0; i < run.pixels; ++i) {
             const uint32_t count = r.resume_film[i].samples;
             const bool bad = st.adaptive_enabled ? count > static_cast<uint32_t>(r.resume_completed_spp)
                                                  : count != static_cast<uint32_t>(r.resume_completed_spp);
@@ -820,122 +843,286 @@ extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* 
     if (status == YRC_OK) status = EnsureCache(s);
     if (status != YRC_OK) return status;
     cudaStream_t stream = s->stream;
-    std::vector<yrc_film_pixel> host_film(static_cast<size_t>(pixels));
+    run.host_film.resize(static_cast<size_t>(run.pixels));
     if (r.resume_film) {
-        std::memcpy(host_film.data(), r.resume_film, sizeof(yrc_film_pixel) * static_cast<size_t>(pixels));
+        std::memcpy(run.host_film.data(), r.resume_film, sizeof(yrc_film_pixel) * static_cast<size_t>(run.pixels));
     } else {
-        std::memset(host_film.data(), 0, sizeof(yrc_film_pixel) * static_cast<size_t>(pixels));
+        std::memset(run.host_film.data(), 0, sizeof(yrc_film_pixel) * static_cast<size_t>(run.pixels));
     }
-    std::vector<int32_t> attempts(static_cast<size_t>(pixels), spp - r.resume_completed_spp);
-    cudaMemcpyAsync(s->film, host_film.data(), sizeof(yrc_film_pixel) * pixels, cudaMemcpyHostToDevice, stream);
-    cudaMemcpyAsync(s->attempts, attempts.data(), sizeof(int32_t) * pixels, cudaMemcpyHostToDevice, stream);
+    std::vector<int32_t> attempts(static_cast<size_t>(run.pixels), run.spp - r.resume_completed_spp);
+    cudaMemcpyAsync(s->film, run.host_film.data(), sizeof(yrc_film_pixel) * run.pixels, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(s->attempts, attempts.data(), sizeof(int32_t) * run.pixels, cudaMemcpyHostToDevice, stream);
     const unsigned long long init_scalars[4] = {0, 0, r.resume_bad_samples, 0};
     cudaMemcpyAsync(s->scalars, init_scalars, sizeof(init_scalars), cudaMemcpyHostToDevice, stream);
     cudaMemsetAsync(s->q.counters, 0, sizeof(unsigned long long) * kCtrCount, stream);
-    const int32_t max_batch = r.progress ? 1 : std::min(spp, kMaxBatch);
+    const int32_t max_batch = r.progress ? 1 : std::min(run.spp, kMaxBatch);
     {
         const DevScene& sc = s->dev;
         BatchArgs b{s->active, s->scalars + 0, s->scalars + 1, s->batch, s->film};
         FilmArgs f{s->attempts, s->scalars + 2, s->scalars + 3, st.adaptive_enabled, st.adaptive_min_spp,
                    st.adaptive_relative_error, st.adaptive_absolute_error, st.adaptive_confidence};
-        LaunchActivePixels(sc, b, f, pixels, s->sm_count, stream);
+        LaunchActivePixels(sc, b, f, run.pixels, s->sm_count, stream);
         LaunchFinishActive(s->scalars + 0, s->scalars + 1, s->batch, max_batch, s->capacity, stream);
     }
     status = EnsureGraph(s, max_batch);
     if (status != YRC_OK) return status;
-
-    int completed_passes = r.resume_completed_spp;
-    uint64_t total_samples = 0;
-    for (int64_t i = 0; i < pixels; ++i) total_samples += host_film[static_cast<size_t>(i)].samples;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, stream);
-    unsigned long long sc_host[4] = {0, 0, 0, 0};
-    int32_t batch_host = 0;
-    cudaMemcpyAsync(sc_host, s->scalars, sizeof(sc_host), cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(&batch_host, s->batch, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
-    cudaError_t err = cudaStreamSynchronize(stream);
+    run.completed_passes = r.resume_completed_spp;
+    cudaMemcpyAsync(run.sc_host, s->scalars, sizeof(run.sc_host), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(&run.batch_host, s->batch, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
+    const cudaError_t err = cudaStreamSynchronize(stream);
     if (err != cudaSuccess) return CudaError(err, "render setup");
-    uint64_t converged = sc_host[3];
-    uint64_t cache_queries = 0, cache_records = 0;
-    while (sc_host[0] > 0) {
-        if (r.stop_flag && *r.stop_flag) return Fail(YRC_ERR_CANCELLED, "render cancelled");
-        const int32_t this_batch = batch_host;
-        cudaMemsetAsync(s->scalars + 3, 0, sizeof(unsigned long long), stream);  // recounted by the batch
-        err = cudaGraphLaunch(s->graph, stream);
-        if (err != cudaSuccess) return CudaError(err, "batch launch");
-        cudaMemcpyAsync(sc_host, s->scalars, sizeof(sc_host), cudaMemcpyDeviceToHost, stream);
-        cudaMemcpyAsync(&batch_host, s->batch, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
-        unsigned long long cache_host[4] = {0, 0, 0, 0};
-        if (s->cargs.enabled) {
-            cudaMemcpyAsync(cache_host, s->cargs.counters, sizeof(cache_host), cudaMemcpyDeviceToHost, stream);
-        }
-        err = cudaStreamSynchronize(stream);
-        if (err != cudaSuccess) return CudaError(err, "batch");
-        cache_queries += cache_host[0];
-        cache_records += std::min<unsigned long long>(cache_host[2], static_cast<unsigned long long>(
-                                                                        std::max(s->cargs.train_records, 0)));
-        completed_passes += this_batch;
-        converged = sc_host[3];
-        if (r.progress) {
-            cudaMemcpy(host_film.data(), s->film, sizeof(yrc_film_pixel) * pixels, cudaMemcpyDeviceToHost);
-            uint64_t done = 0;
-            for (int64_t i = 0; i < pixels; ++i) done += host_film[static_cast<size_t>(i)].samples;
-            unsigned long long counters[kCtrCount];
-            cudaMemcpy(counters, s->q.counters, sizeof(counters), cudaMemcpyDeviceToHost);
-            yrc_render_progress prog{};
-            prog.completed_spp = std::min(completed_passes, spp);
-            prog.target_spp = spp;
-            prog.completed_samples = done;
-            prog.target_samples = static_cast<uint64_t>(spp) * static_cast<uint64_t>(pixels);
-            prog.active_pixels = sc_host[0];
-            prog.converged_pixels = sc_host[3];
-            prog.rays_traced = counters[kCtrStatsBase + 0];
-            prog.elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
-            char msg[512] = {0};
-            if (r.progress(&prog, host_film.data(), sc_host[2], r.user, msg, sizeof(msg))) {
-                return Fail(YRC_ERR_CANCELLED, msg[0] ? msg : "render cancelled by progress callback");
-            }
-        }
+    run.converged = run.sc_host[3];
+    return Ok();
+}
+
+// Work before a batch launch and the readback after it, on `stream`.
+void QueueBatchPrologue(RenderRun& run, cudaStream_t stream) {
+    run.this_batch = run.batch_host;
+    cudaMemsetAsync(run.s->scalars + 3, 0, sizeof(unsigned long long), stream);  // recounted by the batch
+}
+void QueueBatchReadback(RenderRun& run, cudaStream_t stream) {
+    yrc_render_scene* s = run.s;
+    cudaMemcpyAsync(run.sc_host, s->scalars, sizeof(run.sc_host), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(&run.batch_host, s->batch, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
+    if (s->cargs.enabled) {
+        cudaMemcpyAsync(run.cache_host, s->cargs.counters, sizeof(run.cache_host), cudaMemcpyDeviceToHost, stream);
     }
-    cudaEventRecord(e1, stream);
-    err = cudaMemcpyAsync(film_out, s->film, sizeof(yrc_film_pixel) * pixels, cudaMemcpyDeviceToHost, stream);
+}
+// After the readback completed.
+void CollectBatch(RenderRun& run) {
+    yrc_render_scene* s = run.s;
+    if (s->cargs.enabled) {
+        run.cache_queries += run.cache_host[0];
+        run.cache_records += std::min<unsigned long long>(
+            run.cache_host[2], static_cast<unsigned long long>(std::max(s->cargs.train_records, 0)));
+    }
+    run.completed_passes += run.this_batch;
+    run.converged = run.sc_host[3];
+}
+
+yrc_status FinishRender(RenderRun& run, double device_seconds) {
+    yrc_render_scene* s = run.s;
+    cudaStream_t stream = s->stream;
+    const int64_t pixels = run.pixels;
+    cudaError_t err = cudaMemcpyAsync(run.film_out, s->film, sizeof(yrc_film_pixel) * pixels, cudaMemcpyDeviceToHost,
+                                      stream);
     unsigned long long counters[kCtrCount];
-    if (err == cudaSuccess) err = cudaMemcpyAsync(counters, s->q.counters, sizeof(counters), cudaMemcpyDeviceToHost, stream);
+    if (err == cudaSuccess) {
+        err = cudaMemcpyAsync(counters, s->q.counters, sizeof(counters), cudaMemcpyDeviceToHost, stream);
+    }
     unsigned long long fin[4];
     if (err == cudaSuccess) err = cudaMemcpyAsync(fin, s->scalars, sizeof(fin), cudaMemcpyDeviceToHost, stream);
     if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
     if (err != cudaSuccess) return CudaError(err, "render readback");
-    status = CheckDeviceError(s->accel);
+    const yrc_status status = CheckDeviceError(s->accel);
     if (status != YRC_OK) return status;
-    float device_ms = 0.0f;
-    cudaEventElapsedTime(&device_ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (bad_samples_out) *bad_samples_out = fin[2];
-    if (stats) {
+    if (run.bad_out) *run.bad_out = fin[2];
+    if (run.stats) {
+        yrc_render_stats* stats = run.stats;
         std::memset(stats, 0, sizeof(*stats));
         uint64_t done = 0;
-        for (int64_t i = 0; i < pixels; ++i) done += film_out[i].samples;
+        for (int64_t i = 0; i < pixels; ++i) done += run.film_out[i].samples;
         stats->samples_rendered = done;
-        stats->converged_pixels = converged;
+        stats->converged_pixels = run.converged;
         stats->rays_traced = counters[kCtrStatsBase + 0];
         stats->shadow_rays = counters[kCtrStatsBase + 1];
         stats->occluded_shadow_rays = counters[kCtrStatsBase + 2];
         stats->hits = counters[kCtrStatsBase + 3];
         stats->misses = counters[kCtrStatsBase + 4];
-        stats->cache_queries = cache_queries;
-        stats->cache_records = cache_records;
+        stats->cache_queries = run.cache_queries;
+        stats->cache_records = run.cache_records;
         stats->bad_samples = fin[2];
         stats->bvh_nodes = s->bvh_nodes;
         stats->bvh_max_depth = s->bvh_max_depth;
         stats->threads = 1;
-        stats->device_seconds = device_ms / 1e3;
-        stats->elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+        stats->device_seconds = device_seconds;
+        stats->elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - run.start).count();
     }
-    (void)total_samples;
     return Ok();
+}
+
+}  // namespace
+}  // namespace yrc
+
+extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* req, yrc_film_pixel* film_out,
+                                 uint64_t* bad_samples_out, yrc_render_stats* stats) {
+    using namespace yrc;
+    if (!s || !film_out) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render: null argument");
+    std::lock_guard<std::mutex> lock(s->mutex);
+    RenderRun run;
+    run.s = s;
+    if (req) run.r = *req;
+    run.film_out = film_out;
+    run.bad_out = bad_samples_out;
+    run.stats = stats;
+    yrc_status status = BeginRender(run);
+    if (status != YRC_OK) return status;
+    const yrc_render_request& r = run.r;
+    cudaStream_t stream = s->stream;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, stream);
+    while (run.active()) {
+        if (r.stop_flag && *r.stop_flag) return Fail(YRC_ERR_CANCELLED, "render cancelled");
+        QueueBatchPrologue(run, stream);
+        cudaError_t err = cudaGraphLaunch(s->graph, stream);
+        if (err != cudaSuccess) return CudaError(err, "batch launch");
+        QueueBatchReadback(run, stream);
+        err = cudaStreamSynchronize(stream);
+        if (err != cudaSuccess) return CudaError(err, "batch");
+        CollectBatch(run);
+        if (r.progress) {
+            const int64_t pixels = run.pixels;
+            cudaMemcpy(run.host_film.data(), s->film, sizeof(yrc_film_pixel) * pixels, cudaMemcpyDeviceToHost);
+            uint64_t done = 0;
+            for (int64_t i = 0; i < pixels; ++i) done += run.host_film[static_cast<size_t>(i)].samples;
+            unsigned long long counters[kCtrCount];
+            cudaMemcpy(counters, s->q.counters, sizeof(counters), cudaMemcpyDeviceToHost);
+            yrc_render_progress prog{};
+            prog.completed_spp = std::min(run.completed_passes, run.spp);
+            prog.target_spp = run.spp;
+            prog.completed_samples = done;
+            prog.target_samples = static_cast<uint64_t>(run.spp) * static_cast<uint64_t>(pixels);
+            prog.active_pixels = run.sc_host[0];
+            prog.converged_pixels = run.sc_host[3];
+            prog.rays_traced = counters[kCtrStatsBase + 0];
+            prog.elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - run.start).count();
+            char msg[512] = {0};
+            if (r.progress(&prog, run.host_film.data(), run.sc_host[2], r.user, msg, sizeof(msg))) {
+                return Fail(YRC_ERR_CANCELLED, msg[0] ? msg : "render cancelled by progress callback");
+            }
+        }
+    }
+    cudaEventRecord(e1, stream);
+    cudaEventSynchronize(e1);
+    float device_ms = 0.0f;
+    cudaEventElapsedTime(&device_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return FinishRender(run, device_ms / 1e3);
+}
+
+extern "C" yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t count,
+                                      const yrc_render_request* requests, yrc_film_pixel* const* films_out,
+                                      uint64_t* bad_samples_out, yrc_render_stats* stats, double* device_seconds) {
+    using namespace yrc;
+    if (count < 0 || (count > 0 && (!scenes || !films_out))) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: bad argument");
+    }
+    if (count == 0) return Ok();
+    // One lock per scene, taken in address order; every scene on one device.
+    std::vector<yrc_render_scene*> order(scenes, scenes + count);
+    for (int32_t i = 0; i < count; ++i) {
+        if (!order[static_cast<size_t>(i)] || !films_out[i]) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: null scene or film");
+        for (int32_t j = 0; j < i; ++j) {
+            if (order[static_cast<size_t>(j)] == order[static_cast<size_t>(i)]) {
+                return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: a scene appears twice");
+            }
+        }
+        if (order[static_cast<size_t>(i)]->device != order[0]->device) {
+            return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: scenes on different devices");
+        }
+        if (requests && requests[i].progress) {
+            return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: progress callbacks are not supported");
+        }
+        for (int32_t j = 0; j < i; ++j) {
+            if (scenes[i]->cache && scenes[i]->cache == scenes[j]->cache) {
+                return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: two scenes share a radiance cache");
+            }
+        }
+    }
+    std::sort(order.begin(), order.end());
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (yrc_render_scene* s : order) locks.emplace_back(s->mutex);
+    cudaSetDevice(scenes[0]->device);
+    std::vector<RenderRun> runs(static_cast<size_t>(count));
+    for (int32_t i = 0; i < count; ++i) {
+        RenderRun& run = runs[static_cast<size_t>(i)];
+        run.s = scenes[i];
+        if (requests) run.r = requests[i];
+        run.film_out = films_out[i];
+        run.bad_out = bad_samples_out ? bad_samples_out + i : nullptr;
+        run.stats = stats ? stats + i : nullptr;
+        const yrc_status status = BeginRender(run);
+        if (status != YRC_OK) return status;
+    }
+    cudaStream_t stream = nullptr;
+    cudaError_t err = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) return CudaError(err, "render stream");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, stream);
+    // Each step launches one graph holding the batch graph of every scene
+    // still rendering (child graphs, independent of one another); the
+    // combined graph is rebuilt when a scene finishes.
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int32_t> members;
+    yrc_status status = YRC_OK;
+    for (;;) {
+        std::vector<int32_t> live;
+        for (int32_t i = 0; i < count; ++i) {
+            if (runs[static_cast<size_t>(i)].active()) live.push_back(i);
+        }
+        if (live.empty()) break;
+        bool cancelled = false;
+        for (int32_t i : live) {
+            const yrc_render_request& r = runs[static_cast<size_t>(i)].r;
+            if (r.stop_flag && *r.stop_flag) cancelled = true;
+        }
+        if (cancelled) {
+            status = Fail(YRC_ERR_CANCELLED, "render cancelled");
+            break;
+        }
+        if (live != members) {
+            if (exec) cudaGraphExecDestroy(exec);
+            exec = nullptr;
+            cudaGraph_t combined = nullptr;
+            err = cudaGraphCreate(&combined, 0);
+            for (int32_t i : live) {
+                cudaGraphNode_t node = nullptr;
+                if (err == cudaSuccess) {
+                    err = cudaGraphAddChildGraphNode(&node, combined, nullptr, 0,
+                                                     runs[static_cast<size_t>(i)].s->graph_template);
+                }
+            }
+            if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, combined, 0);
+            if (combined) cudaGraphDestroy(combined);
+            if (err != cudaSuccess) {
+                status = CudaError(err, "combined batch graph");
+                break;
+            }
+            members = live;
+        }
+        for (int32_t i : live) QueueBatchPrologue(runs[static_cast<size_t>(i)], stream);
+        err = cudaGraphLaunch(exec, stream);
+        if (err != cudaSuccess) {
+            status = CudaError(err, "combined batch launch");
+            break;
+        }
+        for (int32_t i : live) QueueBatchReadback(runs[static_cast<size_t>(i)], stream);
+        err = cudaStreamSynchronize(stream);
+        if (err != cudaSuccess) {
+            status = CudaError(err, "combined batch");
+            break;
+        }
+        for (int32_t i : live) CollectBatch(runs[static_cast<size_t>(i)]);
+    }
+    cudaEventRecord(e1, stream);
+    cudaEventSynchronize(e1);
+    float device_ms = 0.0f;
+    cudaEventElapsedTime(&device_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaStreamDestroy(stream);
+    if (status != YRC_OK) return status;
+    if (device_seconds) *device_seconds = device_ms / 1e3;
+    for (int32_t i = 0; i < count && status == YRC_OK; ++i) {
+        status = FinishRender(runs[static_cast<size_t>(i)], device_ms / 1e3);
+    }
+    return status;
 }
 
 extern "C" yrc_status yrc_render_scene_set_capacity(yrc_render_scene* s, int64_t capacity) {

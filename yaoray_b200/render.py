@@ -187,6 +187,7 @@ def _bind():
         ("yrc_render_scene_capacity", C.c_int64, [P]),
         ("yrc_render_autotune", C.c_int, [P, C.c_int32, P]),
         ("yrc_render_scene_set_tuning", C.c_int, [P, P]),
+        ("yrc_render_many", C.c_int, [P, C.c_int32, P, P, P, P, P]),
         ("yrc_bssrdf_table_build", C.c_int, [C.c_float, C.c_float, C.c_int32, C.c_int32, P, P, P, P, P]),
         ("yrc_alias_table_build", C.c_int, [P, C.c_int32, P, P, P]),
         ("yrc_environment_distribution_build", C.c_int, [P, C.c_int32, C.c_int32, P, P, P, P, P]),
@@ -520,3 +521,26 @@ class CudaBackend:
             raise YrcError(status, msg)
         stats = {f[0]: getattr(st, f[0]) for f in Stats._fields_}
         return RenderResult(True, "", film, int(bad.value), stats)
+
+    def render_many(self, prepared: list) -> list:
+        """Renders several prepared scenes together (yrc_render_many): each
+        step is one launch of a graph holding every unfinished scene's batch.
+        Films equal render()'s; stats["device_seconds"] is the whole call's."""
+        L = _bind()
+        n = len(prepared)
+        if n == 0:
+            return []
+        films = [np.zeros((p.scene.height, p.scene.width), FILM_PIXEL_DTYPE) for p in prepared]
+        handles = (C.c_void_p * n)(*[p._handle.value for p in prepared])
+        film_ptrs = (C.c_void_p * n)(*[f.ctypes.data for f in films])
+        bads = (C.c_uint64 * n)()
+        stats = (Stats * n)()
+        secs = C.c_double()
+        status = L.yrc_render_many(handles, n, None, film_ptrs, bads, stats, C.byref(secs))
+        if status != _lib.YRC_OK:
+            msg = L.yrc_last_error().decode(errors="replace")
+            if status in (_lib.YRC_ERR_CANCELLED, _lib.YRC_ERR_INVALID_ARGUMENT):
+                return [RenderResult(False, msg) for _ in prepared]
+            raise YrcError(status, msg)
+        return [RenderResult(True, "", films[i], int(bads[i]), {f[0]: getattr(stats[i], f[0]) for f in Stats._fields_})
+                for i in range(n)]
