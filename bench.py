@@ -238,7 +238,11 @@ def run_gpu(args):
 
     # Autotuner: pick the fastest compiled launch shape on a 2M-ray slice of
     # this step's rays (untimed).
-    tune = acc.autotune(rays[: min(n, 1 << 21)], stream=stream)
+    if args.trace_shape is not None:  # a shape fixed by the caller (e.g. to profile the one a plain run chose)
+        acc.set_trace_shape(args.trace_shape)
+        tune = {"shape": args.trace_shape, "times_ms": None}
+    else:
+        tune = acc.autotune(rays[: min(n, 1 << 21)], stream=stream)
 
     for _ in range(args.warmup):
         acc.intersect(rays, hits=hits, stream=stream)
@@ -391,7 +395,11 @@ def run_render(args):
     prepared = backend.prepare(scene)
     prepare_s = time.perf_counter() - t0
     tuning = None
-    if not args.no_autotune:
+    if args.tuning:  # capacity,shape fixed by the caller (e.g. to profile what a plain run chose)
+        cap, shape = (int(x) for x in args.tuning.split(","))
+        tuning = {"capacity": cap, "trace_shape": shape, "fixed": True}
+        prepared.set_tuning(tuning)
+    elif not args.no_autotune:
         t0 = time.perf_counter()
         tuning = prepared.autotune()
         tuning["seconds"] = round(time.perf_counter() - t0, 2)
@@ -399,7 +407,7 @@ def run_render(args):
         res = backend.render(prepared)
         assert res.ok, res.error
     gpu_index = 0
-    times, devs = [], []
+    times, devs, launches = [], [], 0
     with ClockSampler(gpu_index) as clocks:
         for _ in range(args.steps):
             torch.cuda.synchronize()
@@ -407,6 +415,7 @@ def run_render(args):
             res = backend.render(prepared)
             times.append(time.perf_counter() - t0)
             devs.append(res.stats["device_seconds"])
+            launches += int(res.stats["kernel_launches"])
     samples = scene.width * scene.height * scene.spp
     dt = sum(times) / len(times)
     ddt = sum(devs) / len(devs)
@@ -441,6 +450,7 @@ def run_render(args):
             "e2e": {"value": round(samples / dt, 1), "unit": "samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": scene.width * scene.height * 56},
             "path_segments_per_s": round(res.stats["rays_traced"] / ddt, 1),
+            "gpu_launches": launches,
             "cpu_baseline": base, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
 
@@ -532,6 +542,7 @@ def run_nrc(args):
         warm_s += backend.render(w).stats["device_seconds"]
         w.close()
     cached = []
+    launches = 0
     with ClockSampler(0) as clocks:
         for spp in (1, 4, 16):
             errs, secs, queries, segs = [], [], [], []
@@ -543,6 +554,7 @@ def run_nrc(args):
                 secs.append(st["device_seconds"])
                 queries.append(st["cache_queries"])
                 segs.append(st["rays_traced"])
+                launches += int(st["kernel_launches"])
                 p.close()
             cached.append((spp, float(np.mean(errs)), float(np.mean(secs)), int(np.mean(queries)),
                            int(np.mean(segs))))
@@ -575,6 +587,7 @@ def run_nrc(args):
             "cached": [{"spp": s_, "relmse": round(e, 5), "ms": round(t * 1e3, 3), "cache_queries": q,
                         "path_segments": n, "equal_relmse_ratio": round(ratios[s_], 3)}
                        for s_, e, t, q, n in cached],
+            "gpu_launches": launches,
             "e2e": None, "cpu_baseline": None, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
 
@@ -648,6 +661,7 @@ def run_jobs(args):
                               "latency_p50_s": shared_lat["p50"], "latency_p99_s": shared_lat["p99"],
                               "groups_of": args.concurrency},
             "failed_jobs": failed,
+            "gpu_launches": sum(j.kernels for j in jobs),
             "e2e": {"value": round(shared.samples_per_s, 1), "unit": "samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": film_bytes,
                     "note": "value is already host wall clock around the CudaBackend.render calls, films read back"},
@@ -664,6 +678,8 @@ def main():
     ap.add_argument("--spp-scale", type=float, default=1.0, help="spp scale of --workload jobs")
     ap.add_argument("--concurrency", type=int, default=8, help="concurrent jobs of --workload jobs")
     ap.add_argument("--no-autotune", action="store_true", help="render workloads: keep the default queue capacity")
+    ap.add_argument("--trace-shape", type=int, default=None, help="traversal: use this launch shape, no autotune")
+    ap.add_argument("--tuning", default=None, help="render workloads: 'capacity,shape' instead of the autotuner")
     ap.add_argument("--render-spp", type=int, default=16, help="spp per step of --workload instanced")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)

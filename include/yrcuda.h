@@ -604,6 +604,7 @@ typedef struct yrc_render_stats {
     double device_seconds;
     uint64_t cache_queries;    /* paths ended at the radiance cache (0 without one) */
     uint64_t cache_records;    /* training records fed to the cache */
+    uint64_t kernel_launches;  /* kernels this render launched on the device (graph kernel nodes included) */
 } yrc_render_stats;
 
 /*

@@ -50,6 +50,7 @@ class Job:
     tuning: dict | None = None
     tune_s: float = 0.0
     resident: bool = False  # rendered once: its working memory stays allocated
+    kernels: int = 0  # device kernels the last render launched
     latency_s: float = 0.0
     device_s: float = 0.0
     samples: int = 0
@@ -194,6 +195,7 @@ class JobRunner:
         job.resident = job.resident or res.ok
         job.device_s = res.stats.get("device_seconds", 0.0)
         job.samples = int(res.stats.get("samples_rendered", 0))
+        job.kernels = int(res.stats.get("kernel_launches", 0))
         job.film = res.film if self.keep_films else None
 
     def run_sequential(self, jobs: list[Job]) -> BatchResult:
@@ -267,6 +269,7 @@ class JobRunner:
                 job.resident = job.resident or res.ok
                 job.device_s = res.stats.get("device_seconds", 0.0)
                 job.samples = int(res.stats.get("samples_rendered", 0))
+                job.kernels = int(res.stats.get("kernel_launches", 0))
                 job.film = res.film if self.keep_films else None
         wall = time.perf_counter() - t0
         return BatchResult(list(jobs), wall, sum(j.samples for j in jobs), peak, {"budget_bytes": budget})

@@ -107,6 +107,7 @@ struct yrc_render_scene {
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     cudaGraph_t graph_template = nullptr;  // the captured batch, kept for multi-scene launches
+    int64_t graph_kernels = 0;             // kernel nodes of the captured batch
     int32_t graph_max_batch = -1;
     int64_t capacity_choice = 0;  // queue capacity chosen by the autotuner or the caller (0: from the image)
     // Radiance cache (optional).
@@ -737,6 +738,19 @@ yrc_status EnsureGraph(yrc_render_scene* s, int32_t max_batch) {
     }
     s->graph_template = graph;
     s->graph_max_batch = max_batch;
+    size_t nodes = 0;
+    s->graph_kernels = 0;
+    if (cudaGraphGetNodes(graph, nullptr, &nodes) == cudaSuccess && nodes > 0) {
+        std::vector<cudaGraphNode_t> list(nodes);
+        if (cudaGraphGetNodes(graph, list.data(), &nodes) == cudaSuccess) {
+            for (size_t i = 0; i < nodes; ++i) {
+                cudaGraphNodeType type;
+                if (cudaGraphNodeGetType(list[i], &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) {
+                    ++s->graph_kernels;
+                }
+            }
+        }
+    }
     return Ok();
 }
 
@@ -815,6 +829,7 @@ struct RenderRun {
     int32_t this_batch = 0;
     uint64_t converged = 0;
     uint64_t cache_queries = 0, cache_records = 0;
+    uint64_t kernels = 2;  // the active-pixel list of the set-up, then the batch graphs
     bool active() const { return sc_host[0] > 0; }
 };
 
@@ -898,6 +913,7 @@ void CollectBatch(RenderRun& run) {
     }
     run.completed_passes += run.this_batch;
     run.converged = run.sc_host[3];
+    run.kernels += static_cast<uint64_t>(s->graph_kernels);
 }
 
 yrc_status FinishRender(RenderRun& run, double device_seconds) {
@@ -931,6 +947,7 @@ yrc_status FinishRender(RenderRun& run, double device_seconds) {
         stats->misses = counters[kCtrStatsBase + 4];
         stats->cache_queries = run.cache_queries;
         stats->cache_records = run.cache_records;
+        stats->kernel_launches = run.kernels;
         stats->bad_samples = fin[2];
         stats->bvh_nodes = s->bvh_nodes;
         stats->bvh_max_depth = s->bvh_max_depth;

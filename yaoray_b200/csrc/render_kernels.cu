@@ -833,7 +833,6 @@ __global__ void NeeResolveKernel(PathState ps, Queues q, const float4* transmitt
          e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int32_t path = q.nee_paths[e];
         V3 sum{0.0f, 0.0f, 0.0f};
-        bool occluded_any = false;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const int32_t slot = 3 * path + k;
@@ -846,7 +845,6 @@ __global__ void NeeResolveKernel(PathState ps, Queues q, const float4* transmitt
             }
             sum = sum + Mul(c, vis);
             ps.nee[slot] = make_float4(0, 0, 0, 0);
-            (void)occluded_any;
         }
         const V3 tp = F4(ps.nee_tp[path]);
         ps.radiance[path] = ToF4(F4(ps.radiance[path]) + Mul(tp, sum));

@@ -152,7 +152,8 @@ class Stats(C.Structure):
                 ("sphere_tests", C.c_uint64), ("bvh_node_tests", C.c_uint64), ("bvh_nodes", C.c_int32),
                 ("bvh_max_depth", C.c_int32), ("hits", C.c_uint64), ("misses", C.c_uint64),
                 ("bad_samples", C.c_uint64), ("threads", C.c_int32), ("elapsed_seconds", C.c_double),
-                ("device_seconds", C.c_double), ("cache_queries", C.c_uint64), ("cache_records", C.c_uint64)]
+                ("device_seconds", C.c_double), ("cache_queries", C.c_uint64), ("cache_records", C.c_uint64),
+                ("kernel_launches", C.c_uint64)]
 
 
 class RenderTuning(C.Structure):
