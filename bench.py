@@ -238,6 +238,8 @@ def run_gpu(args):
 
     # Autotuner: pick the fastest compiled launch shape on a 2M-ray slice of
     # this step's rays (untimed).
+    if args.four_wide:  # opt-in four-wide traversal of the same BVH (same hits)
+        acc.set_wide(True)
     if args.trace_shape is not None:  # a shape fixed by the caller (e.g. to profile the one a plain run chose)
         acc.set_trace_shape(args.trace_shape)
         tune = {"shape": args.trace_shape, "times_ms": None}
@@ -337,6 +339,7 @@ def run_gpu(args):
                        "l2": f"inputs larger than L2 (rays {n * 32 >> 20} MiB + hits {n * 16 >> 20} MiB + "
                              f"BVH {bvh_mib} MiB, L2 126 MB), no flush",
                        "parallelism": f"replicas x{ws}", "launch_shape": tune["shape"],
+                       "hierarchy": "four-wide copy of the reference BVH" if acc.wide else "binary reference BVH",
                        "autotune_ms": tune["times_ms"],
                        "bvh_build_s": {"device": round(build_device_s, 3), "host": round(build_host_s, 3),
                                        "host_threads": os.cpu_count()}},
@@ -679,6 +682,7 @@ def main():
     ap.add_argument("--concurrency", type=int, default=8, help="concurrent jobs of --workload jobs")
     ap.add_argument("--no-autotune", action="store_true", help="render workloads: keep the default queue capacity")
     ap.add_argument("--trace-shape", type=int, default=None, help="traversal: use this launch shape, no autotune")
+    ap.add_argument("--four-wide", action="store_true", help="traversal: the opt-in four-wide traversal")
     ap.add_argument("--tuning", default=None, help="render workloads: 'capacity,shape' instead of the autotuner")
     ap.add_argument("--render-spp", type=int, default=16, help="spp per step of --workload instanced")
     ap.add_argument("--gpus", type=int, default=1)

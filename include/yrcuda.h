@@ -345,6 +345,21 @@ yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t cou
 yrc_status yrc_accel_set_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t shape);
 int32_t yrc_accel_get_trace_shape(const yrc_accel* accel, int32_t any_hit);
 
+/* Four-wide traversal (opt-in). set_wide(1) builds, for a flat BVH of
+ * triangles only, a four-wide copy of its hierarchy (the binary tree
+ * collapsed two levels at a time, same node boxes and leaves) that later
+ * closest- and any-hit traces without per-ray statistics traverse: half the
+ * dependent node fetches and the same hits, since a triangle tie goes to the
+ * smaller flat index whatever the visiting order (the reference pins BVH4 ==
+ * binary hits in tests/accel/bvh_traversal_tests.cpp:112-138). It fails for
+ * BVHs with spheres (a sphere tie goes to the first visited) and two-level
+ * BVHs. Statistics and probes always use the binary traversal. Off by
+ * default: on B200 it measured slower than the binary kernel (0.91x on
+ * incoherent rays of the 2M-triangle set). No counterpart in the reference
+ * (its BVH4 is a CPU path). */
+yrc_status yrc_accel_set_wide(yrc_accel* accel, int32_t enable);
+int32_t yrc_accel_get_wide(const yrc_accel* accel);
+
 /* ------------------------------------------------------------------ probe */
 
 #define YRC_PROBE_MAX_HITS 64 /* BvhProbeHits::MaxHits (bvh.hpp:122-127) */

@@ -299,3 +299,33 @@ def test_every_launch_shape_is_bit_identical(cuda, full_set):
     tuned = dev.autotune(rays)
     assert 0 <= tuned["shape"] < 7 and min(tuned["times_ms"]) > 0
     dev.check()
+
+
+def test_four_wide_traversal_matches_binary(cuda, full_set):
+    """The four-wide copy of a triangle-only BVH gives the binary traversal's
+    hits bit for bit (closest and any hit, every launch shape), as the
+    reference pins for its BVH4; BVHs with spheres have no four-wide copy."""
+    import torch
+
+    g, b = full_set
+    dev = accel.DeviceAccelerator(g, b)
+    assert not dev.wide  # opt-in
+    rays = torch.from_numpy(np.concatenate([scenes.incoherent_rays(400_000, seed=91),
+                                            scenes.coherent_rays(400, 400),
+                                            scenes.shadow_rays(200_000, seed=92)])).to(cuda)
+    bin_hits = dev.intersect(rays).clone()
+    bin_occ = dev.intersect(rays, any_hit=True).clone()
+    dev.set_wide(True)
+    assert dev.wide
+    wide_hits = dev.intersect(rays)
+    wide_occ = dev.intersect(rays, any_hit=True)
+    assert torch.equal(wide_hits.view(torch.int32), bin_hits.view(torch.int32))
+    assert torch.equal(wide_occ, bin_occ)
+    for shape in range(7):
+        dev.set_trace_shape(shape)
+        assert torch.equal(dev.intersect(rays).view(torch.int32), bin_hits.view(torch.int32)), shape
+    dev.check()
+    gs = geometry(load("trace_spheres"))
+    assert gs.spheres.size > 0
+    with pytest.raises(Exception):
+        accel.DeviceAccelerator(gs, accel.build_bvh(gs)).set_wide(True)

@@ -183,6 +183,8 @@ def lib() -> C.CDLL:
         "yrc_accel_autotune": (C.c_int, [P, P, I64, I32, P, P]),
         "yrc_accel_set_trace_shape": (C.c_int, [P, I32, I32]),
         "yrc_accel_get_trace_shape": (I32, [P, I32]),
+        "yrc_accel_set_wide": (C.c_int, [P, I32]),
+        "yrc_accel_get_wide": (I32, [P]),
         "yrc_stream_synchronize": (C.c_int, [P]),
         "yrc_nrc_create": (C.c_int, [P, C.c_float, C.c_uint64, P]),
         "yrc_nrc_destroy": (None, [P]),

@@ -324,6 +324,15 @@ class DeviceAccelerator:
     def set_trace_shape(self, shape: int, any_hit: bool = False) -> None:
         check(lib().yrc_accel_set_trace_shape(self._handle, int(any_hit), shape))
 
+    @property
+    def wide(self) -> bool:
+        """True while closest / any-hit traces use the four-wide copy of the
+        hierarchy (flat, triangle-only BVHs; same hits as the binary one)."""
+        return bool(lib().yrc_accel_get_wide(self._handle))
+
+    def set_wide(self, enable: bool) -> None:
+        check(lib().yrc_accel_set_wide(self._handle, int(enable)))
+
     def check(self) -> None:
         """Synchronises and raises if a kernel recorded an error status."""
         check(lib().yrc_accel_check(self._handle))

@@ -121,6 +121,95 @@ bool AddBvh(const yrc_bvh_node* nodes, int64_t node_count, SlotFn slot_record, L
     return true;
 }
 
+// Collapses the binary pairs below `root_ref` into four-wide nodes: starting
+// from a pair's two children, the interior entry with the largest box area is
+// replaced by its two children until four entries are held or only leaves
+// remain. Returns the wide root (node 0, or the leaf / absent root itself)
+// and the deepest stack the traversal may need (at most three pushes per
+// wide level).
+struct WideLayout {
+    std::vector<WideNode> nodes;
+    int32_t root = kAbsentRef;
+    int32_t stack = 1;
+};
+
+void BuildWide(const std::vector<NodePair>& pairs, int32_t root_ref, WideLayout& w) {
+    w.nodes.clear();
+    w.root = root_ref;
+    w.stack = 1;
+    if (root_ref < 0) return;  // a leaf or an empty root: nothing to collapse
+    struct Entry {
+        float lo[3], hi[3];
+        int32_t ref;
+    };
+    auto children = [&](int32_t p, Entry out[2]) -> int {
+        const NodePair& q = pairs[static_cast<size_t>(p)];
+        int n = 0;
+        if (q.d.x != kAbsentRef) out[n++] = Entry{{q.a.x, q.a.y, q.a.z}, {q.a.w, q.b.x, q.b.y}, q.d.x};
+        if (q.d.y != kAbsentRef) out[n++] = Entry{{q.b.z, q.b.w, q.c.x}, {q.c.y, q.c.z, q.c.w}, q.d.y};
+        return n;
+    };
+    auto area = [](const Entry& e) {
+        const float x = e.hi[0] - e.lo[0], y = e.hi[1] - e.lo[1], z = e.hi[2] - e.lo[2];
+        return x * y + y * z + z * x;
+    };
+    struct Work {
+        int32_t pair, slot, depth;
+    };
+    std::vector<Work> work{{root_ref, 0, 1}};
+    w.nodes.emplace_back();
+    int32_t deepest = 1;
+    while (!work.empty()) {
+        const Work item = work.back();
+        work.pop_back();
+        Entry e[4];
+        int n = children(item.pair, e);
+        for (;;) {
+            int best = -1;
+            float best_area = -1.0f;
+            for (int k = 0; k < n; ++k) {
+                if (e[k].ref >= 0 && area(e[k]) > best_area) {
+                    best = k;
+                    best_area = area(e[k]);
+                }
+            }
+            if (best < 0) break;
+            Entry c[2];
+            const int m = children(e[best].ref, c);
+            if (n - 1 + m > 4) break;
+            for (int k = best; k + 1 < n; ++k) e[k] = e[k + 1];  // drop the expanded entry
+            --n;
+            for (int k = 0; k < m; ++k) e[n++] = c[k];
+        }
+        WideNode node{};
+        float lox[4] = {0, 0, 0, 0}, hix[4] = {0, 0, 0, 0}, loy[4] = {0, 0, 0, 0}, hiy[4] = {0, 0, 0, 0};
+        float loz[4] = {0, 0, 0, 0}, hiz[4] = {0, 0, 0, 0};
+        int32_t ref[4] = {kAbsentRef, kAbsentRef, kAbsentRef, kAbsentRef};
+        for (int k = 0; k < n; ++k) {
+            lox[k] = e[k].lo[0], loy[k] = e[k].lo[1], loz[k] = e[k].lo[2];
+            hix[k] = e[k].hi[0], hiy[k] = e[k].hi[1], hiz[k] = e[k].hi[2];
+            if (e[k].ref >= 0) {
+                ref[k] = static_cast<int32_t>(w.nodes.size());
+                w.nodes.emplace_back();
+                work.push_back({e[k].ref, ref[k], item.depth + 1});
+            } else {
+                ref[k] = e[k].ref;
+            }
+        }
+        node.lox = make_float4(lox[0], lox[1], lox[2], lox[3]);
+        node.hix = make_float4(hix[0], hix[1], hix[2], hix[3]);
+        node.loy = make_float4(loy[0], loy[1], loy[2], loy[3]);
+        node.hiy = make_float4(hiy[0], hiy[1], hiy[2], hiy[3]);
+        node.loz = make_float4(loz[0], loz[1], loz[2], loz[3]);
+        node.hiz = make_float4(hiz[0], hiz[1], hiz[2], hiz[3]);
+        node.ref = make_int4(ref[0], ref[1], ref[2], ref[3]);
+        w.nodes[static_cast<size_t>(item.slot)] = node;
+        deepest = std::max(deepest, item.depth);
+    }
+    w.root = 0;
+    w.stack = 3 * deepest + 1;
+}
+
 Record TriangleOrSphereRecord(const yrc_geometry& g, const yrc_bvh_view& bvh, int64_t slot) {
     if (slot < 0 || slot >= bvh.primitive_index_count) return SkipRecord(kRecSkip);
     const int32_t pi = bvh.primitive_indices[slot];
@@ -224,6 +313,10 @@ struct yrc_accel {
     int device = 0;
     int sm_count = 148;
     yrc::NodePair* d_pairs = nullptr;
+    yrc::WideNode* d_wide = nullptr;  // four-wide copy, built on the first yrc_accel_set_wide(1)
+    bool wide_enabled = false;
+    bool triangles_only = false;  // flat BVH without spheres: a four-wide copy is allowed
+    int64_t pair_count = 0;
     yrc::Record* d_records = nullptr;
     yrc::Instance* d_instances = nullptr;
     unsigned long long* d_counter = nullptr;
@@ -257,6 +350,7 @@ void FreeAccel(yrc_accel* a) {
     if (!a) return;
     cudaSetDevice(a->device);
     cudaFree(a->d_pairs);
+    cudaFree(a->d_wide);
     cudaFree(a->d_records);
     cudaFree(a->d_instances);
     cudaFree(a->d_counter);
@@ -285,6 +379,7 @@ yrc_status Finalize(Layout& layout, int32_t root_ref, const float lo[3], const f
     if (err == cudaSuccess) err = cudaDeviceGetAttribute(&a->sm_count, cudaDevAttrMultiProcessorCount, a->device);
     if (err == cudaSuccess) err = Upload(&a->d_pairs, layout.pairs, a->device_bytes);
     if (err == cudaSuccess) err = Upload(&a->d_records, layout.records, a->device_bytes);
+    a->pair_count = static_cast<int64_t>(layout.pairs.size());
     if (err == cudaSuccess) err = Upload(&a->d_instances, layout.instances, a->device_bytes);
     if (err == cudaSuccess) err = cudaMalloc(reinterpret_cast<void**>(&a->d_counter), sizeof(unsigned long long));
     if (err == cudaSuccess) err = cudaMalloc(reinterpret_cast<void**>(&a->d_error), sizeof(int));
@@ -304,6 +399,9 @@ yrc_status Finalize(Layout& layout, int32_t root_ref, const float lo[3], const f
     p.root_ref = root_ref;
     p.two_level = two_level;
     p.stack_limit = depth + 1;
+    p.wide = nullptr;
+    p.wide_root = kAbsentRef;
+    p.wide_stack_limit = 0;
     *out = a;
     return Ok();
 }
@@ -413,7 +511,15 @@ yrc_status yrc_accel_create_flat(const yrc_geometry* geometry, const yrc_bvh_vie
     } catch (const std::bad_alloc&) {
         return Fail(YRC_ERR_OUT_OF_MEMORY, "yrc_accel_create_flat: host allocation failed");
     }
-    return Finalize(layout, root, lo, hi, 0, depth, out);
+    const yrc_status st = Finalize(layout, root, lo, hi, 0, depth, out);
+    if (st != YRC_OK) return st;
+    // A four-wide copy is allowed for triangle-only BVHs: their closest hit
+    // does not depend on the visiting order (ties go to the smaller flat
+    // index), while a sphere tie goes to the first visited.
+    bool triangles_only = true;
+    for (int64_t i = 0; i < bvh->primitive_count; ++i) triangles_only = triangles_only && bvh->primitives[i].kind == 0;
+    (*out)->triangles_only = triangles_only;
+    return st;
 }
 
 yrc_status yrc_accel_create_two_level(const yrc_geometry* geometry, const yrc_two_level_view* tl, yrc_accel** out) {
@@ -672,6 +778,39 @@ yrc_status yrc_accel_set_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t 
 int32_t yrc_accel_get_trace_shape(const yrc_accel* accel, int32_t any_hit) {
     return accel ? accel->trace_shape[any_hit ? 1 : 0] : -1;
 }
+
+yrc_status yrc_accel_set_wide(yrc_accel* accel, int32_t enable) {
+    using namespace yrc;
+    if (!accel) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_set_wide: null accelerator");
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    if (enable && !accel->d_wide) {
+        if (!accel->triangles_only || accel->params.two_level || accel->params.root_ref < 0) {
+            return Fail(YRC_ERR_UNSUPPORTED, "yrc_accel_set_wide: no four-wide copy (two-level BVH, spheres or a leaf root)");
+        }
+        cudaSetDevice(accel->device);
+        std::vector<NodePair> pairs(static_cast<size_t>(accel->pair_count));
+        cudaError_t err = cudaMemcpy(pairs.data(), accel->d_pairs, sizeof(NodePair) * pairs.size(), cudaMemcpyDeviceToHost);
+        if (err != cudaSuccess) return CudaFail(err, "yrc_accel_set_wide: reading the binary nodes");
+        WideLayout w;
+        BuildWide(pairs, accel->params.root_ref, w);
+        if (w.nodes.empty() || w.stack > kMaxTraceStack) {
+            return Fail(YRC_ERR_UNSUPPORTED, "yrc_accel_set_wide: four-wide hierarchy too deep");
+        }
+        err = Upload(&accel->d_wide, w.nodes, accel->device_bytes);
+        if (err != cudaSuccess) {
+            cudaFree(accel->d_wide);
+            accel->d_wide = nullptr;
+            return CudaFail(err, "yrc_accel_set_wide: upload");
+        }
+        accel->params.wide_root = w.root;
+        accel->params.wide_stack_limit = w.stack;
+    }
+    accel->wide_enabled = enable != 0;
+    accel->params.wide = accel->wide_enabled ? accel->d_wide : nullptr;
+    return yrc::Ok();
+}
+
+int32_t yrc_accel_get_wide(const yrc_accel* accel) { return accel && accel->wide_enabled ? 1 : 0; }
 
 yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags, void* stream,
                               float* times_ms) {

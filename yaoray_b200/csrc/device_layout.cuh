@@ -65,6 +65,20 @@ struct alignas(16) NodePair {
 };
 static_assert(sizeof(NodePair) == 64, "NodePair must be 64 bytes");
 
+// Four-wide node collapsed from the binary pairs (flat, triangle-only BVHs):
+// child boxes in SoA form (lo x / hi x / lo y / hi y / lo z / hi z of the
+// four children), child refs (wide node index, ~record for a leaf, or
+// kAbsentRef), padded to one 128-byte line. The boxes are the binary tree's
+// own node boxes, so the same slab tests run on them; the binary nodes that
+// the collapse skips contain their children, and the slab test's rounding is
+// monotone, so a box that passes implies that every skipped ancestor passes.
+struct alignas(16) WideNode {
+    float4 lox, hix, loy, hiy, loz, hiz;
+    int4 ref;
+    float4 pad;
+};
+static_assert(sizeof(WideNode) == 128, "WideNode must be 128 bytes");
+
 struct alignas(16) Record {
     float4 v0, v1, v2;
 };
@@ -87,6 +101,9 @@ struct AccelParams {
     int32_t root_ref;     // kAbsentRef for an empty BVH
     int32_t two_level;    // 1: records at the root level are TLAS records
     int32_t stack_limit;  // deepest stack the traversal may need (host-computed)
+    const WideNode* wide;      // four-wide copy of a flat triangle-only BVH, or nullptr
+    int32_t wide_root;         // wide node index, ~record (leaf root) or kAbsentRef
+    int32_t wide_stack_limit;  // deepest stack of the four-wide traversal
 };
 
 #if defined(__CUDACC__)

@@ -210,11 +210,66 @@ struct ClearHits {
 // `sphere_clear` are not accepted; the traversal records that it skipped one
 // (s.saw), adds it to `clear` and goes on, so it ends at the first hit on any
 // other surface.
-template <bool kAny, bool kStats, bool kTwo, typename Stack, bool kFilter = false>
+// Compare-exchange of two (miss, entry, ref) candidates of a four-wide node:
+// hits before misses, then nearer entry first.
+__device__ __forceinline__ void OrderPair(bool& ma, float& ea, int32_t& ra, bool& mb, float& eb, int32_t& rb) {
+    const bool swap = (mb < ma) || (mb == ma && eb < ea);
+    if (swap) {
+        const bool m = ma;
+        const float e = ea;
+        const int32_t r = ra;
+        ma = mb, ea = eb, ra = rb;
+        mb = m, eb = e, rb = r;
+    }
+}
+
+// One step at a four-wide node: the four child boxes are slab-tested with
+// the binary traversal's test; the nearest hit child is taken next and the
+// others are pushed farthest first. Returns 1 when s.cur holds the next
+// node, 0 when no child was hit, -1 on a stack overflow (traversal ends).
+template <typename Stack>
+__device__ __forceinline__ int WideStep(const AccelParams& a, Traversal& s, Stack& st, int2* col, int* error) {
+    const float4* p = reinterpret_cast<const float4*>(a.wide + s.cur);
+    const float4 lx = Ld(p), hx = Ld(p + 1), ly = Ld(p + 2), hy = Ld(p + 3), lz = Ld(p + 4), hz = Ld(p + 5);
+    const int4 rf = __ldg(reinterpret_cast<const int4*>(p + 6));
+    const float limit = s.best.t;
+    bool m0 = true, m1 = true, m2 = true, m3 = true;
+    float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, e3 = 0.0f;
+    int32_t r0 = rf.x, r1 = rf.y, r2 = rf.z, r3 = rf.w;
+    if (r0 != kAbsentRef) m0 = !SlabTest(s.r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, s.tmin, limit, e0);
+    if (r1 != kAbsentRef) m1 = !SlabTest(s.r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, s.tmin, limit, e1);
+    if (r2 != kAbsentRef) m2 = !SlabTest(s.r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, s.tmin, limit, e2);
+    if (r3 != kAbsentRef) m3 = !SlabTest(s.r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, s.tmin, limit, e3);
+    // Sorting network on four.
+    OrderPair(m0, e0, r0, m1, e1, r1);
+    OrderPair(m2, e2, r2, m3, e3, r3);
+    OrderPair(m0, e0, r0, m2, e2, r2);
+    OrderPair(m1, e1, r1, m3, e3, r3);
+    OrderPair(m1, e1, r1, m2, e2, r2);
+    if (m0) return 0;  // no child hit
+    const int pushes = (m1 ? 0 : 1) + (m2 ? 0 : 1) + (m3 ? 0 : 1);
+    if (s.sp + pushes > Stack::kTotalEntries) {  // unreachable when the host's depth bound holds
+        atomicOr(error, kTraceErrorStackOverflow);
+        s.best.hit = false;
+        return -1;
+    }
+    if (!m3) st.Put(col, s.sp++, make_int2(r3, __float_as_int(e3)));
+    if (!m2) st.Put(col, s.sp++, make_int2(r2, __float_as_int(e2)));
+    if (!m1) st.Put(col, s.sp++, make_int2(r1, __float_as_int(e1)));
+    s.cur = r0;
+    return 1;
+}
+
+template <bool kAny, bool kStats, bool kTwo, typename Stack, bool kFilter = false, bool kWide = false>
 __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, int64_t ray, Traversal& s, Stack& st,
                                      int2* col, int* error, const uint8_t* tri_clear = nullptr,
                                      const uint8_t* sphere_clear = nullptr, ClearHits* clear = nullptr) {
     const bool in_blas = kTwo && s.level == 1;
+    if (kWide && s.cur >= 0) {
+        const int r = WideStep(a, s, st, col, error);
+        if (r != 0) return r > 0;
+        return Pop<kAny, kTwo>(rays, ray, s, st, col);
+    }
     if (s.cur >= 0) {
         const float4* p = reinterpret_cast<const float4*>(a.pairs + s.cur);
         const float4 pa = Ld(p), pb = Ld(p + 1), pc = Ld(p + 2);
@@ -386,7 +441,8 @@ __device__ __forceinline__ void WriteResult(const TraceArgs& args, int64_t ray, 
     }
 }
 
-template <bool kAny, bool kStats, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks>
+template <bool kAny, bool kStats, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks,
+          bool kWide = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args) {
     __shared__ int2 s_stack[kShortStack * kBlock];
     int2* col = s_stack + threadIdx.x;
@@ -418,6 +474,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args
                     const float4 b = Ld(args.rays + 2 * ray + 1);
                     const float tmin = Ld(args.rays + 2 * ray).w;
                     alive = Begin(args.accel, args.rays, ray, tmin, b.w, s);
+                    if (kWide && alive) s.cur = args.accel.wide_root;
                     if (!alive) WriteResult<kAny, kStats>(args, ray, s);
                 }
             }
@@ -428,7 +485,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args
         }
 #pragma unroll 1
         for (int k = 0; k < kStepsPerRefill && alive; ++k) {
-            alive = Step<kAny, kStats, kTwo>(args.accel, args.rays, ray, s, st, col, args.error);
+            alive = Step<kAny, kStats, kTwo, StackStore<kTotal, kBlock>, false, kWide>(args.accel, args.rays, ray, s, st,
+                                                                                       col, args.error);
             if (!alive) WriteResult<kAny, kStats>(args, ray, s);
         }
     }
@@ -716,9 +774,10 @@ cudaError_t PersistentGrid(Kernel kernel, int block, int64_t count, int sm_count
     return cudaSuccess;
 }
 
-template <bool kAny, bool kStats, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks>
+template <bool kAny, bool kStats, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks,
+          bool kWide = false>
 cudaError_t LaunchOne(const TraceArgs& args, cudaStream_t stream, int sm_count) {
-    auto kernel = TraceKernel<kAny, kStats, kTwo, kTotal, kBlock, kStepsPerRefill, kMinBlocks>;
+    auto kernel = TraceKernel<kAny, kStats, kTwo, kTotal, kBlock, kStepsPerRefill, kMinBlocks, kWide>;
     int64_t blocks = 0;
     const cudaError_t err = PersistentGrid(kernel, kBlock, args.count, sm_count, blocks);
     if (err != cudaSuccess) return err;
@@ -729,16 +788,16 @@ cudaError_t LaunchOne(const TraceArgs& args, cudaStream_t stream, int sm_count) 
 // The tunable launch shapes (block size, node visits between ray refills,
 // minimum resident blocks for the register budget). Index 0 is the default;
 // the autotuner times the rest on the actual accelerator.
-template <bool kAny, bool kStats, bool kTwo, int kTotal>
+template <bool kAny, bool kStats, bool kTwo, int kTotal, bool kWide = false>
 cudaError_t LaunchShape(const TraceArgs& args, int shape, cudaStream_t stream, int sm_count) {
     switch (kStats || kTwo ? 0 : shape) {
-        case 1: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 4, 1>(args, stream, sm_count);
-        case 2: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 16, 1>(args, stream, sm_count);
-        case 3: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 12>(args, stream, sm_count);
-        case 4: return LaunchOne<kAny, kStats, kTwo, kTotal, 64, 8, 1>(args, stream, sm_count);
-        case 5: return LaunchOne<kAny, kStats, kTwo, kTotal, 256, 8, 1>(args, stream, sm_count);
-        case 6: return LaunchOne<kAny, kStats, kTwo, kTotal, 64, 8, 24>(args, stream, sm_count);
-        default: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1>(args, stream, sm_count);
+        case 1: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 4, 1, kWide>(args, stream, sm_count);
+        case 2: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 16, 1, kWide>(args, stream, sm_count);
+        case 3: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 12, kWide>(args, stream, sm_count);
+        case 4: return LaunchOne<kAny, kStats, kTwo, kTotal, 64, 8, 1, kWide>(args, stream, sm_count);
+        case 5: return LaunchOne<kAny, kStats, kTwo, kTotal, 256, 8, 1, kWide>(args, stream, sm_count);
+        case 6: return LaunchOne<kAny, kStats, kTwo, kTotal, 64, 8, 24, kWide>(args, stream, sm_count);
+        default: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1, kWide>(args, stream, sm_count);
     }
 }
 
@@ -746,6 +805,15 @@ template <bool kAny, bool kStats, bool kTwo>
 cudaError_t LaunchDepth(const TraceArgs& args, int shape, cudaStream_t stream, int sm_count) {
     if (args.accel.stack_limit <= 64) return LaunchShape<kAny, kStats, kTwo, 64>(args, shape, stream, sm_count);
     return LaunchShape<kAny, kStats, kTwo, kMaxTraceStack>(args, 0, stream, sm_count);
+}
+
+// The four-wide traversal (flat, triangle-only, no statistics).
+template <bool kAny>
+cudaError_t LaunchWide(const TraceArgs& args, int shape, cudaStream_t stream, int sm_count) {
+    if (args.accel.wide_stack_limit <= 64) {
+        return LaunchShape<kAny, false, false, 64, true>(args, shape, stream, sm_count);
+    }
+    return LaunchOne<kAny, false, false, kMaxTraceStack, 128, 8, 1, true>(args, stream, sm_count);
 }
 
 template <bool kTwo, int kTotal>
@@ -801,6 +869,9 @@ cudaError_t LaunchShadowTransmittance(const ShadowArgs& args, cudaStream_t strea
 cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, int shape, cudaStream_t stream,
                         int sm_count) {
     const bool two = args.accel.two_level != 0;
+    if (!two && !stats && args.accel.wide) {
+        return any_hit ? LaunchWide<true>(args, shape, stream, sm_count) : LaunchWide<false>(args, shape, stream, sm_count);
+    }
     if (any_hit) {
         if (two) return stats ? LaunchDepth<true, true, true>(args, shape, stream, sm_count)
                               : LaunchDepth<true, false, true>(args, shape, stream, sm_count);
