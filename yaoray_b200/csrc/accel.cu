@@ -297,7 +297,7 @@ bool CheckBvh(const yrc_bvh_view* b, std::string& error) {
 
 // Host pipeline resources for yrc_trace_host (allocated on first use).
 struct HostPipeline {
-    static constexpr int kStreams = 3;
+    static constexpr int kStreams = 4;
     int64_t chunk = 0;
     cudaStream_t streams[kStreams] = {};
     void* d_rays[kStreams] = {};
@@ -674,7 +674,10 @@ yrc_status yrc_trace_host(yrc_accel* accel, const yrc_ray* rays, int64_t count, 
     HostPipeline& p = accel->pipe;
     cudaError_t err = cudaSuccess;
     if (p.chunk == 0) {
-        p.chunk = int64_t{1} << 21;  // 2M rays = 64 MiB of rays per chunk
+        // 512K rays (16 MiB of rays) per chunk: enough chunks in a large
+        // batch that the copies of one overlap the traversal of another and
+        // only one chunk's upload and readback are exposed.
+        p.chunk = int64_t{1} << 19;
         err = cudaMalloc(reinterpret_cast<void**>(&p.d_counters), sizeof(unsigned long long) * HostPipeline::kStreams);
         for (int s = 0; s < HostPipeline::kStreams && err == cudaSuccess; ++s) {
             err = cudaStreamCreateWithFlags(&p.streams[s], cudaStreamNonBlocking);
