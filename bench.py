@@ -429,7 +429,7 @@ def run_render(args):
         if oracle.ref_available():
             job = oracle.RefJob.from_scene(scene)
             job.render(spp=1)
-            base_spp = 8 if args.workload == "cornell" else 1
+            base_spp = 64 if args.workload == "cornell" else 4  # the full Cornell job; 4 spp of the instanced one
             film, st, secs = job.render(spp=base_spp)
             base = {"value": round(scene.width * scene.height * base_spp / secs, 1), "unit": "samples/s",
                     "cores": os.cpu_count(), "kind": "reference",

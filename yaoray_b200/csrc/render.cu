@@ -829,7 +829,7 @@ struct RenderRun {
     int32_t this_batch = 0;
     uint64_t converged = 0;
     uint64_t cache_queries = 0, cache_records = 0;
-    uint64_t kernels = 2;  // the active-pixel list of the set-up, then the batch graphs
+    uint64_t kernels = 3;  // the set-up (attempt counts, active-pixel list), then the batch graphs
     bool active() const { return sc_host[0] > 0; }
 };
 
@@ -858,15 +858,13 @@ yrc_status BeginRender(RenderRun& run) {
     if (status == YRC_OK) status = EnsureCache(s);
     if (status != YRC_OK) return status;
     cudaStream_t stream = s->stream;
-    run.host_film.resize(static_cast<size_t>(run.pixels));
+    if (r.progress) run.host_film.resize(static_cast<size_t>(run.pixels));  // the callback's copy of the film
     if (r.resume_film) {
-        std::memcpy(run.host_film.data(), r.resume_film, sizeof(yrc_film_pixel) * static_cast<size_t>(run.pixels));
+        cudaMemcpyAsync(s->film, r.resume_film, sizeof(yrc_film_pixel) * run.pixels, cudaMemcpyHostToDevice, stream);
     } else {
-        std::memset(run.host_film.data(), 0, sizeof(yrc_film_pixel) * static_cast<size_t>(run.pixels));
+        cudaMemsetAsync(s->film, 0, sizeof(yrc_film_pixel) * run.pixels, stream);
     }
-    std::vector<int32_t> attempts(static_cast<size_t>(run.pixels), run.spp - r.resume_completed_spp);
-    cudaMemcpyAsync(s->film, run.host_film.data(), sizeof(yrc_film_pixel) * run.pixels, cudaMemcpyHostToDevice, stream);
-    cudaMemcpyAsync(s->attempts, attempts.data(), sizeof(int32_t) * run.pixels, cudaMemcpyHostToDevice, stream);
+    LaunchFillInt32(s->attempts, run.pixels, run.spp - r.resume_completed_spp, s->sm_count, stream);
     const unsigned long long init_scalars[4] = {0, 0, r.resume_bad_samples, 0};
     cudaMemcpyAsync(s->scalars, init_scalars, sizeof(init_scalars), cudaMemcpyHostToDevice, stream);
     cudaMemsetAsync(s->q.counters, 0, sizeof(unsigned long long) * kCtrCount, stream);

@@ -1159,6 +1159,15 @@ void LaunchFilm(const DevScene& sc, const PathState& ps, const BatchArgs& b, con
                 int sm_count, cudaStream_t st) {
     FilmKernel<<<Grid(pixels, sm_count), kThreads, 0, st>>>(sc, ps, b, f);
 }
+__global__ void FillInt32Kernel(int32_t* dst, int64_t n, int32_t value) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        dst[i] = value;
+    }
+}
+void LaunchFillInt32(int32_t* dst, int64_t n, int32_t value, int sm_count, cudaStream_t st) {
+    FillInt32Kernel<<<Grid(n, sm_count), kThreads, 0, st>>>(dst, n, value);
+}
 void LaunchActivePixels(const DevScene& sc, const BatchArgs& b, const FilmArgs& f, int64_t pixels, int sm_count,
                         cudaStream_t st) {
     ActivePixelsKernel<<<Grid(pixels, sm_count), kThreads, 0, st>>>(sc, b, f, pixels);

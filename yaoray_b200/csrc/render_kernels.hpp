@@ -52,6 +52,8 @@ void LaunchFilm(const DevScene& sc, const PathState& ps, const BatchArgs& b, con
                 int sm_count, cudaStream_t st);
 void LaunchActivePixels(const DevScene& sc, const BatchArgs& b, const FilmArgs& f, int64_t pixels, int sm_count,
                         cudaStream_t st);
+// dst[0..n) = value.
+void LaunchFillInt32(int32_t* dst, int64_t n, int32_t value, int sm_count, cudaStream_t st);
 void LaunchFinishActive(unsigned long long* active_count, unsigned long long* active_count_next, int32_t* batch,
                         int32_t max_batch, int64_t capacity, cudaStream_t st);
 
