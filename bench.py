@@ -55,6 +55,28 @@ def dist_env():
     return ws, rank, local
 
 
+# Replicas (one process per GPU, no exchange step): each rank traces its own
+# ray set; the job's time is the slowest rank's device time and its value the
+# rays of all ranks over that time.
+def replica_ray_seed(rank: int) -> int:
+    return 2 + 1000 * rank
+
+
+def max_over_ranks(ms: float, ws: int, device) -> float:
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(ws: int, rays_per_rank: int, steps: int, max_ms: float) -> float:
+    """Whole-job Mrays/s of `ws` replicas."""
+    return ws * rays_per_rank * steps / (max_ms / 1e3) / 1e6
+
+
 class ClockSampler:
     """Samples nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -214,7 +236,7 @@ def run_gpu(args):
     assert on_device and host_bvh.nodes.tobytes() == bvh.nodes.tobytes()
     del host_bvh
     acc = accel.DeviceAccelerator(geom, bvh)
-    rays_np = scenes.incoherent_rays(args.rays, seed=2 + 1000 * rank)
+    rays_np = scenes.incoherent_rays(args.rays, seed=replica_ray_seed(rank))
     n = rays_np.shape[0]
     rays = torch.from_numpy(rays_np).to(dev)
     hits = torch.empty((n, 4), dtype=torch.float32, device=dev)
@@ -267,12 +289,9 @@ def run_gpu(args):
     barrier()
     elapsed_ms = start.elapsed_time(end)
     acc.check()
-    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = max_over_ranks(elapsed_ms, ws, dev)
     per_launch_s = elapsed_ms / 1e3 / args.steps
-    value = ws * n * args.steps / (max_ms / 1e3) / 1e6
+    value = replica_value(ws, n, args.steps, max_ms)
 
     # End to end through the C ABI host path (pinned host buffers).
     host_rays = torch.from_numpy(rays_np).pin_memory().numpy()
@@ -284,11 +303,8 @@ def run_gpu(args):
     t0 = time.perf_counter()
     for _ in range(e_steps):
         acc.intersect_host(host_rays, out=host_hits)
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = ws * n * e_steps / float(te.item()) / 1e6
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, ws, dev)
+    e2e_value = replica_value(ws, n, e_steps, e2e_ms)
 
     # The workload's other two query sets, timed the same way (device-resident,
     # CUDA events, max over ranks): coherent primary rays (closest hit) and
@@ -296,7 +312,7 @@ def run_gpu(args):
     del host_rays, host_hits
     other_sets = {}
     for key, make, any_hit in (("coherent_closest_hit", lambda: scenes.coherent_rays(), False),
-                               ("incoherent_any_hit_shadow", lambda: scenes.shadow_rays(seed=3 + 1000 * rank), True)):
+                               ("incoherent_any_hit_shadow", lambda: scenes.shadow_rays(seed=1 + replica_ray_seed(rank)), True)):
         set_rays = torch.from_numpy(make()).to(dev)
         m = set_rays.shape[0]
         if any_hit:
@@ -316,11 +332,9 @@ def run_gpu(args):
         end.record(stream)
         end.synchronize()
         acc.check()
-        ts = torch.tensor([start.elapsed_time(end)], dtype=torch.float64, device=dev)
-        if ws > 1:
-            dist.all_reduce(ts, op=dist.ReduceOp.MAX)
+        set_ms = max_over_ranks(start.elapsed_time(end), ws, dev)
         other_sets[key] = {"rays_per_step_per_gpu": m,
-                           "mrays_s": round(ws * m * args.steps / (float(ts.item()) / 1e3) / 1e6, 2)}
+                           "mrays_s": round(replica_value(ws, m, args.steps, set_ms), 2)}
         del set_rays, out
 
     peak, peak_kind = measured_peak()
