@@ -50,6 +50,22 @@ struct Traversal {
 
 __device__ __forceinline__ float4 Ld(const float4* p) { return __ldg(p); }
 
+// Interior-node loads carry an L2 evict-last policy: the node pairs are read
+// about twenty times per ray and the leaf records and ray streams a few
+// times, so the tree should be what L2 keeps.
+__device__ __forceinline__ unsigned long long NodePolicy() {
+    unsigned long long pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ float4 LdNode(const float4* p, unsigned long long pol) {
+    float4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+
 // Warp-aggregated increment of a statistics counter by the calling lanes.
 __device__ __forceinline__ void CountLanes(unsigned long long* counter) {
     const unsigned mask = __activemask();
@@ -272,8 +288,11 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
     }
     if (s.cur >= 0) {
         const float4* p = reinterpret_cast<const float4*>(a.pairs + s.cur);
-        const float4 pa = Ld(p), pb = Ld(p + 1), pc = Ld(p + 2);
-        const int4 pd = __ldg(reinterpret_cast<const int4*>(p + 3));
+        const unsigned long long pol = NodePolicy();
+        const float4 pa = LdNode(p, pol), pb = LdNode(p + 1, pol), pc = LdNode(p + 2, pol);
+        const float4 pdf = LdNode(p + 3, pol);
+        const int4 pd = make_int4(__float_as_int(pdf.x), __float_as_int(pdf.y), __float_as_int(pdf.z),
+                                  __float_as_int(pdf.w));
         const float limit = in_blas ? s.local.t : s.best.t;
         float le = 0.0f, re = 0.0f;
         bool hl = false, hr = false;
