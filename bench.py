@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import re
 import statistics
@@ -480,9 +481,10 @@ def run_nrc(args):
 
     Reference: `--ref-spp` samples per pixel of the plain tracer, accumulated
     in FP64 over renders of different seeds. Plain curve: renders of 1..64
-    spp. Cached: a fresh cache trained online by 32 warm-up frames of 2 spp
-    (a new sampler seed per frame, 4 optimiser steps per batch; their time is
-    reported separately), then renders of 1, 4 and 16 spp that keep training
+    spp. Cached: a fresh cache trained online by 60 warm-up frames of 2 spp
+    along a seeded camera orbit (0.5 degrees per frame) that ends at the
+    evaluated view (a new sampler seed per frame, 4 optimiser steps per batch;
+    their time is reported separately), then renders of 1, 4 and 16 spp that keep training
     (1 step per batch) and query the moving average of the cache's
     parameters. Every relMSE is the mean over three sampler seeds, every
     time the mean device time of the second render of a prepared scene (the
@@ -496,7 +498,7 @@ def run_nrc(args):
     from yaoray_b200.nrc import RadianceCache
     from yaoray_b200.render import CudaBackend, build_two_level_bvh
 
-    W, H, CLAMP, C_SPREAD, DECAY, WARM = args.nrc_width, args.nrc_height, 20.0, 1.0e-4, 0.995, 32
+    W, H, CLAMP, C_SPREAD, DECAY, WARM, ORBIT_DEG = args.nrc_width, args.nrc_height, 20.0, 1.0e-4, 0.995, 60, 0.5
     SEEDS = (7, 8, 9)
     base = instanced.scene(width=W, height=H, spp=1)
     base.radiance_clamp = CLAMP
@@ -553,8 +555,10 @@ def run_nrc(args):
     cache = RadianceCache(lo, extent, seed=1)
     cache.set_average_decay(DECAY)
     warm_s = 0.0
-    for k in range(WARM):
-        w = backend.prepare(scene(2, 100 + k), accel)
+    for k in range(WARM):  # a seeded camera orbit that ends at the evaluated view
+        frame = dataclasses.replace(base, spp=2, seed=100 + k,
+                                    camera=instanced.camera(orbit=math.radians((k - WARM) * ORBIT_DEG)))
+        w = backend.prepare(frame, accel)
         w.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=4, averaged=True)
         warm_s += backend.render(w).stats["device_seconds"]
         w.close()
@@ -596,6 +600,8 @@ def run_nrc(args):
             "config": {"workload": f"instanced-{W}x{H}-depth16-clamp20", "reference_spp": args.ref_spp,
                        "reference_accumulation": "fp64", "spread_threshold": C_SPREAD,
                        "seeds_per_point": len(SEEDS), "warmup_frames": WARM,
+                       "warmup_orbit": f"{WARM} frames of 2 spp, {ORBIT_DEG} degrees apart about the vertical axis, "
+                                       "ending one step before the evaluated view",
                        "queue_capacity_per_spp": {s_: t["capacity"] for s_, t in tunings.items()},
                        "cache": "16x2^19x2 hash grid + SH4, 64x5 MLP, bf16 tcgen05, Adam 1e-2, "
                                 f"parameter moving average {DECAY}",

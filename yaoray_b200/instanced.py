@@ -233,9 +233,16 @@ def hdri(width: int = 2048, height: int = 1024) -> np.ndarray:
     return tex
 
 
-def camera(spread: float = 1.0) -> dict:
+def camera(spread: float = 1.0, orbit: float = 0.0) -> dict:
+    """The pinhole camera; `orbit` (radians) turns the eye about the vertical
+    axis through the look-at point (a camera orbit; 0 is the default view)."""
     eye = np.array(EYE, np.float32) * np.float32(spread)
-    fwd = np.array(LOOK, np.float32) * np.float32(spread) - eye
+    look = np.array(LOOK, np.float32) * np.float32(spread)
+    if orbit:
+        c, s = np.float32(math.cos(orbit)), np.float32(math.sin(orbit))
+        rel = eye - look
+        eye = (look + np.array([c * rel[0] + s * rel[2], rel[1], -s * rel[0] + c * rel[2]], np.float32)).astype(np.float32)
+    fwd = look - eye
     fwd = fwd / np.float32(np.sqrt(np.float32(np.dot(fwd, fwd))))
     right = np.cross(fwd, np.array([0, 1, 0], np.float32)).astype(np.float32)
     right = right / np.float32(np.sqrt(np.float32(np.dot(right, right))))
