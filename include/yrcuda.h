@@ -656,7 +656,7 @@ int64_t yrc_render_scene_capacity(const yrc_render_scene* scene);
 /* Render autotuner: times short probe renders of this scene (sample indices
  * 0..P-1 of every pixel, P = two batches of the largest candidate) for each
  * candidate queue capacity (whole passes of the image between 2^17 and 2^23
- * paths) and, for single-level accelerators, each closest-hit traversal
+ * paths) and each closest-hit traversal
  * launch shape of the extend stage at the best capacity; keeps the fastest
  * for later yrc_render calls. The traversal stack depth is not a candidate:
  * it follows the BVH's measured depth (64 or 256 entries). Probes run

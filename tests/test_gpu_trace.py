@@ -329,3 +329,25 @@ def test_four_wide_traversal_matches_binary(cuda, full_set):
     assert gs.spheres.size > 0
     with pytest.raises(Exception):
         accel.DeviceAccelerator(gs, accel.build_bvh(gs)).set_wide(True)
+
+
+@pytest.mark.parametrize("name", ["trace_two_level", "trace_spheres"])
+def test_every_launch_shape_matches_golden(cuda, name):
+    """Every compiled launch shape, two-level and sphere BVHs included, gives
+    the reference's hits (the autotuners may pick any of them)."""
+    import torch
+
+    f = load(name)
+    g, b = golden_accel(f, name)
+    dev = accel.DeviceAccelerator(g, b)
+    rays = torch.from_numpy(f["rays"]).to(cuda)
+    exp = {k[4:]: v for k, v in f.items() if k.startswith("out_")}
+    for shape in range(7):
+        dev.set_trace_shape(shape)
+        dev.set_trace_shape(shape, any_hit=True)
+        inst = torch.empty(rays.shape[0], dtype=torch.int32, device=cuda)
+        hits = dev.intersect(rays, instances=inst)
+        occ = dev.intersect(rays, any_hit=True)
+        check_closest(hits, inst, exp, exp["instance"])
+        assert np.array_equal(occ.cpu().numpy().astype(bool), exp["hit"].astype(bool)), shape
+    dev.check()

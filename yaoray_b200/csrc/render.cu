@@ -1206,10 +1206,8 @@ extern "C" yrc_status yrc_render_autotune(yrc_render_scene* s, int32_t flags, yr
             }
         }
     }
-    // Traversal launch shapes (single-level accelerators; the two-level
-    // kernel has one shape).
-    const bool two_level = AccelParamsOf(s->accel).two_level != 0;
-    if (status == YRC_OK && (flags & YRC_TUNE_TRACE_SHAPE) && !two_level) {
+    // Traversal launch shapes of the extend stage.
+    if (status == YRC_OK && (flags & YRC_TUNE_TRACE_SHAPE)) {
         for (int shape = 0; shape < YRC_TRACE_SHAPES; ++shape) {
             double sec = 0.0;
             status = time_config(best_cap, shape, &sec);

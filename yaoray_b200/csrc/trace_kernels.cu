@@ -809,7 +809,7 @@ cudaError_t LaunchOne(const TraceArgs& args, cudaStream_t stream, int sm_count) 
 // the autotuner times the rest on the actual accelerator.
 template <bool kAny, bool kStats, bool kTwo, int kTotal, bool kWide = false>
 cudaError_t LaunchShape(const TraceArgs& args, int shape, cudaStream_t stream, int sm_count) {
-    switch (kStats || kTwo ? 0 : shape) {
+    switch (kStats ? 0 : shape) {
         case 1: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 4, 1, kWide>(args, stream, sm_count);
         case 2: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 16, 1, kWide>(args, stream, sm_count);
         case 3: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 12, kWide>(args, stream, sm_count);
