@@ -51,3 +51,31 @@ def test_shared_launch_matches_single_renders():
                 assert j.film.tobytes() == films[j.name].tobytes(), j.name
     finally:
         runner.close(jobs)
+
+
+def test_shared_launch_rejects_bad_groups():
+    """yrc_render_many refuses a scene given twice and two scenes that share
+    one radiance cache (their training steps would race), with an error."""
+    from yaoray_b200.nrc import RadianceCache
+    from yaoray_b200.render import CudaBackend
+
+    jobs = batch.job_set(2, seed=17, spp_scale=1 / 64, max_triangles=30_000)
+    b = CudaBackend()
+    p0, p1 = b.prepare(jobs[0].scene), b.prepare(jobs[1].scene)
+    try:
+        twice = b.render_many([p0, p0])
+        assert not twice[0].ok and "twice" in twice[0].error
+        lo = jobs[0].scene.geometry.positions.min(0)
+        cache = RadianceCache(lo, 200.0, seed=1)
+        p0.set_radiance_cache(cache)
+        p1.set_radiance_cache(cache)
+        shared = b.render_many([p0, p1])
+        assert not shared[0].ok and "share a radiance cache" in shared[0].error
+        p1.set_radiance_cache(None)
+        ok = b.render_many([p0, p1])
+        assert ok[0].ok and ok[1].ok
+        p0.set_radiance_cache(None)
+        cache.close()
+    finally:
+        p0.close()
+        p1.close()
