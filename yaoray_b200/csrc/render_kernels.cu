@@ -852,15 +852,6 @@ __global__ void NeeResolveKernel(PathState ps, Queues q, const float4* transmitt
     }
 }
 
-// Marks every NEE slot of the queued shadow rays as occluded before the
-// any-hit trace (unused slots then contribute zero as they hold zero).
-__global__ void ClearOcclusionKernel(Queues q, int64_t slots) {
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < slots;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        q.shadow_occluded[i] = 1;
-    }
-}
-
 // ---------------------------------------------------------- subsurface
 
 // The exit half of the subsurface branch (path_integrator.cpp:136-170,
@@ -1151,9 +1142,6 @@ void LaunchNeeResolve(const PathState& ps, const Queues& q, const float4* transm
     } else {
         NeeResolveKernel<false><<<Grid(capacity, sm_count), kThreads, 0, st>>>(ps, q, nullptr);
     }
-}
-void LaunchClearOcclusion(const Queues& q, int64_t slots, int sm_count, cudaStream_t st) {
-    ClearOcclusionKernel<<<Grid(slots, sm_count), kThreads, 0, st>>>(q, slots);
 }
 void LaunchFilm(const DevScene& sc, const PathState& ps, const BatchArgs& b, const FilmArgs& f, int64_t pixels,
                 int sm_count, cudaStream_t st) {

@@ -47,7 +47,6 @@ void LaunchCacheResolve(const PathState& ps, const CacheArgs& cache, int64_t cap
 void LaunchCacheTargets(const PathState& ps, const CacheArgs& cache, int sm_count, cudaStream_t st);
 void LaunchNeeResolve(const PathState& ps, const Queues& q, const float4* transmittance, int64_t capacity,
                       int sm_count, cudaStream_t st);
-void LaunchClearOcclusion(const Queues& q, int64_t slots, int sm_count, cudaStream_t st);
 void LaunchFilm(const DevScene& sc, const PathState& ps, const BatchArgs& b, const FilmArgs& f, int64_t pixels,
                 int sm_count, cudaStream_t st);
 void LaunchActivePixels(const DevScene& sc, const BatchArgs& b, const FilmArgs& f, int64_t pixels, int sm_count,

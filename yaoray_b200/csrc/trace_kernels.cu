@@ -637,6 +637,8 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmi
     int2* col = s_stack + threadIdx.x;
     StackStore<kTotal, kTraceBlock, kShadowShortStack> st;
     Traversal s;
+    s.best.hit = false;  // defined before the first Begin, for the compiler's flow analysis
+    s.saw = false;
     ClearHits clear{s_clear_t + threadIdx.x, s_clear_id + threadIdx.x, 0, false};
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lt_mask = (1u << lane) - 1u;
