@@ -699,7 +699,8 @@ def main():
     ap.add_argument("--nrc-height", type=int, default=540)
     ap.add_argument("--ref-spp", type=int, default=512)
     ap.add_argument("--spp-scale", type=float, default=1.0, help="spp scale of --workload jobs")
-    ap.add_argument("--concurrency", type=int, default=8, help="concurrent jobs of --workload jobs")
+    ap.add_argument("--concurrency", type=int, default=16,
+                    help="--workload jobs: jobs per shared launch (and concurrent streams)")
     ap.add_argument("--no-autotune", action="store_true", help="render workloads: keep the default queue capacity")
     ap.add_argument("--trace-shape", type=int, default=None, help="traversal: use this launch shape, no autotune")
     ap.add_argument("--four-wide", action="store_true", help="traversal: the opt-in four-wide traversal")
