@@ -782,6 +782,27 @@ typedef struct yrc_cache_settings {
  * attachment. */
 yrc_status yrc_render_scene_set_cache(yrc_render_scene* scene, yrc_nrc* cache, const yrc_cache_settings* settings);
 
+/* ---- Sampling primitives evaluated on the device ------------------------
+ * Diagnostics: each evaluates, in a CUDA kernel, the same device code the
+ * path tracer draws its samples with, on host inputs and outputs
+ * (synchronous). */
+
+/* Sampler::Sample1D / Sample2D (src/sampling/sampler.cpp:173-237) of the sampler
+ * `kind` (RenderSamplerKind) constructed for each query's pixel and sample.
+ * `queries` holds n rows of 6 int32 (x, y, sample, bounce, dimension, lane);
+ * a negative bounce counts as 0. `out` receives n floats (two_d == 0) or
+ * 2n floats (x, y per row). */
+yrc_status yrc_sampler_eval(int32_t kind, uint64_t seed, int32_t spp, const int32_t* queries, int64_t n,
+                            int32_t two_d, float* out);
+
+/* Rng(seed) (include/yaoray/core/rng.hpp:15-48) for each of the n seeds,
+ * followed by `draws` calls of NextFloat; out is n x draws floats. */
+yrc_status yrc_rng_eval(const uint64_t* seeds, int64_t n, int32_t draws, float* out);
+
+/* SeedForPixelSample(seed, x, y, sample) (src/sampling/sampler.cpp:304-310)
+ * for n rows of 3 int64 (x, y, sample). */
+yrc_status yrc_pixel_seed_eval(uint64_t seed, const int64_t* queries, int64_t n, uint64_t* out);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
