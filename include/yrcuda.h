@@ -391,6 +391,49 @@ yrc_status yrc_accel_check(yrc_accel* accel);
 
 /* ================================================================= render */
 
+/* TextureFilter / TextureWrap (include/yaoray/scene/texture_options.hpp:7-17). */
+enum {
+    YRC_TEX_NEAREST = 0,
+    YRC_TEX_BILINEAR = 1,
+    YRC_TEX_TRILINEAR = 2,
+    YRC_TEX_EWA = 3
+};
+enum {
+    YRC_WRAP_REPEAT = 0,
+    YRC_WRAP_CLAMP_TO_EDGE = 1,
+    YRC_WRAP_MIRRORED_REPEAT = 2
+};
+
+/* RenderTexture (include/yaoray/scene/texture.hpp:37-51): an RGBA32F image
+ * in the reference's texel order (row y at texels + 4 * y * width). width or
+ * height <= 0, or texels NULL, is a texture without data, which samples as
+ * (0, 0, 0, 1). Mip chains are built on the device at upload. */
+typedef struct yrc_texture {
+    int32_t width;
+    int32_t height;
+    const float* texels; /* width * height * 4 floats */
+    int32_t filter;      /* YRC_TEX_* */
+    int32_t wrap_s;      /* YRC_WRAP_* */
+    int32_t wrap_t;
+    int32_t reserved;
+} yrc_texture;
+
+/* SampleTexture4 (src/shading/texture.cpp:297-309) evaluated on the device
+ * for n (u, v) pairs and, when `footprints` is not NULL, n TextureFootprints
+ * (dudx, dvdx, dudy, dvdy); out receives n RGBA values. Nearest and bilinear
+ * lookups are bit-identical to the reference's; trilinear and EWA lookups
+ * can differ in the last bits of the level-of-detail blend (log2). The mip
+ * chain is built for the call. Synchronous. */
+yrc_status yrc_texture_sample_eval(const yrc_texture* texture, const float* uvs, const float* footprints, int64_t n,
+                                   float* out);
+
+/* BuildTextureMipChain (src/shading/texture.cpp:242-264) on the device:
+ * writes every level, the image first, as RGBA texels into `texels`
+ * (`capacity` texels), (width, height) per level into level_dims and the
+ * number of levels into *level_count (0 for a texture without data). */
+yrc_status yrc_texture_mip_chain_eval(const yrc_texture* texture, float* texels, int64_t capacity, int32_t* level_dims,
+                                      int32_t* level_count);
+
 /* RenderMaterialKind (include/yaoray/scene/material.hpp:7-19). */
 enum {
     YRC_MAT_DIFFUSE = 0,
@@ -406,8 +449,11 @@ enum {
     YRC_MAT_SUBSURFACE_EXIT = 10
 };
 
-/* RenderMaterial (material.hpp:31-65) with texture slots as indices; the
- * device shades untextured materials (every *_texture / normal_map = -1). */
+/* RenderMaterial (material.hpp:31-65) with texture slots as indices into
+ * yrc_scene_desc.textures. The reference samples three of them
+ * (EvaluateMaterialAtSurface, src/shading/material_evaluator.cpp:112-180):
+ * reflectance (multiplied in), alpha (a surface with alpha < 0.5 is skipped
+ * by every ray) and the tangent-space normal map. */
 typedef struct yrc_material {
     int32_t kind;
     float reflectance[3];
@@ -434,10 +480,11 @@ typedef struct yrc_material {
     float alpha;
     float absorption_color[3];
     float absorption_distance;
-    int32_t reflectance_texture;
-    int32_t alpha_texture;
-    int32_t normal_map;
+    int32_t reflectance_texture; /* texture index or -1 */
+    int32_t alpha_texture;       /* texture index or -1 (its red channel scales alpha) */
+    int32_t normal_map;          /* texture index or -1 */
     int32_t measured_index;
+    float normal_scale;          /* scales the normal map's tangent-space x and y (reference default 1) */
 } yrc_material;
 
 /* EmissivePrimitive (include/yaoray/scene/light.hpp:30-34). */
@@ -553,6 +600,16 @@ typedef struct yrc_scene_desc {
     yrc_render_settings settings;
     const yrc_bvh_view* flat;
     const yrc_two_level_view* two_level;
+    /* RenderVertex uv, tangent and tangent_handedness (geometry.hpp:12-18),
+     * read for primitives whose flags say has_uvs / has_tangents: uv is 2
+     * floats at uvs + k * uv_stride bytes, the tangent 3 floats followed by
+     * the handedness at tangents + k * tangent_stride (NULL: none). */
+    const float* uvs;
+    int64_t uv_stride;
+    const float* tangents;
+    int64_t tangent_stride;
+    const yrc_texture* textures;
+    int32_t texture_count;
 } yrc_scene_desc;
 
 /* FilmPixel (include/yaoray/film/film.hpp:19-28), byte-identical, 56 bytes. */
@@ -639,7 +696,7 @@ typedef struct yrc_render_scene yrc_render_scene;
 
 /* CudaBackend::Prepare (src/runtime/cuda_stub_backend.cpp:20-28): uploads the
  * scene and its acceleration structure. Fails with YRC_ERR_UNSUPPORTED for
- * scene features the device does not shade (textures, measured BRDFs). */
+ * scene features the device does not shade (measured BRDFs). */
 yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene** out);
 void yrc_render_scene_destroy(yrc_render_scene* scene);
 int64_t yrc_render_scene_device_bytes(const yrc_render_scene* scene);

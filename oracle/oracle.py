@@ -82,6 +82,9 @@ def oracle_lib() -> C.CDLL:
         L.yo_seed_for_pixel_sample.argtypes = [U64, C.c_int, C.c_int, C.c_int]
         L.yo_seed_for_pixel_sample.restype = U64
         L.yo_rng_floats.argtypes = [U64, C.c_int, P]
+        L.yo_texture_sample.argtypes = [C.c_int, C.c_int, P, C.c_int, C.c_int, C.c_int, P, P, I64, P]
+        L.yo_texture_mip_chain.argtypes = [C.c_int, C.c_int, P, C.c_int, C.c_int, P, P]
+        L.yo_texture_mip_chain.restype = C.c_int
         L.yo_camera_rays.argtypes = [P, C.c_int, C.c_int, P, P, I64, P]
         L.yo_film_accumulate.argtypes = [C.c_int, C.c_int, P, I64, P]
         L.yo_film_accumulate.restype = U64
@@ -237,6 +240,9 @@ def ref_lib() -> C.CDLL:
         L.yrref_camera_rays.argtypes = [P, C.c_int, C.c_int, P, P, I64, P]
         L.yrref_film_accumulate.argtypes = [C.c_int, C.c_int, P, I64, P]
         L.yrref_film_accumulate.restype = U64
+        L.yrref_texture_sample.argtypes = [C.c_int, C.c_int, P, C.c_int, C.c_int, C.c_int, P, P, I64, P]
+        L.yrref_texture_mip_chain.argtypes = [C.c_int, C.c_int, P, C.c_int, C.c_int, P, P]
+        L.yrref_texture_mip_chain.restype = C.c_int
         _REF = L
     return _REF
 
@@ -361,6 +367,70 @@ def ref_sampler(kind: int, seed: int, spp: int, queries: np.ndarray, two_d: bool
     out = np.empty(q.shape[0] * (2 if two_d else 1), np.float32)
     ref_lib().yrref_sampler(kind, seed, spp, q.ctypes.data, q.shape[0], int(two_d), out.ctypes.data)
     return out.reshape(-1, 2) if two_d else out
+
+
+def _texture_args(texels, uvs, footprints):
+    tx = np.ascontiguousarray(texels, np.float32)
+    uv = np.ascontiguousarray(uvs, np.float32).reshape(-1, 2)
+    fp = None if footprints is None else np.ascontiguousarray(footprints, np.float32).reshape(-1, 4)
+    return tx, uv, fp
+
+
+def _mip_buffers(width: int, height: int):
+    return np.zeros((max(width * height, 0) + 64) * 4, np.float32), np.zeros(80, np.int32)
+
+
+def _mip_levels(out, dims, count):
+    levels, at = [], 0
+    for k in range(count):
+        w, h = int(dims[2 * k]), int(dims[2 * k + 1])
+        levels.append(out[4 * at:4 * (at + w * h)].reshape(h, w, 4).copy())
+        at += w * h
+    return levels
+
+
+def ref_texture_sample(texels: np.ndarray, filter: int, wrap_s: int, wrap_t: int, uvs: np.ndarray,
+                       footprints: np.ndarray | None = None) -> np.ndarray:
+    """The reference's SampleTexture4 on an (h, w, 4) RGBA32F image."""
+    tx, uv, fp = _texture_args(texels, uvs, footprints)
+    out = np.empty((uv.shape[0], 4), np.float32)
+    h, w = (tx.shape[0], tx.shape[1]) if tx.ndim == 3 else (0, 0)
+    ref_lib().yrref_texture_sample(w, h, tx.ctypes.data if tx.size else None, filter, wrap_s, wrap_t,
+                                   uv.ctypes.data, None if fp is None else fp.ctypes.data, uv.shape[0],
+                                   out.ctypes.data)
+    return out
+
+
+def ref_texture_mip_chain(texels: np.ndarray, wrap_s: int, wrap_t: int) -> list:
+    """The reference's BuildTextureMipChain levels (after the image)."""
+    tx = np.ascontiguousarray(texels, np.float32)
+    h, w = tx.shape[0], tx.shape[1]
+    out, dims = _mip_buffers(w, h)
+    count = ref_lib().yrref_texture_mip_chain(w, h, tx.ctypes.data, wrap_s, wrap_t, out.ctypes.data,
+                                              dims.ctypes.data)
+    return _mip_levels(out, dims, count)
+
+
+def oracle_texture_sample(texels: np.ndarray, filter: int, wrap_s: int, wrap_t: int, uvs: np.ndarray,
+                          footprints: np.ndarray | None = None) -> np.ndarray:
+    """The C restatement's SampleTexture4 on an (h, w, 4) RGBA32F image."""
+    tx, uv, fp = _texture_args(texels, uvs, footprints)
+    out = np.empty((uv.shape[0], 4), np.float32)
+    h, w = (tx.shape[0], tx.shape[1]) if tx.ndim == 3 else (0, 0)
+    oracle_lib().yo_texture_sample(w, h, tx.ctypes.data if tx.size else None, filter, wrap_s, wrap_t,
+                                   uv.ctypes.data, None if fp is None else fp.ctypes.data, uv.shape[0],
+                                   out.ctypes.data)
+    return out
+
+
+def oracle_texture_mip_chain(texels: np.ndarray, wrap_s: int, wrap_t: int) -> list:
+    """The C restatement's BuildTextureMipChain levels (after the image)."""
+    tx = np.ascontiguousarray(texels, np.float32)
+    h, w = tx.shape[0], tx.shape[1]
+    out, dims = _mip_buffers(w, h)
+    count = oracle_lib().yo_texture_mip_chain(w, h, tx.ctypes.data, wrap_s, wrap_t, out.ctypes.data,
+                                              dims.ctypes.data)
+    return _mip_levels(out, dims, count)
 
 
 def ref_bssrdf_table(g: float, eta: float, rho_count: int = 100, radius_count: int = 64) -> dict:

@@ -17,6 +17,7 @@
 #include <yaoray/sampling/sampler.hpp>
 #include <yaoray/scene/camera.hpp>
 #include <yaoray/scene/render_scene.hpp>
+#include <yaoray/shading/texture.hpp>
 
 #include <algorithm>
 #include <atomic>
@@ -328,6 +329,65 @@ void yrref_sampler(int kind, std::uint64_t seed, int spp, const int* queries, st
 
 std::uint64_t yrref_seed_for_pixel_sample(std::uint64_t seed, int x, int y, int sample) {
     return yr::SeedForPixelSample(seed, x, y, sample);
+}
+
+// ------------------------------------------------------------------ texture ---
+// An RGBA32F image prepared as the reference prepares scene textures
+// (BuildTextureSamplingCaches) and looked up with SampleTexture4; footprints
+// are 4 floats per lookup or NULL (no footprint).
+static yr::RenderTexture MakeTexture(int width, int height, const float* texels, int filter, int wrap_s,
+    int wrap_t) {
+    yr::RenderTexture t;
+    t.width = width;
+    t.height = height;
+    if (texels && width > 0 && height > 0) {
+        t.texels.resize(static_cast<std::size_t>(width) * static_cast<std::size_t>(height));
+        for (std::size_t i = 0; i < t.texels.size(); ++i) {
+            t.texels[i] = yr::Color4f{texels[4 * i], texels[4 * i + 1], texels[4 * i + 2], texels[4 * i + 3]};
+        }
+    }
+    t.filter = static_cast<yr::TextureFilter>(filter);
+    t.wrap_s = static_cast<yr::TextureWrap>(wrap_s);
+    t.wrap_t = static_cast<yr::TextureWrap>(wrap_t);
+    return t;
+}
+
+void yrref_texture_sample(int width, int height, const float* texels, int filter, int wrap_s, int wrap_t,
+    const float* uvs, const float* footprints, std::int64_t n, float* out) {
+    std::vector<yr::RenderTexture> textures;
+    textures.push_back(MakeTexture(width, height, texels, filter, wrap_s, wrap_t));
+    yr::BuildTextureSamplingCaches(textures);
+    for (std::int64_t i = 0; i < n; ++i) {
+        const yr::Vec2f uv{uvs[2 * i], uvs[2 * i + 1]};
+        yr::TextureFootprint f;
+        if (footprints) f = yr::TextureFootprint{footprints[4 * i], footprints[4 * i + 1], footprints[4 * i + 2],
+            footprints[4 * i + 3]};
+        const yr::Color4f c = yr::SampleTexture4(textures[0], uv, f);
+        out[4 * i] = c.x;
+        out[4 * i + 1] = c.y;
+        out[4 * i + 2] = c.z;
+        out[4 * i + 3] = c.w;
+    }
+}
+
+// BuildTextureMipChain: the levels after the image into `out`, (w, h) per
+// level into dims; returns the level count.
+int yrref_texture_mip_chain(int width, int height, const float* texels, int wrap_s, int wrap_t, float* out,
+    int* dims) {
+    yr::RenderTexture t = MakeTexture(width, height, texels, 1, wrap_s, wrap_t);
+    yr::BuildTextureMipChain(t);
+    std::size_t at = 0;
+    for (std::size_t l = 0; l < t.mip_levels.size(); ++l) {
+        dims[2 * l] = t.mip_levels[l].width;
+        dims[2 * l + 1] = t.mip_levels[l].height;
+        for (const yr::Color4f& c : t.mip_levels[l].texels) {
+            out[at++] = c.x;
+            out[at++] = c.y;
+            out[at++] = c.z;
+            out[at++] = c.w;
+        }
+    }
+    return static_cast<int>(t.mip_levels.size());
 }
 
 // First `count` NextFloat() draws of Rng(seed).

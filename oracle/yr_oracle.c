@@ -710,3 +710,271 @@ uint64_t yo_film_accumulate(int width, int height, const float* samples, int64_t
     }
     return bad;
 }
+
+/* ----------------------------------------------------------------- texture */
+
+/* RenderTexture sampling (src/shading/texture.cpp:14-322). A texture is the
+ * image plus its mip chain, levels stored one after the other. */
+typedef struct tex_level {
+    int w, h;
+    const float* t; /* RGBA rows */
+} tex_level;
+
+typedef struct tex_view {
+    int width, height, filter, wrap_s, wrap_t, levels;
+    tex_level lv[40];
+} tex_view;
+
+typedef struct rgba {
+    float x, y, z, w;
+} rgba;
+
+static rgba rgba_black(void) { rgba c = {0.0f, 0.0f, 0.0f, 1.0f}; return c; } /* Color4f{} */
+static rgba rgba_add(rgba a, rgba b) { rgba c = {a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; return c; }
+static rgba rgba_scale(rgba a, float s) { rgba c = {a.x * s, a.y * s, a.z * s, a.w * s}; return c; }
+static rgba rgba_div(rgba a, float s) { rgba c = {a.x / s, a.y / s, a.z / s, a.w / s}; return c; }
+/* Lerp (texture.cpp:101-103). */
+static rgba rgba_lerp(rgba a, rgba b, float t) { return rgba_add(rgba_scale(a, 1.0f - t), rgba_scale(b, t)); }
+static float fmax_std(float a, float b) { return a < b ? b : a; }
+static float fmin_std(float a, float b) { return b < a ? b : a; }
+static int clampi(int v, int lo, int hi) { return v < lo ? lo : (hi < v ? hi : v); }
+
+/* ApplyWrap (texture.cpp:20-28): 0 repeat, 1 clamp, 2 mirrored repeat. */
+static float apply_wrap(float v, int wrap) {
+    if (wrap == 1) return v < 0.0f ? 0.0f : (1.0f < v ? 1.0f : v);
+    const float base = floorf(v);
+    const float fraction = v - base;
+    if (wrap == 2) return (((int)base) & 1) == 0 ? fraction : 1.0f - fraction;
+    return fraction < 0.0f ? fraction + 1.0f : fraction;
+}
+
+/* WrappedTexelIndex (texture.cpp:30-40). */
+static int wrapped_index(int value, int count, int wrap) {
+    if (wrap == 1) return clampi(value, 0, count - 1);
+    if (wrap == 2) {
+        const int period = count * 2;
+        int w = value % period;
+        if (w < 0) w += period;
+        return w < count ? w : period - 1 - w;
+    }
+    int w = value % count;
+    if (w < 0) w += count;
+    return w;
+}
+
+/* TexelAt (texture.cpp:90-99). */
+static rgba texel_at(tex_level l, int x, int y, int ws, int wt) {
+    if (l.w <= 0 || l.h <= 0 || !l.t) return rgba_black();
+    const int ix = wrapped_index(x, l.w, ws), iy = wrapped_index(y, l.h, wt);
+    const float* p = l.t + 4 * ((int64_t)iy * l.w + ix);
+    rgba c = {p[0], p[1], p[2], p[3]};
+    return c;
+}
+
+/* Level (texture.cpp:42-60). */
+static tex_level tex_level_of(const tex_view* t, int level) {
+    const int i = level <= 0 ? 0 : (level < t->levels - 1 ? level : t->levels - 1);
+    return t->lv[i];
+}
+
+/* SampleNearest (texture.cpp:105-113). */
+static rgba sample_nearest(tex_level l, const tex_view* t, float u, float v) {
+    if (l.w <= 0 || l.h <= 0 || !l.t) return rgba_black();
+    const int x = clampi((int)floorf(apply_wrap(u, t->wrap_s) * (float)l.w), 0, l.w - 1);
+    const int y = clampi((int)floorf(apply_wrap(v, t->wrap_t) * (float)l.h), 0, l.h - 1);
+    return texel_at(l, x, y, t->wrap_s, t->wrap_t);
+}
+
+/* SampleBilinear (texture.cpp:115-130). */
+static rgba sample_bilinear(tex_level l, const tex_view* t, float u, float v) {
+    if (l.w <= 0 || l.h <= 0 || !l.t) return rgba_black();
+    if (l.w == 1 && l.h == 1) {
+        rgba c = {l.t[0], l.t[1], l.t[2], l.t[3]};
+        return c;
+    }
+    const float s = apply_wrap(u, t->wrap_s) * (float)l.w - 0.5f;
+    const float tt = apply_wrap(v, t->wrap_t) * (float)l.h - 0.5f;
+    const int s0 = (int)floorf(s), t0 = (int)floorf(tt);
+    const float ds = s - (float)s0, dt = tt - (float)t0;
+    const rgba c00 = texel_at(l, s0, t0, t->wrap_s, t->wrap_t);
+    const rgba c10 = texel_at(l, s0 + 1, t0, t->wrap_s, t->wrap_t);
+    const rgba c01 = texel_at(l, s0, t0 + 1, t->wrap_s, t->wrap_t);
+    const rgba c11 = texel_at(l, s0 + 1, t0 + 1, t->wrap_s, t->wrap_t);
+    return rgba_lerp(rgba_lerp(c00, c10, ds), rgba_lerp(c01, c11, ds), dt);
+}
+
+/* LodForFootprint (texture.cpp:132-138). */
+static float lod_for_footprint(const tex_view* t, const float* f) {
+    const float w = (float)(t->width > 1 ? t->width : 1), h = (float)(t->height > 1 ? t->height : 1);
+    const float dx = hypotf(f[0] * w, f[1] * h);
+    const float dy = hypotf(f[2] * w, f[3] * h);
+    return fmax_std(0.0f, log2f(fmax_std(1.0f, fmax_std(dx, dy))));
+}
+
+/* EwaWeights (texture.cpp:140-152). */
+static float ewa_weight(size_t i) {
+    static float weights[128];
+    static int ready = 0;
+    if (!ready) {
+        const float alpha = 2.0f, edge = expf(-alpha);
+        for (size_t k = 0; k < 128; ++k) {
+            const float r2 = (float)k / (float)(128 - 1);
+            weights[k] = expf(-alpha * r2) - edge;
+        }
+        ready = 1;
+    }
+    return weights[i];
+}
+
+/* SampleEwaLevel (texture.cpp:154-213). */
+static rgba sample_ewa_level(const tex_view* t, float u, float v, const float* f, int level) {
+    const tex_level l = tex_level_of(t, level);
+    if (l.w <= 0 || l.h <= 0 || !l.t) return rgba_black();
+    float dsdx = f[0] * (float)l.w, dtdx = f[1] * (float)l.h;
+    float dsdy = f[2] * (float)l.w, dtdy = f[3] * (float)l.h;
+    if (dsdx * dsdx + dtdx * dtdx < dsdy * dsdy + dtdy * dtdy) {
+        float tmp = dsdx; dsdx = dsdy; dsdy = tmp;
+        tmp = dtdx; dtdx = dtdy; dtdy = tmp;
+    }
+    const float major = hypotf(dsdx, dtdx);
+    float minor = hypotf(dsdy, dtdy);
+    const float max_anisotropy = 8.0f;
+    if (minor > 0.0f && major > minor * max_anisotropy) {
+        const float scale = major / (minor * max_anisotropy);
+        dsdy *= scale;
+        dtdy *= scale;
+        minor *= scale;
+    }
+    if (minor == 0.0f) return sample_bilinear(l, t, u, v);
+    const float s = apply_wrap(u, t->wrap_s) * (float)l.w - 0.5f;
+    const float tc = apply_wrap(v, t->wrap_t) * (float)l.h - 0.5f;
+    float a = dtdx * dtdx + dtdy * dtdy + 1.0f;
+    float b = -2.0f * (dsdx * dtdx + dsdy * dtdy);
+    float c = dsdx * dsdx + dsdy * dsdy + 1.0f;
+    const float inverse = 1.0f / (a * c - 0.25f * b * b);
+    a *= inverse;
+    b *= inverse;
+    c *= inverse;
+    const float determinant = -b * b + 4.0f * a * c;
+    if (determinant <= 0.0f) return sample_bilinear(l, t, u, v);
+    const float inverse_det = 1.0f / determinant;
+    const float radius_s = 2.0f * sqrtf(c * inverse_det);
+    const float radius_t = 2.0f * sqrtf(a * inverse_det);
+    const int s0 = (int)ceilf(s - radius_s), s1 = (int)floorf(s + radius_s);
+    const int t0 = (int)ceilf(tc - radius_t), t1 = (int)floorf(tc + radius_t);
+    rgba sum = rgba_black();
+    float weight_sum = 0.0f;
+    for (int it = t0; it <= t1; ++it) {
+        for (int is = s0; is <= s1; ++is) {
+            const float ss = (float)is - s, tt = (float)it - tc;
+            const float r2 = a * ss * ss + b * ss * tt + c * tt * tt;
+            if (r2 >= 1.0f) continue;
+            size_t wi = (size_t)(r2 * 128.0f);
+            if (wi > 127) wi = 127;
+            const float weight = ewa_weight(wi);
+            sum = rgba_add(sum, rgba_scale(texel_at(l, is, it, t->wrap_s, t->wrap_t), weight));
+            weight_sum += weight;
+        }
+    }
+    return weight_sum > 0.0f ? rgba_div(sum, weight_sum) : sample_bilinear(l, t, u, v);
+}
+
+/* SampleTrilinear (texture.cpp:215-223). */
+static rgba sample_trilinear(const tex_view* t, float u, float v, const float* f) {
+    const float lod = fmin_std(lod_for_footprint(t, f), (float)(t->levels - 1));
+    const int l0 = (int)floorf(lod);
+    const int l1 = l0 + 1 < t->levels - 1 ? l0 + 1 : t->levels - 1;
+    return rgba_lerp(sample_bilinear(tex_level_of(t, l0), t, u, v), sample_bilinear(tex_level_of(t, l1), t, u, v),
+                     lod - (float)l0);
+}
+
+/* SampleEwa (texture.cpp:225-238). */
+static rgba sample_ewa(const tex_view* t, float u, float v, const float* f) {
+    const float w = (float)(t->width > 1 ? t->width : 1), h = (float)(t->height > 1 ? t->height : 1);
+    const float dx = hypotf(f[0] * w, f[1] * h);
+    const float dy = hypotf(f[2] * w, f[3] * h);
+    const float minor = fmax_std(1.0f, fmin_std(dx, dy));
+    const float lod = fmin_std(fmax_std(0.0f, log2f(minor)), (float)(t->levels - 1));
+    const int l0 = (int)floorf(lod);
+    const int l1 = l0 + 1 < t->levels - 1 ? l0 + 1 : t->levels - 1;
+    return rgba_lerp(sample_ewa_level(t, u, v, f, l0), sample_ewa_level(t, u, v, f, l1), lod - (float)l0);
+}
+
+/* BuildTextureMipChain (texture.cpp:242-264): level dims halve with
+ * round-up; each texel is ((a + b) + c) + d of the 2x2 block, times 0.25.
+ * Writes the levels after the image into `out`; returns their count. */
+int yo_texture_mip_chain(int width, int height, const float* texels, int wrap_s, int wrap_t, float* out, int32_t* dims) {
+    if (width <= 0 || height <= 0 || !texels) return 0;
+    tex_level src = {width, height, texels};
+    int count = 0;
+    float* dst = out;
+    while (src.w > 1 || src.h > 1) {
+        const int w = (src.w + 1) / 2 > 1 ? (src.w + 1) / 2 : 1;
+        const int h = (src.h + 1) / 2 > 1 ? (src.h + 1) / 2 : 1;
+        for (int y = 0; y < h; ++y) {
+            for (int x = 0; x < w; ++x) {
+                rgba f = texel_at(src, x * 2, y * 2, wrap_s, wrap_t);
+                f = rgba_add(f, texel_at(src, x * 2 + 1, y * 2, wrap_s, wrap_t));
+                f = rgba_add(f, texel_at(src, x * 2, y * 2 + 1, wrap_s, wrap_t));
+                f = rgba_add(f, texel_at(src, x * 2 + 1, y * 2 + 1, wrap_s, wrap_t));
+                f = rgba_scale(f, 0.25f);
+                float* p = dst + 4 * ((int64_t)y * w + x);
+                p[0] = f.x; p[1] = f.y; p[2] = f.z; p[3] = f.w;
+            }
+        }
+        dims[2 * count] = w;
+        dims[2 * count + 1] = h;
+        ++count;
+        src.w = w;
+        src.h = h;
+        src.t = dst;
+        dst += 4 * (int64_t)w * h;
+    }
+    return count;
+}
+
+/* SampleTexture4 (texture.cpp:297-309) after BuildTextureMipChain. */
+void yo_texture_sample(int width, int height, const float* texels, int filter, int wrap_s, int wrap_t,
+                       const float* uvs, const float* footprints, int64_t n, float* out) {
+    tex_view t;
+    memset(&t, 0, sizeof t);
+    t.width = width;
+    t.height = height;
+    t.filter = filter;
+    t.wrap_s = wrap_s;
+    t.wrap_t = wrap_t;
+    float* chain = NULL;
+    if (width > 0 && height > 0 && texels) {
+        chain = (float*)malloc(sizeof(float) * 4 * ((size_t)width * height + 64));
+        int32_t dims[80];
+        const int mips = yo_texture_mip_chain(width, height, texels, wrap_s, wrap_t, chain, dims);
+        t.levels = 1 + mips;
+        t.lv[0].w = width;
+        t.lv[0].h = height;
+        t.lv[0].t = texels;
+        const float* at = chain;
+        for (int l = 0; l < mips; ++l) {
+            t.lv[1 + l].w = dims[2 * l];
+            t.lv[1 + l].h = dims[2 * l + 1];
+            t.lv[1 + l].t = at;
+            at += 4 * (int64_t)dims[2 * l] * dims[2 * l + 1];
+        }
+    }
+    static const float zero[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int64_t i = 0; i < n; ++i) {
+        const float u = uvs[2 * i], v = uvs[2 * i + 1];
+        const float* f = footprints ? footprints + 4 * i : zero;
+        const int fzero = f[0] == 0.0f && f[1] == 0.0f && f[2] == 0.0f && f[3] == 0.0f;
+        rgba c;
+        if (t.width <= 0 || t.height <= 0 || t.levels == 0) c = rgba_black();
+        else if (t.filter == 0) c = sample_nearest(t.lv[0], &t, u, v);
+        else if (t.filter == 2 && !fzero && t.levels > 1) c = sample_trilinear(&t, u, v, f);
+        else if (t.filter == 3 && !fzero && t.levels > 1) c = sample_ewa(&t, u, v, f);
+        else c = sample_bilinear(t.lv[0], &t, u, v);
+        out[4 * i] = c.x;
+        out[4 * i + 1] = c.y;
+        out[4 * i + 2] = c.z;
+        out[4 * i + 3] = c.w;
+    }
+    free(chain);
+}

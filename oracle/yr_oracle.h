@@ -113,6 +113,19 @@ void yo_camera_rays(const float* camera, int width, int height, const int32_t* p
  * pixels_out: 14 x 4 bytes per pixel in FilmPixel order. Returns bad count. */
 uint64_t yo_film_accumulate(int width, int height, const float* samples, int64_t n, void* pixels_out);
 
+/* RenderTexture lookups (src/shading/texture.cpp): SampleTexture4 after
+ * BuildTextureMipChain. texels: RGBA32F rows; filter 0 nearest, 1 bilinear,
+ * 2 trilinear, 3 EWA; wrap 0 repeat, 1 clamp-to-edge, 2 mirrored repeat.
+ * uvs: 2 floats per lookup; footprints: 4 per lookup (dudx, dvdx, dudy,
+ * dvdy) or NULL; out: 4 per lookup. */
+void yo_texture_sample(int width, int height, const float* texels, int filter, int wrap_s, int wrap_t,
+                       const float* uvs, const float* footprints, int64_t n, float* out);
+/* BuildTextureMipChain: the levels after the image, one after the other, in
+ * `out` (sized for width * height + 64 texels suffices); dims: (w, h) per
+ * level. Returns the number of levels written. */
+int yo_texture_mip_chain(int width, int height, const float* texels, int wrap_s, int wrap_t, float* out,
+                         int32_t* dims);
+
 #ifdef __cplusplus
 }
 #endif

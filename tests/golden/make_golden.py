@@ -5,11 +5,13 @@ fixtures are outputs of the unmodified reference code, compiled from its
 sources by oracle/Makefile into oracle/_ref/libyaoray_ref.so and called
 through oracle/ref_shim.cpp: IntersectAcceleration / IntersectTwoLevelBvh /
 IntersectAccelerationProbe, BuildBvh / BuildTwoLevelBvh, Sampler, Rng,
-GeneratePerspectiveCameraRay and Film::AddSample. Inputs are small seeded
+GeneratePerspectiveCameraRay, Film::AddSample, SampleTexture4 and
+BuildTextureMipChain. Inputs are small seeded
 cases; each file stores inputs and expected outputs so the CPU tests can pin
 the oracle restatement without the reference present.
 
-Run: python tests/golden/make_golden.py   (needs oracle/_ref built)
+Run: python tests/golden/make_golden.py [texture]   (needs oracle/_ref built;
+`texture` writes only texture.npz)
 """
 from __future__ import annotations
 
@@ -197,8 +199,43 @@ def main() -> None:
     film, nbad = oracle.ref_film(w, h, s)
     np.savez_compressed(HERE / "camera_film.npz", camera=cam, pixels=px, samples=sm, rays=cam_rays, film_samples=s,
                         film_w=w, film_h=h, film_pixels=film.view(np.uint8), film_bad=np.int64(nbad))
+    texture_fixture()
     print("golden fixtures written to", HERE)
 
 
+def texture_fixture() -> None:
+    """7. Texture lookups (SampleTexture4 after BuildTextureSamplingCaches)
+    and mip chains (BuildTextureMipChain): odd and degenerate sizes, every
+    wrap mode, every filter, lookups with and without footprints, uvs on
+    texel edges, far outside [0, 1] and non-finite."""
+    rng = np.random.default_rng(0x7E57)
+    shapes = [(1, 1), (1, 37), (37, 1), (2, 2), (4, 4), (5, 3), (23, 37), (32, 32)]
+    wraps = [(0, 0), (1, 1), (2, 2), (0, 2), (2, 1)]
+    fx = {"shapes": np.array(shapes, np.int32), "wraps": np.array(wraps, np.int32)}
+    n = 160
+    for si, (h, w) in enumerate(shapes):
+        tx = rng.random((h, w, 4), dtype=np.float32)
+        tx[..., 3] = rng.choice(np.array([0.0, 0.3, 0.7, 1.0], np.float32), (h, w))
+        fx[f"t{si}_texels"] = tx
+        for wi, (ws, wt) in enumerate(wraps):
+            uv = rng.uniform(-2.5, 3.5, (n, 2)).astype(np.float32)
+            uv[:16] = rng.integers(-3 * w, 4 * w, (16, 2)) / np.array([w, h], np.float32)
+            uv[16:20] = np.array([[0, 0], [1, 1], [0.5, 0.5], [1e3, -1e3]], np.float32)
+            uv[20:22] = np.array([[np.nan, 0.25], [np.inf, 0.5]], np.float32)
+            fp = (rng.standard_normal((n, 4)) * np.exp(rng.uniform(-10.0, 2.0, (n, 1)))).astype(np.float32)
+            fp[:40] = 0.0
+            fp[40:50, 1:3] = 0.0  # axis-aligned footprints
+            fx[f"t{si}_w{wi}_uv"] = uv
+            fx[f"t{si}_w{wi}_fp"] = fp
+            for f in range(4):
+                fx[f"t{si}_w{wi}_f{f}"] = oracle.ref_texture_sample(tx, f, ws, wt, uv, fp)
+            for li, lv in enumerate(oracle.ref_texture_mip_chain(tx, ws, wt)):
+                fx[f"t{si}_w{wi}_mip{li}"] = lv
+    np.savez_compressed(HERE / "texture.npz", **fx)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["texture"]:
+        texture_fixture()
+    else:
+        main()

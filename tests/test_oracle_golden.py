@@ -124,6 +124,32 @@ def test_film_matches_reference_golden():
     assert px.view(np.uint8).tobytes() == f["film_pixels"].tobytes()
 
 
+def same_values(a, b):
+    """Bit-equal, except that any NaN matches any NaN (x86-64 and CUDA
+    produce NaNs with different payloads)."""
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    na, nb = np.isnan(a), np.isnan(b)
+    return np.array_equal(na, nb) and np.array_equal(bits(np.where(na, 0, a)), bits(np.where(nb, 0, b)))
+
+
+def test_texture_matches_reference_golden():
+    f = load("texture")
+    for si in range(len(f["shapes"])):
+        tx = f[f"t{si}_texels"]
+        for wi, (ws, wt) in enumerate(f["wraps"]):
+            uv, fp = f[f"t{si}_w{wi}_uv"], f[f"t{si}_w{wi}_fp"]
+            for filt in range(4):
+                got = oracle.oracle_texture_sample(tx, filt, int(ws), int(wt), uv, fp)
+                assert same_values(got, f[f"t{si}_w{wi}_f{filt}"]), (si, wi, filt)
+            mips = oracle.oracle_texture_mip_chain(tx, int(ws), int(wt))
+            expect = [f[k] for k in sorted((k for k in f if k.startswith(f"t{si}_w{wi}_mip")),
+                                           key=lambda k: int(k.split("mip")[1]))]
+            assert len(mips) == len(expect)
+            for a, b in zip(mips, expect):
+                assert np.array_equal(bits(a), bits(b))
+
+
 # ---------------------------------------------------------- live reference
 
 def test_oracle_matches_live_reference_on_traversal_set(ref):
@@ -148,3 +174,16 @@ def test_oracle_sampler_matches_live_reference_random(ref):
                 a = oracle.oracle_sampler(kind, 99, spp, q, d2)
                 b = ref.ref_sampler(kind, 99, spp, q, d2)
                 assert np.array_equal(bits(a), bits(b))
+
+
+def test_oracle_texture_matches_live_reference_random(ref):
+    rng = np.random.default_rng(12)
+    for h, w in [(3, 7), (64, 48), (1, 129)]:
+        tx = rng.random((h, w, 4), dtype=np.float32)
+        uv = rng.uniform(-4, 4, (4000, 2)).astype(np.float32)
+        fp = (rng.standard_normal((4000, 4)) * np.exp(rng.uniform(-9, 1, (4000, 1)))).astype(np.float32)
+        for ws, wt in [(0, 1), (2, 0), (1, 2)]:
+            for filt in range(4):
+                a = oracle.oracle_texture_sample(tx, filt, ws, wt, uv, fp)
+                b = ref.ref_texture_sample(tx, filt, ws, wt, uv, fp)
+                assert same_values(a, b), (h, w, ws, wt, filt)

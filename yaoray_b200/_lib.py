@@ -199,6 +199,8 @@ def lib() -> C.CDLL:
         "yrc_sampler_eval": (C.c_int, [I32, C.c_uint64, I32, P, I64, I32, P]),
         "yrc_rng_eval": (C.c_int, [P, I64, I32, P]),
         "yrc_pixel_seed_eval": (C.c_int, [C.c_uint64, P, I64, P]),
+        "yrc_texture_sample_eval": (C.c_int, [P, P, P, I64, P]),
+        "yrc_texture_mip_chain_eval": (C.c_int, [P, P, I64, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
