@@ -201,13 +201,27 @@ BackendPrepareResult CudaBackend::Prepare(RenderJob job) {
         o.alpha = m.alpha.value;
         Rgb(m.absorption_color, o.absorption_color);
         o.absorption_distance = m.absorption_distance;
-        // The device shades untextured materials; a texture is only looked up
-        // on primitives with UVs, so report it only where one could apply.
         o.reflectance_texture = m.reflectance.texture;
         o.alpha_texture = m.alpha.texture;
         o.normal_map = m.normal_map;
         o.measured_index = m.measured_index;
+        o.normal_scale = m.normal_scale;
     }
+    // Vertex uvs and tangents, and every texture of the IR by index (the
+    // device builds the mip chains).
+    d.uvs = ir.vertices.empty() ? nullptr : &ir.vertices[0].uv.x;
+    d.uv_stride = sizeof(RenderVertex);
+    d.tangents = ir.vertices.empty() ? nullptr : &ir.vertices[0].tangent.x;
+    d.tangent_stride = sizeof(RenderVertex);
+    std::vector<yrc_texture> textures;
+    for (const RenderTexture& t : ir.textures) {
+        const std::vector<Color4f>& texels = t.sampling_cache ? t.sampling_cache->texels : t.texels;
+        textures.push_back(yrc_texture{t.width, t.height, texels.empty() ? nullptr : &texels[0].x,
+                                       static_cast<int32_t>(t.filter), static_cast<int32_t>(t.wrap_s),
+                                       static_cast<int32_t>(t.wrap_t), 0});
+    }
+    d.textures = textures.data();
+    d.texture_count = static_cast<int32_t>(textures.size());
     d.materials = materials.data();
     d.material_count = static_cast<int32_t>(materials.size());
     std::vector<yrc_emissive_primitive> emissive;

@@ -552,6 +552,8 @@ class RefJob:
         return RenderScene(geom, mats, camd, st.width, st.height, spp=st.spp, max_depth=st.max_depth, seed=st.seed,
                            sampler=st.sampler, radiance_clamp=st.radiance_clamp,
                            normals=verts[:, 3:6].copy() if (prims["flags"] & 1).any() else None, emissive=em,
+                           uvs=verts[:, 6:8].copy() if (prims["flags"] & 2).any() else None,
+                           tangents=verts[:, 8:12].copy() if (prims["flags"] & 4).any() else None,
                            alias=(prob, alias, pmf) if na else None,
                            adaptive={"enabled": bool(st.adaptive_enabled), "min_spp": st.adaptive_min_spp,
                                      "relative_error": st.adaptive_relative_error,

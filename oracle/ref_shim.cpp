@@ -590,6 +590,7 @@ void yrref_job_materials(void* handle, yrc_material* out) {
         o.alpha_texture = m.alpha.texture;
         o.normal_map = m.normal_map;
         o.measured_index = m.measured_index;
+        o.normal_scale = m.normal_scale;
     }
 }
 
@@ -625,8 +626,8 @@ void yrref_job_lights(void* handle, yrc_emissive_primitive* emissive, float* ali
     settings->adaptive_confidence = s.adaptive_sampling.confidence;
 }
 
-// Builds a job from the C-ABI scene description (textures, BSSRDF tables and
-// analytic lights are not carried). The environment texture becomes a
+// Builds a job from the C-ABI scene description (analytic lights are not
+// carried). The environment texture becomes a
 // bilinear, repeat-wrapped RGBA texture with its distribution rebuilt by
 // BuildEnvironmentDistribution.
 void* yrref_job_from_desc(const yrc_scene_desc* d) {
@@ -640,6 +641,16 @@ void* yrref_job_from_desc(const yrc_scene_desc* d) {
         if (d->normals) {
             const float* n = reinterpret_cast<const float*>(reinterpret_cast<const char*>(d->normals) + v * d->normal_stride);
             ir.vertices[v].normal = yr::Vec3f{n[0], n[1], n[2]};
+        }
+        if (d->uvs) {
+            const float* t = reinterpret_cast<const float*>(reinterpret_cast<const char*>(d->uvs) + v * d->uv_stride);
+            ir.vertices[v].uv = yr::Vec2f{t[0], t[1]};
+        }
+        if (d->tangents) {
+            const float* t =
+                reinterpret_cast<const float*>(reinterpret_cast<const char*>(d->tangents) + v * d->tangent_stride);
+            ir.vertices[v].tangent = yr::Vec3f{t[0], t[1], t[2]};
+            ir.vertices[v].tangent_handedness = t[3];
         }
     }
     ir.indices.assign(g.indices, g.indices + g.index_count);
@@ -684,7 +695,17 @@ void* yrref_job_from_desc(const yrc_scene_desc* d) {
         r.alpha.value = m.alpha;
         r.absorption_color = Rgb(m.absorption_color);
         r.absorption_distance = m.absorption_distance;
+        r.reflectance.texture = m.reflectance_texture;
+        r.alpha.texture = m.alpha_texture;
+        r.normal_map = m.normal_map;
+        r.normal_scale = m.normal_scale;
         ir.materials.push_back(r);
+    }
+    // Scene textures keep their indices; the environment texture follows them.
+    for (int32_t i = 0; d->textures && i < d->texture_count; ++i) {
+        const yrc_texture& t = d->textures[i];
+        yr::RenderTexture tex = MakeTexture(t.width, t.height, t.texels, t.filter, t.wrap_s, t.wrap_t);
+        ir.textures.push_back(std::move(tex));
     }
     for (int32_t i = 0; i < d->emissive_count; ++i) {
         const yrc_emissive_primitive& e = d->emissive[i];

@@ -165,3 +165,92 @@ def subsurface_scene(width: int = 256, height: int = 256, spp: int = 64, max_dep
     s.geometry.primitives[tall_box]["material_index"] = len(s.materials) - 1
     s.bssrdf_tables = [build_bssrdf_table(eta)]
     return s
+
+
+def _checker(n: int, tiles: int, a, b) -> np.ndarray:
+    y, x = np.mgrid[0:n, 0:n]
+    on = ((x * tiles // n) + (y * tiles // n)) % 2 == 0
+    tex = np.where(on[..., None], np.array([*a, 1.0], np.float32), np.array([*b, 1.0], np.float32))
+    return tex.astype(np.float32)
+
+
+def _bump_normal_map(n: int, waves: int = 4, slope: float = 0.35) -> np.ndarray:
+    """A tangent-space normal map of sine bumps, encoded n * 0.5 + 0.5."""
+    v, u = (np.mgrid[0:n, 0:n] + 0.5) / n
+    nx = slope * np.sin(2.0 * np.pi * waves * u)
+    ny = slope * np.cos(2.0 * np.pi * waves * v)
+    nz = np.ones_like(nx)
+    ln = np.sqrt(nx * nx + ny * ny + nz * nz)
+    enc = np.stack([nx / ln, ny / ln, nz / ln], -1) * 0.5 + 0.5
+    return np.concatenate([enc, np.ones((n, n, 1))], -1).astype(np.float32)
+
+
+def textured_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8,
+                   filters=(3, 2, 1, 0), seed: int = 7) -> RenderScene:
+    """The Cornell box with textured surfaces: the floor carries a checker
+    reflectance texture (filters[0], repeat), the back wall a noise texture
+    (filters[1], mirrored repeat), the red wall a coarse texture
+    (filters[2], clamp to edge), the short box a checker (filters[3],
+    repeat), and the tall box a tangent-space normal map (bilinear) with
+    per-vertex tangents. Every wall and box has planar uvs spanning several
+    texture repeats."""
+    from .texture import Texture
+
+    s = scene(width, height, spp, max_depth)
+    g = s.geometry
+    rng = np.random.default_rng(seed)
+    nv = g.positions.shape[0]
+    uvs = np.zeros((nv, 2), np.float32)
+    tangents = np.zeros((nv, 4), np.float32)
+    tangents[:, 3] = 1.0
+    prims = g.primitives
+    idx = g.indices
+    # Planar uvs per shape: walls and boxes are parameterised by the two
+    # axes of largest extent, in units of 1.39 (a quarter of the box).
+    for k in range(7):
+        first, count = int(prims[k]["first_index"]), int(prims[k]["index_count"])
+        verts = np.unique(idx[first:first + count])
+        p = g.positions[verts]
+        ext = p.max(0) - p.min(0)
+        if k >= 5:  # boxes: (x + z, y)
+            uvs[verts, 0] = (p[:, 0] + p[:, 2]) / 1.39
+            uvs[verts, 1] = p[:, 1] / 1.39
+        else:
+            a, b = np.argsort(-ext)[:2]
+            uvs[verts, 0] = p[:, a] / 1.39
+            uvs[verts, 1] = p[:, b] / 1.39
+        prims[k]["flags"] = prims[k]["flags"] | 2
+    # Tall box: tangents along its rotated x axis (17 degrees about y).
+    a = math.radians(17.0)
+    first, count = int(prims[6]["first_index"]), int(prims[6]["index_count"])
+    verts = np.unique(idx[first:first + count])
+    tangents[verts, 0:3] = (math.cos(a), 0.0, -math.sin(a))
+    tangents[verts, 3] = np.where(np.arange(verts.size) % 2 == 0, 1.0, -1.0)
+    prims[6]["flags"] = prims[6]["flags"] | 4
+    noise = (0.35 + 0.6 * rng.random((23, 37, 4))).astype(np.float32)
+    noise[..., 3] = 1.0
+    coarse = (0.3 + 0.7 * rng.random((5, 3, 4))).astype(np.float32)
+    s.textures = [
+        Texture(_checker(64, 8, (0.9, 0.9, 0.85), (0.15, 0.2, 0.3)), filters[0], 0, 0),
+        Texture(noise, filters[1], 2, 2),
+        Texture(coarse, filters[2], 1, 1),
+        Texture(_checker(16, 4, (0.95, 0.6, 0.3), (0.3, 0.5, 0.9)), filters[3], 0, 0),
+        Texture(_bump_normal_map(32), 1, 0, 0),
+    ]
+    white, red = s.materials[2].copy(), s.materials[1].copy()
+    new = []
+    for base, key, t in ((white, "reflectance_texture", 0), (white, "reflectance_texture", 1),
+                         (red, "reflectance_texture", 2), (white, "reflectance_texture", 3),
+                         (white, "normal_map", 4)):
+        m = base.copy()
+        m[key] = t
+        if key == "normal_map":
+            m["normal_scale"] = 0.8
+        new.append(m)
+    base_index = len(s.materials)
+    s.materials = np.concatenate([s.materials, np.stack(new)])
+    for shape, k in ((0, 0), (2, 1), (3, 2), (5, 3), (6, 4)):  # floor, back, red wall, short box, tall box
+        prims[shape]["material_index"] = base_index + k
+    s.uvs = uvs
+    s.tangents = tangents
+    return s

@@ -24,6 +24,7 @@
 #include "nrc.hpp"
 #include "render_kernels.hpp"
 #include "render_types.hpp"
+#include "texture.hpp"
 #include "trace_kernels.hpp"
 #include "yrc_internal.hpp"
 
@@ -115,6 +116,7 @@ struct yrc_render_scene {
     yrc_cache_settings cache_settings{};
     yrc::DeviceArena cache_work;
     int64_t cache_capacity = 0;
+    yrc::TextureSet textures;  // scene textures and their mip chains
     yrc::CacheArgs cargs{};
     std::mutex mutex;
 };
@@ -141,6 +143,7 @@ void yrc_render_scene_destroy(yrc_render_scene* scene) {
     scene->cache_work.Release();
     scene->work.Release();
     scene->arena.Release();
+    scene->textures.Release();
     yrc_accel_destroy(scene->accel);
     delete scene;
 }
@@ -167,7 +170,8 @@ yrc_status yrc_render_scene_set_cache(yrc_render_scene* scene, yrc_nrc* cache, c
 }
 
 int64_t yrc_render_scene_device_bytes(const yrc_render_scene* scene) {
-    return scene ? scene->arena.bytes + scene->work.bytes + yrc_accel_device_bytes(scene->accel) : 0;
+    return scene ? scene->arena.bytes + scene->work.bytes + scene->textures.bytes + yrc_accel_device_bytes(scene->accel)
+                 : 0;
 }
 
 yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene** out) {
@@ -187,10 +191,13 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
     if (desc->analytic_count > 0) {
         return Fail(YRC_ERR_UNSUPPORTED, "analytic (point/spot/distant) lights are not rendered on the device");
     }
+    if (desc->texture_count < 0 || (desc->texture_count > 0 && !desc->textures)) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "invalid texture array");
+    }
     for (int32_t i = 0; i < desc->material_count; ++i) {
         const yrc_material& m = desc->materials[i];
-        if (m.reflectance_texture >= 0 || m.alpha_texture >= 0 || m.normal_map >= 0) {
-            return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": textured materials are not shaded on the device");
+        if (m.alpha_texture >= 0 && m.alpha_texture < desc->texture_count) {
+            return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": alpha-textured surfaces are not traced on the device");
         }
         if (m.kind == YRC_MAT_MEASURED && m.measured_index >= 0) {
             return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": measured BRDFs are not shaded on the device");
@@ -306,6 +313,24 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
     d.sphere_material = A.Upload(sphere_material);
     d.sphere_flip = A.Upload(sphere_flip);
     d.instance_o2w = A.Upload(o2w);
+    // RenderVertex uv and tangent (+ handedness), when given.
+    if (desc->uvs) {
+        std::vector<float2> uv(static_cast<size_t>(g.vertex_count));
+        for (int64_t v = 0; v < g.vertex_count; ++v) {
+            const float* q = reinterpret_cast<const float*>(reinterpret_cast<const char*>(desc->uvs) + v * desc->uv_stride);
+            uv[static_cast<size_t>(v)] = make_float2(q[0], q[1]);
+        }
+        d.uvs = A.Upload(uv);
+    }
+    if (desc->tangents) {
+        std::vector<float4> tg(static_cast<size_t>(g.vertex_count));
+        for (int64_t v = 0; v < g.vertex_count; ++v) {
+            const float* q =
+                reinterpret_cast<const float*>(reinterpret_cast<const char*>(desc->tangents) + v * desc->tangent_stride);
+            tg[static_cast<size_t>(v)] = make_float4(q[0], q[1], q[2], q[3]);
+        }
+        d.tangents = A.Upload(tg);
+    }
     d.primitive_count = g.primitive_count;
     d.sphere_count = g.sphere_count;
     d.instance_count = desc->two_level ? desc->two_level->instance_count : 0;
@@ -334,6 +359,11 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
         std::memcpy(dm.sigma_s, m.sigma_s, sizeof(dm.sigma_s));
         dm.bssrdf_eta = m.bssrdf_eta;
         dm.bssrdf_index = m.bssrdf_index;
+        dm.reflectance_texture = m.reflectance_texture;
+        dm.alpha_texture = m.alpha_texture;
+        dm.normal_map = m.normal_map;
+        dm.alpha = m.alpha;
+        dm.normal_scale = m.normal_scale;
         if (m.kind == YRC_MAT_DIELECTRIC || m.kind == YRC_MAT_THIN_DIELECTRIC) transparent = true;
     }
     d.materials = A.Upload(mats);
@@ -473,6 +503,18 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
         yrc_render_scene_destroy(s);
         return CudaError(err, "render scene upload");
     }
+    // Textures: BuildTextureSamplingCaches on the device.
+    if (desc->texture_count > 0) {
+        const yrc_status ts = UploadTextures(desc->textures, desc->texture_count, nullptr, s->textures);
+        if (ts != YRC_OK) {
+            const std::string msg = yrc_last_error();
+            yrc_render_scene_destroy(s);
+            return Fail(ts, msg);
+        }
+        d.textures = s->textures.textures;
+        d.texture_count = s->textures.count;
+        d.ewa_weights = s->textures.ewa_weights;
+    }
     *out = s;
     return Ok();
 }
@@ -529,6 +571,8 @@ yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     q.nee_paths = W.Alloc<int32_t>(capacity);
     q.order = W.Alloc<int32_t>(capacity);
     q.shade_class = W.Alloc<uint8_t>(capacity);
+    q.tex_normal = s->dev.texture_count > 0 ? W.Alloc<float4>(capacity) : nullptr;
+    q.tex_scale = s->dev.texture_count > 0 ? W.Alloc<float4>(capacity) : nullptr;
     q.counters = W.Alloc<unsigned long long>(kCtrCount);
     s->transmittance = s->dev.any_transparent ? W.Alloc<float4>(3 * capacity) : nullptr;
     if (s->dev.any_subsurface) {

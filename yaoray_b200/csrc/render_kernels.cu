@@ -240,6 +240,7 @@ struct Surface {
     V3 p;        // hit point
     V3 n;        // shading normal (face-forwarded as the reference does)
     V3 ng_obj;   // object-space geometric normal of a triangle (emission MIS)
+    V3 reflectance_scale;  // reflectance texture lookup (1, 1, 1 when untextured)
     int32_t material;
     int32_t prim;  // mesh primitive, -1 for spheres
     bool triangle;
@@ -278,10 +279,154 @@ __device__ inline V3 ResolveShadingNormal(const DevScene& sc, int32_t prim, int4
     return n;
 }
 
+// ------------------------------------------------------ textured shading
+
+__device__ __forceinline__ bool TextureValid(const DevScene& sc, int32_t t) { return t >= 0 && t < sc.texture_count; }
+
+__device__ __forceinline__ V3 TransformPointV(const float* m, V3 p) {
+    const float in[3] = {p.x, p.y, p.z};
+    float out[3];
+    TransformPointRef(m, in, out);
+    return V3{out[0], out[1], out[2]};
+}
+
+__device__ __forceinline__ V3 TransformVectorV(const float* m, V3 v) {
+    const float in[3] = {v.x, v.y, v.z};
+    float out[3];
+    TransformVectorRef(m, in, out);
+    return V3{out[0], out[1], out[2]};
+}
+
+// The pixel-step differentials of a camera ray (GeneratePerspectiveCameraRay,
+// src/scene/camera.cpp:33-37): both start at the camera origin and pass
+// through (film_x + 1, film_y) and (film_x, film_y + 1).
+__device__ inline void CameraDifferentials(const DevScene& sc, int32_t pixel, int32_t sample, V3& dx, V3& dy) {
+    const int x = pixel % sc.width, y = pixel / sc.width;
+    PixelSampler smp;
+    smp.Init(sc.sampler, sc.seed, x, y, sample, sc.spp);
+    float sx, sy;
+    smp.Sample2D(kDimPixel, 0, sx, sy);
+    const float fx = static_cast<float>(x) + sx;
+    const float fy = static_cast<float>(y) + sy;
+    dx = CameraDirection(sc, fx + 1.0f, fy);
+    dy = CameraDirection(sc, fx, fy + 1.0f);
+}
+
+// ComputeTextureFootprint (src/integrators/surface_query.cpp:35-97) for a
+// camera ray from `origin` with pixel differentials dx, dy; o2w is the
+// instance transform (null for world-space geometry).
+__device__ inline TexFootprint ComputeFootprint(const DevScene& sc, int4 tv, const float* o2w, V3 hit_point, V3 gn,
+                                                V3 origin, V3 dx, V3 dy) {
+    const TexFootprint zero{0.0f, 0.0f, 0.0f, 0.0f};
+    V3 p0 = VertexPos(sc, tv.x), p1 = VertexPos(sc, tv.y), p2 = VertexPos(sc, tv.z);
+    if (o2w) {
+        p0 = TransformPointV(o2w, p0);
+        p1 = TransformPointV(o2w, p1);
+        p2 = TransformPointV(o2w, p2);
+    }
+    const float2 uv0 = sc.uvs[tv.x], uv1 = sc.uvs[tv.y], uv2 = sc.uvs[tv.z];
+    const float du1 = uv1.x - uv0.x;
+    const float dv1 = uv1.y - uv0.y;
+    const float du2 = uv2.x - uv0.x;
+    const float dv2 = uv2.y - uv0.y;
+    const float uv_det = du1 * dv2 - dv1 * du2;
+    if (fabsf(uv_det) < 1.0e-12f) return zero;
+    const float inverse_uv_det = 1.0f / uv_det;
+    const V3 dp1 = p1 - p0;
+    const V3 dp2 = p2 - p0;
+    const V3 dpdu = (dp1 * dv2 - dp2 * dv1) * inverse_uv_det;
+    const V3 dpdv = (dp2 * du1 - dp1 * du2) * inverse_uv_det;
+    auto differential_point = [&](V3 direction) {
+        const float denominator = Dot(gn, direction);
+        if (fabsf(denominator) < 1.0e-12f) return hit_point;
+        const float t = Dot(gn, hit_point - origin) / denominator;
+        return origin + direction * t;
+    };
+    const V3 dpdx = differential_point(dx) - hit_point;
+    const V3 dpdy = differential_point(dy) - hit_point;
+    const float a = Dot(dpdu, dpdu);
+    const float b = Dot(dpdu, dpdv);
+    const float c = Dot(dpdv, dpdv);
+    const float gram_det = a * c - b * b;
+    if (fabsf(gram_det) < 1.0e-20f) return zero;
+    const float inverse_gram_det = 1.0f / gram_det;
+    auto solve = [&](V3 dp) {
+        const float u_rhs = Dot(dp, dpdu);
+        const float v_rhs = Dot(dp, dpdv);
+        return make_float2((u_rhs * c - v_rhs * b) * inverse_gram_det, (v_rhs * a - u_rhs * b) * inverse_gram_det);
+    };
+    const float2 fdx = solve(dpdx);
+    const float2 fdy = solve(dpdy);
+    if (!isfinite(fdx.x) || !isfinite(fdx.y) || !isfinite(fdy.x) || !isfinite(fdy.y)) return zero;
+    return TexFootprint{fdx.x, fdx.y, fdy.x, fdy.y};
+}
+
+// The textured part of EvaluateMaterialAtSurface
+// (src/shading/material_evaluator.cpp:131-176) for a triangle with uvs:
+// the reflectance texture (multiplied into the reflectance) and the normal
+// map (ResolveNormalMap, :35-96) applied to the shading normal `n`, before
+// the final face-forward. At a camera-ray hit (depth 0) the lookups use the
+// ray-differential footprint; other rays have none.
+__device__ __forceinline__ void ApplySurfaceTextures(const DevScene& sc, const DevMaterial& dm, int32_t prim, int4 tv,
+                                                  float u, float v, const float* o2w, V3 o, V3 hit_point, V3 gn,
+                                                  int depth, int32_t pixel, int32_t sample, V3& n, V3& refl_scale) {
+    const bool refl = TextureValid(sc, dm.reflectance_texture);
+    const bool nmap = TextureValid(sc, dm.normal_map) && (sc.prim_flags[prim] & 4u) && sc.tangents;
+    if (!refl && !nmap) return;
+    // InterpolateUv (src/geometry/intersection.cpp:20-32).
+    const float w = 1.0f - u - v;
+    const float2 a = sc.uvs[tv.x], b = sc.uvs[tv.y], c = sc.uvs[tv.z];
+    const float tu = a.x * w + b.x * u + c.x * v;
+    const float tv2 = a.y * w + b.y * u + c.y * v;
+    TexFootprint fp{0.0f, 0.0f, 0.0f, 0.0f};
+    if (depth == 0) {
+        V3 dx, dy;
+        CameraDifferentials(sc, pixel, sample, dx, dy);
+        fp = ComputeFootprint(sc, tv, o2w, hit_point, gn, o, dx, dy);
+    }
+    if (refl) {
+        const float4 t = SampleTexture4(sc.textures[dm.reflectance_texture], tu, tv2, fp, sc.ewa_weights);
+        refl_scale = V3{t.x, t.y, t.z};
+    }
+    if (!nmap) return;
+    const float4 enc = SampleTexture4(sc.textures[dm.normal_map], tu, tv2, fp, sc.ewa_weights);
+    V3 ts{enc.x * 2.0f - 1.0f, enc.y * 2.0f - 1.0f, enc.z * 2.0f - 1.0f};
+    ts.x = ts.x * dm.normal_scale;
+    ts.y = ts.y * dm.normal_scale;
+    ts = Normalize(ts);
+    if (LengthSq(ts) == 0.0f) return;
+    // InterpolateTangent / InterpolateHandedness (intersection.cpp:49-73).
+    const float4 t0 = sc.tangents[tv.x], t1 = sc.tangents[tv.y], t2 = sc.tangents[tv.z];
+    V3 tangent = Normalize(V3{t0.x * w + t1.x * u + t2.x * v, t0.y * w + t1.y * u + t2.y * v,
+                              t0.z * w + t1.z * u + t2.z * v});
+    if (o2w) tangent = TransformVectorV(o2w, tangent);
+    // OrthogonalizeTangent (material_evaluator.cpp:27-33).
+    const V3 projected = tangent - n * Dot(tangent, n);
+    if (LengthSq(projected) <= 1.0e-12f) return;
+    tangent = Normalize(projected);
+    if (LengthSq(tangent) == 0.0f) return;
+    float orientation = 1.0f;
+    if (o2w) {
+        const float* m = o2w;
+        const float det = m[0] * (m[5] * m[10] - m[9] * m[6]) - m[4] * (m[1] * m[10] - m[9] * m[2]) +
+                          m[8] * (m[1] * m[6] - m[5] * m[2]);
+        orientation = det < 0.0f ? -1.0f : 1.0f;
+    }
+    const float handedness = (t0.w * w + t1.w * u + t2.w * v) * orientation;
+    const V3 bitangent = Cross(n, tangent) * handedness;
+    const V3 mapped = Normalize(tangent * ts.x + bitangent * ts.y + n * ts.z);
+    if (LengthSq(mapped) > 0.0f) n = mapped;
+}
+
 // TraceVisibleSurface's surface resolve (src/integrators/surface_query.cpp:129-187)
-// and EvaluateMaterialAtSurface (src/shading/material_evaluator.cpp:112-180),
-// untextured. Returns false for a hit on an invalid triangle material.
-__device__ inline bool ResolveSurface(const DevScene& sc, V3 o, V3 d, float4 hit, int32_t inst, Surface& s) {
+// and EvaluateMaterialAtSurface (src/shading/material_evaluator.cpp:112-180).
+// Returns false for a hit on an invalid triangle material. kTextured adds
+// the texture lookups (the texture stage); depth, pixel and sample locate
+// the camera ray of a depth-0 hit (texture footprints).
+template <bool kTextured>
+__device__ inline bool ResolveSurface(const DevScene& sc, V3 o, V3 d, float4 hit, int32_t inst, Surface& s,
+                                      int depth, int32_t pixel, int32_t sample) {
+    s.reflectance_scale = V3{1.0f, 1.0f, 1.0f};
     const int32_t id = __float_as_int(hit.y);
     s.p = o + d * hit.x;
     if (id <= -2) {
@@ -308,16 +453,25 @@ __device__ inline bool ResolveSurface(const DevScene& sc, V3 o, V3 d, float4 hit
     s.ng_obj = raw;
     const float u = hit.z, v = hit.w;
     const V3 wo = -d;
+    const bool textured = kTextured && sc.texture_count > 0 && sc.uvs && (sc.prim_flags[prim] & 2u);
     if (inst >= 0) {
         const float* m = sc.instance_o2w + 16 * inst;
         const V3 wraw = TransformNormal(m, raw);
         const V3 gn = Dot(wraw, wo) < 0.0f ? -wraw : wraw;
         V3 n = TransformNormal(m, ResolveShadingNormal(sc, prim, tv, u, v, raw));
         if (Dot(n, gn) < 0.0f) n = -n;
+        if (textured) {
+            ApplySurfaceTextures(sc, sc.materials[s.material], prim, tv, u, v, m, o, s.p, gn, depth, pixel, sample,
+                                 n, s.reflectance_scale);
+        }
         s.n = Dot(n, wo) < 0.0f ? -n : n;
     } else {
         const V3 gn = Dot(raw, wo) < 0.0f ? -raw : raw;
-        const V3 n = ResolveShadingNormal(sc, prim, tv, u, v, gn);
+        V3 n = ResolveShadingNormal(sc, prim, tv, u, v, gn);
+        if (textured) {
+            ApplySurfaceTextures(sc, sc.materials[s.material], prim, tv, u, v, nullptr, o, s.p, gn, depth, pixel,
+                                 sample, n, s.reflectance_scale);
+        }
         s.n = Dot(n, wo) < 0.0f ? -n : n;
     }
     return true;
@@ -565,6 +719,42 @@ __device__ constexpr int32_t ClassKind() {
          : kClass == kClassCoatedDiffuse ? kCoatedDiffuse : -1;
 }
 
+// Texture stage of a bounce: for every extend-queue entry that hit a
+// triangle with uvs whose material has a reflectance texture or a normal
+// map, the textured surface resolve (EvaluateMaterialAtSurface,
+// src/shading/material_evaluator.cpp:112-180): the reflectance scale and
+// the final shading normal, w = 1; other entries get w = 0. Kept apart from
+// the shade kernels so that their register budget does not carry the
+// texture filters.
+__global__ void __launch_bounds__(256) SurfaceTextureKernel(DevScene sc, PathState ps, Queues q, int depth) {
+    const int64_t n = static_cast<int64_t>(q.counters[kCtrIn]);
+    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const float4 hit = q.hits[e];
+        const int32_t id = __float_as_int(hit.y);
+        bool textured = false;
+        if (id >= 0) {
+            const int32_t prim = sc.tri_prim[id];
+            const int32_t mi = sc.prim_material[prim];
+            if (mi >= 0 && (sc.prim_flags[prim] & 2u)) {
+                const DevMaterial& dm = sc.materials[mi];
+                textured = TextureValid(sc, dm.reflectance_texture) ||
+                           (TextureValid(sc, dm.normal_map) && (sc.prim_flags[prim] & 4u) && sc.tangents);
+            }
+        }
+        if (!textured) {
+            q.tex_normal[e] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            continue;
+        }
+        const int32_t path = q.path_in[e];
+        const V3 o = F4(q.ray_in[2 * e]), d = F4(q.ray_in[2 * e + 1]);
+        Surface s;
+        ResolveSurface<true>(sc, o, d, hit, q.inst[e], s, depth, ps.pixel[path], ps.sample[path]);
+        q.tex_normal[e] = make_float4(s.n.x, s.n.y, s.n.z, 1.0f);
+        q.tex_scale[e] = make_float4(s.reflectance_scale.x, s.reflectance_scale.y, s.reflectance_scale.z, 0.0f);
+    }
+}
+
 // IntegratePathSample's per-bounce body (src/integrators/path_integrator.cpp:23-197)
 // for the entries of one shading class.
 template <int kClass>
@@ -618,16 +808,24 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
         }
 
         Surface s;
-        if (!ResolveSurface(sc, o, d, hit, inst, s)) {
+        if (!ResolveSurface<false>(sc, o, d, hit, inst, s, depth, 0, 0)) {
             rad = rad + Mul(tp, V3{1.0f, 0.0f, 1.0f});  // invalid material marker
             ps.radiance[path] = ToF4(rad);
             continue;
+        }
+        if (sc.texture_count > 0 && s.triangle) {  // the texture stage's result for this entry
+            const float4 tn = q.tex_normal[e];
+            if (tn.w != 0.0f) {
+                s.n = F4(tn);
+                s.reflectance_scale = F4(q.tex_scale[e]);
+            }
         }
         Mat m;
         V3 emission{0.0f, 0.0f, 0.0f};
         if (s.material >= 0) {
             const DevMaterial& dm = sc.materials[s.material];
             m = LoadMat(dm);
+            m.reflectance = Mul(m.reflectance, s.reflectance_scale);
             emission = Ld3(dm.emission);
         } else {  // default RenderMaterial: diffuse 0.5
             m = Mat{kDiffuse, {0.5f, 0.5f, 0.5f}, 1.5f, 0.0f, 0.0f, 1.5f, 0.01f, {0, 0, 0}, 10, 1};
@@ -1115,6 +1313,7 @@ void LaunchResetCounters(const Queues& q, cudaStream_t st) { ResetCountersKernel
 void LaunchAdvanceQueue(const Queues& q, cudaStream_t st) { AdvanceQueueKernel<<<1, 32, 0, st>>>(q); }
 void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, const CacheArgs& cache, int depth,
                  int64_t capacity, int sm_count, cudaStream_t st) {
+    if (sc.texture_count > 0) SurfaceTextureKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
     ClassifyKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, q);
     ScatterByClassKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(q);
     ShadeKernel<kClassMiss><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);

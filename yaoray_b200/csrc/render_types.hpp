@@ -16,6 +16,7 @@
 #include <cstdint>
 
 #include "device_layout.cuh"
+#include "texture.cuh"
 
 namespace yrc {
 
@@ -51,7 +52,12 @@ struct alignas(16) DevMaterial {
     float sigma_s[3];
     float bssrdf_eta;
     int32_t bssrdf_index;
-    int32_t pad[3];
+    int32_t reflectance_texture;  // scene texture indices, -1 = none
+    int32_t alpha_texture;
+    int32_t normal_map;
+    float alpha;
+    float normal_scale;
+    int32_t pad[2];
 };
 
 struct DevBssrdf {
@@ -129,6 +135,12 @@ struct DevScene {
     float radiance_clamp;
     int32_t any_transparent;  // scene has Dielectric / ThinDielectric materials
     int32_t any_subsurface;   // scene has Subsurface materials (probe stage needed)
+    // textured shading
+    const float2* uvs;           // per vertex, may be null
+    const float4* tangents;      // per vertex: tangent xyz, handedness in w; may be null
+    const DevTexture* textures;  // texture_count entries
+    int32_t texture_count;
+    const float* ewa_weights;
 };
 
 // Path state, structure of arrays over `capacity` slots.
@@ -206,6 +218,8 @@ struct Queues {
     float4* probe_entry;
     float4* probe_hit;
     int32_t* probe_count;
+    float4* tex_normal;   // texture stage: final shading normal per entry, w = 1 when textured
+    float4* tex_scale;    // texture stage: reflectance scale per entry
     int32_t* order;       // extend-queue entries sorted by shading class
     uint8_t* shade_class; // shading class per extend-queue entry
     unsigned long long* counters;  // see kCounter*

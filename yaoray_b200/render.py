@@ -20,6 +20,7 @@ import numpy as np
 from . import _lib
 from ._lib import YrcError, check, lib, ptr
 from .accel import SceneGeometry, build_bvh, build_bvh_device, build_two_level_bvh
+from .texture import textures_array
 
 # --------------------------------------------------------------- C mirrors
 
@@ -34,7 +35,7 @@ class Material(C.Structure):
                 ("bssrdf_eta", C.c_float), ("bssrdf_index", C.c_int32), ("emission", C.c_float * 3),
                 ("alpha", C.c_float), ("absorption_color", C.c_float * 3), ("absorption_distance", C.c_float),
                 ("reflectance_texture", C.c_int32), ("alpha_texture", C.c_int32), ("normal_map", C.c_int32),
-                ("measured_index", C.c_int32)]
+                ("measured_index", C.c_int32), ("normal_scale", C.c_float)]
 
 
 MATERIAL_DTYPE = np.dtype([("kind", "<i4"), ("reflectance", "<f4", 3), ("eta", "<f4", 3), ("k", "<f4", 3),
@@ -46,7 +47,7 @@ MATERIAL_DTYPE = np.dtype([("kind", "<i4"), ("reflectance", "<f4", 3), ("eta", "
                            ("bssrdf_index", "<i4"), ("emission", "<f4", 3), ("alpha", "<f4"),
                            ("absorption_color", "<f4", 3), ("absorption_distance", "<f4"),
                            ("reflectance_texture", "<i4"), ("alpha_texture", "<i4"), ("normal_map", "<i4"),
-                           ("measured_index", "<i4")])
+                           ("measured_index", "<i4"), ("normal_scale", "<f4")])
 assert MATERIAL_DTYPE.itemsize == C.sizeof(Material)
 
 EMISSIVE_DTYPE = np.dtype([("primitive_index", "<i4"), ("radiance", "<f4", 3), ("area", "<f4")])
@@ -81,6 +82,7 @@ def default_material(**kw) -> np.void:
     m["absorption_color"] = (1.0, 1.0, 1.0)
     m["absorption_distance"] = 1.0
     m["reflectance_texture"] = m["alpha_texture"] = m["normal_map"] = m["measured_index"] = -1
+    m["normal_scale"] = 1.0
     for k, v in kw.items():
         m[k] = v
     return m
@@ -127,7 +129,9 @@ class SceneDesc(C.Structure):
                 ("emissive_count", C.c_int32), ("emissive_power", AliasTable), ("analytic", C.c_void_p),
                 ("analytic_count", C.c_int32), ("analytic_power", AliasTable), ("environment", Environment),
                 ("bssrdf_tables", C.c_void_p), ("bssrdf_count", C.c_int32), ("camera", Camera),
-                ("settings", Settings), ("flat", C.c_void_p), ("two_level", C.c_void_p)]
+                ("settings", Settings), ("flat", C.c_void_p), ("two_level", C.c_void_p),
+                ("uvs", C.c_void_p), ("uv_stride", C.c_int64), ("tangents", C.c_void_p),
+                ("tangent_stride", C.c_int64), ("textures", C.c_void_p), ("texture_count", C.c_int32)]
 
 
 class Progress(C.Structure):
@@ -259,7 +263,7 @@ def build_alias_table(weights: np.ndarray):
 
 @dataclass
 class RenderScene:
-    """RenderSceneIR + RenderSettings (untextured subset) as numpy arrays."""
+    """RenderSceneIR + RenderSettings as numpy arrays."""
 
     geometry: SceneGeometry
     materials: np.ndarray                      # MATERIAL_DTYPE
@@ -277,6 +281,9 @@ class RenderScene:
     environment: EnvironmentMap = field(default_factory=EnvironmentMap)
     bssrdf_tables: list = field(default_factory=list)  # build_bssrdf_table() dicts, by bssrdf_index
     adaptive: dict | None = None               # enabled/min_spp/relative_error/absolute_error/confidence
+    uvs: np.ndarray | None = None              # (V, 2) RenderVertex::uv
+    tangents: np.ndarray | None = None         # (V, 4) RenderVertex::tangent xyz + tangent_handedness
+    textures: list = field(default_factory=list)  # texture.Texture, by material texture index
 
     def emissive_power_alias(self):
         """The alias table PrepareLightSampling builds (emissive power = area * luminance)."""
@@ -337,6 +344,21 @@ class PreparedScene:
             self._keep.append(nrm)
             d.normals = ptr(nrm)
             d.normal_stride = 12
+        if scene.uvs is not None:
+            uv = np.ascontiguousarray(scene.uvs, np.float32).reshape(-1, 2)
+            self._keep.append(uv)
+            d.uvs = ptr(uv)
+            d.uv_stride = 8
+        if scene.tangents is not None:
+            tg = np.ascontiguousarray(scene.tangents, np.float32).reshape(-1, 4)
+            self._keep.append(tg)
+            d.tangents = ptr(tg)
+            d.tangent_stride = 16
+        if scene.textures:
+            tarr, tkeep = textures_array(scene.textures)
+            self._keep += [tarr, tkeep]
+            d.textures = C.addressof(tarr)
+            d.texture_count = len(scene.textures)
         mats = np.ascontiguousarray(scene.materials, MATERIAL_DTYPE)
         em = np.ascontiguousarray(scene.emissive, EMISSIVE_DTYPE)
         self._keep += [mats, em]
