@@ -84,3 +84,29 @@ def test_textures_change_the_render_and_share_pyramids(cuda):
     one = plain.prepare(s).device_bytes
     s.textures = s.textures + [s.textures[0], s.textures[0]]  # two more copies of the floor's image
     assert plain.prepare(s).device_bytes - one < 4096
+
+
+def test_cutout_scene_matches_reference_cpu(cuda, ref):
+    """Alpha: a screen with an alpha texture cutting round holes in front
+    of the boxes, a pane with constant alpha 0.2 under the light (every ray
+    skips it, shadow rays included), and thin glass with a textured
+    reflectance (shadow rays take its textured transmittance). The skip
+    loops re-trace from just past each cut-out hit as the reference does,
+    so first hits, and with them the depth and normal sums, stay
+    bit-identical."""
+    def make(seed):
+        s = cornell.cutout_scene(96, 96, 64, 8)
+        s.seed = seed
+        return s
+
+    res, cpu_film, cpu_stats, cpu2 = render_pair(ref, make)
+    check_aovs(res, cpu_film)
+    g, c, c2 = linear(res.film), linear(cpu_film), linear(cpu2)
+    noise = relmse(c2, c)
+    err = relmse(g, c)
+    assert err < 0.25 * noise, (err, noise)
+    assert abs(g.mean() / c.mean() - 1.0) < 0.01
+    assert res.bad_samples == 0
+    assert abs(res.stats["rays_traced"] / cpu_stats["rays_traced"] - 1) < 0.02
+    assert abs(res.stats["shadow_rays"] / cpu_stats["shadow_rays"] - 1) < 0.02
+    assert abs(res.stats["occluded_shadow_rays"] / cpu_stats["occluded_shadow_rays"] - 1) < 0.03

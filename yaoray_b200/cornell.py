@@ -254,3 +254,59 @@ def textured_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth
     s.uvs = uvs
     s.tangents = tangents
     return s
+
+
+def _append_quad(s: RenderScene, corners, material: int, uv_scale: float = 3.0) -> None:
+    """Appends a two-triangle quad (corners in order) with uvs spanning
+    uv_scale repeats as a new mesh primitive of material `material`."""
+    from . import _lib
+
+    g = s.geometry
+    base = g.positions.shape[0]
+    g.positions = np.concatenate([g.positions, np.asarray(corners, np.float32)])
+    first = g.indices.size
+    g.indices = np.concatenate([g.indices, (np.array([0, 1, 2, 0, 2, 3], np.uint32) + base)])
+    prim = np.zeros(1, _lib.PRIM_DTYPE)
+    prim[0]["first_index"], prim[0]["index_count"] = first, 6
+    prim[0]["material_index"], prim[0]["flags"] = material, 2
+    g.primitives = np.concatenate([g.primitives, prim])
+    quad_uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32) * np.float32(uv_scale)
+    s.uvs = np.concatenate([s.uvs, quad_uv])
+    tg = np.zeros((4, 4), np.float32)
+    tg[:, 3] = 1.0
+    s.tangents = np.concatenate([s.tangents, tg])
+    if s.normals is not None:
+        s.normals = np.concatenate([s.normals, np.zeros((4, 3), np.float32)])
+
+
+def cutout_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8) -> RenderScene:
+    """textured_scene() plus three panes that exercise alpha and shadows: a
+    screen in front of the boxes whose alpha texture (red channel, bilinear)
+    cuts round holes, a pane under the light with constant alpha 0.2 (cut out
+    everywhere: camera and shadow rays skip it), and a thin-glass pane whose
+    reflectance is textured (shadow rays through it take the textured
+    transmittance)."""
+    from .render import THIN_DIELECTRIC
+    from .texture import Texture
+
+    s = textured_scene(width, height, spp, max_depth)
+    n = 32
+    v, u = (np.mgrid[0:n, 0:n] + 0.5) / n
+    holes = ((u - 0.5) ** 2 + (v - 0.5) ** 2) > 0.09
+    alpha_tex = np.stack([holes.astype(np.float32), 0.5 * np.ones((n, n)), u, np.ones((n, n))], -1).astype(np.float32)
+    s.textures = s.textures + [Texture(alpha_tex, 1, 0, 0),
+                               Texture(_checker(8, 2, (0.9, 0.7, 0.5), (0.4, 0.8, 0.95)), 0, 0, 0)]
+    t_alpha, t_glass = len(s.textures) - 2, len(s.textures) - 1
+    white = s.materials[2].copy()
+    screen = white.copy()
+    screen["alpha_texture"] = t_alpha
+    ghost = white.copy()
+    ghost["alpha"] = 0.2
+    glass = default_material(kind=THIN_DIELECTRIC, reflectance=(1.0, 1.0, 1.0), ior=1.5)
+    glass["reflectance_texture"] = t_glass
+    base = len(s.materials)
+    s.materials = np.concatenate([s.materials, np.stack([screen, ghost, glass])])
+    _append_quad(s, [(0.6, 0.4, 1.0), (4.9, 0.4, 1.0), (4.9, 3.9, 1.0), (0.6, 3.9, 1.0)], base, 2.0)
+    _append_quad(s, [(1.6, 5.2, 1.8), (3.9, 5.2, 1.8), (3.9, 5.2, 3.9), (1.6, 5.2, 3.9)], base + 1)
+    _append_quad(s, [(0.8, 2.2, 0.6), (2.0, 2.2, 0.6), (2.0, 2.2, 2.9), (0.8, 2.2, 2.9)], base + 2, 1.0)
+    return s

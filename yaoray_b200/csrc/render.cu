@@ -196,9 +196,6 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
     }
     for (int32_t i = 0; i < desc->material_count; ++i) {
         const yrc_material& m = desc->materials[i];
-        if (m.alpha_texture >= 0 && m.alpha_texture < desc->texture_count) {
-            return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": alpha-textured surfaces are not traced on the device");
-        }
         if (m.kind == YRC_MAT_MEASURED && m.measured_index >= 0) {
             return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": measured BRDFs are not shaded on the device");
         }
@@ -212,9 +209,6 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
                 !t.rho_eff || !t.profile_cdf) {
                 return Fail(YRC_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + ": malformed BSSRDF table");
             }
-        }
-        if (m.alpha < 0.5f) {
-            return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": alpha-cut-out surfaces are not traced on the device");
         }
     }
     auto* s = new (std::nothrow) yrc_render_scene();
@@ -365,6 +359,10 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
         dm.alpha = m.alpha;
         dm.normal_scale = m.normal_scale;
         if (m.kind == YRC_MAT_DIELECTRIC || m.kind == YRC_MAT_THIN_DIELECTRIC) transparent = true;
+        const bool tex_alpha = m.alpha_texture >= 0 && m.alpha_texture < desc->texture_count;
+        const bool tex_refl = m.reflectance_texture >= 0 && m.reflectance_texture < desc->texture_count;
+        if (m.alpha < 0.5f || tex_alpha) d.any_alpha = 1;
+        if (m.alpha < 0.5f || tex_alpha || (m.kind == YRC_MAT_THIN_DIELECTRIC && tex_refl)) d.exact_shadows = 1;
     }
     d.materials = A.Upload(mats);
     d.material_count = desc->material_count;
@@ -574,7 +572,7 @@ yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     q.tex_normal = s->dev.texture_count > 0 ? W.Alloc<float4>(capacity) : nullptr;
     q.tex_scale = s->dev.texture_count > 0 ? W.Alloc<float4>(capacity) : nullptr;
     q.counters = W.Alloc<unsigned long long>(kCtrCount);
-    s->transmittance = s->dev.any_transparent ? W.Alloc<float4>(3 * capacity) : nullptr;
+    s->transmittance = (s->dev.any_transparent || s->dev.exact_shadows) ? W.Alloc<float4>(3 * capacity) : nullptr;
     if (s->dev.any_subsurface) {
         q.probe_ray = W.Alloc<float4>(2 * capacity);
         q.probe_target = W.Alloc<int4>(capacity);
@@ -681,6 +679,7 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
         ta.error = AccelErrorWord(s->accel);
         cudaError_t err = LaunchTrace(ta, false, false, TraceShapeOf(s->accel, 0), st, s->sm_count);
         if (err != cudaSuccess) return CudaError(err, "extend trace");
+        if (sc.any_alpha) LaunchAlphaExtend(sc, s->ps, q, depth, C, s->sm_count, ta.error, st);
         LaunchShade(sc, s->ps, q, cache, depth, C, s->sm_count, st);
         if (sc.any_subsurface) {
             RenderProbeArgs pa{};
@@ -697,7 +696,11 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
             if (perr != cudaSuccess) return CudaError(perr, "subsurface probe");
             LaunchSubsurfaceExit(sc, s->ps, q, depth, C, s->sm_count, st);
         }
-        if (sc.any_transparent) {
+        if (sc.exact_shadows) {
+            LaunchShadowExact(sc, q, s->transmittance, q.counters + kCtrStatsBase + 2, 2 * C, s->sm_count, ta.error,
+                              st);
+            err = cudaGetLastError();
+        } else if (sc.any_transparent) {
             ShadowArgs sa{};
             sa.accel = sc.accel;
             sa.rays = q.shadow_ray;

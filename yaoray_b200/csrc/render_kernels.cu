@@ -12,12 +12,15 @@
 // one CUDA graph.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "bsdf.cuh"
 #include "bssrdf.cuh"
 #include "render_kernels.hpp"
 #include "render_types.hpp"
 #include "sampler.cuh"
 #include "shading.cuh"
+#include "traversal.cuh"
 
 namespace yrc {
 namespace {
@@ -755,6 +758,222 @@ __global__ void __launch_bounds__(256) SurfaceTextureKernel(DevScene sc, PathSta
     }
 }
 
+// ----------------------------------------------------------- alpha cut-outs
+
+constexpr int kMaxAlphaSkips = 64;          // MaxAlphaSkippedHits (surface_query.cpp:12)
+constexpr float kAlphaSkipOffset = 1.0e-4f;  // AlphaSkipTOffset (surface_query.cpp:13)
+
+struct TraceHit {
+    float4 h;      // t, id bits (-1 miss), u, v
+    int32_t inst;
+};
+
+// Closest hit of (o, d) over [tmin, tmax], one ray per thread (IntersectBvh /
+// IntersectTwoLevelBvh); col is the thread's shared-memory stack column.
+template <bool kTwo, int kTotal>
+__device__ inline TraceHit ClosestHit(const AccelParams& a, V3 o, V3 d, float tmin, float tmax,
+                                      StackStore<kTotal>& st, int2* col, int* error) {
+    Traversal t;
+    const float of[3] = {o.x, o.y, o.z};
+    const float df[3] = {d.x, d.y, d.z};
+    bool alive = BeginRay(a, of, df, tmin, tmax, t);
+    while (alive) alive = Step<false, false, kTwo>(a, nullptr, 0, t, st, col, error);
+    TraceHit r;
+    r.h = make_float4(t.best.t, __int_as_float(t.best.hit ? t.best.id : -1), t.best.u, t.best.v);
+    r.inst = t.best.hit ? t.best_inst : -1;
+    return r;
+}
+
+// The resolved alpha of a triangle hit (EvaluateMaterialAtSurface,
+// src/shading/material_evaluator.cpp:130-149) compared with IsAlphaVisible's
+// 0.5 (:182-184). Spheres and hits on invalid materials are visible. At a
+// camera-ray hit (depth 0) the alpha texture uses the ray-differential
+// footprint.
+__device__ inline bool AlphaVisible(const DevScene& sc, V3 o, V3 d, float4 hit, int32_t inst, int depth, int32_t pixel,
+                                    int32_t sample) {
+    const int32_t id = __float_as_int(hit.y);
+    if (id < 0) return true;
+    const int32_t prim = sc.tri_prim[id];
+    const int32_t mi = sc.prim_material[prim];
+    if (mi < 0) return true;
+    const DevMaterial& dm = sc.materials[mi];
+    float alpha = dm.alpha;
+    if (sc.uvs && (sc.prim_flags[prim] & 2u) && TextureValid(sc, dm.alpha_texture)) {
+        const int4 tv = sc.tri_vertices[id];
+        const float u = hit.z, v = hit.w;
+        const float w = 1.0f - u - v;
+        const float2 a = sc.uvs[tv.x], b = sc.uvs[tv.y], c = sc.uvs[tv.z];
+        const float tu = a.x * w + b.x * u + c.x * v;
+        const float tw = a.y * w + b.y * u + c.y * v;
+        TexFootprint fp{0.0f, 0.0f, 0.0f, 0.0f};
+        if (depth == 0) {
+            const float* m = inst >= 0 ? sc.instance_o2w + 16 * inst : nullptr;
+            const V3 p0 = VertexPos(sc, tv.x), p1 = VertexPos(sc, tv.y), p2 = VertexPos(sc, tv.z);
+            V3 raw = Normalize(Cross(p1 - p0, p2 - p0));
+            if (m) raw = TransformNormal(m, raw);
+            const V3 gn = Dot(raw, -d) < 0.0f ? -raw : raw;
+            V3 dx, dy;
+            CameraDifferentials(sc, pixel, sample, dx, dy);
+            fp = ComputeFootprint(sc, tv, m, o + d * hit.x, gn, o, dx, dy);
+        }
+        alpha = alpha * SampleTexture4(sc.textures[dm.alpha_texture], tu, tw, fp, sc.ewa_weights).x;
+    }
+    return alpha >= 0.5f;
+}
+
+// TraceVisibleSurface's skip loop (src/integrators/surface_query.cpp:108-199)
+// after a first closest hit `first`: while the hit surface is cut out, trace
+// again from just past it, at most kMaxAlphaSkips traces in all. Returns the
+// visible hit, or a miss (exhausted = true when the trace budget ran out).
+template <bool kTwo, int kTotal>
+__device__ inline TraceHit SkipCutOuts(const DevScene& sc, V3 o, V3 d, float tmax, TraceHit first, int depth,
+                                       int32_t pixel, int32_t sample, StackStore<kTotal>& st, int2* col, int* error,
+                                       bool& exhausted) {
+    exhausted = false;
+    TraceHit h = first;
+    const TraceHit miss{make_float4(tmax, __int_as_float(-1), 0.0f, 0.0f), -1};
+    for (int traces = 1;; ++traces) {
+        if (__float_as_int(h.h.y) == -1) return miss;
+        if (AlphaVisible(sc, o, d, h.h, h.inst, depth, pixel, sample)) return h;
+        const float tmin = h.h.x + kAlphaSkipOffset;
+        if (tmin >= tmax) return miss;
+        if (traces >= kMaxAlphaSkips) {
+            exhausted = true;
+            return miss;
+        }
+        h = ClosestHit<kTwo, kTotal>(sc.accel, o, d, tmin, tmax, st, col, error);
+    }
+}
+
+// Extend-stage fix-up for scenes with cut-out materials: every entry whose
+// closest hit is cut out continues past it (an exhausted skip loop counts as
+// a miss, as the path integrator treats it).
+template <bool kTwo, int kTotal>
+__global__ void __launch_bounds__(kTraceBlock) AlphaExtendKernel(DevScene sc, PathState ps, Queues q, int depth,
+                                                                 int* error) {
+    __shared__ int2 s_stack[kShortStack * kTraceBlock];
+    int2* col = s_stack + threadIdx.x;
+    StackStore<kTotal> st;
+    const int64_t n = static_cast<int64_t>(q.counters[kCtrIn]);
+    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const float4 hit = q.hits[e];
+        const V3 o = F4(q.ray_in[2 * e]);
+        const float4 rb = q.ray_in[2 * e + 1];
+        const V3 d = F4(rb);
+        const int32_t path = q.path_in[e];
+        const int32_t inst = q.inst[e];
+        if (__float_as_int(hit.y) == -1) continue;
+        const int32_t pixel = depth == 0 ? ps.pixel[path] : 0;
+        const int32_t sample = depth == 0 ? ps.sample[path] : 0;
+        if (AlphaVisible(sc, o, d, hit, inst, depth, pixel, sample)) continue;
+        bool exhausted;
+        const TraceHit r = SkipCutOuts<kTwo, kTotal>(sc, o, d, rb.w, TraceHit{hit, inst}, depth, pixel, sample, st,
+                                                     col, error, exhausted);
+        q.hits[e] = r.h;
+        q.inst[e] = r.inst;
+    }
+}
+
+// TraceShadowVisibility (src/integrators/path_direct_lighting.cpp:23-113)
+// one shadow ray per thread, each query a closest hit with the cut-out skip
+// loop, for scenes where the single-pass shadow kernel does not apply (cut-out
+// materials, or thin dielectrics whose reflectance is textured). Writes the
+// transmittance (w = 1 visible, all 0 occluded) to the ray's slot.
+template <bool kTwo, int kTotal>
+__global__ void __launch_bounds__(kTraceBlock) ShadowExactKernel(DevScene sc, Queues q, float4* transmittance,
+                                                                 unsigned long long* occluded_count, int* error) {
+    __shared__ int2 s_stack[kShortStack * kTraceBlock];
+    int2* col = s_stack + threadIdx.x;
+    StackStore<kTotal> st;
+    const int64_t n = static_cast<int64_t>(q.counters[kCtrShadow]);
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const float4 ra = q.shadow_ray[2 * k], rb = q.shadow_ray[2 * k + 1];
+        V3 o = F4(ra);
+        const V3 d = F4(rb);
+        float remaining = rb.w;
+        float qmin = ra.w;
+        V3 T{1.0f, 1.0f, 1.0f}, mc{1.0f, 1.0f, 1.0f};
+        float md = 1.0f;
+        bool medium = false;
+        auto black = [&]() { return fmaxf(T.x, fmaxf(T.y, T.z)) <= 1.0e-6f; };
+        auto beer = [&](float dist) {
+            if (dist <= 0.0f || md <= 0.0f) return;
+            const float inv = 1.0f / md;
+            const float c0 = fminf(fmaxf(mc.x, 1.0e-6f), 1.0f), c1 = fminf(fmaxf(mc.y, 1.0e-6f), 1.0f),
+                        c2 = fminf(fmaxf(mc.z, 1.0e-6f), 1.0f);
+            T = V3{T.x * expf(logf(c0) * dist * inv), T.y * expf(logf(c1) * dist * inv),
+                   T.z * expf(logf(c2) * dist * inv)};
+        };
+        float4 result = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (int query = 0; query < kClearHits; ++query) {
+            const bool finite = isfinite(remaining);
+            const TraceHit first = ClosestHit<kTwo, kTotal>(sc.accel, o, d, qmin, remaining, st, col, error);
+            bool exhausted;
+            const TraceHit h =
+                SkipCutOuts<kTwo, kTotal>(sc, o, d, remaining, first, 1, 0, 0, st, col, error, exhausted);
+            if (exhausted) break;
+            const int32_t id = __float_as_int(h.h.y);
+            if (id == -1) {
+                if (medium) {
+                    if (!finite) break;
+                    beer(remaining);
+                }
+                if (!black()) result = make_float4(T.x, T.y, T.z, 1.0f);
+                break;
+            }
+            const float t = h.h.x;
+            if (medium) {
+                beer(t);
+                if (black()) break;
+            }
+            const int32_t prim = id >= 0 ? sc.tri_prim[id] : -1;
+            const int32_t material = id >= 0 ? sc.prim_material[prim] : sc.sphere_material[-2 - id];
+            if (material < 0) break;
+            const DevMaterial& m = sc.materials[material];
+            if (m.kind != kDielectric && m.kind != kThinDielectric) break;
+            const V3 hp = o + d * t;
+            if (m.kind == kThinDielectric) {
+                V3 refl = Ld3(m.reflectance);
+                if (id >= 0 && sc.uvs && (sc.prim_flags[prim] & 2u) && TextureValid(sc, m.reflectance_texture)) {
+                    const int4 tv = sc.tri_vertices[id];
+                    const float u = h.h.z, v = h.h.w;
+                    const float w = 1.0f - u - v;
+                    const float2 a = sc.uvs[tv.x], b = sc.uvs[tv.y], c = sc.uvs[tv.z];
+                    const float4 tx = SampleTexture4(sc.textures[m.reflectance_texture], a.x * w + b.x * u + c.x * v,
+                                                     a.y * w + b.y * u + c.y * v,
+                                                     TexFootprint{0.0f, 0.0f, 0.0f, 0.0f}, sc.ewa_weights);
+                    refl = Mul(refl, V3{tx.x, tx.y, tx.z});
+                }
+                T = V3{T.x * Clampf(refl.x, 0.0f, 1.0f), T.y * Clampf(refl.y, 0.0f, 1.0f),
+                       T.z * Clampf(refl.z, 0.0f, 1.0f)};
+                if (black()) break;
+            } else if (medium) {
+                medium = false;
+                mc = V3{1.0f, 1.0f, 1.0f};
+                md = 1.0f;
+            } else {
+                medium = true;
+                mc = Ld3(m.absorption_color);
+                md = m.absorption_distance;
+            }
+            const float bias = SurfaceBias(hp);
+            if (finite) {
+                remaining = remaining - (t + bias);
+                if (remaining <= 0.0f) {
+                    if (!black()) result = make_float4(T.x, T.y, T.z, 1.0f);
+                    break;
+                }
+            }
+            o = hp + d * bias;
+            qmin = 1.0e-5f;
+        }
+        transmittance[q.shadow_slot[k]] = result;
+        if (result.w == 0.0f) atomicAdd(occluded_count, 1ull);
+    }
+}
+
 // IntegratePathSample's per-bounce body (src/integrators/path_integrator.cpp:23-197)
 // for the entries of one shading class.
 template <int kClass>
@@ -1323,6 +1542,43 @@ void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, const
     ShadeKernel<kClassCoatedDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
     ShadeKernel<kClassGeneric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
 }
+template <bool kTwo, int kTotal>
+void LaunchAlphaOne(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
+                    int sm_count, int* error, float4* transmittance, unsigned long long* occluded_count,
+                    bool shadows, cudaStream_t st) {
+    const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((capacity + kTraceBlock - 1) / kTraceBlock,
+                                                                    static_cast<int64_t>(sm_count) * 16));
+    if (shadows) {
+        ShadowExactKernel<kTwo, kTotal><<<blocks * 2, kTraceBlock, 0, st>>>(sc, q, transmittance, occluded_count, error);
+    } else {
+        AlphaExtendKernel<kTwo, kTotal><<<blocks, kTraceBlock, 0, st>>>(sc, ps, q, depth, error);
+    }
+}
+
+void LaunchAlpha(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity, int sm_count,
+                 int* error, float4* transmittance, unsigned long long* occluded_count, bool shadows,
+                 cudaStream_t st) {
+    const bool two = sc.accel.two_level != 0;
+    const bool deep = sc.accel.stack_limit > 64;
+    if (two) {
+        if (deep) LaunchAlphaOne<true, kMaxTraceStack>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, st);
+        else LaunchAlphaOne<true, 64>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, st);
+    } else {
+        if (deep) LaunchAlphaOne<false, kMaxTraceStack>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, st);
+        else LaunchAlphaOne<false, 64>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, st);
+    }
+}
+
+void LaunchAlphaExtend(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
+                       int sm_count, int* error, cudaStream_t st) {
+    LaunchAlpha(sc, ps, q, depth, capacity, sm_count, error, nullptr, nullptr, false, st);
+}
+
+void LaunchShadowExact(const DevScene& sc, const Queues& q, float4* transmittance, unsigned long long* occluded_count,
+                       int64_t capacity, int sm_count, int* error, cudaStream_t st) {
+    LaunchAlpha(sc, PathState{}, q, 0, capacity, sm_count, error, transmittance, occluded_count, true, st);
+}
+
 void LaunchSubsurfaceExit(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
                           int sm_count, cudaStream_t st) {
     SubsurfaceExitKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);

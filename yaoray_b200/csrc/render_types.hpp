@@ -141,6 +141,8 @@ struct DevScene {
     const DevTexture* textures;  // texture_count entries
     int32_t texture_count;
     const float* ewa_weights;
+    int32_t any_alpha;      // a material can cut surfaces out (alpha < 0.5 or an alpha texture)
+    int32_t exact_shadows;  // shadow rays take the per-thread reference loop (cut-outs, textured thin glass)
 };
 
 // Path state, structure of arrays over `capacity` slots.
