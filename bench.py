@@ -380,13 +380,15 @@ RENDER_WORKLOADS = {
     "cornell": ("samples/s (plain MIS path tracer, Cornell box)", "cornell-256x256-64spp-depth8"),
     "instanced": ("samples/s (plain wavefront path tracer, instanced scene)",
                   "instanced-256inst-31M-tris-1920x1080-depth16"),
+    "textured": ("samples/s (MIS path tracer, textured Cornell box)", "cornell-textured-256x256-64spp-depth8"),
+    "cutout": ("samples/s (MIS path tracer, Cornell box with alpha cut-outs)", "cornell-cutout-256x256-64spp-depth8"),
 }
 
 
 def render_scene(workload: str, spp: int):
-    if workload == "cornell":
+    if workload in ("cornell", "textured", "cutout"):
         from yaoray_b200 import cornell
-        return cornell.scene()
+        return {"cornell": cornell.scene, "textured": cornell.textured_scene, "cutout": cornell.cutout_scene}[workload]()
     from yaoray_b200 import instanced
     return instanced.scene(spp=spp)
 
@@ -394,7 +396,9 @@ def render_scene(workload: str, spp: int):
 def run_render(args):
     """--workload cornell: the plain MIS path tracer on the Cornell box
     (256x256, 64 spp, Owen-Sobol seed 0, max depth 8); one step = one full
-    64-spp render.
+    64-spp render. --workload textured / cutout: the same box with
+    reflectance textures under every filter and a normal map, and with alpha
+    cut-outs and textured thin glass on top of that.
     --workload instanced: the instanced scene (256 affine instances of four
     procedural meshes, 31.4M instanced triangles, HDRI + 64 emissive
     triangles, 1920x1080, max depth 16); one step = one render of
@@ -444,7 +448,7 @@ def run_render(args):
         if oracle.ref_available():
             job = oracle.RefJob.from_scene(scene)
             job.render(spp=1)
-            base_spp = 64 if args.workload == "cornell" else 4  # the full Cornell job; 4 spp of the instanced one
+            base_spp = 4 if args.workload == "instanced" else 64  # the full Cornell jobs; 4 spp of the instanced one
             film, st, secs = job.render(spp=base_spp)
             base = {"value": round(scene.width * scene.height * base_spp / secs, 1), "unit": "samples/s",
                     "cores": os.cpu_count(), "kind": "reference",
@@ -694,7 +698,8 @@ def run_jobs(args):
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--workload", choices=["traversal", "cornell", "instanced", "nrc", "jobs"], default="traversal")
+    ap.add_argument("--workload", choices=["traversal", "cornell", "textured", "cutout", "instanced", "nrc", "jobs"],
+                    default="traversal")
     ap.add_argument("--nrc-width", type=int, default=960)
     ap.add_argument("--nrc-height", type=int, default=540)
     ap.add_argument("--ref-spp", type=int, default=512)
