@@ -110,3 +110,24 @@ def test_cutout_scene_matches_reference_cpu(cuda, ref):
     assert abs(res.stats["rays_traced"] / cpu_stats["rays_traced"] - 1) < 0.02
     assert abs(res.stats["shadow_rays"] / cpu_stats["shadow_rays"] - 1) < 0.02
     assert abs(res.stats["occluded_shadow_rays"] / cpu_stats["occluded_shadow_rays"] - 1) < 0.03
+
+
+def test_instanced_cutout_scene_matches_reference_cpu(cuda, ref):
+    """The cut-out scene as a two-level scene: the normal map on a mirrored
+    instance (negative determinant: the tangent frame flips), the alpha
+    screen under a tilt and a translation (footprints from transformed
+    triangles), every other primitive under an identity instance."""
+    def make(seed):
+        s = cornell.instanced_cutout_scene(96, 96, 64, 8)
+        s.seed = seed
+        return s
+
+    res, cpu_film, cpu_stats, cpu2 = render_pair(ref, make)
+    check_aovs(res, cpu_film)
+    g, c, c2 = linear(res.film), linear(cpu_film), linear(cpu2)
+    noise = relmse(c2, c)
+    err = relmse(g, c)
+    assert err < 0.25 * noise, (err, noise)
+    assert abs(g.mean() / c.mean() - 1.0) < 0.01
+    assert res.bad_samples == 0
+    assert abs(res.stats["rays_traced"] / cpu_stats["rays_traced"] - 1) < 0.02

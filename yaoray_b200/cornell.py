@@ -310,3 +310,33 @@ def cutout_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: 
     _append_quad(s, [(1.6, 5.2, 1.8), (3.9, 5.2, 1.8), (3.9, 5.2, 3.9), (1.6, 5.2, 3.9)], base + 1)
     _append_quad(s, [(0.8, 2.2, 0.6), (2.0, 2.2, 0.6), (2.0, 2.2, 2.9), (0.8, 2.2, 2.9)], base + 2, 1.0)
     return s
+
+
+def instanced_cutout_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8) -> RenderScene:
+    """cutout_scene() traversed as a two-level scene: every primitive is an
+    explicit instance, the identity except for the normal-mapped tall box,
+    mirrored in x about its centre (a negative-determinant transform: its
+    tangent frame flips orientation), and the cut-out screen, moved 0.3
+    towards the camera and tilted 10 degrees about x."""
+    from . import _lib
+
+    s = cutout_scene(width, height, spp, max_depth)
+    g = s.geometry
+    n = g.primitives.size
+    eye = np.eye(4, dtype=np.float32)
+    inst = np.zeros(n, _lib.INSTANCE_DTYPE)
+    for k in range(n):
+        m = eye.copy()
+        if k == 6:  # tall box: x -> 2 cx - x
+            first, count = int(g.primitives[k]["first_index"]), int(g.primitives[k]["index_count"])
+            cx = float(g.positions[np.unique(g.indices[first:first + count])][:, 0].mean())
+            m[0, 0] = -1.0
+            m[0, 3] = 2.0 * cx
+        elif k == n - 3:  # the screen (first of the three appended panes)
+            a = math.radians(10.0)
+            m[1, 1], m[1, 2], m[2, 1], m[2, 2] = math.cos(a), -math.sin(a), math.sin(a), math.cos(a)
+            m[2, 3] = -0.3
+        inst[k]["primitive"] = k
+        inst[k]["object_to_world"] = m.T.reshape(16)  # column-major
+    g.instances = inst
+    return s
