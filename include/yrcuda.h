@@ -434,6 +434,45 @@ yrc_status yrc_texture_sample_eval(const yrc_texture* texture, const float* uvs,
 yrc_status yrc_texture_mip_chain_eval(const yrc_texture* texture, float* texels, int64_t capacity, int32_t* level_dims,
                                       int32_t* level_count);
 
+/* MeasuredBrdf (include/yaoray/shading/measured_brdf.hpp:10-24): the RGL
+ * tensors LoadMeasuredBrdf reads (src/shading/measured_brdf.cpp:33-190),
+ * isotropic only (n_phi_i <= 2), row-major:
+ *   ndf, sigma   [ndf_rows][ndf_cols]                   (theta_m x phi_m)
+ *   vndf         [n_phi_i][n_theta_i][vndf_rows][vndf_cols]
+ *   luminance    [n_phi_i][n_theta_i][res][res]
+ *   spectra      [n_phi_i][n_theta_i][n_wavelengths][res][res]
+ * The library builds the reference's five warps from them. */
+typedef struct yrc_measured_brdf {
+    int32_t n_theta_i;
+    int32_t n_phi_i;
+    int32_t n_wavelengths;
+    int32_t ndf_rows;
+    int32_t ndf_cols;
+    int32_t vndf_rows;
+    int32_t vndf_cols;
+    int32_t res;
+    const float* theta_i;
+    const float* phi_i;
+    const float* wavelengths;
+    const float* ndf;
+    const float* sigma;
+    const float* vndf;
+    const float* luminance;
+    const float* spectra;
+} yrc_measured_brdf;
+
+/* EvaluateMeasured and PdfMeasured (src/shading/bsdf_measured.cpp:10-61,
+ * 177-238) on the device for n rows of 9 floats (wo, wi, normal): f gets 3
+ * floats per row, pdf 1. The warp arithmetic follows the reference's
+ * (including its fused multiply-adds); the angles go through CUDA's
+ * acosf/atan2f, so values agree within rounding. Synchronous. */
+yrc_status yrc_measured_eval(const yrc_measured_brdf* brdf, const float* queries, int64_t n, float* f, float* pdf);
+
+/* SampleMeasured (src/shading/bsdf_measured.cpp:67-128) on the device for n
+ * rows of 8 floats (wo, normal, u.x, u.y): out gets 8 floats per row (wi,
+ * weight, pdf, valid 0/1). Synchronous. */
+yrc_status yrc_measured_sample(const yrc_measured_brdf* brdf, const float* queries, int64_t n, float* out);
+
 /* RenderMaterialKind (include/yaoray/scene/material.hpp:7-19). */
 enum {
     YRC_MAT_DIFFUSE = 0,
@@ -610,6 +649,11 @@ typedef struct yrc_scene_desc {
     int64_t tangent_stride;
     const yrc_texture* textures;
     int32_t texture_count;
+    /* RenderSceneIR::measured_brdfs, indexed by yrc_material.measured_index;
+     * a Measured material whose index has no entry renders as the
+     * reference's conductor fallback. */
+    const yrc_measured_brdf* measured;
+    int32_t measured_count;
 } yrc_scene_desc;
 
 /* FilmPixel (include/yaoray/film/film.hpp:19-28), byte-identical, 56 bytes. */
@@ -696,7 +740,7 @@ typedef struct yrc_render_scene yrc_render_scene;
 
 /* CudaBackend::Prepare (src/runtime/cuda_stub_backend.cpp:20-28): uploads the
  * scene and its acceleration structure. Fails with YRC_ERR_UNSUPPORTED for
- * scene features the device does not shade (measured BRDFs). */
+ * scene features the device does not shade (analytic lights). */
 yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene** out);
 void yrc_render_scene_destroy(yrc_render_scene* scene);
 int64_t yrc_render_scene_device_bytes(const yrc_render_scene* scene);

@@ -243,6 +243,8 @@ def ref_lib() -> C.CDLL:
         L.yrref_texture_sample.argtypes = [C.c_int, C.c_int, P, C.c_int, C.c_int, C.c_int, P, P, I64, P]
         L.yrref_texture_mip_chain.argtypes = [C.c_int, C.c_int, P, C.c_int, C.c_int, P, P]
         L.yrref_texture_mip_chain.restype = C.c_int
+        L.yrref_measured_eval.argtypes = [P, P, I64, P, P]
+        L.yrref_measured_sample.argtypes = [P, P, I64, P]
         _REF = L
     return _REF
 
@@ -431,6 +433,30 @@ def oracle_texture_mip_chain(texels: np.ndarray, wrap_s: int, wrap_t: int) -> li
     count = oracle_lib().yo_texture_mip_chain(w, h, tx.ctypes.data, wrap_s, wrap_t, out.ctypes.data,
                                               dims.ctypes.data)
     return _mip_levels(out, dims, count)
+
+
+def ref_measured_eval(brdf, wo, wi, n):
+    """The reference's EvaluateMeasured / PdfMeasured (brdf: a
+    yaoray_b200.measured.MeasuredBrdf): (f (n, 3), pdf (n,))."""
+    q = np.ascontiguousarray(np.concatenate([np.reshape(wo, (-1, 3)), np.reshape(wi, (-1, 3)),
+                                             np.reshape(n, (-1, 3))], 1), np.float32)
+    f = np.empty((q.shape[0], 3), np.float32)
+    pdf = np.empty(q.shape[0], np.float32)
+    st, keep = brdf.c_struct()
+    ref_lib().yrref_measured_eval(C.addressof(st), q.ctypes.data, q.shape[0], f.ctypes.data, pdf.ctypes.data)
+    del keep
+    return f, pdf
+
+
+def ref_measured_sample(brdf, wo, n, u):
+    """The reference's SampleMeasured: (n, 8) rows of wi, weight, pdf, valid."""
+    q = np.ascontiguousarray(np.concatenate([np.reshape(wo, (-1, 3)), np.reshape(n, (-1, 3)),
+                                             np.reshape(u, (-1, 2))], 1), np.float32)
+    out = np.empty((q.shape[0], 8), np.float32)
+    st, keep = brdf.c_struct()
+    ref_lib().yrref_measured_sample(C.addressof(st), q.ctypes.data, q.shape[0], out.ctypes.data)
+    del keep
+    return out
 
 
 def ref_bssrdf_table(g: float, eta: float, rho_count: int = 100, radius_count: int = 64) -> dict:

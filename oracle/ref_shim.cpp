@@ -18,6 +18,9 @@
 #include <yaoray/scene/camera.hpp>
 #include <yaoray/scene/render_scene.hpp>
 #include <yaoray/shading/texture.hpp>
+#include <yaoray/shading/measured_brdf.hpp>
+#include "shading/bsdf_internal.hpp"
+#include "yrcuda.h"
 
 #include <algorithm>
 #include <atomic>
@@ -390,6 +393,69 @@ int yrref_texture_mip_chain(int width, int height, const float* texels, int wrap
     return static_cast<int>(t.mip_levels.size());
 }
 
+// ------------------------------------------------------------ measured BRDF ---
+// A MeasuredBrdf from the C-ABI arrays, with its five warps built exactly as
+// LoadMeasuredBrdf builds them from a tensor file.
+static std::shared_ptr<yr::MeasuredBrdf> MakeMeasured(const yrc_measured_brdf& b) {
+    auto m = std::make_shared<yr::MeasuredBrdf>();
+    const std::size_t nv = static_cast<std::size_t>(b.n_phi_i) * b.n_theta_i;
+    m->theta_i.assign(b.theta_i, b.theta_i + b.n_theta_i);
+    m->phi_i.assign(b.phi_i, b.phi_i + b.n_phi_i);
+    m->wavelengths.assign(b.wavelengths, b.wavelengths + b.n_wavelengths);
+    const std::size_t nd = static_cast<std::size_t>(b.ndf_rows) * b.ndf_cols;
+    m->ndf.assign(b.ndf, b.ndf + nd);
+    m->sigma.assign(b.sigma, b.sigma + nd);
+    m->vndf.assign(b.vndf, b.vndf + nv * b.vndf_rows * b.vndf_cols);
+    m->luminance.assign(b.luminance, b.luminance + nv * b.res * b.res);
+    m->spectra.assign(b.spectra, b.spectra + nv * b.n_wavelengths * b.res * b.res);
+    m->isotropic = b.n_phi_i <= 2;
+    m->res = b.res;
+    m->ndf_warp = yr::PiecewiseLinear2D<0>(m->ndf.data(), b.ndf_cols, b.ndf_rows, {}, {}, false, false);
+    m->sigma_warp = yr::PiecewiseLinear2D<0>(m->sigma.data(), b.ndf_cols, b.ndf_rows, {}, {}, false, false);
+    m->vndf_warp = yr::PiecewiseLinear2D<2>(m->vndf.data(), b.vndf_cols, b.vndf_rows, {b.n_phi_i, b.n_theta_i},
+                                            {m->phi_i.data(), m->theta_i.data()}, true, true);
+    m->luminance_warp = yr::PiecewiseLinear2D<2>(m->luminance.data(), b.res, b.res, {b.n_phi_i, b.n_theta_i},
+                                                 {m->phi_i.data(), m->theta_i.data()}, true, true);
+    m->spectra_warp = yr::PiecewiseLinear2D<3>(m->spectra.data(), b.res, b.res,
+                                               {b.n_phi_i, b.n_theta_i, b.n_wavelengths},
+                                               {m->phi_i.data(), m->theta_i.data(), m->wavelengths.data()},
+                                               false, false);
+    return m;
+}
+
+// EvaluateMeasured / PdfMeasured for rows of (wo, wi, normal).
+void yrref_measured_eval(const yrc_measured_brdf* b, const float* q, std::int64_t n, float* f, float* pdf) {
+    const auto m = MakeMeasured(*b);
+    for (std::int64_t i = 0; i < n; ++i) {
+        const float* r = q + 9 * i;
+        const yr::Vec3f wo{r[0], r[1], r[2]}, wi{r[3], r[4], r[5]}, nn{r[6], r[7], r[8]};
+        const yr::Color3f c = yr::EvaluateMeasured(*m, wo, wi, nn);
+        f[3 * i] = c.x;
+        f[3 * i + 1] = c.y;
+        f[3 * i + 2] = c.z;
+        pdf[i] = yr::PdfMeasured(*m, wo, wi, nn);
+    }
+}
+
+// SampleMeasured for rows of (wo, normal, u): out rows (wi, weight, pdf, valid).
+void yrref_measured_sample(const yrc_measured_brdf* b, const float* q, std::int64_t n, float* out) {
+    const auto m = MakeMeasured(*b);
+    for (std::int64_t i = 0; i < n; ++i) {
+        const float* r = q + 8 * i;
+        const yr::BsdfSample s = yr::SampleMeasured(*m, yr::Vec3f{r[0], r[1], r[2]}, yr::Vec3f{r[3], r[4], r[5]},
+                                                    yr::Vec2f{r[6], r[7]});
+        float* o = out + 8 * i;
+        o[0] = s.wi.x;
+        o[1] = s.wi.y;
+        o[2] = s.wi.z;
+        o[3] = s.weight.x;
+        o[4] = s.weight.y;
+        o[5] = s.weight.z;
+        o[6] = s.pdf;
+        o[7] = s.valid ? 1.0f : 0.0f;
+    }
+}
+
 // First `count` NextFloat() draws of Rng(seed).
 void yrref_rng_floats(std::uint64_t seed, int count, float* out) {
     yr::Rng rng(seed);
@@ -699,8 +765,10 @@ void* yrref_job_from_desc(const yrc_scene_desc* d) {
         r.alpha.texture = m.alpha_texture;
         r.normal_map = m.normal_map;
         r.normal_scale = m.normal_scale;
+        r.measured_index = m.measured_index;
         ir.materials.push_back(r);
     }
+    for (int32_t i = 0; d->measured && i < d->measured_count; ++i) ir.measured_brdfs.push_back(MakeMeasured(d->measured[i]));
     // Scene textures keep their indices; the environment texture follows them.
     for (int32_t i = 0; d->textures && i < d->texture_count; ++i) {
         const yrc_texture& t = d->textures[i];

@@ -201,6 +201,8 @@ def lib() -> C.CDLL:
         "yrc_pixel_seed_eval": (C.c_int, [C.c_uint64, P, I64, P]),
         "yrc_texture_sample_eval": (C.c_int, [P, P, P, I64, P]),
         "yrc_texture_mip_chain_eval": (C.c_int, [P, P, I64, P, P]),
+        "yrc_measured_eval": (C.c_int, [P, P, I64, P, P]),
+        "yrc_measured_sample": (C.c_int, [P, P, I64, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -340,3 +340,18 @@ def instanced_cutout_scene(width: int = 256, height: int = 256, spp: int = 64, m
         inst[k]["object_to_world"] = m.T.reshape(16)  # column-major
     g.instances = inst
     return s
+
+
+def measured_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8) -> RenderScene:
+    """The Cornell box with both boxes made of a measured (RGL-layout) BRDF:
+    the seeded synthetic tensors of measured.synthetic_brdf()."""
+    from .measured import synthetic_brdf
+    from .render import MEASURED
+
+    s = scene(width, height, spp, max_depth)
+    m = default_material(kind=MEASURED, reflectance=WHITE, measured_index=0, uroughness=0.3, vroughness=0.3)
+    s.materials = np.concatenate([s.materials, m[None]])
+    for box in (5, 6):
+        s.geometry.primitives[box]["material_index"] = len(s.materials) - 1
+    s.measured = [synthetic_brdf(3)]
+    return s

@@ -5,6 +5,7 @@
 // within one call.
 #pragma once
 
+#include "measured.cuh"
 #include "sampler.cuh"
 #include "shading.cuh"
 
@@ -35,6 +36,7 @@ struct Mat {
     V3 coat_absorption;
     int32_t coat_maxdepth;
     int32_t coat_nsamples;
+    const DevMeasuredBrdf* measured;  // kMeasured with data; null: the conductor fallback
 };
 
 __device__ inline Mat LoadMat(const DevMaterial& m) {
@@ -49,6 +51,7 @@ __device__ inline Mat LoadMat(const DevMaterial& m) {
     r.coat_absorption = Ld3(m.coat_absorption);
     r.coat_maxdepth = m.coat_maxdepth;
     r.coat_nsamples = m.coat_nsamples;
+    r.measured = nullptr;
     return r;
 }
 
@@ -117,6 +120,8 @@ __device__ inline V3 EvalSimple(const Mat& m, V3 wo, V3 wi, V3 n) {
             if (!IsAbove(wo, n) || !IsAbove(wi, n)) return {0, 0, 0};
             return m.reflectance / kPi;
         case kMeasured:
+            if (m.measured) return EvalMeasured(*m.measured, wo, wi, n);
+            [[fallthrough]];
         case kConductor:
             if (m.ur <= kDeltaRoughness && m.vr <= kDeltaRoughness) return {0, 0, 0};
             return GgxSpecularBrdf(m.reflectance, m.ur, wo, wi, n);
@@ -150,6 +155,8 @@ __device__ inline float PdfSimple(const Mat& m, V3 wo, V3 wi, V3 n) {
             if (!IsAbove(wo, n) || !IsAbove(wi, n)) return 0.0f;
             return fmaxf(0.0f, Dot(n, wi)) / kPi;
         case kMeasured:
+            if (m.measured) return PdfMeasuredBrdf(*m.measured, wo, wi, n);
+            [[fallthrough]];
         case kConductor:
             if (m.ur <= kDeltaRoughness && m.vr <= kDeltaRoughness) return 0.0f;
             return GgxReflectionPdf(m.ur, wo, wi, n);
@@ -176,6 +183,8 @@ __device__ inline BsdfSample SampleSimple(const Mat& m, V3 wo, V3 n, float sx, f
             return BsdfSample{wi, m.reflectance, PdfSimple(m, wo, wi, n), true, false};
         }
         case kMeasured:
+            if (m.measured) return SampleMeasuredBrdf(*m.measured, wo, n, sx, sy);
+            [[fallthrough]];
         case kConductor:
             if (m.ur <= kDeltaRoughness && m.vr <= kDeltaRoughness) {
                 if (!IsAbove(wo, n) || IsBlack(m.reflectance)) return NoSample();

@@ -24,6 +24,7 @@
 #include "nrc.hpp"
 #include "render_kernels.hpp"
 #include "render_types.hpp"
+#include "measured.hpp"
 #include "texture.hpp"
 #include "trace_kernels.hpp"
 #include "yrc_internal.hpp"
@@ -117,6 +118,7 @@ struct yrc_render_scene {
     yrc::DeviceArena cache_work;
     int64_t cache_capacity = 0;
     yrc::TextureSet textures;  // scene textures and their mip chains
+    yrc::MeasuredSet measured;  // measured BRDF warps
     yrc::CacheArgs cargs{};
     std::mutex mutex;
 };
@@ -144,6 +146,7 @@ void yrc_render_scene_destroy(yrc_render_scene* scene) {
     scene->work.Release();
     scene->arena.Release();
     scene->textures.Release();
+    scene->measured.Release();
     yrc_accel_destroy(scene->accel);
     delete scene;
 }
@@ -170,7 +173,8 @@ yrc_status yrc_render_scene_set_cache(yrc_render_scene* scene, yrc_nrc* cache, c
 }
 
 int64_t yrc_render_scene_device_bytes(const yrc_render_scene* scene) {
-    return scene ? scene->arena.bytes + scene->work.bytes + scene->textures.bytes + yrc_accel_device_bytes(scene->accel)
+    return scene ? scene->arena.bytes + scene->work.bytes + scene->textures.bytes + scene->measured.bytes +
+                       yrc_accel_device_bytes(scene->accel)
                  : 0;
 }
 
@@ -196,9 +200,6 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
     }
     for (int32_t i = 0; i < desc->material_count; ++i) {
         const yrc_material& m = desc->materials[i];
-        if (m.kind == YRC_MAT_MEASURED && m.measured_index >= 0) {
-            return Fail(YRC_ERR_UNSUPPORTED, "material " + std::to_string(i) + ": measured BRDFs are not shaded on the device");
-        }
         if (m.kind == YRC_MAT_SUBSURFACE) {
             if (m.bssrdf_index < 0 || m.bssrdf_index >= desc->bssrdf_count || !desc->bssrdf_tables) {
                 return Fail(YRC_ERR_UNSUPPORTED,
@@ -358,6 +359,9 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
         dm.normal_map = m.normal_map;
         dm.alpha = m.alpha;
         dm.normal_scale = m.normal_scale;
+        dm.measured_index = (m.kind == YRC_MAT_MEASURED && m.measured_index >= 0 && m.measured_index < desc->measured_count)
+                                ? m.measured_index
+                                : -1;
         if (m.kind == YRC_MAT_DIELECTRIC || m.kind == YRC_MAT_THIN_DIELECTRIC) transparent = true;
         const bool tex_alpha = m.alpha_texture >= 0 && m.alpha_texture < desc->texture_count;
         const bool tex_refl = m.reflectance_texture >= 0 && m.reflectance_texture < desc->texture_count;
@@ -512,6 +516,16 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
         d.textures = s->textures.textures;
         d.texture_count = s->textures.count;
         d.ewa_weights = s->textures.ewa_weights;
+    }
+    if (desc->measured_count > 0) {
+        const yrc_status ms = UploadMeasured(desc->measured, desc->measured_count, s->measured);
+        if (ms != YRC_OK) {
+            const std::string msg = yrc_last_error();
+            yrc_render_scene_destroy(s);
+            return Fail(ms, msg);
+        }
+        d.measured = s->measured.brdfs;
+        d.measured_count = s->measured.count;
     }
     *out = s;
     return Ok();

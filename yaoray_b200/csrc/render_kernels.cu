@@ -1045,6 +1045,7 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
             const DevMaterial& dm = sc.materials[s.material];
             m = LoadMat(dm);
             m.reflectance = Mul(m.reflectance, s.reflectance_scale);
+            m.measured = dm.measured_index >= 0 ? sc.measured + dm.measured_index : nullptr;
             emission = Ld3(dm.emission);
         } else {  // default RenderMaterial: diffuse 0.5
             m = Mat{kDiffuse, {0.5f, 0.5f, 0.5f}, 1.5f, 0.0f, 0.0f, 1.5f, 0.01f, {0, 0, 0}, 10, 1};

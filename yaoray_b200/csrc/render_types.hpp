@@ -57,7 +57,8 @@ struct alignas(16) DevMaterial {
     int32_t normal_map;
     float alpha;
     float normal_scale;
-    int32_t pad[2];
+    int32_t measured_index;  // into DevScene::measured, -1 = none
+    int32_t pad;
 };
 
 struct DevBssrdf {
@@ -77,6 +78,8 @@ struct DevAnalytic {
     float cone_angle;
     float cone_cos_inner;
 };
+
+struct DevMeasuredBrdf;  // measured.cuh
 
 struct DevScene {
     AccelParams accel;
@@ -141,6 +144,8 @@ struct DevScene {
     const DevTexture* textures;  // texture_count entries
     int32_t texture_count;
     const float* ewa_weights;
+    const DevMeasuredBrdf* measured;  // measured BRDFs (RGL warps)
+    int32_t measured_count;
     int32_t any_alpha;      // a material can cut surfaces out (alpha < 0.5 or an alpha texture)
     int32_t exact_shadows;  // shadow rays take the per-thread reference loop (cut-outs, textured thin glass)
 };

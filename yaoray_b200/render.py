@@ -20,6 +20,7 @@ import numpy as np
 from . import _lib
 from ._lib import YrcError, check, lib, ptr
 from .accel import SceneGeometry, build_bvh, build_bvh_device, build_two_level_bvh
+from .measured import measured_array
 from .texture import textures_array
 
 # --------------------------------------------------------------- C mirrors
@@ -131,7 +132,8 @@ class SceneDesc(C.Structure):
                 ("bssrdf_tables", C.c_void_p), ("bssrdf_count", C.c_int32), ("camera", Camera),
                 ("settings", Settings), ("flat", C.c_void_p), ("two_level", C.c_void_p),
                 ("uvs", C.c_void_p), ("uv_stride", C.c_int64), ("tangents", C.c_void_p),
-                ("tangent_stride", C.c_int64), ("textures", C.c_void_p), ("texture_count", C.c_int32)]
+                ("tangent_stride", C.c_int64), ("textures", C.c_void_p), ("texture_count", C.c_int32),
+                ("measured", C.c_void_p), ("measured_count", C.c_int32)]
 
 
 class Progress(C.Structure):
@@ -284,6 +286,7 @@ class RenderScene:
     uvs: np.ndarray | None = None              # (V, 2) RenderVertex::uv
     tangents: np.ndarray | None = None         # (V, 4) RenderVertex::tangent xyz + tangent_handedness
     textures: list = field(default_factory=list)  # texture.Texture, by material texture index
+    measured: list = field(default_factory=list)  # measured.MeasuredBrdf, by material measured_index
 
     def emissive_power_alias(self):
         """The alias table PrepareLightSampling builds (emissive power = area * luminance)."""
@@ -359,6 +362,11 @@ class PreparedScene:
             self._keep += [tarr, tkeep]
             d.textures = C.addressof(tarr)
             d.texture_count = len(scene.textures)
+        if scene.measured:
+            marr, mkeep = measured_array(scene.measured)
+            self._keep += [marr, mkeep]
+            d.measured = C.addressof(marr)
+            d.measured_count = len(scene.measured)
         mats = np.ascontiguousarray(scene.materials, MATERIAL_DTYPE)
         em = np.ascontiguousarray(scene.emissive, EMISSIVE_DTYPE)
         self._keep += [mats, em]
