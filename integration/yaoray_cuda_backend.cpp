@@ -9,6 +9,7 @@
 // pass loop on the device with the RenderRequest's resume film, stop token and
 // per-pass progress callback, and returns a yr::Film and RenderStats.
 // Only the C ABI (include/yrcuda.h) crosses into the CUDA library.
+#include <yaoray/shading/measured_brdf.hpp>
 #include <yaoray/accel/acceleration.hpp>
 #include <yaoray/lighting/light_sampling.hpp>
 #include <yaoray/runtime/cuda_stub_backend.hpp>
@@ -222,6 +223,19 @@ BackendPrepareResult CudaBackend::Prepare(RenderJob job) {
     }
     d.textures = textures.data();
     d.texture_count = static_cast<int32_t>(textures.size());
+    // Measured BRDFs: the raw RGL tensors (the library builds the warps).
+    std::vector<yrc_measured_brdf> measured;
+    for (const std::shared_ptr<MeasuredBrdf>& mb : ir.measured_brdfs) {
+        const MeasuredBrdf& m = *mb;
+        measured.push_back(yrc_measured_brdf{
+            static_cast<int32_t>(m.theta_i.size()), static_cast<int32_t>(m.phi_i.size()),
+            static_cast<int32_t>(m.wavelengths.size()), static_cast<int32_t>(m.ndf_shape[0]),
+            static_cast<int32_t>(m.ndf_shape[1]), static_cast<int32_t>(m.vndf_shape[2]),
+            static_cast<int32_t>(m.vndf_shape[3]), m.res, m.theta_i.data(), m.phi_i.data(), m.wavelengths.data(),
+            m.ndf.data(), m.sigma.data(), m.vndf.data(), m.luminance.data(), m.spectra.data()});
+    }
+    d.measured = measured.data();
+    d.measured_count = static_cast<int32_t>(measured.size());
     d.materials = materials.data();
     d.material_count = static_cast<int32_t>(materials.size());
     std::vector<yrc_emissive_primitive> emissive;
