@@ -692,8 +692,7 @@ void yrref_job_lights(void* handle, yrc_emissive_primitive* emissive, float* ali
     settings->adaptive_confidence = s.adaptive_sampling.confidence;
 }
 
-// Builds a job from the C-ABI scene description (analytic lights are not
-// carried). The environment texture becomes a
+// Builds a job from the C-ABI scene description. The environment texture becomes a
 // bilinear, repeat-wrapped RGBA texture with its distribution rebuilt by
 // BuildEnvironmentDistribution.
 void* yrref_job_from_desc(const yrc_scene_desc* d) {
@@ -778,6 +777,17 @@ void* yrref_job_from_desc(const yrc_scene_desc* d) {
     for (int32_t i = 0; i < d->emissive_count; ++i) {
         const yrc_emissive_primitive& e = d->emissive[i];
         ir.emissive_primitives.push_back(yr::EmissivePrimitive{e.primitive_index, Rgb(e.radiance), e.area});
+    }
+    for (int32_t i = 0; d->analytic && i < d->analytic_count; ++i) {
+        const yrc_analytic_light& a = d->analytic[i];
+        yr::AnalyticLight l;
+        l.kind = static_cast<yr::AnalyticLightKind>(a.kind);
+        l.position = yr::Point3f{a.position[0], a.position[1], a.position[2]};
+        l.direction = yr::Vec3f{a.direction[0], a.direction[1], a.direction[2]};
+        l.intensity = Rgb(a.intensity);
+        l.cone_angle = a.cone_angle;
+        l.cone_cos_inner = a.cone_cos_inner;
+        ir.analytic_lights.push_back(l);
     }
     const yrc_environment& env = d->environment;
     for (int32_t i = 0; d->bssrdf_tables && i < d->bssrdf_count; ++i) {

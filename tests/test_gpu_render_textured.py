@@ -131,3 +131,24 @@ def test_instanced_cutout_scene_matches_reference_cpu(cuda, ref):
     assert abs(g.mean() / c.mean() - 1.0) < 0.01
     assert res.bad_samples == 0
     assert abs(res.stats["rays_traced"] / cpu_stats["rays_traced"] - 1) < 0.02
+
+
+@pytest.mark.parametrize("many", [False, True])
+def test_analytic_lights_match_reference_cpu(cuda, ref, many):
+    """Point, spot and distant lights (many=False: power alias selection;
+    many=True: twelve local lights, light-tree selection by power over
+    distance) together with the area light."""
+    def make(seed):
+        s = cornell.analytic_scene(96, 96, 64, 8, many=many)
+        s.seed = seed
+        return s
+
+    res, cpu_film, cpu_stats, cpu2 = render_pair(ref, make)
+    g, c, c2 = linear(res.film), linear(cpu_film), linear(cpu2)
+    noise = relmse(c2, c)
+    err = relmse(g, c)
+    assert err < 0.25 * noise, (err, noise)
+    assert abs(g.mean() / c.mean() - 1.0) < 0.01
+    assert res.film["depth_sum"].tobytes() == cpu_film["depth_sum"].tobytes()
+    assert abs(res.stats["shadow_rays"] / cpu_stats["shadow_rays"] - 1) < 0.02
+    assert abs(res.stats["occluded_shadow_rays"] / cpu_stats["occluded_shadow_rays"] - 1) < 0.03

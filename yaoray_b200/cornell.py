@@ -355,3 +355,31 @@ def measured_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth
         s.geometry.primitives[box]["material_index"] = len(s.materials) - 1
     s.measured = [synthetic_brdf(3)]
     return s
+
+
+def analytic_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8,
+                   many: bool = False) -> RenderScene:
+    """The Cornell box lit by analytic lights as well as its area light:
+    a point, a spot and a distant light (selected through the power alias
+    table), or with many=True twelve point and spot lights spread under the
+    ceiling (more than 8 local lights: selected through the light tree)."""
+    from .render import ANALYTIC_DTYPE
+
+    s = scene(width, height, spp, max_depth)
+    if many:
+        rng = np.random.default_rng(11)
+        a = np.zeros(12, ANALYTIC_DTYPE)
+        a["kind"] = np.where(np.arange(12) % 3 == 2, 1, 0)
+        a["position"] = np.stack([rng.uniform(0.5, 5.0, 12), rng.uniform(3.5, 5.3, 12), rng.uniform(0.5, 5.0, 12)], 1)
+        a["direction"] = (0.0, -1.0, 0.0)
+        a["intensity"] = rng.uniform(0.5, 2.5, (12, 3))
+        a["cone_angle"] = np.float32(math.cos(math.radians(40.0)))
+        a["cone_cos_inner"] = np.float32(math.cos(math.radians(25.0)))
+    else:
+        a = np.zeros(3, ANALYTIC_DTYPE)
+        a[0] = (0, (1.2, 4.5, 2.0), (0, 0, 0), (6.0, 5.0, 4.0), 0.0, 0.0)
+        a[1] = (1, (4.0, 5.0, 3.5), (-0.3, -1.0, 0.1), (12.0, 12.0, 16.0), math.cos(math.radians(30.0)),
+                math.cos(math.radians(20.0)))
+        a[2] = (2, (0, 0, 0), (0.2, -1.0, 0.6), (0.6, 0.55, 0.5), 0.0, 0.0)
+    s.analytic = a
+    return s

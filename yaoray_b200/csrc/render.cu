@@ -17,6 +17,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -192,8 +193,8 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
         (desc->emissive_count > 0 && !desc->emissive)) {
         return Fail(YRC_ERR_INVALID_ARGUMENT, "invalid material or light arrays");
     }
-    if (desc->analytic_count > 0) {
-        return Fail(YRC_ERR_UNSUPPORTED, "analytic (point/spot/distant) lights are not rendered on the device");
+    if (desc->analytic_count < 0 || (desc->analytic_count > 0 && !desc->analytic)) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "invalid analytic light array");
     }
     if (desc->texture_count < 0 || (desc->texture_count > 0 && !desc->textures)) {
         return Fail(YRC_ERR_INVALID_ARGUMENT, "invalid texture array");
@@ -483,6 +484,88 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
     }
     for (int32_t i = 0; i < desc->material_count; ++i) {
         if (desc->materials[i].kind == YRC_MAT_SUBSURFACE) d.any_subsurface = 1;
+    }
+
+    // Analytic lights (PrepareLightSampling, src/lighting/light_sampling.cpp:
+    // 205-275): the power alias table (the caller's, else built here from the
+    // same weights) and, when every light is local and there are more than
+    // 8, the power / distance tree.
+    d.analytic_count = desc->analytic_count;
+    d.analytic_tree_root = -1;
+    if (desc->analytic_count > 0) {
+        const int32_t n = desc->analytic_count;
+        std::vector<DevAnalytic> lights(static_cast<size_t>(n));
+        std::vector<float> weights(static_cast<size_t>(n));
+        std::vector<int> local;
+        for (int32_t i = 0; i < n; ++i) {
+            const yrc_analytic_light& l = desc->analytic[i];
+            DevAnalytic& a = lights[static_cast<size_t>(i)];
+            a.kind = l.kind;
+            std::memcpy(a.position, l.position, sizeof(a.position));
+            std::memcpy(a.direction, l.direction, sizeof(a.direction));
+            std::memcpy(a.intensity, l.intensity, sizeof(a.intensity));
+            a.cone_angle = l.cone_angle;
+            a.cone_cos_inner = l.cone_cos_inner;
+            float power = std::max(0.0f, 0.2126f * l.intensity[0] + 0.7152f * l.intensity[1] + 0.0722f * l.intensity[2]);
+            if (l.kind == 1) {
+                power *= std::max(0.0f, 2.0f * 3.14159265358979323846f * (1.0f - l.cone_angle));
+            } else if (l.kind == 0) {
+                power *= 4.0f * 3.14159265358979323846f;
+            }
+            weights[static_cast<size_t>(i)] = power;
+            if (l.kind != 2 && power > 0.0f) local.push_back(i);
+        }
+        d.analytic = A.Upload(lights);
+        std::vector<float> prob(static_cast<size_t>(n)), pmf(static_cast<size_t>(n));
+        std::vector<int32_t> alias(static_cast<size_t>(n));
+        const yrc_alias_table& at = desc->analytic_power;
+        if (at.count == n && at.probability && at.alias && at.pmf) {
+            prob.assign(at.probability, at.probability + n);
+            alias.assign(at.alias, at.alias + n);
+            pmf.assign(at.pmf, at.pmf + n);
+        } else {
+            yrc_alias_table_build(weights.data(), n, prob.data(), alias.data(), pmf.data());
+        }
+        d.analytic_alias_prob = A.Upload(prob);
+        d.analytic_alias_index = A.Upload(alias);
+        d.analytic_alias_pmf = A.Upload(pmf);
+        if (static_cast<int32_t>(local.size()) == n && n > 8) {
+            std::vector<DevLightNode> nodes;
+            nodes.reserve(local.size() * 2);
+            std::function<int(size_t, size_t)> build = [&](size_t begin, size_t end) -> int {
+                float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+                float power = 0.0f;
+                for (size_t i = begin; i < end; ++i) {
+                    const float* pos = desc->analytic[local[i]].position;
+                    for (int k = 0; k < 3; ++k) {
+                        lo[k] = std::min(lo[k], pos[k]);
+                        hi[k] = std::max(hi[k], pos[k]);
+                    }
+                    power += weights[static_cast<size_t>(local[i])];
+                }
+                const int node = static_cast<int>(nodes.size());
+                nodes.push_back(DevLightNode{{lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}, power, -1, -1, -1});
+                if (end - begin == 1) {
+                    nodes[static_cast<size_t>(node)].light_index = local[begin];
+                    return node;
+                }
+                const float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+                const int axis = ex >= ey && ex >= ez ? 0 : (ey >= ez ? 1 : 2);
+                const size_t middle = begin + (end - begin) / 2;
+                std::nth_element(local.begin() + static_cast<std::ptrdiff_t>(begin),
+                                 local.begin() + static_cast<std::ptrdiff_t>(middle),
+                                 local.begin() + static_cast<std::ptrdiff_t>(end), [&](int a, int b) {
+                                     return desc->analytic[a].position[axis] < desc->analytic[b].position[axis];
+                                 });
+                const int left = build(begin, middle);
+                const int right = build(middle, end);
+                nodes[static_cast<size_t>(node)].left = left;
+                nodes[static_cast<size_t>(node)].right = right;
+                return node;
+            };
+            d.analytic_tree_root = build(0, local.size());
+            d.analytic_tree = A.Upload(nodes);
+        }
     }
 
     // Camera and settings.

@@ -622,6 +622,109 @@ __device__ __forceinline__ void PushShadow(Queues& q, V3 o, V3 d, float tmax, in
 
 }  // namespace
 
+// --------------------------------------------------------- analytic lights
+
+struct AnalyticSample {
+    V3 wi, radiance;
+    float distance, selection_pdf;
+    bool valid;
+};
+
+// DistanceSquaredToBounds / TreeImportance
+// (src/lighting/analytic_light_sampling.cpp:8-20).
+__device__ __forceinline__ float StdMax3(float a, float b, float c) {
+    float r = a;
+    if (r < b) r = b;
+    if (r < c) r = c;
+    return r;
+}
+__device__ inline float TreeImportance(const DevLightNode& n, V3 p) {
+    const float dx = StdMax3(n.lo[0] - p.x, 0.0f, p.x - n.hi[0]);
+    const float dy = StdMax3(n.lo[1] - p.y, 0.0f, p.y - n.hi[1]);
+    const float dz = StdMax3(n.lo[2] - p.z, 0.0f, p.z - n.hi[2]);
+    const float d2 = dx * dx + dy * dy + dz * dz;
+    return n.power / fmaxf(1.0e-4f, d2);
+}
+
+// SampleAnalyticLight (src/lighting/analytic_light_sampling.cpp:22-142):
+// the light chosen by the tree walk (power over distance), else the power
+// alias table, else uniformly; then the point / spot / distant sample.
+__device__ inline AnalyticSample SampleAnalytic(const DevScene& sc, V3 p, float select) {
+    AnalyticSample out{{0, 0, 0}, {0, 0, 0}, 0.0f, 0.0f, false};
+    int light = -1;
+    float pdf = 1.0f;
+    float u = select < 0.0f ? 0.0f : (0.99999994f < select ? 0.99999994f : select);
+    if (sc.analytic_tree_root >= 0) {
+        int node = sc.analytic_tree_root;
+        for (int guard = 0; node >= 0 && guard < 64; ++guard) {
+            const DevLightNode& n = sc.analytic_tree[node];
+            if (n.light_index >= 0) {
+                light = n.light_index;
+                break;
+            }
+            if (n.left < 0 || n.right < 0) return out;
+            const float lw = TreeImportance(sc.analytic_tree[n.left], p);
+            const float rw = TreeImportance(sc.analytic_tree[n.right], p);
+            const float total = lw + rw;
+            const float lp = total > 0.0f ? lw / total : 0.5f;
+            if (u < lp) {
+                pdf *= lp;
+                u = lp > 0.0f ? u / lp : 0.0f;
+                node = n.left;
+            } else {
+                const float rp = 1.0f - lp;
+                pdf *= rp;
+                u = rp > 0.0f ? (u - lp) / rp : 0.0f;
+                node = n.right;
+            }
+        }
+    } else if (sc.analytic_alias_pmf) {
+        float r;
+        light = SampleAlias(sc.analytic_alias_prob, sc.analytic_alias_index, sc.analytic_alias_pmf, sc.analytic_count,
+                            u, pdf, r);
+    } else {
+        light = min(static_cast<int>(u * static_cast<float>(sc.analytic_count)), sc.analytic_count - 1);
+        pdf = 1.0f / static_cast<float>(sc.analytic_count);
+    }
+    if (light < 0 || light >= sc.analytic_count || pdf <= 0.0f) return out;
+    const DevAnalytic& l = sc.analytic[light];
+    const V3 intensity = Ld3(l.intensity);
+    if (l.kind == 2) {  // distant
+        const V3 to_light = -Ld3(l.direction);
+        if (LengthSq(to_light) == 0.0f) return out;
+        out.wi = Normalize(to_light);
+        out.distance = 1.0e6f;
+        out.radiance = intensity;
+    } else {
+        const V3 delta = Ld3(l.position) - p;
+        const float dsq = Dot(delta, delta);
+        if (dsq <= 0.0f) return out;
+        const float dist = sqrtf(dsq);
+        if (l.kind == 0) {  // point
+            out.wi = Normalize(delta);
+            out.radiance = intensity / dsq;
+        } else {  // spot
+            const V3 wi = delta / dist;
+            const V3 ld = Ld3(l.direction);
+            const V3 axis = LengthSq(ld) > 0.0f ? Normalize(ld) : V3{0.0f, 0.0f, 1.0f};
+            const float cc = -Dot(wi, axis);
+            float falloff = 0.0f;
+            if (cc >= l.cone_cos_inner) {
+                falloff = 1.0f;
+            } else if (cc > l.cone_angle) {
+                const float t = (cc - l.cone_angle) / (l.cone_cos_inner - l.cone_angle);
+                falloff = t * t * (3.0f - 2.0f * t);
+            }
+            out.wi = wi;
+            out.radiance = intensity * (falloff / dsq);
+        }
+        out.distance = dist;
+    }
+    out.valid = true;
+    out.selection_pdf = pdf;
+    return out;
+}
+
 // EstimateDirectLight (src/integrators/path_direct_lighting.cpp:170-283) with
 // visibility deferred: draws the light samples of vertex p (normal n, towards
 // the viewer wo), stores each contribution without visibility in the path's
@@ -666,6 +769,22 @@ __device__ inline void NextEvent(const DevScene& sc, PathState& ps, Queues& q, i
                             }
                         }
                     }
+                }
+            }
+        }
+    }
+    if (sc.analytic_count > 0) {  // delta lights: no MIS against the BSDF
+        const AnalyticSample as = SampleAnalytic(sc, p, smp.Sample1D(kDimAnalyticLightSelect, depth));
+        if (as.valid && as.selection_pdf > 0.0f && !IsBlack(as.radiance)) {
+            const float cs = fmaxf(0.0f, Dot(n, as.wi));
+            if (cs > 0.0f) {
+                const V3 f = EvalBsdf(m, wo, as.wi, n, rng);
+                if (!IsBlack(f)) {
+                    CountStat(q.counters, kStatShadow);
+                    const float sb = SurfaceBias(p);
+                    ps.nee[3 * path + 1] = ToF4(Mul(f, as.radiance) * (cs / as.selection_pdf));
+                    PushShadow(q, p + n * sb, as.wi, as.distance - sb, 3 * path + 1);
+                    any = true;
                 }
             }
         }

@@ -79,6 +79,13 @@ struct DevAnalytic {
     float cone_cos_inner;
 };
 
+// LightTreeNode (include/yaoray/scene/light.hpp:53-59).
+struct DevLightNode {
+    float lo[3], hi[3];
+    float power;
+    int32_t left, right, light_index;
+};
+
 struct DevMeasuredBrdf;  // measured.cuh
 
 struct DevScene {
@@ -123,7 +130,9 @@ struct DevScene {
     const DevAnalytic* analytic;
     const float* analytic_alias_prob;
     const int32_t* analytic_alias_index;
-    const float* analytic_alias_pmf;
+    const float* analytic_alias_pmf;   // null: uniform selection
+    const DevLightNode* analytic_tree;  // power/distance tree (more than 8 lights, none distant)
+    int32_t analytic_tree_root;         // -1: no tree
     // environment
     DevEnvironment env;
     // subsurface

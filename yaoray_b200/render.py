@@ -52,6 +52,9 @@ MATERIAL_DTYPE = np.dtype([("kind", "<i4"), ("reflectance", "<f4", 3), ("eta", "
 assert MATERIAL_DTYPE.itemsize == C.sizeof(Material)
 
 EMISSIVE_DTYPE = np.dtype([("primitive_index", "<i4"), ("radiance", "<f4", 3), ("area", "<f4")])
+# AnalyticLight (include/yaoray/scene/light.hpp:38-45); kind 0 point, 1 spot, 2 distant.
+ANALYTIC_DTYPE = np.dtype([("kind", "<i4"), ("position", "<f4", 3), ("direction", "<f4", 3), ("intensity", "<f4", 3),
+                           ("cone_angle", "<f4"), ("cone_cos_inner", "<f4")])
 FILM_PIXEL_DTYPE = np.dtype([("sum", "<f4", 3), ("samples", "<u4"), ("luminance_mean", "<f4"),
                              ("luminance_m2", "<f4"), ("albedo_sum", "<f4", 3), ("normal_sum", "<f4", 3),
                              ("depth_sum", "<f4"), ("aov_samples", "<u4")])
@@ -287,6 +290,7 @@ class RenderScene:
     tangents: np.ndarray | None = None         # (V, 4) RenderVertex::tangent xyz + tangent_handedness
     textures: list = field(default_factory=list)  # texture.Texture, by material texture index
     measured: list = field(default_factory=list)  # measured.MeasuredBrdf, by material measured_index
+    analytic: np.ndarray = field(default_factory=lambda: np.zeros(0, ANALYTIC_DTYPE))  # point/spot/distant lights
 
     def emissive_power_alias(self):
         """The alias table PrepareLightSampling builds (emissive power = area * luminance)."""
@@ -367,6 +371,11 @@ class PreparedScene:
             self._keep += [marr, mkeep]
             d.measured = C.addressof(marr)
             d.measured_count = len(scene.measured)
+        if scene.analytic.size:
+            an = np.ascontiguousarray(scene.analytic, ANALYTIC_DTYPE)
+            self._keep.append(an)
+            d.analytic = ptr(an)
+            d.analytic_count = an.size  # the power alias table is built by the library
         mats = np.ascontiguousarray(scene.materials, MATERIAL_DTYPE)
         em = np.ascontiguousarray(scene.emissive, EMISSIVE_DTYPE)
         self._keep += [mats, em]
