@@ -631,7 +631,7 @@ typedef struct yrc_scene_desc {
     yrc_alias_table emissive_power;
     const yrc_analytic_light* analytic;
     int32_t analytic_count;
-    yrc_alias_table analytic_power;
+    yrc_alias_table analytic_power; /* count 0: built by the library from the lights' power */
     yrc_environment environment;
     const yrc_bssrdf_table* bssrdf_tables;
     int32_t bssrdf_count;
