@@ -238,7 +238,7 @@ __device__ __forceinline__ float MeasuredPhi2U(float p) { return p * (1.0f / (2.
 __device__ __forceinline__ float ClampUnit(float v) { return v < -1.0f ? -1.0f : (v > 1.0f ? 1.0f : v); }
 
 // EvaluateMeasured (bsdf_measured.cpp:10-61).
-__device__ inline V3 EvalMeasured(const DevMeasuredBrdf& m, V3 wo, V3 wi, V3 n) {
+static __device__ __noinline__ V3 EvalMeasured(const DevMeasuredBrdf& m, V3 wo, V3 wi, V3 n) {
     const MeasuredFrame f = MakeMeasuredFrame(n);
     V3 lwo = ToLocal(f, wo), lwi = ToLocal(f, wi);
     if (lwo.z * lwi.z <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
@@ -273,7 +273,7 @@ __device__ inline V3 EvalMeasured(const DevMeasuredBrdf& m, V3 wo, V3 wi, V3 n) 
 }
 
 // PdfMeasured (bsdf_measured.cpp:177-238).
-__device__ inline float PdfMeasuredBrdf(const DevMeasuredBrdf& m, V3 wo, V3 wi, V3 n) {
+static __device__ __noinline__ float PdfMeasuredBrdf(const DevMeasuredBrdf& m, V3 wo, V3 wi, V3 n) {
     const MeasuredFrame f = MakeMeasuredFrame(n);
     V3 lwo = ToLocal(f, wo), lwi = ToLocal(f, wi);
     if (lwo.z * lwi.z <= 0.0f) return 0.0f;
@@ -297,8 +297,10 @@ __device__ inline float PdfMeasuredBrdf(const DevMeasuredBrdf& m, V3 wo, V3 wi, 
     return jac > 0.0f ? ui.pdf * lum / jac : 0.0f;
 }
 
-// SampleMeasured (bsdf_measured.cpp:67-128).
-__device__ inline BsdfSample SampleMeasuredBrdf(const DevMeasuredBrdf& m, V3 wo, V3 n, float sx, float sy) {
+// SampleMeasured (bsdf_measured.cpp:67-128). The three entry points are not
+// inlined, so that the generic shading class carries their registers only
+// inside the call.
+static __device__ __noinline__ BsdfSample SampleMeasuredBrdf(const DevMeasuredBrdf& m, V3 wo, V3 n, float sx, float sy) {
     const MeasuredFrame f = MakeMeasuredFrame(n);
     V3 lwo = ToLocal(f, wo);
     const bool flip = lwo.z <= 0.0f;

@@ -649,7 +649,21 @@ __device__ inline float TreeImportance(const DevLightNode& n, V3 p) {
 // SampleAnalyticLight (src/lighting/analytic_light_sampling.cpp:22-142):
 // the light chosen by the tree walk (power over distance), else the power
 // alias table, else uniformly; then the point / spot / distant sample.
-__device__ inline AnalyticSample SampleAnalytic(const DevScene& sc, V3 p, float select) {
+// Not inlined, and given pointers rather than the scene, so that the shade
+// kernels do not carry its registers when a scene has no analytic lights.
+__device__ __noinline__ AnalyticSample SampleAnalyticLight(const DevAnalytic* analytic, int32_t analytic_count,
+                                                           const float* alias_prob, const int32_t* alias_index,
+                                                           const float* alias_pmf, const DevLightNode* tree,
+                                                           int32_t tree_root, V3 p, float select) {
+    struct {
+        const DevAnalytic* analytic;
+        int32_t analytic_count;
+        const float* analytic_alias_prob;
+        const int32_t* analytic_alias_index;
+        const float* analytic_alias_pmf;
+        const DevLightNode* analytic_tree;
+        int32_t analytic_tree_root;
+    } sc{analytic, analytic_count, alias_prob, alias_index, alias_pmf, tree, tree_root};
     AnalyticSample out{{0, 0, 0}, {0, 0, 0}, 0.0f, 0.0f, false};
     int light = -1;
     float pdf = 1.0f;
@@ -774,7 +788,10 @@ __device__ inline void NextEvent(const DevScene& sc, PathState& ps, Queues& q, i
         }
     }
     if (sc.analytic_count > 0) {  // delta lights: no MIS against the BSDF
-        const AnalyticSample as = SampleAnalytic(sc, p, smp.Sample1D(kDimAnalyticLightSelect, depth));
+        const AnalyticSample as = SampleAnalyticLight(sc.analytic, sc.analytic_count, sc.analytic_alias_prob,
+                                                      sc.analytic_alias_index, sc.analytic_alias_pmf,
+                                                      sc.analytic_tree, sc.analytic_tree_root, p,
+                                                      smp.Sample1D(kDimAnalyticLightSelect, depth));
         if (as.valid && as.selection_pdf > 0.0f && !IsBlack(as.radiance)) {
             const float cs = fmaxf(0.0f, Dot(n, as.wi));
             if (cs > 0.0f) {
