@@ -10,8 +10,8 @@ BuildTextureMipChain. Inputs are small seeded
 cases; each file stores inputs and expected outputs so the CPU tests can pin
 the oracle restatement without the reference present.
 
-Run: python tests/golden/make_golden.py [texture]   (needs oracle/_ref built;
-`texture` writes only texture.npz)
+Run: python tests/golden/make_golden.py [texture|measured]   (needs oracle/_ref
+built; `texture` / `measured` write only that fixture)
 """
 from __future__ import annotations
 
@@ -200,6 +200,7 @@ def main() -> None:
     np.savez_compressed(HERE / "camera_film.npz", camera=cam, pixels=px, samples=sm, rays=cam_rays, film_samples=s,
                         film_w=w, film_h=h, film_pixels=film.view(np.uint8), film_bad=np.int64(nbad))
     texture_fixture()
+    measured_fixture()
     print("golden fixtures written to", HERE)
 
 
@@ -234,8 +235,31 @@ def texture_fixture() -> None:
     np.savez_compressed(HERE / "texture.npz", **fx)
 
 
+def measured_fixture() -> None:
+    """8. Measured BRDF: EvaluateMeasured / PdfMeasured / SampleMeasured of
+    the seeded synthetic RGL-layout BRDF (yaoray_b200.measured.synthetic_brdf
+    seed 5, rebuilt from its seed by the tests) on seeded directions."""
+    from yaoray_b200 import measured as M
+
+    rng = np.random.default_rng(0xB8DF)
+    brdf = M.synthetic_brdf(5)
+    n = 4000
+    nrm = rng.normal(size=(n, 3))
+    nrm = (nrm / np.linalg.norm(nrm, axis=1, keepdims=True)).astype(np.float32)
+    wo = nrm * rng.uniform(0.05, 1.0, (n, 1)) + rng.normal(size=(n, 3)) * 0.6
+    wo = (wo / np.linalg.norm(wo, axis=1, keepdims=True)).astype(np.float32)
+    wi = nrm * rng.uniform(-0.2, 1.0, (n, 1)) + rng.normal(size=(n, 3)) * 0.6
+    wi = (wi / np.linalg.norm(wi, axis=1, keepdims=True)).astype(np.float32)
+    u = rng.random((n, 2)).astype(np.float32)
+    f, pdf = oracle.ref_measured_eval(brdf, wo, wi, nrm)
+    smp = oracle.ref_measured_sample(brdf, wo, nrm, u)
+    np.savez_compressed(HERE / "measured.npz", seed=np.int64(5), wo=wo, wi=wi, n=nrm, u=u, f=f, pdf=pdf, sample=smp)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["texture"]:
         texture_fixture()
+    elif sys.argv[1:] == ["measured"]:
+        measured_fixture()
     else:
         main()

@@ -107,3 +107,24 @@ def test_measured_rejects_anisotropic_tensors():
     b.spectra = np.repeat(b.spectra, 3, axis=0)
     with pytest.raises(YrcError, match="anisotropic"):
         M.evaluate(b, np.zeros((1, 3)), np.zeros((1, 3)), np.zeros((1, 3)))
+
+
+@pytest.mark.gpu
+def test_measured_matches_reference_golden(cuda):
+    """The same comparison against outputs of the reference committed in
+    tests/golden/measured.npz (needs no reference build)."""
+    from pathlib import Path
+
+    f = dict(np.load(Path(__file__).resolve().parent / "golden" / "measured.npz"))
+    brdf = M.synthetic_brdf(int(f["seed"]))
+    fv, pdf = M.evaluate(brdf, f["wo"], f["wi"], f["n"])
+    assert np.array_equal(fv > 0, f["f"] > 0) and np.array_equal(pdf > 0, f["pdf"] > 0)
+    assert np.allclose(fv, f["f"], rtol=1e-3, atol=1e-6 * f["f"].max())
+    assert np.allclose(pdf, f["pdf"], rtol=1e-3, atol=1e-6 * f["pdf"].max())
+    got = M.sample(brdf, f["wo"], f["n"], f["u"])
+    want = f["sample"]
+    both = (got[:, 7] > 0) & (want[:, 7] > 0)
+    assert np.mean((got[:, 7] > 0) == (want[:, 7] > 0)) > 0.999
+    assert np.allclose(got[both, :3], want[both, :3], atol=2e-4)
+    rel = np.abs(got[both, 6] - want[both, 6]) / want[both, 6]
+    assert np.mean(rel <= 1e-3) >= 0.99 and np.median(rel) < 1e-5
