@@ -79,3 +79,22 @@ def test_shared_launch_rejects_bad_groups():
     finally:
         p0.close()
         p1.close()
+
+
+def test_shared_launch_renders_every_scene_kind():
+    """The stages that only some scenes need (texture stage, cut-out skip
+    loop, exact shadow loop, measured BRDFs, analytic lights with the light
+    tree) inside one shared launch: films equal one-at-a-time renders."""
+    from yaoray_b200 import cornell
+    from yaoray_b200.render import CudaBackend
+
+    scenes = [cornell.textured_scene(48, 48, 8, 6), cornell.cutout_scene(48, 48, 8, 6),
+              cornell.instanced_cutout_scene(48, 48, 8, 6), cornell.measured_scene(48, 48, 8, 6),
+              cornell.analytic_scene(48, 48, 8, 6, many=True), cornell.scene(48, 48, 8, 6)]
+    b = CudaBackend()
+    prepared = [b.prepare(s) for s in scenes]
+    singles = [b.render(p) for p in prepared]
+    many = b.render_many(prepared)
+    for k, (one, shared) in enumerate(zip(singles, many)):
+        assert one.ok and shared.ok, (k, one.error, shared.error)
+        assert shared.film.tobytes() == one.film.tobytes(), k
