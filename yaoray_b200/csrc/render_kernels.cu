@@ -865,7 +865,7 @@ __device__ constexpr int32_t ClassKind() {
 // the final shading normal, w = 1; other entries get w = 0. Kept apart from
 // the shade kernels so that their register budget does not carry the
 // texture filters.
-__global__ void __launch_bounds__(256) SurfaceTextureKernel(DevScene sc, PathState ps, Queues q, int depth) {
+__global__ void __launch_bounds__(256, 4) SurfaceTextureKernel(DevScene sc, PathState ps, Queues q, int depth) {
     const int64_t n = static_cast<int64_t>(q.counters[kCtrIn]);
     for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
          e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
