@@ -6,7 +6,8 @@
     result = backend.render(prepared, request)    # RenderBackend::Render(PreparedScene, RenderRequest)
 
 `RenderScene` holds a RenderSceneIR + RenderSettings as numpy arrays (the
-same fields the reference's IR carries for untextured scenes). Errors come
+reference IR's fields, textures, measured BRDFs and analytic lights
+included). Errors come
 back as `RenderResult(ok=False, error=...)` like the reference's result
 structs; programming errors raise `YrcError`.
 """
