@@ -38,3 +38,34 @@ def test_reference_cli_path_with_cuda_backend(cuda, tmp_path):
     assert abs(g.mean() / c.mean() - 1) < 0.01
     assert info["cuda_progress_calls"] == 32
     assert abs(info["cuda_rays"] / info["cpu_rays"] - 1) < 0.02
+
+
+def test_reference_cli_path_textured_scene(cuda, tmp_path):
+    """Image-map textures through the reference's own frontend (TGA loading,
+    sRGB decoding, uvs from "point2 uv") and the drop-in adapter's texture
+    and uv marshalling: the floor bilinear, the back wall with the
+    frontend's default EWA filter."""
+    if not DRIVER.exists():
+        pytest.skip("drop-in driver not built (needs the reference sources)")
+    rng = np.random.default_rng(4)
+    y, x = np.mgrid[0:32, 0:32]
+    checks = np.where((((x // 4) + (y // 4)) % 2 == 0)[..., None], [230, 220, 200], [40, 60, 120]).astype(np.uint8)
+    cornell.write_tga(tmp_path / "floor.tga", checks)
+    cornell.write_tga(tmp_path / "wall.tga", rng.integers(60, 250, (24, 40, 3)).astype(np.uint8))
+    scene = tmp_path / "textured.pbrt"
+    scene.write_text(cornell.pbrt_text_textured(80, 64, 32, 8, "floor.tga", "wall.tga"))
+    out = subprocess.run([str(DRIVER), str(scene), str(tmp_path / "r")], capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr
+    cpu = np.fromfile(tmp_path / "r.cpu.film", FILM_PIXEL_DTYPE)
+    gpu = np.fromfile(tmp_path / "r.cuda.film", FILM_PIXEL_DTYPE)
+    assert np.array_equal(cpu["samples"], gpu["samples"])
+    for k in ("normal_sum", "depth_sum", "aov_samples"):
+        assert cpu[k].tobytes() == gpu[k].tobytes(), k
+    a, b = gpu["albedo_sum"], cpu["albedo_sum"]
+    assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
+    assert np.mean(np.all(a.view(np.uint32) == b.view(np.uint32), axis=-1)) >= 0.99
+    assert len(np.unique(b.round(3), axis=0)) > 50  # the textures are visible in the albedo
+    c = cpu["sum"] / cpu["samples"][:, None]
+    g = gpu["sum"] / gpu["samples"][:, None]
+    assert abs(g.mean() / c.mean() - 1) < 0.01

@@ -383,3 +383,35 @@ def analytic_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth
         a[2] = (2, (0, 0, 0), (0.2, -1.0, 0.6), (0.6, 0.55, 0.5), 0.0, 0.0)
     s.analytic = a
     return s
+
+
+def write_tga(path, rgb: np.ndarray) -> None:
+    """Writes an (h, w, 3) uint8 image as an uncompressed 24-bit TGA, top row
+    first."""
+    h, w, _ = rgb.shape
+    header = bytes([0, 0, 2, 0, 0, 0, 0, 0, 0, 0, 0, 0, w & 255, w >> 8, h & 255, h >> 8, 24, 0x20])
+    with open(path, "wb") as f:
+        f.write(header + np.ascontiguousarray(rgb[..., ::-1], np.uint8).tobytes())
+
+
+def pbrt_text_textured(width: int, height: int, spp: int, max_depth: int, floor_tex: str, wall_tex: str) -> str:
+    """pbrt_text() with image-map textures: the floor's reflectance from
+    `floor_tex` (bilinear) and the back wall's from `wall_tex` (the
+    frontend's default EWA filter), both with uvs spanning 3 repeats."""
+    lines = pbrt_text(width, height, spp, max_depth).splitlines()
+    world = lines.index("WorldBegin")
+    tex = [f'Texture "floorimg" "spectrum" "imagemap" "string filename" ["{floor_tex}"] "string filter" ["bilinear"]',
+           f'Texture "wallimg" "spectrum" "imagemap" "string filename" ["{wall_tex}"]',
+           'MakeNamedMaterial "floortex" "string type" ["diffuse"] "texture reflectance" ["floorimg"]',
+           'MakeNamedMaterial "walltex" "string type" ["diffuse"] "texture reflectance" ["wallimg"]']
+    out = lines[:world + 1] + tex
+    shape = 0
+    for line in lines[world + 1:]:
+        if line.startswith('NamedMaterial "white"') and shape in (0, 2):
+            line = 'NamedMaterial "floortex"' if shape == 0 else 'NamedMaterial "walltex"'
+        if line.startswith('Shape "trianglemesh"'):
+            if shape in (0, 2):
+                line += ' "point2 uv" [0 0 3 0 3 3 0 3]'
+            shape += 1
+        out.append(line)
+    return "\n".join(out) + "\n"
