@@ -69,3 +69,32 @@ def test_reference_cli_path_textured_scene(cuda, tmp_path):
     c = cpu["sum"] / cpu["samples"][:, None]
     g = gpu["sum"] / gpu["samples"][:, None]
     assert abs(g.mean() / c.mean() - 1) < 0.01
+
+
+def test_reference_cli_path_analytic_lights(cuda, tmp_path):
+    """Point, spot and distant LightSources compiled by the reference's
+    frontend and passed through the adapter (the library builds their power
+    alias table), next to the box's area light."""
+    if not DRIVER.exists():
+        pytest.skip("drop-in driver not built (needs the reference sources)")
+    lines = cornell.pbrt_text(80, 64, 32, 8).splitlines()
+    world = lines.index("WorldBegin")
+    lights = ['LightSource "point" "rgb I" [3 2.5 2] "point3 from" [1.2 4.5 2.0]',
+              'LightSource "spot" "rgb I" [8 8 10] "point3 from" [4.0 5.0 3.5] "point3 to" [3.5 0 3.0] '
+              '"float coneangle" [30] "float conedeltaangle" [8]',
+              'LightSource "distant" "rgb L" [0.4 0.4 0.35] "point3 from" [0 0 0] "point3 to" [0.2 -1 0.6]']
+    scene = tmp_path / "lights.pbrt"
+    scene.write_text("\n".join(lines[:world + 1] + lights + lines[world + 1:]) + "\n")
+    out = subprocess.run([str(DRIVER), str(scene), str(tmp_path / "r")], capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr
+    info = json.loads(out.stdout.strip().splitlines()[-1])
+    cpu = np.fromfile(tmp_path / "r.cpu.film", FILM_PIXEL_DTYPE)
+    gpu = np.fromfile(tmp_path / "r.cuda.film", FILM_PIXEL_DTYPE)
+    assert np.array_equal(cpu["samples"], gpu["samples"])
+    for k in ("albedo_sum", "normal_sum", "depth_sum", "aov_samples"):
+        assert cpu[k].tobytes() == gpu[k].tobytes(), k
+    c = cpu["sum"] / cpu["samples"][:, None]
+    g = gpu["sum"] / gpu["samples"][:, None]
+    assert abs(g.mean() / c.mean() - 1) < 0.01
+    assert abs(info["cuda_rays"] / info["cpu_rays"] - 1) < 0.02
