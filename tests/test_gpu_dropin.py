@@ -98,3 +98,38 @@ def test_reference_cli_path_analytic_lights(cuda, tmp_path):
     g = gpu["sum"] / gpu["samples"][:, None]
     assert abs(g.mean() / c.mean() - 1) < 0.01
     assert abs(info["cuda_rays"] / info["cpu_rays"] - 1) < 0.02
+
+
+def test_reference_cli_path_measured_material(cuda, tmp_path):
+    """A measured material read by the reference's loader from an RGL
+    tensor file (the seeded synthetic BRDF written by
+    measured.write_tensor_file) on both boxes, passed through the adapter's
+    measured-BRDF marshalling."""
+    if not DRIVER.exists():
+        pytest.skip("drop-in driver not built (needs the reference sources)")
+    from yaoray_b200 import measured
+
+    measured.write_tensor_file(tmp_path / "synthetic.bsdf", measured.synthetic_brdf(3))
+    lines = cornell.pbrt_text(80, 64, 32, 8).splitlines()
+    world = lines.index("WorldBegin")
+    out_lines = lines[:world + 1] + ['MakeNamedMaterial "meas" "string type" ["measured"] '
+                                     '"string filename" ["synthetic.bsdf"]']
+    shape = 0
+    for line in lines[world + 1:]:
+        if line.startswith('NamedMaterial "white"') and shape in (5, 6):
+            line = 'NamedMaterial "meas"'
+        if line.startswith('Shape "trianglemesh"'):
+            shape += 1
+        out_lines.append(line)
+    scene = tmp_path / "measured.pbrt"
+    scene.write_text("\n".join(out_lines) + "\n")
+    out = subprocess.run([str(DRIVER), str(scene), str(tmp_path / "r")], capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr
+    cpu = np.fromfile(tmp_path / "r.cpu.film", FILM_PIXEL_DTYPE)
+    gpu = np.fromfile(tmp_path / "r.cuda.film", FILM_PIXEL_DTYPE)
+    for k in ("normal_sum", "depth_sum", "aov_samples"):
+        assert cpu[k].tobytes() == gpu[k].tobytes(), k
+    c = cpu["sum"] / cpu["samples"][:, None]
+    g = gpu["sum"] / gpu["samples"][:, None]
+    assert abs(g.mean() / c.mean() - 1) < 0.01

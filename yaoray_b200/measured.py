@@ -97,3 +97,25 @@ def synthetic_brdf(seed: int = 0, n_theta_i: int = 6, res: int = 16, wavelengths
             tint = 0.3 + 0.6 * np.exp(-((w - 600.0) / 120.0) ** 2)
             spec[0, k, j] = lum[0, k] * tint * (1.0 + 0.1 * rng.random((res, res)))
     return MeasuredBrdf(th, phi, wl, ndf, sigma, vndf, lum, spec)
+
+
+def write_tensor_file(path, brdf: MeasuredBrdf) -> None:
+    """Saves `brdf` as an RGL .bsdf file in the Mitsuba tensor-file layout
+    (the format the reference's LoadMeasuredBrdf reads): magic
+    "tensor_file\\0", version 1.0, the field count, then per field its name,
+    rank, dtype (10 = float32), absolute data offset and shape, followed by
+    the little-endian data."""
+    import struct
+
+    fields = [(k, np.ascontiguousarray(getattr(brdf, k), np.float32))
+              for k in ("theta_i", "phi_i", "wavelengths", "ndf", "sigma", "vndf", "luminance", "spectra")]
+    header = b"tensor_file\0" + bytes([1, 0]) + struct.pack("<I", len(fields))
+    size = len(header) + sum(2 + len(k) + 2 + 1 + 8 + 8 * a.ndim for k, a in fields)
+    descs, blobs, offset = b"", b"", size
+    for k, a in fields:
+        descs += struct.pack("<H", len(k)) + k.encode() + struct.pack("<HBQ", a.ndim, 10, offset)
+        descs += b"".join(struct.pack("<Q", d) for d in a.shape)
+        blobs += a.tobytes()
+        offset += a.nbytes
+    with open(path, "wb") as f:
+        f.write(header + descs + blobs)
