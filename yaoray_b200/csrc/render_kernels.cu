@@ -1380,29 +1380,57 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
 
 // Adds each path's visible next-event contributions:
 // radiance += throughput_at_vertex * ((emissive + analytic) + environment).
+// Each thread resolves kNeePerThread entries (e, e + stride, ...) with all
+// of their paths' loads issued before any store: the accesses follow the
+// shading order through the path state, so the kernel waits on latency, and
+// independent paths per thread multiply the loads in flight.
+constexpr int kNeePerThread = 2;
+
 template <bool kTransmittance>
 __global__ void NeeResolveKernel(PathState ps, Queues q, const float4* transmittance) {
     const int64_t count = static_cast<int64_t>(q.counters[kCtrNee]);
-    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < count;
-         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int32_t path = q.nee_paths[e];
-        V3 sum{0.0f, 0.0f, 0.0f};
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t e0 = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e0 < count;
+         e0 += kNeePerThread * stride) {
+        int32_t path[kNeePerThread];
+        bool live[kNeePerThread];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const int32_t slot = 3 * path + k;
-            const V3 c = F4(ps.nee[slot]);
-            V3 vis{0.0f, 0.0f, 0.0f};
-            if (kTransmittance) {
-                vis = F4(transmittance[slot]);
-            } else {
-                vis = q.shadow_occluded[slot] ? V3{0, 0, 0} : V3{1, 1, 1};
-            }
-            sum = sum + Mul(c, vis);
-            ps.nee[slot] = make_float4(0, 0, 0, 0);
+        for (int j = 0; j < kNeePerThread; ++j) {
+            const int64_t e = e0 + j * stride;
+            live[j] = e < count;
+            path[j] = live[j] ? q.nee_paths[e] : q.nee_paths[e0];
         }
-        const V3 tp = F4(ps.nee_tp[path]);
-        ps.radiance[path] = ToF4(F4(ps.radiance[path]) + Mul(tp, sum));
-        ps.flags[path] &= ~kPathNee;
+        float4 c[kNeePerThread][3], vis[kNeePerThread][3], tp[kNeePerThread], rad[kNeePerThread];
+        uint32_t fl[kNeePerThread];
+#pragma unroll
+        for (int j = 0; j < kNeePerThread; ++j) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int32_t slot = 3 * path[j] + k;
+                c[j][k] = ps.nee[slot];
+                if (kTransmittance) {
+                    vis[j][k] = transmittance[slot];
+                } else {
+                    const float v = q.shadow_occluded[slot] ? 0.0f : 1.0f;
+                    vis[j][k] = make_float4(v, v, v, 0.0f);
+                }
+            }
+            tp[j] = ps.nee_tp[path[j]];
+            rad[j] = ps.radiance[path[j]];
+            fl[j] = ps.flags[path[j]];
+        }
+#pragma unroll
+        for (int j = 0; j < kNeePerThread; ++j) {
+            if (!live[j]) continue;
+            V3 sum{0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                sum = sum + Mul(F4(c[j][k]), F4(vis[j][k]));
+                ps.nee[3 * path[j] + k] = make_float4(0, 0, 0, 0);
+            }
+            ps.radiance[path[j]] = ToF4(F4(rad[j]) + Mul(F4(tp[j]), sum));
+            ps.flags[path[j]] = fl[j] & ~kPathNee;
+        }
     }
 }
 
