@@ -314,9 +314,14 @@ yrc_status yrc_trace_stats_device(yrc_accel* accel, const yrc_ray* rays, int64_t
  *
  * - count above YRC_NOALLOC_STATS_MAX_RAYS returns YRC_ERR_INVALID_ARGUMENT
  *   before any work is queued; split larger batches.
- * - The first call on each device looks up the scratch array's device address
- *   (with that device current) and caches it. Make that first call before any
- *   stream capture begins.
+ * - The scratch array's device address is looked up (with the device current)
+ *   and cached when an accelerator is created on that device, and the
+ *   statistics kernels this accelerator uses are loaded then too. Under lazy
+ *   module loading (the CUDA 12 default) both steps take device memory, so
+ *   create the accelerator before the caller reserves its pool; later calls
+ *   on it allocate nothing. Should the lookup have failed at creation, the
+ *   first call retries it (and that retry may allocate): make the first call
+ *   before any stream capture begins.
  * - All calls on one device share the scratch array, which keeps whatever the
  *   last call left there. The part that must start at zero (the ray-refill
  *   counter) is reset on `stream` before each launch; the rest is write-only.

@@ -19,7 +19,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libyaoray_ref.so"
-REFERENCE_SRC = Path(os.environ.get("YAORAY_REFERENCE", "/root/reference"))
+# The reference checkout: $YAORAY_REFERENCE, else "reference" beside the repository root.
+REFERENCE_SRC = Path(os.environ.get("YAORAY_REFERENCE", str(HERE.parent.parent / "reference")))
 
 P, I64, I32, U64 = C.c_void_p, C.c_int64, C.c_int32, C.c_uint64
 
@@ -513,6 +514,7 @@ def _bind_jobs(L):
     L.yrref_job_from_desc.restype = P
     L.yrref_job_from_desc.argtypes = [P]
     L.yrref_job_render.argtypes = [P, C.c_int, C.c_int, P, P, P]
+    L.yrref_job_render_resume.argtypes = [P, C.c_int, C.c_int, P, C.c_int, P, P, P]
     L._jobs_bound = True
     return L
 
@@ -586,8 +588,10 @@ class RefJob:
                                      "absolute_error": st.adaptive_absolute_error,
                                      "confidence": st.adaptive_confidence})
 
-    def render(self, threads: int = 0, spp: int = 0):
-        """CpuBackend render -> (film FILM_PIXEL_DTYPE (H*W), stats dict, seconds)."""
+    def render(self, threads: int = 0, spp: int = 0, resume_film=None, resume_spp: int = 0):
+        """CpuBackend render -> (film FILM_PIXEL_DTYPE (H*W), stats dict, seconds).
+        With `resume_film` (FILM_PIXEL_DTYPE, H x W) the render resumes from it
+        after `resume_spp` passes, and the stats carry converged_pixels."""
         L = _bind_jobs(ref_lib())
         c = np.zeros(11, np.int64)
         L.yrref_job_counts(self.h, c.ctypes.data)
@@ -601,11 +605,18 @@ class RefJob:
         L.yrref_job_lights(self.h, _p(em), _p(np.zeros(na, np.float32)), _p(np.zeros(na, np.int32)),
                            _p(np.zeros(na, np.float32)), C.addressof(cam), C.addressof(st))
         film = np.zeros(st.width * st.height, FILM_PIXEL_DTYPE)
-        stats = np.zeros(7, np.uint64)
+        stats = np.zeros(8, np.uint64)
         secs = C.c_double()
-        rc = L.yrref_job_render(self.h, threads, spp, film.ctypes.data, stats.ctypes.data, C.byref(secs))
-        if rc != 0:
-            raise RuntimeError(L.yrref_last_error().decode())
         keys = ["samples_rendered", "rays_traced", "shadow_rays", "occluded_shadow_rays", "hits", "misses",
                 "bad_samples"]
+        if resume_film is None:
+            rc = L.yrref_job_render(self.h, threads, spp, film.ctypes.data, stats.ctypes.data, C.byref(secs))
+        else:
+            resume = np.ascontiguousarray(resume_film, FILM_PIXEL_DTYPE).reshape(-1)
+            assert resume.size == film.size
+            rc = L.yrref_job_render_resume(self.h, threads, spp, resume.ctypes.data, resume_spp, film.ctypes.data,
+                                           stats.ctypes.data, C.byref(secs))
+            keys.append("converged_pixels")
+        if rc != 0:
+            raise RuntimeError(L.yrref_last_error().decode())
         return film.reshape(st.height, st.width), dict(zip(keys, map(int, stats))), float(secs.value)

@@ -842,16 +842,15 @@ void* yrref_job_from_desc(const yrc_scene_desc* d) {
     return job;
 }
 
-// Renders the job with the reference CPU backend. film_out: width*height
-// FilmPixel (56 bytes each). stats: samples, rays_traced, shadow_rays,
-// occluded, hits, misses, bad samples (7 uint64). Returns 0 on success.
-int yrref_job_render(void* handle, int threads, int spp_override, void* film_out, std::uint64_t* stats,
-                     double* seconds) {
-    const RefJob& j = *static_cast<RefJob*>(handle);
+namespace {
+
+int RenderJobImpl(const RefJob& j, int threads, int spp_override, const void* resume_film, int resume_spp,
+                  void* film_out, std::uint64_t* stats, int stat_count, double* seconds) {
     yr::RenderJob job{j.ir, j.settings};
     job.settings.requested_backend = yr::RenderBackendKind::Cpu;
     job.settings.threads = threads;
     if (spp_override > 0) job.settings.spp = spp_override;
+    const int width = job.settings.width, height = job.settings.height;
     yr::CpuBackend backend;
     yr::BackendPrepareResult prepared = backend.Prepare(std::move(job));
     if (!prepared.ok) {
@@ -859,6 +858,16 @@ int yrref_job_render(void* handle, int threads, int spp_override, void* film_out
         return 1;
     }
     yr::RenderRequest request;
+    std::unique_ptr<yr::Film> resume;
+    if (resume_film) {
+        resume = std::make_unique<yr::Film>(width, height);
+        const auto* px = static_cast<const yr::FilmPixel*>(resume_film);
+        for (int y = 0; y < height; ++y) {
+            for (int x = 0; x < width; ++x) resume->SetPixelForCheckpoint(x, y, px[y * width + x]);
+        }
+        request.resume_film = resume.get();
+        request.resume_completed_spp = resume_spp;
+    }
     yr::RenderResult result = backend.Render(*prepared.scene, request);
     if (!result.ok || !result.film) {
         g_last_error = result.error;
@@ -866,16 +875,35 @@ int yrref_job_render(void* handle, int threads, int spp_override, void* film_out
     }
     std::memcpy(film_out, result.film->Pixels().data(), result.film->Pixels().size() * sizeof(yr::FilmPixel));
     if (stats) {
-        stats[0] = result.stats.samples_rendered;
-        stats[1] = result.stats.rays_traced;
-        stats[2] = result.stats.shadow_rays;
-        stats[3] = result.stats.occluded_shadow_rays;
-        stats[4] = result.stats.hits;
-        stats[5] = result.stats.misses;
-        stats[6] = result.film->BadSampleCount();
+        const std::uint64_t all[8] = {result.stats.samples_rendered, result.stats.rays_traced,
+                                      result.stats.shadow_rays,      result.stats.occluded_shadow_rays,
+                                      result.stats.hits,             result.stats.misses,
+                                      result.film->BadSampleCount(), result.stats.converged_pixels};
+        for (int k = 0; k < stat_count; ++k) stats[k] = all[k];
     }
     if (seconds) *seconds = result.stats.elapsed_seconds;
     return 0;
+}
+
+}  // namespace
+
+// Renders the job with the reference CPU backend. film_out: width*height
+// FilmPixel (56 bytes each). stats: samples, rays_traced, shadow_rays,
+// occluded, hits, misses, bad samples (7 uint64). Returns 0 on success.
+int yrref_job_render(void* handle, int threads, int spp_override, void* film_out, std::uint64_t* stats,
+                     double* seconds) {
+    return RenderJobImpl(*static_cast<RefJob*>(handle), threads, spp_override, nullptr, 0, film_out, stats, 7,
+                         seconds);
+}
+
+// The same render resumed from `resume_film` (width*height FilmPixel, no bad
+// samples) after `resume_spp` completed passes, as RenderRequest's
+// resume_film / resume_completed_spp do; stats gets an eighth entry, the
+// converged pixels of the last pass (RenderStats::converged_pixels).
+int yrref_job_render_resume(void* handle, int threads, int spp_override, const void* resume_film, int resume_spp,
+                            void* film_out, std::uint64_t* stats, double* seconds) {
+    return RenderJobImpl(*static_cast<RefJob*>(handle), threads, spp_override, resume_film, resume_spp, film_out,
+                         stats, 8, seconds);
 }
 
 // ComputeBeamDiffusionBSSRDF of the reference, for checking the product's

@@ -184,6 +184,41 @@ def test_full_traversal_set_bit_exact(cuda, full_set, kind):
     dev.check()
 
 
+@pytest.fixture(scope="module")
+def live_full_set(ref):
+    """The traversal set's BVH as the compiled reference's own BuildBvh made it."""
+    g = scenes.traversal_scene()
+    rs = ref.RefScene(g)
+    nodes, pi, prims, depth = rs.flat_bvh()
+    return g, rs, RenderBvh(nodes, pi, prims, depth)
+
+
+@pytest.mark.parametrize("kind", ["incoherent", "coherent", "shadow"])
+def test_full_set_against_live_reference(cuda, live_full_set, kind):
+    """Every one of the 7,997,584 rays of a set, traced on the device over the
+    reference's own BVH and by the compiled reference's IntersectBvh
+    (src/accel/bvh_traversal.cpp:253-345) on the host: ids, t, u and v
+    bit-identical and per-ray node and triangle test counts equal; for the
+    shadow set, occlusion equals IntersectBvh(ray, t_min, t_max).hit."""
+    import torch
+
+    g, rs, b = live_full_set
+    rays = {"incoherent": lambda: scenes.incoherent_rays(seed=2), "coherent": lambda: scenes.coherent_rays(),
+            "shadow": lambda: scenes.shadow_rays(seed=3)}[kind]()
+    assert rays.shape[0] == 2828 * 2828
+    exp = rs.trace(rays)
+    dev = accel.DeviceAccelerator(g, b)
+    rd = torch.from_numpy(rays).to(cuda)
+    if kind == "shadow":
+        occ = dev.intersect(rd, any_hit=True).cpu().numpy()
+        assert np.array_equal(occ.astype(bool), exp["hit"].astype(bool))
+    else:
+        check_closest(dev.intersect(rd), None, exp)
+        gst = dev.trace_stats(rd).cpu().numpy()
+        assert np.array_equal(gst[0], exp["node_tests"]) and np.array_equal(gst[1], exp["triangle_tests"])
+    dev.check()
+
+
 def test_full_size_properties(cuda, full_set):
     """At the full 7,997,584-ray size: closest-hit t never exceeds the any-hit
     t_max window when occluded, and any-hit == (closest hit exists)."""

@@ -8,6 +8,11 @@ rays; its per-ray counters must equal the allocating entry point's bit for bit
 reuse one fixed scratch array that keeps the previous call's contents. Batches
 larger than that array are refused before any work is queued.
 
+It also checks the property itself: after the accelerator is created, free
+device memory and the stream-ordered pool's usage stay the same across
+no-allocation calls (the first one included), while the allocating entry point
+does show up in the pool's high-water mark, so the check can see an allocation.
+
 This file is named to be collected last."""
 import ctypes as C
 
@@ -47,6 +52,61 @@ def _compare_two_calls(handle, rays, n, flags):
         got = _counts(L.yrc_trace_stats_device_noalloc, handle, rays, n, flags, sentinel)
         assert np.array_equal(got, want)
     assert L.yrc_accel_check(handle) == _lib.YRC_OK
+
+
+# CUmemPool_attribute values (cuda.h): pool usage as the driver counts it.
+_USED_MEM_CURRENT, _USED_MEM_HIGH = 7, 8
+
+
+def _default_pool():
+    """The current device's default stream-ordered memory pool, through the
+    driver API (libyrcuda links its own CUDA runtime, so torch's allocator
+    statistics would not see its allocations)."""
+    import torch
+
+    cu = C.CDLL("libcuda.so.1")
+    dev = C.c_int()
+    assert cu.cuDeviceGet(C.byref(dev), torch.cuda.current_device()) == 0
+    pool = C.c_void_p()
+    assert cu.cuDeviceGetDefaultMemPool(C.byref(pool), dev) == 0
+    return cu, pool
+
+
+def _pool_attr(cu, pool, attr):
+    v = C.c_uint64()
+    assert cu.cuMemPoolGetAttribute(pool, attr, C.byref(v)) == 0
+    return v.value
+
+
+def test_noalloc_calls_take_no_device_memory(cuda):
+    import torch
+
+    geom = scenes.traversal_scene(seed=3, spheres=16)
+    dev = accel.DeviceAccelerator(geom, accel.build_bvh(geom))
+    n = 65536
+    rays = torch.from_numpy(scenes.incoherent_rays(n, seed=4)).to(cuda)
+    out = torch.full((3, n), -1, dtype=torch.int32, device=cuda)
+    L = _lib.lib()
+    torch.cuda.synchronize()
+    cu, pool = _default_pool()
+    zero = C.c_uint64(0)
+    assert cu.cuMemPoolSetAttribute(pool, _USED_MEM_HIGH, C.byref(zero)) == 0  # restart the high-water mark
+    used0 = _pool_attr(cu, pool, _USED_MEM_CURRENT)
+    free0 = torch.cuda.mem_get_info()[0]
+    for flags in (_lib.YRC_TRACE_CLOSEST, _lib.YRC_TRACE_ANY, _lib.YRC_TRACE_CLOSEST):
+        status = L.yrc_trace_stats_device_noalloc(dev._handle, _lib.ptr(rays), n, flags, _lib.ptr(out[0]),
+                                                  _lib.ptr(out[1]), _lib.ptr(out[2]), _stream())
+        assert status == _lib.YRC_OK, L.yrc_last_error().decode()
+        torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert _pool_attr(cu, pool, _USED_MEM_HIGH) <= used0
+    assert (out[0] > 0).any()
+    # control: the allocating entry point takes its scratch from that pool
+    status = L.yrc_trace_stats_device(dev._handle, _lib.ptr(rays), n, _lib.YRC_TRACE_CLOSEST, _lib.ptr(out[0]),
+                                      _lib.ptr(out[1]), _lib.ptr(out[2]), _stream())
+    assert status == _lib.YRC_OK
+    torch.cuda.synchronize()
+    assert _pool_attr(cu, pool, _USED_MEM_HIGH) >= used0 + 16 * n
 
 
 @pytest.fixture(scope="module")

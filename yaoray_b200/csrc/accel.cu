@@ -487,6 +487,23 @@ yrc_status NoAllocScratch(int device, unsigned char** out) {
     return Ok();
 }
 
+// Called when an accelerator is created on its device (current): looks up
+// the scratch address there and loads the statistics kernels that
+// yrc_trace_stats_device_noalloc launches for this accelerator. With lazy
+// module loading (the CUDA 12 default) a module is loaded, and a kernel's
+// code placed in device memory, only when first used; this file has no
+// kernels, so the module that holds the scratch array is loaded only by the
+// address lookup. Doing both at creation, which allocates anyway, leaves
+// nothing for the first no-allocation call to allocate. A failure here is
+// not the creation's: the no-allocation call retries the lookup and reports.
+void ResolveNoAllocScratch(const yrc_accel* a) {
+    unsigned char* ignored = nullptr;
+    const bool looked_up = NoAllocScratch(a->device, &ignored) == YRC_OK;
+    const bool loaded = PreloadStatsKernels(a->params.two_level != 0, a->params.stack_limit) == cudaSuccess;
+    if (!looked_up || !loaded) cudaGetLastError();
+    Ok();
+}
+
 }  // namespace
 }  // namespace yrc
 
@@ -513,6 +530,7 @@ yrc_status yrc_accel_create_flat(const yrc_geometry* geometry, const yrc_bvh_vie
     }
     const yrc_status st = Finalize(layout, root, lo, hi, 0, depth, out);
     if (st != YRC_OK) return st;
+    ResolveNoAllocScratch(*out);
     // A four-wide copy is allowed for triangle-only BVHs: their closest hit
     // does not depend on the visiting order (ties go to the smaller flat
     // index), while a sphere tie goes to the first visited.
@@ -589,7 +607,9 @@ yrc_status yrc_accel_create_two_level(const yrc_geometry* geometry, const yrc_tw
     } catch (const std::bad_alloc&) {
         return Fail(YRC_ERR_OUT_OF_MEMORY, "yrc_accel_create_two_level: host allocation failed");
     }
-    return Finalize(layout, tlas_root, lo, hi, 1, tlas_depth, out);
+    const yrc_status st = Finalize(layout, tlas_root, lo, hi, 1, tlas_depth, out);
+    if (st == YRC_OK) ResolveNoAllocScratch(*out);
+    return st;
 }
 
 void yrc_accel_destroy(yrc_accel* accel) { yrc::FreeAccel(accel); }

@@ -492,6 +492,22 @@ cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, int sha
                  : LaunchDepth<false, false, false>(args, shape, stream, sm_count);
 }
 
+template <bool kTwo, int kTotal>
+cudaError_t PreloadStatsPair() {
+    cudaFuncAttributes attr;
+    cudaError_t err = cudaFuncGetAttributes(&attr, TraceKernel<false, true, kTwo, kTotal, 128, 8, 1>);
+    if (err == cudaSuccess) err = cudaFuncGetAttributes(&attr, TraceKernel<true, true, kTwo, kTotal, 128, 8, 1>);
+    return err;
+}
+
+cudaError_t PreloadStatsKernels(bool two_level, int stack_limit) {
+    // The kernels LaunchDepth picks for statistics (shape 0 whatever the
+    // tuned shape, the depth class of the BVH).
+    const bool deep = stack_limit > 64;
+    if (two_level) return deep ? PreloadStatsPair<true, kMaxTraceStack>() : PreloadStatsPair<true, 64>();
+    return deep ? PreloadStatsPair<false, kMaxTraceStack>() : PreloadStatsPair<false, 64>();
+}
+
 cudaError_t LaunchProbe(const ProbeArgs& args, cudaStream_t stream, int sm_count) {
     const bool two = args.accel.two_level != 0;
     const bool deep = args.accel.stack_limit > 64;

@@ -101,5 +101,9 @@ cudaError_t LaunchShadowTransmittance(const ShadowArgs& args, cudaStream_t strea
 cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, int shape, cudaStream_t stream,
                         int sm_count);
 cudaError_t LaunchProbe(const ProbeArgs& args, cudaStream_t stream, int sm_count);
+// Loads the code of the two statistics traversal kernels (closest and any
+// hit) that a BVH of this kind and stack limit uses, so that their first
+// launch under lazy module loading does not take device memory.
+cudaError_t PreloadStatsKernels(bool two_level, int stack_limit);
 
 }  // namespace yrc
