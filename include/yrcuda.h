@@ -531,6 +531,26 @@ typedef struct yrc_material {
     float normal_scale;          /* scales the normal map's tangent-space x and y (reference default 1) */
 } yrc_material;
 
+/* ---- Scattering functions evaluated on the device ------------------------
+ * Diagnostics: each evaluates, in a CUDA kernel, the same device code the
+ * path tracer shades with, on host inputs and outputs (synchronous), so that
+ * it can be checked function by function against the reference's. */
+
+/* EvaluateBsdf then PdfBsdf (src/shading/bsdf.cpp:17-148) for one material
+ * (any kind but Measured, which has yrc_measured_eval) on n rows of 9 floats
+ * (wo, wi, normal): f gets 3 floats per row, pdf 1. Each row's PCG32 stream
+ * is Rng(seeds[i]) (include/yaoray/core/rng.hpp:15-48), drawn by the layered
+ * kinds' stochastic walk (src/shading/bsdf_layered.cpp:13-349) in the
+ * evaluation and then the pdf, as a path vertex evaluates a light sample. */
+yrc_status yrc_bsdf_eval(const yrc_material* material, const float* queries, const uint64_t* seeds, int64_t n,
+                         float* f, float* pdf);
+
+/* SampleBsdf (src/shading/bsdf.cpp:150-310) on n rows of 8 floats (wo,
+ * normal, u.x, u.y) with Rng(seeds[i]): out gets 9 floats per row (wi,
+ * weight, pdf, valid 0/1, specular 0/1). */
+yrc_status yrc_bsdf_sample(const yrc_material* material, const float* queries, const uint64_t* seeds, int64_t n,
+                           float* out);
+
 /* EmissivePrimitive (include/yaoray/scene/light.hpp:30-34). */
 typedef struct yrc_emissive_primitive {
     int32_t primitive_index;
@@ -592,6 +612,20 @@ typedef struct yrc_bssrdf_table {
  */
 yrc_status yrc_bssrdf_table_build(float g, float eta, int32_t rho_count, int32_t radius_count, float* rho_samples,
                                   float* radius_samples, float* profile, float* rho_eff, float* profile_cdf);
+
+/* TabulatedBSSRDF(sigma_a, sigma_s, eta, table) (src/shading/bssrdf.cpp:
+ * 153-266) on the device for n queries: sample_r[i] = Sample_Sr(channels[i],
+ * u[i]) (-1 for a channel without extinction), pdf_sr[i] = Pdf_Sr(channels[i],
+ * r[i]), sr[3i..3i+2] = Sr(r[i]). Channels are 0..2. */
+yrc_status yrc_bssrdf_eval(const yrc_bssrdf_table* table, const float sigma_a[3], const float sigma_s[3], float eta,
+                           const int32_t* channels, const float* u, const float* r, int64_t n, float* sample_r,
+                           float* pdf_sr, float* sr);
+
+/* TabulatedBSSRDF::Pdf_Sp (src/shading/bssrdf.cpp:244-266) on n rows of 18 floats
+ * (po, ss, ts, ns, pi, ni): the area-measure pdf of exit point pi with normal
+ * ni for entry po with shading frame (ss, ts, ns). */
+yrc_status yrc_bssrdf_pdf_sp(const yrc_bssrdf_table* table, const float sigma_a[3], const float sigma_s[3], float eta,
+                             const float* queries, int64_t n, float* pdf);
 
 /* RenderCamera (include/yaoray/scene/camera.hpp:7-13). */
 typedef struct yrc_camera {
@@ -807,6 +841,18 @@ yrc_status yrc_render(yrc_render_scene* scene, const yrc_render_request* request
 yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t count, const yrc_render_request* requests,
                            yrc_film_pixel* const* films_out, uint64_t* bad_samples_out, yrc_render_stats* stats,
                            double* device_seconds);
+
+/*
+ * TraceShadowVisibility (src/integrators/path_direct_lighting.cpp:23-113) for
+ * n caller rays (host, synchronous) through the scene's own shadow stage, the
+ * code the path tracer runs for its next-event rays: each ray's origin,
+ * direction and t_max = max_distance, t_min = the first query's t_min (the
+ * reference uses 1e-5). `transmittance` gets 4 floats per ray: the RGB
+ * transmittance and 1 when visible, all 0 when occluded. No counterpart in
+ * the reference's public API (its loop is internal to the integrator).
+ */
+yrc_status yrc_render_scene_shadow_eval(yrc_render_scene* scene, const yrc_ray* rays, int64_t n,
+                                        float* transmittance);
 
 /* Wait for all work the library queued on `stream` (NULL = legacy default). */
 yrc_status yrc_stream_synchronize(void* stream);

@@ -472,6 +472,66 @@ def ref_bssrdf_table(g: float, eta: float, rho_count: int = 100, radius_count: i
     return t
 
 
+def ref_bsdf_eval(material, wo, wi, n, seeds):
+    """The reference's EvaluateBsdf then PdfBsdf (one RenderMaterial from a
+    MATERIAL_DTYPE record) with Rng(seeds[i]) per row: (f (n, 3), pdf (n,))."""
+    from yaoray_b200.render import MATERIAL_DTYPE
+    m = np.ascontiguousarray(np.asarray(material, MATERIAL_DTYPE).reshape(1))
+    q = np.ascontiguousarray(np.concatenate([np.reshape(wo, (-1, 3)), np.reshape(wi, (-1, 3)),
+                                             np.reshape(n, (-1, 3))], 1), np.float32)
+    s = np.ascontiguousarray(seeds, np.uint64).reshape(-1)
+    f = np.empty((q.shape[0], 3), np.float32)
+    pdf = np.empty(q.shape[0], np.float32)
+    L = ref_lib()
+    L.yrref_bsdf_eval.argtypes = [P, P, P, I64, P, P]
+    L.yrref_bsdf_eval(m.ctypes.data, q.ctypes.data, s.ctypes.data, q.shape[0], f.ctypes.data, pdf.ctypes.data)
+    return f, pdf
+
+
+def ref_bsdf_sample(material, wo, n, u, seeds) -> np.ndarray:
+    """The reference's SampleBsdf with Rng(seeds[i]) per row: (n, 9) rows of
+    wi, weight, pdf, valid, specular."""
+    from yaoray_b200.render import MATERIAL_DTYPE
+    m = np.ascontiguousarray(np.asarray(material, MATERIAL_DTYPE).reshape(1))
+    q = np.ascontiguousarray(np.concatenate([np.reshape(wo, (-1, 3)), np.reshape(n, (-1, 3)),
+                                             np.reshape(u, (-1, 2))], 1), np.float32)
+    s = np.ascontiguousarray(seeds, np.uint64).reshape(-1)
+    out = np.empty((q.shape[0], 9), np.float32)
+    L = ref_lib()
+    L.yrref_bsdf_sample.argtypes = [P, P, P, I64, P]
+    L.yrref_bsdf_sample(m.ctypes.data, q.ctypes.data, s.ctypes.data, q.shape[0], out.ctypes.data)
+    return out
+
+
+def ref_bssrdf_eval(sigma_a, sigma_s, eta: float, channels, u, r, g: float = 0.0):
+    """The reference TabulatedBSSRDF (100 x 64 table for g, eta):
+    (Sample_Sr(ch, u), Pdf_Sr(ch, r), Sr(r) (n, 3)) per row."""
+    ch = np.ascontiguousarray(channels, np.int32).reshape(-1)
+    uu = np.ascontiguousarray(u, np.float32).reshape(-1)
+    rr = np.ascontiguousarray(r, np.float32).reshape(-1)
+    n = ch.size
+    sa = np.ascontiguousarray(sigma_a, np.float32)
+    ss = np.ascontiguousarray(sigma_s, np.float32)
+    sample_r, pdf, sr = np.empty(n, np.float32), np.empty(n, np.float32), np.empty((n, 3), np.float32)
+    L = ref_lib()
+    L.yrref_bssrdf_eval.argtypes = [P, P, C.c_float, C.c_float, C.c_int, P, P, P, P, P, P]
+    L.yrref_bssrdf_eval(sa.ctypes.data, ss.ctypes.data, eta, g, n, ch.ctypes.data, uu.ctypes.data, rr.ctypes.data,
+                        sample_r.ctypes.data, pdf.ctypes.data, sr.ctypes.data)
+    return sample_r, pdf, sr
+
+
+def ref_bssrdf_pdf_sp(sigma_a, sigma_s, eta: float, queries, g: float = 0.0) -> np.ndarray:
+    """The reference TabulatedBSSRDF::Pdf_Sp per row of (po, ss, ts, ns, pi, ni)."""
+    q = np.ascontiguousarray(queries, np.float32).reshape(-1, 18)
+    sa = np.ascontiguousarray(sigma_a, np.float32)
+    ss = np.ascontiguousarray(sigma_s, np.float32)
+    out = np.empty(q.shape[0], np.float32)
+    L = ref_lib()
+    L.yrref_bssrdf_pdf_sp.argtypes = [P, P, C.c_float, C.c_float, C.c_int, P, P]
+    L.yrref_bssrdf_pdf_sp(sa.ctypes.data, ss.ctypes.data, eta, g, q.shape[0], q.ctypes.data, out.ctypes.data)
+    return out
+
+
 def ref_rng(seed: int, count: int) -> np.ndarray:
     out = np.empty(count, np.float32)
     ref_lib().yrref_rng_floats(seed, count, out.ctypes.data)
@@ -587,6 +647,18 @@ class RefJob:
                                      "relative_error": st.adaptive_relative_error,
                                      "absolute_error": st.adaptive_absolute_error,
                                      "confidence": st.adaptive_confidence})
+
+    def shadow_visibility(self, rays: np.ndarray) -> np.ndarray:
+        """The reference's TraceShadowVisibility on this job's scene (prepared
+        as the CPU backend prepares it) for (n, 8) rays (origin, unused,
+        direction, max_distance) -> (n, 4): RGB transmittance, visible."""
+        L = _bind_jobs(ref_lib())
+        L.yrref_job_shadow_visibility.argtypes = [P, P, I64, P]
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        out = np.empty((r.shape[0], 4), np.float32)
+        if L.yrref_job_shadow_visibility(self.h, r.ctypes.data, r.shape[0], out.ctypes.data) != 0:
+            raise RuntimeError(L.yrref_last_error().decode())
+        return out
 
     def render(self, threads: int = 0, spp: int = 0, resume_film=None, resume_spp: int = 0):
         """CpuBackend render -> (film FILM_PIXEL_DTYPE (H*W), stats dict, seconds).

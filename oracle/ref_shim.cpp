@@ -522,6 +522,7 @@ std::uint64_t yrref_film_accumulate(int width, int height, const float* samples,
 #include <yaoray/lighting/environment.hpp>
 #include <yaoray/lighting/light_sampling.hpp>
 #include <yaoray/shading/bssrdf.hpp>
+#include "integrators/path_integrator_internal.hpp"
 
 namespace {
 
@@ -540,6 +541,38 @@ void CopyRgb(const yr::Color3f& c, float* out) {
 }
 
 yr::Color3f Rgb(const float* c) { return yr::Color3f{c[0], c[1], c[2]}; }
+
+yr::RenderMaterial MaterialFrom(const yrc_material& m) {
+    yr::RenderMaterial r;
+    r.kind = static_cast<yr::RenderMaterialKind>(m.kind);
+    r.reflectance.value = Rgb(m.reflectance);
+    r.eta.value = Rgb(m.eta);
+    r.k.value = Rgb(m.k);
+    r.ior = m.ior;
+    r.uroughness.value = m.uroughness;
+    r.vroughness.value = m.vroughness;
+    r.remap_roughness = m.remap_roughness != 0;
+    r.coating_ior = m.coating_ior;
+    r.coating_roughness.value = m.coating_roughness;
+    r.coat_thickness = m.coat_thickness;
+    r.coat_absorption = Rgb(m.coat_absorption);
+    r.coat_maxdepth = m.coat_maxdepth;
+    r.coat_nsamples = m.coat_nsamples;
+    r.sigma_a = Rgb(m.sigma_a);
+    r.sigma_s = Rgb(m.sigma_s);
+    r.bssrdf_eta = m.bssrdf_eta;
+    r.bssrdf_index = m.bssrdf_index;
+    r.emission = Rgb(m.emission);
+    r.alpha.value = m.alpha;
+    r.absorption_color = Rgb(m.absorption_color);
+    r.absorption_distance = m.absorption_distance;
+    r.reflectance.texture = m.reflectance_texture;
+    r.alpha.texture = m.alpha_texture;
+    r.normal_map = m.normal_map;
+    r.normal_scale = m.normal_scale;
+    r.measured_index = m.measured_index;
+    return r;
+}
 
 void PrepareAlias(RefJob& job) {
     yr::RenderSceneIR copy = job.ir;
@@ -735,38 +768,7 @@ void* yrref_job_from_desc(const yrc_scene_desc* d) {
         std::copy(g.instances[i].object_to_world, g.instances[i].object_to_world + 16, inst.object_to_world.m.begin());
         ir.instances.push_back(inst);
     }
-    for (int32_t i = 0; i < d->material_count; ++i) {
-        const yrc_material& m = d->materials[i];
-        yr::RenderMaterial r;
-        r.kind = static_cast<yr::RenderMaterialKind>(m.kind);
-        r.reflectance.value = Rgb(m.reflectance);
-        r.eta.value = Rgb(m.eta);
-        r.k.value = Rgb(m.k);
-        r.ior = m.ior;
-        r.uroughness.value = m.uroughness;
-        r.vroughness.value = m.vroughness;
-        r.remap_roughness = m.remap_roughness != 0;
-        r.coating_ior = m.coating_ior;
-        r.coating_roughness.value = m.coating_roughness;
-        r.coat_thickness = m.coat_thickness;
-        r.coat_absorption = Rgb(m.coat_absorption);
-        r.coat_maxdepth = m.coat_maxdepth;
-        r.coat_nsamples = m.coat_nsamples;
-        r.sigma_a = Rgb(m.sigma_a);
-        r.sigma_s = Rgb(m.sigma_s);
-        r.bssrdf_eta = m.bssrdf_eta;
-        r.bssrdf_index = m.bssrdf_index;
-        r.emission = Rgb(m.emission);
-        r.alpha.value = m.alpha;
-        r.absorption_color = Rgb(m.absorption_color);
-        r.absorption_distance = m.absorption_distance;
-        r.reflectance.texture = m.reflectance_texture;
-        r.alpha.texture = m.alpha_texture;
-        r.normal_map = m.normal_map;
-        r.normal_scale = m.normal_scale;
-        r.measured_index = m.measured_index;
-        ir.materials.push_back(r);
-    }
+    for (int32_t i = 0; i < d->material_count; ++i) ir.materials.push_back(MaterialFrom(d->materials[i]));
     for (int32_t i = 0; d->measured && i < d->measured_count; ++i) ir.measured_brdfs.push_back(MakeMeasured(d->measured[i]));
     // Scene textures keep their indices; the environment texture follows them.
     for (int32_t i = 0; d->textures && i < d->texture_count; ++i) {
@@ -906,6 +908,65 @@ int yrref_job_render_resume(void* handle, int threads, int spp_override, const v
                          stats, 8, seconds);
 }
 
+// TraceShadowVisibility (src/integrators/path_direct_lighting.cpp:23-113) on
+// the job's scene, prepared as the CPU backend prepares it, for n rays of 8
+// floats (origin, unused, direction, max_distance): out rows of 4 floats
+// (transmittance RGB, visible 0/1). Returns 0, or 1 on a build error.
+int yrref_job_shadow_visibility(void* handle, const float* rays, std::int64_t n, float* out) {
+    const RefJob& j = *static_cast<RefJob*>(handle);
+    yr::RenderSceneIR ir = j.ir;
+    yr::BuildTextureSamplingCaches(ir.textures);
+    yr::PrepareLightSampling(ir);
+    yr::RenderAccelerationBuildResult build = yr::BuildRenderAcceleration(ir.Geometry());
+    if (!build.errors.empty()) {
+        g_last_error = build.errors.front();
+        return 1;
+    }
+    for (std::int64_t i = 0; i < n; ++i) {
+        const float* r = rays + 8 * i;
+        yr::PathTraceStats stats;
+        const yr::ShadowVisibility v = yr::TraceShadowVisibility(
+            ir, build.acceleration, yr::Ray3f{yr::Point3f{r[0], r[1], r[2]}, yr::Vec3f{r[4], r[5], r[6]}}, r[7], stats);
+        CopyRgb(v.transmittance, out + 4 * i);
+        out[4 * i + 3] = v.visible ? 1.0f : 0.0f;
+    }
+    return 0;
+}
+
+// EvaluateBsdf then PdfBsdf with Rng(seeds[i]) for rows of (wo, wi, normal).
+void yrref_bsdf_eval(const yrc_material* material, const float* q, const std::uint64_t* seeds, std::int64_t n,
+                     float* f, float* pdf) {
+    const yr::RenderMaterial m = MaterialFrom(*material);
+    for (std::int64_t i = 0; i < n; ++i) {
+        const float* r = q + 9 * i;
+        const yr::Vec3f wo{r[0], r[1], r[2]}, wi{r[3], r[4], r[5]}, nn{r[6], r[7], r[8]};
+        yr::Rng rng{seeds[i]};
+        CopyRgb(yr::EvaluateBsdf(m, wo, wi, nn, rng), f + 3 * i);
+        pdf[i] = yr::PdfBsdf(m, wo, wi, nn, rng);
+    }
+}
+
+// SampleBsdf with Rng(seeds[i]) for rows of (wo, normal, u): out rows (wi,
+// weight, pdf, valid, specular).
+void yrref_bsdf_sample(const yrc_material* material, const float* q, const std::uint64_t* seeds, std::int64_t n,
+                       float* out) {
+    const yr::RenderMaterial m = MaterialFrom(*material);
+    for (std::int64_t i = 0; i < n; ++i) {
+        const float* r = q + 8 * i;
+        yr::Rng rng{seeds[i]};
+        const yr::BsdfSample s =
+            yr::SampleBsdf(m, yr::Vec3f{r[0], r[1], r[2]}, yr::Vec3f{r[3], r[4], r[5]}, yr::Vec2f{r[6], r[7]}, rng);
+        float* o = out + 9 * i;
+        o[0] = s.wi.x;
+        o[1] = s.wi.y;
+        o[2] = s.wi.z;
+        CopyRgb(s.weight, o + 3);
+        o[6] = s.pdf;
+        o[7] = s.valid ? 1.0f : 0.0f;
+        o[8] = s.specular ? 1.0f : 0.0f;
+    }
+}
+
 // ComputeBeamDiffusionBSSRDF of the reference, for checking the product's
 // table builder.
 void yrref_bssrdf_table(float g, float eta, int rho_count, int radius_count, float* rho, float* radius,
@@ -935,6 +996,21 @@ void yrref_bssrdf_eval(const float* sigma_a, const float* sigma_s, float eta, fl
         sr[3 * i] = c.x;
         sr[3 * i + 1] = c.y;
         sr[3 * i + 2] = c.z;
+    }
+}
+
+// TabulatedBSSRDF::Pdf_Sp for rows of (po, ss, ts, ns, pi, ni).
+void yrref_bssrdf_pdf_sp(const float* sigma_a, const float* sigma_s, float eta, float g, int n, const float* q,
+                         float* pdf) {
+    yr::BSSRDFTable t(100, 64);
+    yr::ComputeBeamDiffusionBSSRDF(g, eta, t);
+    const yr::TabulatedBSSRDF b(yr::Color3f{sigma_a[0], sigma_a[1], sigma_a[2]},
+                                yr::Color3f{sigma_s[0], sigma_s[1], sigma_s[2]}, eta, t);
+    for (int i = 0; i < n; ++i) {
+        const float* p = q + 18 * i;
+        pdf[i] = b.Pdf_Sp(yr::Point3f{p[0], p[1], p[2]}, yr::Vec3f{p[3], p[4], p[5]}, yr::Vec3f{p[6], p[7], p[8]},
+                          yr::Vec3f{p[9], p[10], p[11]}, yr::Point3f{p[12], p[13], p[14]},
+                          yr::Vec3f{p[15], p[16], p[17]});
     }
 }
 

@@ -1,0 +1,102 @@
+"""Per-ray shadow visibility against the reference's TraceShadowVisibility
+(src/integrators/path_direct_lighting.cpp:23-113), through the render path's
+own shadow stage (yrc_render_scene_shadow_eval) and the compiled reference on
+the same scene and rays.
+
+The scene is a stack of 20 pairs of parallel glass quads, the two quads of a
+pair 2e-5 apart, alternating Dielectric (a Beer-Lambert medium toggles at
+each crossing) and ThinDielectric (a clamped reflectance factor), with an
+opaque quad over part of the stack. A ray crossing k pairs meets 2k surfaces
+that pass light. The reference re-spawns each query just past the previous
+hit, so the second quad of a pair is skipped whenever it lies within the bias
+(about 1e-4 along the ray): such a ray takes about k queries, and it is
+visible when it ends before its 17th query. The device's single pass keeps
+only the 16 nearest clear surfaces; rays that need a surface beyond those go
+to the exact loop. Rays with 9 or more pairs before their end point exercise
+exactly that hand-off (more than 16 clear surfaces, some of them closer than
+the next query's t_min).
+
+Stated bounds: visibility identical for every ray; transmittance within a
+relative 1e-4 (CUDA's expf/logf in Beer-Lambert differ from glibc's in the
+last bits) on at least 99.9 % of the visible rays. The rest are rounding
+ties: the single pass measures a surface's t from the ray origin less the
+distance already advanced, the reference from the re-spawned origin, and
+when that t lies within rounding of the 1e-5 t_min the two can disagree on
+whether the surface counts (3 of 40,902 visible rays here, grazing rays
+whose pair gap is about bias + t_min along the ray).
+"""
+import numpy as np
+import pytest
+
+from yaoray_b200.accel import SceneGeometry
+from yaoray_b200.render import DIELECTRIC, DIFFUSE, THIN_DIELECTRIC, CudaBackend, RenderScene, default_material
+
+pytestmark = pytest.mark.gpu
+
+PAIRS, GAP, SPACING, Z0 = 20, 2.0e-5, 0.6, 1.0
+
+
+def _quad(z, x0=-6.0, x1=6.0, y0=-6.0, y1=6.0):
+    pts = np.array([(x0, y0, z), (x1, y0, z), (x1, y1, z), (x0, y1, z)], np.float32)
+    return pts, np.array([(0, 1, 2), (0, 2, 3)], np.uint32)
+
+
+def slab_stack_scene() -> RenderScene:
+    meshes, mat_of = [], []
+    for i in range(PAIRS):
+        z = np.float32(Z0 + i * SPACING)
+        for dz in (0.0, GAP):
+            meshes.append(_quad(np.float32(z + np.float32(dz))))
+            mat_of.append(0 if i % 2 == 0 else 1)
+    meshes.append(_quad(np.float32(Z0 + 10.3 * SPACING), x0=2.0))  # opaque, over x > 2 only
+    mat_of.append(2)
+    geom = SceneGeometry.from_meshes(meshes)
+    geom.primitives["material_index"] = np.array(mat_of, np.int32)
+    mats = np.stack([default_material(kind=DIELECTRIC, ior=1.5, reflectance=(1.0, 1.0, 1.0),
+                                      absorption_color=(0.8, 0.6, 0.9), absorption_distance=3.0),
+                     default_material(kind=THIN_DIELECTRIC, ior=1.5, reflectance=(0.97, 0.93, 0.9)),
+                     default_material(kind=DIFFUSE, reflectance=(0.5, 0.5, 0.5))])
+    cam = {"origin": (0.0, 0.0, -5.0), "forward": (0.0, 0.0, 1.0), "right": (1.0, 0.0, 0.0), "up": (0.0, 1.0, 0.0),
+           "fov_y_radians": 0.7}
+    return RenderScene(geom, mats, cam, 16, 16, spp=1, max_depth=2)
+
+
+def shadow_rays(n, seed):
+    rng = np.random.default_rng(seed)
+    o = np.concatenate([rng.uniform(-3, 3, (n, 2)), np.full((n, 1), 0.2)], 1).astype(np.float32)
+    e = np.concatenate([rng.uniform(-3, 3, (n, 2)), rng.uniform(0.5, Z0 + PAIRS * SPACING + 1.0, (n, 1))],
+                       1).astype(np.float32)
+    d = (e - o).astype(np.float32)
+    dist = np.sqrt(np.sum(d.astype(np.float32) ** 2, 1, dtype=np.float32)).astype(np.float32)
+    d = (d / dist[:, None]).astype(np.float32)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3] = o
+    rays[:, 3] = 1.0e-5
+    rays[:, 4:7] = d
+    rays[:, 7] = dist
+    pairs = np.floor((e[:, 2] - Z0) / SPACING).astype(np.int64) + 1
+    return rays, np.clip(pairs, 0, PAIRS)
+
+
+def test_shadow_visibility_matches_reference_per_ray(cuda, ref):
+    scene = slab_stack_scene()
+    rays, pairs = shadow_rays(60000, seed=5)
+    want = ref.RefJob.from_scene(scene).shadow_visibility(rays)
+    backend = CudaBackend()
+    prepared = backend.prepare(scene)
+    got = prepared.shadow_visibility(rays)
+    vis_w = want[:, 3] == 1.0
+    vis_g = got[:, 3] == 1.0
+    mism = np.nonzero(vis_w != vis_g)[0]
+    assert mism.size == 0, (mism.size, mism[:5], pairs[mism[:5]], got[mism[:5]], want[mism[:5]])
+    assert (got[~vis_g] == 0).all()
+    rel = np.abs(got[vis_g, :3].astype(np.float64) - want[vis_g, :3]) / np.maximum(want[vis_g, :3], 1e-30)
+    close = rel.max(1) <= 1e-4
+    assert close.mean() >= 0.999, (close.mean(), rel.max())
+    # the cases this scene exists for: visible rays past more than 16 clear
+    # surfaces, occluded rays past more than 16 queries, and opaque hits
+    deep = pairs >= 9
+    assert (vis_w & deep).sum() > 1000
+    assert close[deep[vis_g]].all()  # the rays the exact loop took over match to rounding
+    assert (~vis_w & (pairs >= 17)).sum() > 1000
+    assert 0.3 < vis_w.mean() < 0.9

@@ -203,6 +203,10 @@ def lib() -> C.CDLL:
         "yrc_texture_mip_chain_eval": (C.c_int, [P, P, I64, P, P]),
         "yrc_measured_eval": (C.c_int, [P, P, I64, P, P]),
         "yrc_measured_sample": (C.c_int, [P, P, I64, P]),
+        "yrc_bsdf_eval": (C.c_int, [P, P, P, I64, P, P]),
+        "yrc_bsdf_sample": (C.c_int, [P, P, P, I64, P]),
+        "yrc_bssrdf_eval": (C.c_int, [P, P, P, C.c_float, P, P, P, I64, P, P, P]),
+        "yrc_bssrdf_pdf_sp": (C.c_int, [P, P, P, C.c_float, P, I64, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

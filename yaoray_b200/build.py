@@ -25,7 +25,8 @@ OBJ = PKG / "_build"
 LIB = PKG / "libyrcuda.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NO_FMA_UNITS = {"render_kernels.cu": ["-fmad=false"], "sample_eval.cu": ["-fmad=false"], "measured.cu": ["-fmad=false"]}
+NO_FMA_UNITS = {"render_kernels.cu": ["-fmad=false"], "sample_eval.cu": ["-fmad=false"], "measured.cu": ["-fmad=false"],
+                "shading_eval.cu": ["-fmad=false"]}
 
 
 def _nvcc() -> str:

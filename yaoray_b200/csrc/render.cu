@@ -663,6 +663,8 @@ yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     q.shadow_ray = W.Alloc<float4>(2 * 2 * capacity);
     q.shadow_slot = W.Alloc<int32_t>(2 * capacity);
     q.shadow_occluded = W.Alloc<uint8_t>(3 * capacity);
+    q.shadow_overflow =
+        (s->dev.any_transparent && !s->dev.exact_shadows) ? W.Alloc<int32_t>(2 * capacity) : nullptr;
     q.nee_paths = W.Alloc<int32_t>(capacity);
     q.order = W.Alloc<int32_t>(capacity);
     q.shade_class = W.Alloc<uint8_t>(capacity);
@@ -813,8 +815,16 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
             sa.sphere_clear = sc.sphere_clear;
             sa.counter = q.counters + kCtrShadowTrace;
             sa.occluded_count = q.counters + kCtrStatsBase + 2;
+            sa.overflow = q.shadow_overflow;
+            sa.overflow_count = q.counters + kCtrShadowOverflow;
             sa.error = ta.error;
             err = LaunchShadowTransmittance(sa, st, s->sm_count);
+            // Rays past more than 16 clear surfaces: the exact loop.
+            if (err == cudaSuccess) {
+                LaunchShadowExact(sc, q, s->transmittance, q.counters + kCtrStatsBase + 2, 2 * C, s->sm_count,
+                                  ta.error, st, q.shadow_overflow);
+                err = cudaGetLastError();
+            }
         } else {
             TraceArgs sh{};
             sh.accel = sc.accel;
@@ -1392,4 +1402,98 @@ extern "C" yrc_status yrc_render_scene_set_tuning(yrc_render_scene* s, const yrc
     if (st != YRC_OK) return st;
     DropGraph(s);
     return Ok();
+}
+
+// TraceShadowVisibility (src/integrators/path_direct_lighting.cpp:23-113) for
+// caller rays, through the scene's own shadow stage: the single-pass
+// transmittance kernel with its exact-loop overflow, the exact loop for
+// scenes with cut-outs, or the any-hit kernel for scenes without surfaces
+// that pass light.
+extern "C" yrc_status yrc_render_scene_shadow_eval(yrc_render_scene* s, const yrc_ray* rays, int64_t n,
+                                                   float* transmittance) {
+    using namespace yrc;
+    if (!s || n < 0 || n > (int64_t{1} << 30) || (n > 0 && (!rays || !transmittance))) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_scene_shadow_eval: bad argument");
+    }
+    if (n == 0) return Ok();
+    std::lock_guard<std::mutex> lock(s->mutex);
+    cudaSetDevice(s->device);
+    const size_t un = static_cast<size_t>(n);
+    const DevScene& sc = s->dev;
+    DeviceArena a;
+    Queues q{};
+    q.shadow_ray = a.Upload(reinterpret_cast<const float4*>(rays), 2 * un);
+    std::vector<int32_t> slot(un);
+    for (size_t i = 0; i < un; ++i) slot[i] = static_cast<int32_t>(i);
+    q.shadow_slot = a.Upload(slot);
+    q.shadow_overflow = a.Alloc<int32_t>(un);
+    q.shadow_occluded = a.Alloc<uint8_t>(un);
+    q.counters = a.Alloc<unsigned long long>(kCtrCount);
+    float4* tr = a.Alloc<float4>(un);
+    std::vector<unsigned long long> counters(kCtrCount, 0);
+    counters[kCtrShadow] = static_cast<unsigned long long>(n);
+    cudaError_t err = a.err;
+    if (err == cudaSuccess) {
+        err = cudaMemcpy(q.counters, counters.data(), sizeof(unsigned long long) * kCtrCount, cudaMemcpyHostToDevice);
+    }
+    int* error = AccelErrorWord(s->accel);
+    const cudaStream_t st = nullptr;
+    const bool opaque = !sc.exact_shadows && !sc.any_transparent;
+    if (err == cudaSuccess) {
+        if (sc.exact_shadows) {
+            LaunchShadowExact(sc, q, tr, q.counters + kCtrStatsBase + 2, n, s->sm_count, error, st);
+            err = cudaGetLastError();
+        } else if (sc.any_transparent) {
+            ShadowArgs sa{};
+            sa.accel = sc.accel;
+            sa.rays = q.shadow_ray;
+            sa.count_ptr = q.counters + kCtrShadow;
+            sa.capacity = n;
+            sa.out_index = q.shadow_slot;
+            sa.transmittance = tr;
+            sa.tri_prim = sc.tri_prim;
+            sa.prim_material = sc.prim_material;
+            sa.sphere_material = sc.sphere_material;
+            sa.materials = sc.materials;
+            sa.tri_clear = sc.tri_clear;
+            sa.sphere_clear = sc.sphere_clear;
+            sa.counter = q.counters + kCtrShadowTrace;
+            sa.occluded_count = q.counters + kCtrStatsBase + 2;
+            sa.overflow = q.shadow_overflow;
+            sa.overflow_count = q.counters + kCtrShadowOverflow;
+            sa.error = error;
+            err = LaunchShadowTransmittance(sa, st, s->sm_count);
+            if (err == cudaSuccess) {
+                LaunchShadowExact(sc, q, tr, q.counters + kCtrStatsBase + 2, n, s->sm_count, error, st,
+                                  q.shadow_overflow);
+                err = cudaGetLastError();
+            }
+        } else {
+            TraceArgs sh{};
+            sh.accel = sc.accel;
+            sh.rays = q.shadow_ray;
+            sh.count = n;
+            sh.count_ptr = q.counters + kCtrShadow;
+            sh.occluded = q.shadow_occluded;
+            sh.out_index = q.shadow_slot;
+            sh.counter = q.counters + kCtrShadowTrace;
+            sh.occluded_count = q.counters + kCtrStatsBase + 2;
+            sh.error = error;
+            err = LaunchTrace(sh, true, false, TraceShapeOf(s->accel, 1), st, s->sm_count);
+        }
+    }
+    if (err == cudaSuccess) err = cudaDeviceSynchronize();
+    if (err == cudaSuccess && opaque) {
+        std::vector<uint8_t> occ(un);
+        err = cudaMemcpy(occ.data(), q.shadow_occluded, un, cudaMemcpyDeviceToHost);
+        for (size_t i = 0; err == cudaSuccess && i < un; ++i) {
+            const float v = occ[i] ? 0.0f : 1.0f;
+            for (int c = 0; c < 4; ++c) transmittance[4 * i + c] = v;
+        }
+    } else if (err == cudaSuccess) {
+        err = cudaMemcpy(transmittance, tr, sizeof(float4) * un, cudaMemcpyDeviceToHost);
+    }
+    a.Release();
+    if (err != cudaSuccess) return CudaError(err, "yrc_render_scene_shadow_eval");
+    return CheckDeviceError(s->accel);
 }

@@ -144,6 +144,7 @@ __global__ void ResetCountersKernel(Queues q) {
         q.counters[kCtrNee] = 0;
         q.counters[kCtrTrace] = 0;
         q.counters[kCtrShadowTrace] = 0;
+        q.counters[kCtrShadowOverflow] = 0;
         q.counters[kCtrProbe] = 0;
         for (int c = 0; c < kShadeClasses; ++c) {
             q.counters[kCtrClass0 + c] = 0;
@@ -1014,17 +1015,21 @@ __global__ void __launch_bounds__(kTraceBlock) AlphaExtendKernel(DevScene sc, Pa
 // TraceShadowVisibility (src/integrators/path_direct_lighting.cpp:23-113)
 // one shadow ray per thread, each query a closest hit with the cut-out skip
 // loop, for scenes where the single-pass shadow kernel does not apply (cut-out
-// materials, or thin dielectrics whose reflectance is textured). Writes the
-// transmittance (w = 1 visible, all 0 occluded) to the ray's slot.
+// materials, or thin dielectrics whose reflectance is textured), and for the
+// rays that kernel leaves to it (`list`: shadow entries past more than 16
+// clear surfaces, counted in kCtrShadowOverflow). Writes the transmittance
+// (w = 1 visible, all 0 occluded) to the ray's slot.
 template <bool kTwo, int kTotal>
-__global__ void __launch_bounds__(kTraceBlock) ShadowExactKernel(DevScene sc, Queues q, float4* transmittance,
+__global__ void __launch_bounds__(kTraceBlock) ShadowExactKernel(DevScene sc, Queues q, const int32_t* list,
+                                                                 float4* transmittance,
                                                                  unsigned long long* occluded_count, int* error) {
     __shared__ int2 s_stack[kShortStack * kTraceBlock];
     int2* col = s_stack + threadIdx.x;
     StackStore<kTotal> st;
-    const int64_t n = static_cast<int64_t>(q.counters[kCtrShadow]);
-    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
-         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t n = static_cast<int64_t>(list ? q.counters[kCtrShadowOverflow] : q.counters[kCtrShadow]);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t k = list ? static_cast<int64_t>(list[i]) : i;
         const float4 ra = q.shadow_ray[2 * k], rb = q.shadow_ray[2 * k + 1];
         V3 o = F4(ra);
         const V3 d = F4(rb);
@@ -1710,11 +1715,13 @@ void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, const
 template <bool kTwo, int kTotal>
 void LaunchAlphaOne(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
                     int sm_count, int* error, float4* transmittance, unsigned long long* occluded_count,
-                    bool shadows, cudaStream_t st) {
+                    bool shadows, const int32_t* list, cudaStream_t st) {
     const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((capacity + kTraceBlock - 1) / kTraceBlock,
                                                                     static_cast<int64_t>(sm_count) * 16));
     if (shadows) {
-        ShadowExactKernel<kTwo, kTotal><<<blocks * 2, kTraceBlock, 0, st>>>(sc, q, transmittance, occluded_count, error);
+        // An overflow list is rare and short: one block per SM covers it.
+        const unsigned grid = list ? static_cast<unsigned>(sm_count) : blocks * 2;
+        ShadowExactKernel<kTwo, kTotal><<<grid, kTraceBlock, 0, st>>>(sc, q, list, transmittance, occluded_count, error);
     } else {
         AlphaExtendKernel<kTwo, kTotal><<<blocks, kTraceBlock, 0, st>>>(sc, ps, q, depth, error);
     }
@@ -1722,26 +1729,26 @@ void LaunchAlphaOne(const DevScene& sc, const PathState& ps, const Queues& q, in
 
 void LaunchAlpha(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity, int sm_count,
                  int* error, float4* transmittance, unsigned long long* occluded_count, bool shadows,
-                 cudaStream_t st) {
+                 const int32_t* list, cudaStream_t st) {
     const bool two = sc.accel.two_level != 0;
     const bool deep = sc.accel.stack_limit > 64;
     if (two) {
-        if (deep) LaunchAlphaOne<true, kMaxTraceStack>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, st);
-        else LaunchAlphaOne<true, 64>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, st);
+        if (deep) LaunchAlphaOne<true, kMaxTraceStack>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, list, st);
+        else LaunchAlphaOne<true, 64>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, list, st);
     } else {
-        if (deep) LaunchAlphaOne<false, kMaxTraceStack>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, st);
-        else LaunchAlphaOne<false, 64>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, st);
+        if (deep) LaunchAlphaOne<false, kMaxTraceStack>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, list, st);
+        else LaunchAlphaOne<false, 64>(sc, ps, q, depth, capacity, sm_count, error, transmittance, occluded_count, shadows, list, st);
     }
 }
 
 void LaunchAlphaExtend(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
                        int sm_count, int* error, cudaStream_t st) {
-    LaunchAlpha(sc, ps, q, depth, capacity, sm_count, error, nullptr, nullptr, false, st);
+    LaunchAlpha(sc, ps, q, depth, capacity, sm_count, error, nullptr, nullptr, false, nullptr, st);
 }
 
 void LaunchShadowExact(const DevScene& sc, const Queues& q, float4* transmittance, unsigned long long* occluded_count,
-                       int64_t capacity, int sm_count, int* error, cudaStream_t st) {
-    LaunchAlpha(sc, PathState{}, q, 0, capacity, sm_count, error, transmittance, occluded_count, true, st);
+                       int64_t capacity, int sm_count, int* error, cudaStream_t st, const int32_t* list) {
+    LaunchAlpha(sc, PathState{}, q, 0, capacity, sm_count, error, transmittance, occluded_count, true, list, st);
 }
 
 void LaunchSubsurfaceExit(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,

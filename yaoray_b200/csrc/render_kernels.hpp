@@ -39,11 +39,13 @@ void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, const
 // Subsurface: close the probes traced by LaunchRenderProbe (exit point,
 // Sp / pdf, NEE at the exit, continuation).
 // Scenes with cut-out (alpha) materials: the extend stage's skip loop over
-// cut-out hits, and the exact per-thread shadow-visibility loop.
+// cut-out hits, and the exact per-thread shadow-visibility loop, over the
+// whole shadow queue or (`list`) over the entries the single-pass shadow
+// kernel left to it (q.shadow_overflow, counted in kCtrShadowOverflow).
 void LaunchAlphaExtend(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
                        int sm_count, int* error, cudaStream_t st);
 void LaunchShadowExact(const DevScene& sc, const Queues& q, float4* transmittance, unsigned long long* occluded_count,
-                       int64_t capacity, int sm_count, int* error, cudaStream_t st);
+                       int64_t capacity, int sm_count, int* error, cudaStream_t st, const int32_t* list = nullptr);
 void LaunchSubsurfaceExit(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
                           int sm_count, cudaStream_t st);
 // Radiance cache: add cached radiance to the paths that ended at the cache;

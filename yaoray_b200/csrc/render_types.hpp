@@ -222,6 +222,7 @@ struct Queues {
     float4* shadow_ray;   // 2 per shadow entry
     int32_t* shadow_slot; // path * 3 + light type
     uint8_t* shadow_occluded;
+    int32_t* shadow_overflow;  // shadow entries the exact loop traces (see ShadowArgs::overflow)
     int32_t* nee_paths;   // paths with pending NEE
     // Subsurface probes (BSSRDF entry -> probe traversal -> exit), one per
     // path at most: probe_ray 2 per entry (base.xyz + t_min, direction.xyz +
@@ -250,6 +251,7 @@ enum CounterIndex {
     kCtrProbe = 10,  // subsurface probes queued at this depth
     kCtrTrace = 12,  // traversal work counter
     kCtrShadowTrace = 13,
+    kCtrShadowOverflow = 14,  // entries in shadow_overflow
     kCtrStatsBase = 16,  // rays, shadow rays, occluded, hits, misses, bad
     kCtrCursor0 = 24,  // scatter cursors per shading class
     kCtrCount = 32,

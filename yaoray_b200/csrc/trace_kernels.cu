@@ -212,10 +212,14 @@ __global__ void __launch_bounds__(kTraceBlock) RenderProbeKernel(RenderProbeArgs
 // all the ray is fully visible. Otherwise the reference's loop is replayed
 // over the kept list in t order: each query returns the first kept surface
 // beyond the query's origin plus t_min (1e-5), t measured from that origin,
-// with the same bias, remaining-distance and 16-query rules. What differs
-// from re-tracing is rounding: t is the traversal's t from the ray origin
-// less the distance already advanced, not a new intersection from the
-// re-spawned origin. Persistent warps with per-lane refill, like TraceKernel.
+// with the same bias, remaining-distance and 16-query rules. When more than
+// 16 clear surfaces were seen and a query would need one beyond the kept
+// list, the ray's queue index goes to an overflow list that the exact loop
+// (ShadowExactKernel, re-spawning each query) traces afterwards, and this
+// kernel writes nothing for it. What differs from re-tracing is rounding: t
+// is the traversal's t from the ray origin less the distance already
+// advanced, not a new intersection from the re-spawned origin. Persistent
+// warps with per-lane refill, like TraceKernel.
 template <bool kTwo, int kTotal>
 __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmittanceKernel(ShadowArgs args) {
     __shared__ int2 s_stack[kShadowShortStack * kTraceBlock];
@@ -273,8 +277,9 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmi
                 }
             }
             if (!found) {
-                // A surface beyond the kept ones would be this query's answer.
-                if (clear.dropped) return occluded;
+                // A surface beyond the kept ones would be this query's
+                // answer: the exact loop traces this ray instead.
+                if (clear.dropped) return make_float4(0.0f, 0.0f, 0.0f, -1.0f);
                 if (medium) {
                     if (!finite) return occluded;
                     beer(remaining);
@@ -329,6 +334,11 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmi
             tr = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
         } else {
             tr = replay();
+            if (tr.w < 0.0f) {
+                const unsigned long long o = atomicAdd(args.overflow_count, 1ull);
+                args.overflow[o] = static_cast<int32_t>(ray);
+                return;
+            }
         }
         args.transmittance[slot] = tr;
         if (tr.w == 0.0f) CountLanes(args.occluded_count);

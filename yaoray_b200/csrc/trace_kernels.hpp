@@ -69,6 +69,8 @@ struct ShadowArgs {
     const uint8_t* sphere_clear;          // per sphere
     unsigned long long* counter;          // ray work counter, zeroed before the launch
     unsigned long long* occluded_count;   // shadow rays found not visible (RenderStats::occluded_shadow_rays)
+    int32_t* overflow;                    // queue indices left to the exact loop (more than 16 clear surfaces)
+    unsigned long long* overflow_count;   // entries in `overflow`, zeroed before the launch
     int* error;
 };
 

@@ -198,6 +198,7 @@ def _bind():
         ("yrc_render_scene_capacity", C.c_int64, [P]),
         ("yrc_render_autotune", C.c_int, [P, C.c_int32, P]),
         ("yrc_render_scene_set_tuning", C.c_int, [P, P]),
+        ("yrc_render_scene_shadow_eval", C.c_int, [P, P, C.c_int64, P]),
         ("yrc_render_many", C.c_int, [P, C.c_int32, P, P, P, P, P]),
         ("yrc_bssrdf_table_build", C.c_int, [C.c_float, C.c_float, C.c_int32, C.c_int32, P, P, P, P, P]),
         ("yrc_alias_table_build", C.c_int, [P, C.c_int32, P, P, P]),
@@ -465,6 +466,15 @@ class PreparedScene:
         e.g. one found on a scene of the same image size and spp."""
         t = RenderTuning(int(tuning["capacity"]), int(tuning["trace_shape"]), 0, 0.0)
         check(_bind().yrc_render_scene_set_tuning(self._handle, C.byref(t)))
+
+    def shadow_visibility(self, rays: np.ndarray) -> np.ndarray:
+        """TraceShadowVisibility through this scene's shadow stage for (n, 8)
+        rays (origin, t_min, direction, max_distance) -> (n, 4): RGB
+        transmittance and 1 when visible, all 0 when occluded."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        out = np.empty((r.shape[0], 4), np.float32)
+        check(_bind().yrc_render_scene_shadow_eval(self._handle, ptr(r), r.shape[0], ptr(out)))
+        return out
 
     def set_radiance_cache(self, cache, spread_threshold: float = 0.01, train_one_in: int = 16,
                            train_records: int = 65536, train: bool = True, train_steps: int = 1,
