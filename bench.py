@@ -378,10 +378,37 @@ def run_gpu(args):
             "cpu_baseline": base,
             "clocks": clocks.summary(),
         }
-        print(json.dumps(line), flush=True)
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
+    return line if rank == 0 else None
+
+
+# The other halves of the metric, run after the traversal line at N = 1 as
+# their own processes (their own memory, device-timed regions, CPU baselines
+# and clock samples): the Cornell box at its configured size, the instanced
+# scene, and the radiance cache's equal-relMSE ratio.
+EXTRA_LEGS = (("cornell", ["--workload", "cornell", "--steps", "10", "--warmup", "3"]),
+              ("instanced", ["--workload", "instanced", "--steps", "4", "--warmup", "3"]),
+              ("nrc", ["--workload", "nrc"]))
+
+
+def run_extra_legs():
+    legs = {}
+    for name, argv in EXTRA_LEGS:
+        t0 = time.perf_counter()
+        res = subprocess.run([sys.executable, str(ROOT / "bench.py"), *argv], capture_output=True, text=True,
+                             timeout=1200)
+        leg = None
+        for row in reversed(res.stdout.splitlines()):
+            if row.startswith("{"):
+                leg = json.loads(row)
+                break
+        if leg is None:
+            leg = {"error": f"exit {res.returncode}: {res.stderr.strip()[-600:]}"}
+        leg["leg_wall_s"] = round(time.perf_counter() - t0, 1)
+        legs[name] = leg
+    return legs
 
 
 RENDER_WORKLOADS = {
@@ -487,22 +514,27 @@ def run_render(args):
 
 def run_nrc(args):
     """--workload nrc: equal-relMSE time of the neural-cached path tracer
-    against the plain one on the instanced scene (960x540, max depth 16,
-    radiance clamp 20 for every render so that the reference's rare
-    numerically extreme samples do not dominate the error).
+    against the plain one on the instanced scene (max depth 16, radiance
+    clamp 20 for every render so that the reference integrator's rare
+    numerically extreme samples do not dominate the error), per frame of a
+    seeded camera orbit, in steady state.
 
-    Reference: `--ref-spp` samples per pixel of the plain tracer, accumulated
-    in FP64 over renders of different seeds. Plain curve: renders of 1..64
-    spp. Cached: a fresh cache trained online by 60 warm-up frames of 2 spp
-    along a seeded camera orbit (0.5 degrees per frame) that ends at the
-    evaluated view (a new sampler seed per frame, 4 optimiser steps per batch;
-    their time is reported separately), then renders of 1, 4 and 16 spp that keep training
-    (1 step per batch) and query the moving average of the cache's
-    parameters. Every relMSE is the mean over three sampler seeds, every
-    time the mean device time of the second render of a prepared scene (the
-    first captures the batch graph). For each cached render, the time the
-    plain tracer needs for the same relMSE is interpolated on its log-log
-    time/error curve; value = that time / the cached render's time at 16 spp."""
+    The cached tracer renders a 60-frame orbit (0.5 degrees per frame about
+    the vertical axis, a new sampler seed per frame) at --nrc-spp samples per
+    pixel, training the cache online in every frame (--nrc-train-steps
+    optimiser steps per batch on that frame's own unbiased training paths)
+    and querying the moving average of its parameters. Nothing is trained
+    outside the frames themselves, and every frame is charged its own
+    training: each frame is the first render of a freshly prepared scene, its
+    time the device time (wall time beside it) of that render. The last
+    --nrc-eval-frames frames are evaluated: per frame a reference of
+    --ref-spp samples per pixel of the plain tracer accumulated in FP64 over
+    renders of other seeds, and the plain tracer's curve of device time
+    against relMSE (renders of 1..64 spp, each the first render of a fresh
+    prepared scene too). For each evaluated frame the time the plain tracer
+    needs for the cached frame's relMSE is interpolated on that curve;
+    value = the geometric mean over the evaluated frames of that time / the
+    cached frame's time."""
     import dataclasses
 
     import torch
@@ -510,14 +542,17 @@ def run_nrc(args):
     from yaoray_b200.nrc import RadianceCache
     from yaoray_b200.render import CudaBackend, build_two_level_bvh
 
-    W, H, CLAMP, C_SPREAD, DECAY, WARM, ORBIT_DEG = args.nrc_width, args.nrc_height, 20.0, 1.0e-4, 0.995, 60, 0.5
-    SEEDS = (7, 8, 9)
+    W, H, CLAMP, C_SPREAD, DECAY, ORBIT_DEG = args.nrc_width, args.nrc_height, 20.0, 1.0e-4, 0.995, 0.5
+    FRAMES, EVAL, SPP = args.nrc_frames, args.nrc_eval_frames, args.nrc_spp
     base = instanced.scene(width=W, height=H, spp=1)
     base.radiance_clamp = CLAMP
     accel = build_two_level_bvh(base.geometry)
 
-    def scene(spp, seed):
-        return dataclasses.replace(base, spp=spp, seed=seed)
+    def view(k):  # orbit frame k; the last frame is the canonical view
+        return instanced.camera(orbit=math.radians((k - FRAMES + 1) * ORBIT_DEG))
+
+    def scene(spp, seed, k):
+        return dataclasses.replace(base, spp=spp, seed=seed, camera=view(k))
 
     def relmse(img, ref):
         return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
@@ -525,105 +560,112 @@ def run_nrc(args):
     backend = CudaBackend()
     lo = base.geometry.positions.min(0)
     extent = float((base.geometry.positions.max(0) - lo).max())
-    ref = np.zeros((H, W, 3), np.float64)
-    per = 128
-    for k in range(max(1, args.ref_spp // per)):
-        p = backend.prepare(scene(per, 1000 + k), accel)
-        ref += backend.render(p).linear()
-        p.close()
-    ref /= max(1, args.ref_spp // per)
-
-    def timed(prep):
-        backend.render(prep)  # graph capture
-        torch.cuda.synchronize()
-        r = backend.render(prep)
-        return r.linear(), r.stats
 
     # The render autotuner's queue capacity and launch shape per spp level,
-    # found on the plain tracer and used by both tracers.
+    # found on the plain tracer at the canonical view and used by both tracers.
+    levels = (1, 2, 4, 8, 16, 32, 64)
     tunings = {}
     if not args.no_autotune:
-        for spp in (1, 2, 4, 8, 16, 32, 64):
-            p = backend.prepare(scene(spp, SEEDS[0]), accel)
+        for spp in sorted(set(levels) | {SPP}):
+            p = backend.prepare(scene(spp, 7, FRAMES - 1), accel)
             tunings[spp] = p.autotune()
             p.close()
 
-    def prepare(spp, seed):
-        p = backend.prepare(scene(spp, seed), accel)
+    def prepare(spp, seed, k):
+        p = backend.prepare(scene(spp, seed, k), accel)
         if spp in tunings:
             p.set_tuning(tunings[spp])
         return p
 
-    plain = []
-    for spp in (1, 2, 4, 8, 16, 32, 64):
-        errs, secs = [], []
-        for seed in SEEDS:
-            p = prepare(spp, seed)
-            img, st = timed(p)
-            errs.append(relmse(img, ref))
-            secs.append(st["device_seconds"])
+    def first_render(p):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = backend.render(p)
+        wall = time.perf_counter() - t0
+        return r.linear(), r.stats, wall
+
+    evaluated = list(range(FRAMES - EVAL, FRAMES))
+    refs, curves = {}, {}
+    for k in evaluated:
+        ref = np.zeros((H, W, 3), np.float64)
+        per = min(128, args.ref_spp)
+        for j in range(max(1, args.ref_spp // per)):
+            p = backend.prepare(scene(per, 1000 + 97 * k + j, k), accel)
+            ref += backend.render(p).linear()
             p.close()
-        plain.append((spp, float(np.mean(errs)), float(np.mean(secs))))
+        refs[k] = ref / max(1, args.ref_spp // per)
+        curve = []
+        for spp in levels:
+            p = prepare(spp, 5000 + 13 * k + spp, k)
+            img, st, wall = first_render(p)
+            curve.append((spp, relmse(img, refs[k]), st["device_seconds"], wall))
+            p.close()
+        curves[k] = curve
+
     cache = RadianceCache(lo, extent, seed=1)
     cache.set_average_decay(DECAY)
-    warm_s = 0.0
-    for k in range(WARM):  # a seeded camera orbit that ends at the evaluated view
-        frame = dataclasses.replace(base, spp=2, seed=100 + k,
-                                    camera=instanced.camera(orbit=math.radians((k - WARM) * ORBIT_DEG)))
-        w = backend.prepare(frame, accel)
-        w.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=4, averaged=True)
-        warm_s += backend.render(w).stats["device_seconds"]
-        w.close()
-    cached = []
+    frames = []
     launches = 0
     with ClockSampler(0) as clocks:
-        for spp in (1, 4, 16):
-            errs, secs, queries, segs = [], [], [], []
-            for seed in SEEDS:
-                p = prepare(spp, seed)
-                p.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=1, averaged=True)
-                img, st = timed(p)
-                errs.append(relmse(img, ref))
-                secs.append(st["device_seconds"])
-                queries.append(st["cache_queries"])
-                segs.append(st["rays_traced"])
-                launches += int(st["kernel_launches"])
-                p.close()
-            cached.append((spp, float(np.mean(errs)), float(np.mean(secs)), int(np.mean(queries)),
-                           int(np.mean(segs))))
+        for k in range(FRAMES):
+            p = prepare(SPP, 100 + k, k)
+            p.set_radiance_cache(cache, spread_threshold=C_SPREAD, train_steps=args.nrc_train_steps, averaged=True)
+            img, st, wall = first_render(p)
+            launches += int(st["kernel_launches"])
+            frames.append({"frame": k, "ms": st["device_seconds"] * 1e3, "wall_ms": wall * 1e3,
+                           "relmse": relmse(img, refs[k]) if k in refs else None,
+                           "cache_queries": int(st["cache_queries"]), "path_segments": int(st["rays_traced"])})
+            p.close()
     cache.check()
     cache.close()
 
-    def plain_time_for(err):
-        pts = sorted(plain, key=lambda x: -x[1])  # decreasing error
-        for (s0, e0, t0), (s1, e1, t1) in zip(pts, pts[1:]):
-            if e1 <= err <= e0:
-                f = (np.log(err) - np.log(e0)) / (np.log(e1) - np.log(e0))
-                return float(np.exp(np.log(t0) + f * (np.log(t1) - np.log(t0))))
-        # beyond the curve: extrapolate with relMSE ~ 1/time from the last point
-        s1, e1, t1 = pts[-1]
-        return float(t1 * e1 / err)
+    def plain_time_for(curve, err, col):
+        pts = sorted(curve, key=lambda x: -x[1])  # decreasing error
+        for a, b in zip(pts, pts[1:]):
+            if b[1] <= err <= a[1]:
+                f = (np.log(err) - np.log(a[1])) / (np.log(b[1]) - np.log(a[1]))
+                return float(np.exp(np.log(a[col]) + f * (np.log(b[col]) - np.log(a[col]))))
+        last = pts[-1] if err < pts[-1][1] else pts[0]
+        return float(last[col] * last[1] / err)  # beyond the curve: relMSE ~ 1 / time
 
-    ratios = {spp: plain_time_for(e) / t for spp, e, t, _, _ in cached}
-    line = {"metric": "equal-relMSE time ratio, plain / neural-cached (instanced scene)",
-            "value": round(ratios[16], 3), "unit": "x", "n_gpus": 1, "steps": 1, "warmup": 1,
-            "ms_per_step": round(cached[-1][2] * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 render, bf16 MLP", "data": "synthetic",
-            "config": {"workload": f"instanced-{W}x{H}-depth16-clamp20", "reference_spp": args.ref_spp,
-                       "reference_accumulation": "fp64", "spread_threshold": C_SPREAD,
-                       "seeds_per_point": len(SEEDS), "warmup_frames": WARM,
-                       "warmup_orbit": f"{WARM} frames of 2 spp, {ORBIT_DEG} degrees apart about the vertical axis, "
-                                       "ending one step before the evaluated view",
+    per_frame = []
+    for f in frames:
+        k = f["frame"]
+        if k not in refs:
+            continue
+        dev = plain_time_for(curves[k], f["relmse"], 2) / (f["ms"] / 1e3)
+        wall = plain_time_for(curves[k], f["relmse"], 3) / (f["wall_ms"] / 1e3)
+        per_frame.append({"frame": k, "cached_ms": round(f["ms"], 3), "cached_wall_ms": round(f["wall_ms"], 2),
+                          "relmse": round(f["relmse"], 5), "cache_queries": f["cache_queries"],
+                          "path_segments": f["path_segments"], "ratio_device_time": round(dev, 3),
+                          "ratio_wall_time": round(wall, 3),
+                          "plain": [{"spp": s_, "relmse": round(e, 5), "ms": round(t * 1e3, 3),
+                                     "wall_ms": round(w_ * 1e3, 2)} for s_, e, t, w_ in curves[k]]})
+    value = float(np.exp(np.mean([np.log(x["ratio_device_time"]) for x in per_frame])))
+    wall_value = float(np.exp(np.mean([np.log(x["ratio_wall_time"]) for x in per_frame])))
+    train_ms = [f["ms"] for f in frames]
+    line = {"metric": "equal-relMSE time ratio, plain / neural-cached (instanced scene, steady-state orbit frames)",
+            "value": round(value, 3), "unit": "x", "n_gpus": 1, "steps": EVAL, "warmup": FRAMES - EVAL,
+            "ms_per_step": round(float(np.mean([x["cached_ms"] for x in per_frame])), 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 render, bf16 MLP", "data": "synthetic",
+            "config": {"workload": f"instanced-{W}x{H}-depth16-clamp20-orbit{FRAMES}", "reference_spp": args.ref_spp,
+                       "reference_accumulation": "fp64", "spread_threshold": C_SPREAD, "spp_per_frame": SPP,
+                       "train_steps_per_batch": args.nrc_train_steps,
+                       "orbit": f"{FRAMES} frames, {ORBIT_DEG} degrees apart about the vertical axis, a new sampler "
+                                "seed per frame; the cache trains online in every frame and nowhere else",
+                       "evaluated_frames": evaluated, "timing": "every render is the first of a freshly prepared "
+                       "scene: device time excludes its graph capture, wall time includes it",
                        "queue_capacity_per_spp": {s_: t["capacity"] for s_, t in tunings.items()},
                        "cache": "16x2^19x2 hash grid + SH4, 64x5 MLP, bf16 tcgen05, Adam 1e-2, "
                                 f"parameter moving average {DECAY}",
-                       "cache_warmup_ms": round(warm_s * 1e3, 2)},
-            "plain": [{"spp": s_, "relmse": round(e, 5), "ms": round(t * 1e3, 3)} for s_, e, t in plain],
-            "cached": [{"spp": s_, "relmse": round(e, 5), "ms": round(t * 1e3, 3), "cache_queries": q,
-                        "path_segments": n, "equal_relmse_ratio": round(ratios[s_], 3)}
-                       for s_, e, t, q, n in cached],
+                       "orbit_frame_ms": {"first": round(train_ms[0], 3), "median": round(float(np.median(train_ms)), 3)}},
+            "per_frame": per_frame,
+            "wall_time_ratio": round(wall_value, 3),
             "gpu_launches": launches,
-            "e2e": None, "cpu_baseline": None, "clocks": clocks.summary()}
+            "e2e": {"value": round(wall_value, 3), "unit": "x", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": W * H * 56,
+                    "note": "the same ratio from host wall clock around each render call (films read back)"},
+            "cpu_baseline": None, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
 
 
@@ -708,9 +750,13 @@ def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--workload", choices=["traversal", "cornell", "textured", "cutout", "instanced", "nrc", "jobs"],
                     default="traversal")
-    ap.add_argument("--nrc-width", type=int, default=960)
-    ap.add_argument("--nrc-height", type=int, default=540)
+    ap.add_argument("--nrc-width", type=int, default=1920)
+    ap.add_argument("--nrc-height", type=int, default=1080)
     ap.add_argument("--ref-spp", type=int, default=512)
+    ap.add_argument("--nrc-frames", type=int, default=60, help="--workload nrc: orbit frames")
+    ap.add_argument("--nrc-eval-frames", type=int, default=2, help="--workload nrc: last frames evaluated")
+    ap.add_argument("--nrc-spp", type=int, default=4, help="--workload nrc: spp per orbit frame")
+    ap.add_argument("--nrc-train-steps", type=int, default=2, help="--workload nrc: optimiser steps per batch")
     ap.add_argument("--spp-scale", type=float, default=1.0, help="spp scale of --workload jobs")
     ap.add_argument("--concurrency", type=int, default=16,
                     help="--workload jobs: jobs per shared launch (and concurrent streams)")
@@ -725,6 +771,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="traversal: skip the Cornell, instanced and radiance-cache legs of the default line")
     ap.add_argument("--rays", type=int, default=RAYS_PER_STEP,
                     help="rays per step (default: the full 7,997,584; smaller only for profiling captures)")
     args = ap.parse_args()
@@ -739,7 +787,11 @@ def main():
     elif args.workload == "jobs":
         run_jobs(args)
     else:
-        run_gpu(args)
+        line = run_gpu(args)
+        if line is not None:
+            if line["n_gpus"] == 1 and not args.no_extras:
+                line["workloads"] = run_extra_legs()
+            print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

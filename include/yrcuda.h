@@ -882,6 +882,12 @@ typedef struct yrc_nrc yrc_nrc;
 yrc_status yrc_nrc_create(const float box_lo[3], float box_extent, uint64_t seed, yrc_nrc** out);
 void yrc_nrc_destroy(yrc_nrc* cache);
 
+/* Makes `dst` an exact copy of `src` (same device): parameters, optimiser
+ * moments, step count, moving average and its decay, and the encoding's box.
+ * Synchronous. For evaluating a trained cache several times from the same
+ * state. No counterpart in the reference. */
+yrc_status yrc_nrc_copy_state(yrc_nrc* dst, yrc_nrc* src);
+
 /* Host copies of the fp32 master parameters (either pointer may be NULL). */
 yrc_status yrc_nrc_set_params(yrc_nrc* cache, const float* weights, const float* grid);
 yrc_status yrc_nrc_get_params(yrc_nrc* cache, float* weights_out, float* grid_out);

@@ -177,3 +177,44 @@ def test_training_learns_a_radiance_function(cuda):
     c.close()
     assert after < 0.1 * before, (before, after)
     assert after < 0.05, after
+
+
+def test_copied_state_matches_and_trains_alike(cuda):
+    """yrc_nrc_copy_state copies everything an optimiser step reads. Right
+    after the copy, parameters, moving averages and inference are
+    bit-identical. After the same further steps the two stay within the
+    run-to-run spread of training (gradients are summed with fp32 atomics, so
+    training is not bit-reproducible), far closer than a cache that got only
+    the parameters (fresh Adam moments and step count)."""
+    import torch
+    a = RadianceCache(LO, EXTENT, seed=5)
+    b = RadianceCache(LO, EXTENT, seed=6)
+    c = RadianceCache(LO, EXTENT, seed=7)
+    data = []
+    rng = np.random.default_rng(8)
+    for k in range(6):
+        _, flat = queries(4096, 500 + k)
+        data.append((torch.from_numpy(flat).to(cuda),
+                     torch.from_numpy(rng.uniform(0.1, 2.0, (4096, 4)).astype(np.float32)).to(cuda)))
+    for q, t in data[:3]:
+        a.train_step(q, t)
+    b.copy_from(a)
+    c.set_params(*a.get_params())
+    for x, y in zip(a.get_params() + a.get_averaged_params(), b.get_params() + b.get_averaged_params()):
+        assert x.tobytes() == y.tobytes()
+    _, flat = queries(2048, 77)
+    qt = torch.from_numpy(flat).to(cuda)
+    assert torch.equal(a.infer(qt), b.infer(qt))
+    for q, t in data[3:]:
+        for m in (a, b, c):
+            m.train_step(q, t)
+    for m in (a, b, c):
+        m.check()
+    wa, ga = a.get_params()
+    wb, gb = b.get_params()
+    wc, gc = c.get_params()
+    copy_gap = rel_fro(wb, wa) + rel_fro(gb, ga)
+    params_only_gap = rel_fro(wc, wa) + rel_fro(gc, ga)
+    assert copy_gap < 1e-3 and copy_gap < 0.05 * params_only_gap, (copy_gap, params_only_gap)
+    for m in (a, b, c):
+        m.close()

@@ -196,6 +196,7 @@ def lib() -> C.CDLL:
         "yrc_nrc_train_step": (C.c_int, [P, P, P, I64, P, P]),
         "yrc_nrc_gradients": (C.c_int, [P, P, P, I64, P, P, P]),
         "yrc_nrc_check": (C.c_int, [P]),
+        "yrc_nrc_copy_state": (C.c_int, [P, P]),
         "yrc_sampler_eval": (C.c_int, [I32, C.c_uint64, I32, P, I64, I32, P]),
         "yrc_rng_eval": (C.c_int, [P, I64, I32, P]),
         "yrc_pixel_seed_eval": (C.c_int, [C.c_uint64, P, I64, P]),

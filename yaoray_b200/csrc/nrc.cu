@@ -784,6 +784,44 @@ void yrc_nrc_destroy(yrc_nrc* c) {
     delete c;
 }
 
+yrc_status yrc_nrc_copy_state(yrc_nrc* dst, yrc_nrc* src) {
+    using namespace yrc;
+    using namespace yrc::nrc;
+    if (!dst || !src || dst == src) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_nrc_copy_state: bad argument");
+    if (dst->device != src->device) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_nrc_copy_state: caches on different devices");
+    }
+    std::scoped_lock lock(dst->mutex, src->mutex);
+    cudaSetDevice(src->device);
+    cudaError_t err = cudaDeviceSynchronize();
+    auto copy = [&](void* d, const void* s_, size_t bytes) {
+        if (err == cudaSuccess) err = cudaMemcpy(d, s_, bytes, cudaMemcpyDeviceToDevice);
+    };
+    copy(dst->table, src->table, sizeof(__half) * kGridParams);
+    copy(dst->table_master, src->table_master, sizeof(float) * kGridParams);
+    copy(dst->table_m, src->table_m, sizeof(float) * kGridParams);
+    copy(dst->table_v, src->table_v, sizeof(float) * kGridParams);
+    copy(dst->w, src->w, sizeof(__nv_bfloat16) * kWeightCount);
+    copy(dst->w_master, src->w_master, sizeof(float) * kWeightCount);
+    copy(dst->w_m, src->w_m, sizeof(float) * kWeightCount);
+    copy(dst->w_v, src->w_v, sizeof(float) * kWeightCount);
+    copy(dst->table_avg_master, src->table_avg_master, sizeof(float) * kGridParams);
+    copy(dst->table_avg, src->table_avg, sizeof(__half) * kGridParams);
+    copy(dst->w_avg_master, src->w_avg_master, sizeof(float) * kWeightCount);
+    copy(dst->w_avg, src->w_avg, sizeof(__nv_bfloat16) * kWeightCount);
+    copy(dst->step, src->step, sizeof(int64_t));
+    if (err != cudaSuccess) return CudaFailN(err, "state copy");
+    // The encoding's box and level scales; the table pointer stays dst's own.
+    for (int l = 0; l < kLevels; ++l) {
+        dst->grid.scale[l] = src->grid.scale[l];
+        dst->grid.side[l] = src->grid.side[l];
+    }
+    for (int k = 0; k < 3; ++k) dst->grid.lo[k] = src->grid.lo[k];
+    dst->grid.inv = src->grid.inv;
+    dst->avg_decay = src->avg_decay;
+    return Ok();
+}
+
 yrc_status yrc_nrc_set_params(yrc_nrc* c, const float* weights, const float* grid) {
     using namespace yrc;
     using namespace yrc::nrc;

@@ -39,6 +39,12 @@ class RadianceCache:
         except Exception:
             pass
 
+    def copy_from(self, other: "RadianceCache") -> None:
+        """Makes this cache an exact copy of `other` (parameters, optimiser
+        state, moving average), e.g. to evaluate one trained state several
+        times."""
+        check(lib().yrc_nrc_copy_state(self._handle, other._handle))
+
     def set_params(self, weights: np.ndarray | None = None, grid: np.ndarray | None = None) -> None:
         """weights (6, 64, 64) and grid (16, 2^19, 2) float32 master values."""
         w = None if weights is None else np.ascontiguousarray(weights, np.float32)
