@@ -126,6 +126,59 @@ struct yrc_render_scene {
 
 namespace yrc {
 namespace {
+// The shadow stage of a bounce over the queued shadow rays: the exact
+// per-thread loop (cut-outs, textured thin glass), the single-pass
+// transmittance kernel with its exact-loop overflow (surfaces that pass
+// light), or the any-hit kernel.
+cudaError_t ShadowStage(yrc_render_scene* s, const Queues& q, int64_t C, int* error, cudaStream_t st) {
+    const DevScene& sc = s->dev;
+    cudaError_t err = cudaSuccess;
+    if (sc.exact_shadows) {
+        LaunchShadowExact(sc, q, s->transmittance, q.counters + kCtrStatsBase + 2, 2 * C, s->sm_count, error,
+                          st);
+        err = cudaGetLastError();
+    } else if (sc.any_transparent) {
+        ShadowArgs sa{};
+        sa.accel = sc.accel;
+        sa.rays = q.shadow_ray;
+        sa.count_ptr = q.counters + kCtrShadow;
+        sa.capacity = 2 * C;
+        sa.out_index = q.shadow_slot;
+        sa.transmittance = s->transmittance;
+        sa.tri_prim = sc.tri_prim;
+        sa.prim_material = sc.prim_material;
+        sa.sphere_material = sc.sphere_material;
+        sa.materials = sc.materials;
+        sa.tri_clear = sc.tri_clear;
+        sa.sphere_clear = sc.sphere_clear;
+        sa.counter = q.counters + kCtrShadowTrace;
+        sa.occluded_count = q.counters + kCtrStatsBase + 2;
+        sa.overflow = q.shadow_overflow;
+        sa.overflow_count = q.counters + kCtrShadowOverflow;
+        sa.error = error;
+        err = LaunchShadowTransmittance(sa, st, s->sm_count);
+        // Rays past more than 16 clear surfaces: the exact loop.
+        if (err == cudaSuccess) {
+            LaunchShadowExact(sc, q, s->transmittance, q.counters + kCtrStatsBase + 2, 2 * C, s->sm_count,
+                              error, st, q.shadow_overflow);
+            err = cudaGetLastError();
+        }
+    } else {
+        TraceArgs sh{};
+        sh.accel = sc.accel;
+        sh.rays = q.shadow_ray;
+        sh.count = 2 * C;
+        sh.count_ptr = q.counters + kCtrShadow;
+        sh.occluded = q.shadow_occluded;
+        sh.out_index = q.shadow_slot;
+        sh.counter = q.counters + kCtrShadowTrace;
+        sh.occluded_count = q.counters + kCtrStatsBase + 2;
+        sh.error = error;
+        err = LaunchTrace(sh, true, false, TraceShapeOf(s->accel, 1), st, s->sm_count);
+    }
+    return err;
+}
+
 // Releases the scene's captured batch (executable and template).
 void DropGraph(yrc_render_scene* s) {
     if (s->graph) cudaGraphExecDestroy(s->graph);
@@ -364,6 +417,7 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
                                 ? m.measured_index
                                 : -1;
         if (m.kind == YRC_MAT_DIELECTRIC || m.kind == YRC_MAT_THIN_DIELECTRIC) transparent = true;
+        if (m.kind == YRC_MAT_COATED_DIFFUSE || m.kind == YRC_MAT_COATED_CONDUCTOR) d.any_layered = 1;
         const bool tex_alpha = m.alpha_texture >= 0 && m.alpha_texture < desc->texture_count;
         const bool tex_refl = m.reflectance_texture >= 0 && m.reflectance_texture < desc->texture_count;
         if (m.alpha < 0.5f || tex_alpha) d.any_alpha = 1;
@@ -653,6 +707,7 @@ yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     ps.nee_tp = W.Alloc<float4>(capacity);
     ps.spread = W.Alloc<float2>(capacity);
     ps.nee_vis = nullptr;
+    ps.defer = s->dev.any_layered ? W.Alloc<float4>(5 * capacity) : nullptr;
     Queues& q = s->q;
     q.ray_in = W.Alloc<float4>(2 * capacity);
     q.path_in = W.Alloc<int32_t>(capacity);
@@ -666,6 +721,8 @@ yrc_status EnsureWork(yrc_render_scene* s, int64_t capacity) {
     q.shadow_overflow =
         (s->dev.any_transparent && !s->dev.exact_shadows) ? W.Alloc<int32_t>(2 * capacity) : nullptr;
     q.nee_paths = W.Alloc<int32_t>(capacity);
+    q.defer_paths = s->dev.any_layered ? W.Alloc<int32_t>(capacity) : nullptr;
+    q.defer_paths2 = s->dev.any_layered ? W.Alloc<int32_t>(capacity) : nullptr;
     q.order = W.Alloc<int32_t>(capacity);
     q.shade_class = W.Alloc<uint8_t>(capacity);
     q.tex_normal = s->dev.texture_count > 0 ? W.Alloc<float4>(capacity) : nullptr;
@@ -795,51 +852,17 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
             if (perr != cudaSuccess) return CudaError(perr, "subsurface probe");
             LaunchSubsurfaceExit(sc, s->ps, q, depth, C, s->sm_count, st);
         }
-        if (sc.exact_shadows) {
-            LaunchShadowExact(sc, q, s->transmittance, q.counters + kCtrStatsBase + 2, 2 * C, s->sm_count, ta.error,
-                              st);
-            err = cudaGetLastError();
-        } else if (sc.any_transparent) {
-            ShadowArgs sa{};
-            sa.accel = sc.accel;
-            sa.rays = q.shadow_ray;
-            sa.count_ptr = q.counters + kCtrShadow;
-            sa.capacity = 2 * C;
-            sa.out_index = q.shadow_slot;
-            sa.transmittance = s->transmittance;
-            sa.tri_prim = sc.tri_prim;
-            sa.prim_material = sc.prim_material;
-            sa.sphere_material = sc.sphere_material;
-            sa.materials = sc.materials;
-            sa.tri_clear = sc.tri_clear;
-            sa.sphere_clear = sc.sphere_clear;
-            sa.counter = q.counters + kCtrShadowTrace;
-            sa.occluded_count = q.counters + kCtrStatsBase + 2;
-            sa.overflow = q.shadow_overflow;
-            sa.overflow_count = q.counters + kCtrShadowOverflow;
-            sa.error = ta.error;
-            err = LaunchShadowTransmittance(sa, st, s->sm_count);
-            // Rays past more than 16 clear surfaces: the exact loop.
-            if (err == cudaSuccess) {
-                LaunchShadowExact(sc, q, s->transmittance, q.counters + kCtrStatsBase + 2, 2 * C, s->sm_count,
-                                  ta.error, st, q.shadow_overflow);
-                err = cudaGetLastError();
-            }
-        } else {
-            TraceArgs sh{};
-            sh.accel = sc.accel;
-            sh.rays = q.shadow_ray;
-            sh.count = 2 * C;
-            sh.count_ptr = q.counters + kCtrShadow;
-            sh.occluded = q.shadow_occluded;
-            sh.out_index = q.shadow_slot;
-            sh.counter = q.counters + kCtrShadowTrace;
-            sh.occluded_count = q.counters + kCtrStatsBase + 2;
-            sh.error = ta.error;
-            err = LaunchTrace(sh, true, false, TraceShapeOf(s->accel, 1), st, s->sm_count);
-        }
+        err = ShadowStage(s, q, C, ta.error, st);
         if (err != cudaSuccess) return CudaError(err, "shadow trace");
         LaunchNeeResolve(s->ps, q, s->transmittance, C, s->sm_count, st);
+        if (sc.any_layered) {
+            // Coated vertices: their next events in the reference's PCG32
+            // order, with a second shadow stage in between.
+            LaunchLayeredNee(sc, s->ps, q, s->transmittance, depth, C, s->sm_count, st);
+            err = ShadowStage(s, q, C, ta.error, st);
+            if (err != cudaSuccess) return CudaError(err, "coated-vertex shadow trace");
+            LaunchLayeredContinue(sc, s->ps, q, s->transmittance, depth, C, s->sm_count, st);
+        }
         LaunchAdvanceQueue(q, st);
         std::swap(q.ray_in, q.ray_out);
         std::swap(q.path_in, q.path_out);

@@ -146,6 +146,8 @@ __global__ void ResetCountersKernel(Queues q) {
         q.counters[kCtrShadowTrace] = 0;
         q.counters[kCtrShadowOverflow] = 0;
         q.counters[kCtrProbe] = 0;
+        q.counters[kCtrDefer] = 0;
+        q.counters[kCtrDefer2] = 0;
         for (int c = 0; c < kShadeClasses; ++c) {
             q.counters[kCtrClass0 + c] = 0;
             q.counters[kCtrCursor0 + c] = 0;
@@ -835,6 +837,64 @@ __device__ inline void NextEvent(const DevScene& sc, PathState& ps, Queues& q, i
     }
 }
 
+// A coated (layered) vertex, whose BSDF evaluations draw from the path's
+// PCG32 stream. EstimateDirectLight (src/integrators/path_direct_lighting.cpp:
+// 170-283) evaluates the BSDF for an emissive light sample only after its
+// shadow ray came back visible, then evaluates it for the analytic and the
+// environment samples before their shadow rays, draws the environment pdf
+// after its ray, and the continuation is sampled after all of that
+// (path_integrator.cpp:93-173). To draw in that order the vertex is kept
+// (PathState::defer) and finished in two later stages: here only the
+// emissive light sample and its shadow ray, which need no BSDF; then
+// LayeredNeeKernel after the shadow stage, and LayeredContinueKernel after a
+// second shadow stage for the analytic and environment rays.
+__device__ inline void DeferLayeredVertex(const DevScene& sc, PathState& ps, Queues& q, int32_t path,
+                                          PixelSampler& smp, int depth, const Mat& m, int32_t material, V3 p, V3 n,
+                                          V3 wo, uint32_t& flags) {
+    float4* v = ps.defer + 5 * static_cast<int64_t>(path);
+    v[0] = ToF4(p, __int_as_float(material));
+    v[1] = ToF4(n, __int_as_float(m.kind));
+    v[2] = ToF4(wo, 0.0f);
+    v[3] = ToF4(m.reflectance, 0.0f);
+    flags &= ~(kPathDeferEmissive | kPathDeferAnalytic | kPathDeferEnvironment);
+    if (sc.emissive_count > 0) {
+        const float us = smp.Sample1D(kDimDirectLightSelect, depth);
+        float tx, ty;
+        smp.Sample2D(kDimDirectLightSurface, depth, tx, ty);
+        const LightSample ls = SampleEmissive(sc, us, tx, ty);
+        if (ls.valid && ls.pdf > 0.0f && !IsBlack(ls.radiance)) {
+            const V3 to_light = ls.point - p;
+            const float dsq = LengthSq(to_light);
+            if (dsq > kMinShadowBias * kMinShadowBias) {
+                const float dist = sqrtf(dsq);
+                const float sb = ShadowBias(p, ls.point, dist);
+                if (dist > sb) {
+                    const V3 so = p + n * sb;
+                    const V3 stl = ls.point - so;
+                    const float sdsq = LengthSq(stl);
+                    if (sdsq > kMinShadowBias * kMinShadowBias) {
+                        const float sd = sqrtf(sdsq);
+                        const V3 wi = stl / sd;
+                        const float cs = fmaxf(0.0f, Dot(n, wi));
+                        if (cs > 0.0f) {
+                            const float pl = PdfEmissiveSolidAngle(sc, p, ls.point, ls.normal, ls.emissive);
+                            if (pl > 0.0f) {
+                                CountStat(q.counters, kStatShadow);
+                                ps.nee[3 * path + 0] = ToF4(ls.radiance, cs);
+                                v[4] = ToF4(wi, pl);
+                                PushShadow(q, so, wi, sd - sb, 3 * path + 0);
+                                flags |= kPathDeferEmissive;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    const unsigned long long k = QueueAppend(q.counters + kCtrDefer);
+    q.defer_paths[k] = path;
+}
+
 // Radiance-cache query of a surface vertex (the 16-float layout of
 // yrc_nrc_infer): position, roughness, direction towards the viewer,
 // shading normal, diffuse and specular albedo.
@@ -848,6 +908,62 @@ __device__ __forceinline__ void WriteCacheQuery(float* out, V3 p, V3 wo, V3 n, c
     o[1] = make_float4(wo.x, wo.y, wo.z, n.x);
     o[2] = make_float4(n.y, n.z, kd.x, kd.y);
     o[3] = make_float4(kd.z, ks, ks, ks);
+}
+
+// The end of a surface vertex of IntegratePathSample (src/integrators/
+// path_integrator.cpp:171-192): the continuation sampled from the BSDF,
+// Russian roulette from depth 3, the medium state after a thick-dielectric
+// transmission and the next bounce's ray queued; then the path's throughput,
+// radiance, flags and PCG32 state are stored.
+__device__ inline void ContinuePath(const DevScene& sc, PathState& ps, Queues& q, int32_t path, int depth,
+                                    const Mat& m, int32_t material, V3 p, V3 n, V3 wo, V3 tp, V3 rad,
+                                    uint32_t flags, PixelSampler& smp, Pcg32& rng) {
+    bool cont = depth + 1 < sc.max_depth;
+    BsdfSample bs = NoSample();
+    if (cont) {
+        float bx, by;
+        smp.Sample2D(kDimBsdf, depth, bx, by);
+        bs = SampleBsdf(m, wo, n, bx, by, rng);
+        cont = bs.valid && !IsBlack(bs.weight);
+    }
+    if (cont) {
+        tp = Mul(tp, bs.weight);
+        // SurviveRussianRoulette (path_integrator_common.cpp:185-201)
+        if (depth >= 3) {
+            const float survival = Clampf(MaxComp(tp), 0.05f, 0.95f);
+            if (smp.Sample1D(kDimRussianRoulette, depth) >= survival) {
+                cont = false;
+            } else {
+                tp = tp / survival;
+            }
+        }
+    }
+    if (cont) {
+        // UpdateMediumStateAfterBsdf (path_integrator_common.cpp:108-123)
+        if (m.kind == kDielectric && Dot(bs.wi, n) < 0.0f) {
+            if (flags & kPathMedium) {
+                flags &= ~kPathMedium;
+            } else {
+                flags |= kPathMedium;
+                const DevMaterial& dm = sc.materials[material];
+                ps.medium[path] = make_float4(dm.absorption_color[0], dm.absorption_color[1],
+                                              dm.absorption_color[2], dm.absorption_distance);
+            }
+        }
+        flags |= kPathPrevValid;
+        flags = bs.specular ? (flags | kPathPrevDelta) : (flags & ~kPathPrevDelta);
+        ps.prev[path] = ToF4(p, bs.pdf);
+        const V3 bn = Dot(bs.wi, n) >= 0.0f ? n : -n;
+        const V3 no = p + bn * SurfaceBias(p);
+        const unsigned long long k = QueueAppend(q.counters + kCtrOut);
+        q.ray_out[2 * k] = make_float4(no.x, no.y, no.z, 1.0e-5f);
+        q.ray_out[2 * k + 1] = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, __int_as_float(0x7f800000));
+        q.path_out[k] = path;
+    }
+    ps.throughput[path] = ToF4(tp);
+    ps.radiance[path] = ToF4(rad);
+    ps.flags[path] = flags;
+    ps.rng_state[path] = rng.state;
 }
 
 // The material kind a shading class folds to (-1: any kind).
@@ -1259,6 +1375,16 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
         smp.Init(sc.sampler, sc.seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
         Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
 
+        // --- coated vertex: next events and continuation in the reference's
+        // PCG32 order, after the shadow stages (DeferLayeredVertex)
+        if ((kClass == kClassCoatedDiffuse || kClass == kClassGeneric) && IsLayered(m.kind) && !IsDelta(m)) {
+            DeferLayeredVertex(sc, ps, q, path, smp, depth, m, s.material, s.p, s.n, wo, flags);
+            ps.throughput[path] = ToF4(tp);
+            ps.radiance[path] = ToF4(rad);
+            ps.flags[path] = flags;
+            continue;
+        }
+
         // --- next-event estimation: samples now, visibility in the shadow stage
         if (!IsDelta(m)) NextEvent(sc, ps, q, path, smp, rng, depth, m, s.p, s.n, wo, tp, flags);
 
@@ -1334,52 +1460,7 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
             continue;
         }
 
-        bool cont = depth + 1 < sc.max_depth;
-        BsdfSample bs = NoSample();
-        if (cont) {
-            float bx, by;
-            smp.Sample2D(kDimBsdf, depth, bx, by);
-            bs = SampleBsdf(m, wo, s.n, bx, by, rng);
-            cont = bs.valid && !IsBlack(bs.weight);
-        }
-        if (cont) {
-            tp = Mul(tp, bs.weight);
-            // SurviveRussianRoulette (path_integrator_common.cpp:185-201)
-            if (depth >= 3) {
-                const float survival = Clampf(MaxComp(tp), 0.05f, 0.95f);
-                if (smp.Sample1D(kDimRussianRoulette, depth) >= survival) {
-                    cont = false;
-                } else {
-                    tp = tp / survival;
-                }
-            }
-        }
-        if (cont) {
-            // UpdateMediumStateAfterBsdf (path_integrator_common.cpp:108-123)
-            if (m.kind == kDielectric && Dot(bs.wi, s.n) < 0.0f) {
-                if (flags & kPathMedium) {
-                    flags &= ~kPathMedium;
-                } else {
-                    flags |= kPathMedium;
-                    const DevMaterial& dm = sc.materials[s.material];
-                    ps.medium[path] = make_float4(dm.absorption_color[0], dm.absorption_color[1],
-                                                  dm.absorption_color[2], dm.absorption_distance);
-                }
-            }
-            flags |= kPathPrevValid;
-            flags = bs.specular ? (flags | kPathPrevDelta) : (flags & ~kPathPrevDelta);
-            ps.prev[path] = ToF4(s.p, bs.pdf);
-            const V3 bn = Dot(bs.wi, s.n) >= 0.0f ? s.n : -s.n;
-            const V3 no = s.p + bn * SurfaceBias(s.p);
-            const unsigned long long k = QueueAppend(q.counters + kCtrOut);
-            q.ray_out[2 * k] = make_float4(no.x, no.y, no.z, 1.0e-5f);
-            q.ray_out[2 * k + 1] = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, __int_as_float(0x7f800000));
-            q.path_out[k] = path;
-        }
-        ps.throughput[path] = ToF4(tp);
-        ps.radiance[path] = ToF4(rad);
-        ps.flags[path] = flags;
-        ps.rng_state[path] = rng.state;
+        ContinuePath(sc, ps, q, path, depth, m, s.material, s.p, s.n, wo, tp, rad, flags, smp, rng);
     }
 }
 
@@ -1436,6 +1517,170 @@ __global__ void NeeResolveKernel(PathState ps, Queues q, const float4* transmitt
             ps.radiance[path[j]] = ToF4(F4(rad[j]) + Mul(F4(tp[j]), sum));
             ps.flags[path[j]] = fl[j] & ~kPathNee;
         }
+    }
+}
+
+// ------------------------------------------------------ coated vertices
+
+// A queued shadow ray's outcome by its slot: the transmittance (w = 1
+// visible, all 0 occluded) or, in scenes without surfaces that pass light,
+// the any-hit flag.
+template <bool kTransmittance>
+__device__ __forceinline__ float4 SlotVisibility(const Queues& q, const float4* transmittance, int32_t slot) {
+    if (kTransmittance) return transmittance[slot];
+    const float v = q.shadow_occluded[slot] ? 0.0f : 1.0f;
+    return make_float4(v, v, v, v);
+}
+
+// The BSDF of a deferred coated vertex (the shade kernel's Mat).
+__device__ inline Mat DeferredMat(const DevScene& sc, const float4* v) {
+    Mat m = LoadMat(sc.materials[__float_as_int(v[0].w)]);
+    m.kind = __float_as_int(v[1].w);
+    m.reflectance = F4(v[3]);
+    m.measured = nullptr;
+    return m;
+}
+
+// After the shadow stage: the emissive next event of each deferred coated
+// vertex (BSDF value and pdf drawn only when its shadow ray was visible),
+// then the analytic and environment samples with their BSDF values and
+// shadow rays (queued for a second shadow stage), as EstimateDirectLight
+// orders them (path_direct_lighting.cpp:185-262, 115-168). A vertex with no
+// second-stage ray samples its continuation right away.
+template <bool kTransmittance>
+__global__ void __launch_bounds__(256, 2) LayeredNeeKernel(DevScene sc, PathState ps, Queues q,
+                                                            const float4* transmittance, int depth) {
+    const int64_t count = static_cast<int64_t>(q.counters[kCtrDefer]);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t path = q.defer_paths[i];
+        float4* v = ps.defer + 5 * static_cast<int64_t>(path);
+        const V3 p = F4(v[0]), n = F4(v[1]), wo = F4(v[2]);
+        const int32_t material = __float_as_int(v[0].w);
+        const Mat m = DeferredMat(sc, v);
+        uint32_t flags = ps.flags[path];
+        Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
+        PixelSampler smp;
+        const int32_t pixel = ps.pixel[path];
+        smp.Init(sc.sampler, sc.seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
+        V3 sum{0.0f, 0.0f, 0.0f};
+        if (flags & kPathDeferEmissive) {
+            const float4 vis = SlotVisibility<kTransmittance>(q, transmittance, 3 * path + 0);
+            if (vis.w == 1.0f) {
+                const float4 lc = ps.nee[3 * path + 0];  // radiance, cosine
+                const float4 wl = v[4];                  // direction, light pdf
+                const V3 wi = F4(wl);
+                const V3 f = EvalBsdf(m, wo, wi, n, rng);
+                if (!IsBlack(f)) {
+                    const float pb = PdfBsdf(m, wo, wi, n, rng);
+                    const float mis = PowerHeuristic(1, wl.w, 1, pb);
+                    sum = sum + Mul(f, Mul(F4(vis), F4(lc))) * (lc.w * mis / wl.w);
+                }
+            }
+            ps.nee[3 * path + 0] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        flags &= ~(kPathDeferEmissive | kPathDeferAnalytic | kPathDeferEnvironment);
+        if (sc.analytic_count > 0) {  // delta lights: no MIS against the BSDF
+            const AnalyticSample as = SampleAnalyticLight(sc.analytic, sc.analytic_count, sc.analytic_alias_prob,
+                                                          sc.analytic_alias_index, sc.analytic_alias_pmf,
+                                                          sc.analytic_tree, sc.analytic_tree_root, p,
+                                                          smp.Sample1D(kDimAnalyticLightSelect, depth));
+            if (as.valid && as.selection_pdf > 0.0f && !IsBlack(as.radiance)) {
+                const float cs = fmaxf(0.0f, Dot(n, as.wi));
+                if (cs > 0.0f) {
+                    const V3 f = EvalBsdf(m, wo, as.wi, n, rng);
+                    if (!IsBlack(f)) {
+                        CountStat(q.counters, kStatShadow);
+                        const float sb = SurfaceBias(p);
+                        ps.nee[3 * path + 1] = ToF4(Mul(f, as.radiance) * (cs / as.selection_pdf));
+                        PushShadow(q, p + n * sb, as.wi, as.distance - sb, 3 * path + 1);
+                        flags |= kPathDeferAnalytic;
+                    }
+                }
+            }
+        }
+        if (EnvSampleable(sc.env)) {
+            float tx, ty;
+            smp.Sample2D(kDimDirectLightSurface, depth, tx, ty);
+            const EnvSample es = SampleEnvironment(sc.env, tx, ty);
+            if (es.valid && es.pdf > 0.0f && !IsBlack(es.radiance)) {
+                const float cs = fmaxf(0.0f, Dot(n, es.dir));
+                if (cs > 0.0f) {
+                    const V3 f = EvalBsdf(m, wo, es.dir, n, rng);
+                    if (!IsBlack(f)) {
+                        CountStat(q.counters, kStatShadow);
+                        ps.nee[3 * path + 2] = ToF4(Mul(f, es.radiance), es.pdf);
+                        v[4] = ToF4(es.dir, cs);
+                        PushShadow(q, p + n * SurfaceBias(p), es.dir, __int_as_float(0x7f800000), 3 * path + 2);
+                        flags |= kPathDeferEnvironment;
+                    }
+                }
+            }
+        }
+        const V3 tp = F4(ps.throughput[path]);
+        const V3 rad = F4(ps.radiance[path]) + Mul(tp, sum);
+        if (flags & (kPathDeferAnalytic | kPathDeferEnvironment)) {
+            ps.radiance[path] = ToF4(rad);
+            ps.flags[path] = flags;
+            ps.rng_state[path] = rng.state;
+            const unsigned long long k = QueueAppend(q.counters + kCtrDefer2);
+            q.defer_paths2[k] = path;
+            continue;
+        }
+        ContinuePath(sc, ps, q, path, depth, m, material, p, n, wo, tp, rad, flags, smp, rng);
+    }
+}
+
+// After the second shadow stage: the analytic contribution, the environment
+// pdf (drawn only when its shadow ray was visible) and MIS weight, then the
+// continuation of each deferred coated vertex.
+template <bool kTransmittance>
+__global__ void __launch_bounds__(256, 2) LayeredContinueKernel(DevScene sc, PathState ps, Queues q,
+                                                                 const float4* transmittance, int depth) {
+    const int64_t count = static_cast<int64_t>(q.counters[kCtrDefer2]);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int32_t path = q.defer_paths2[i];
+        const float4* v = ps.defer + 5 * static_cast<int64_t>(path);
+        const V3 p = F4(v[0]), n = F4(v[1]), wo = F4(v[2]);
+        const int32_t material = __float_as_int(v[0].w);
+        const Mat m = DeferredMat(sc, v);
+        uint32_t flags = ps.flags[path];
+        Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
+        PixelSampler smp;
+        const int32_t pixel = ps.pixel[path];
+        smp.Init(sc.sampler, sc.seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
+        V3 sum{0.0f, 0.0f, 0.0f};
+        if (flags & kPathDeferAnalytic) {
+            const float4 vis = SlotVisibility<kTransmittance>(q, transmittance, 3 * path + 1);
+            if (vis.w == 1.0f) sum = sum + Mul(F4(ps.nee[3 * path + 1]), F4(vis));
+            ps.nee[3 * path + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        if (flags & kPathDeferEnvironment) {
+            const float4 vis = SlotVisibility<kTransmittance>(q, transmittance, 3 * path + 2);
+            if (vis.w == 1.0f) {
+                const float4 fl = ps.nee[3 * path + 2];  // BSDF x radiance, environment pdf
+                const float4 dc = v[4];                  // direction, cosine
+                const float pb = PdfBsdf(m, wo, F4(dc), n, rng);
+                const float mis = PowerHeuristic(1, fl.w, 1, pb);
+                sum = sum + Mul(F4(fl), F4(vis)) * (dc.w * mis / fl.w);
+            }
+            ps.nee[3 * path + 2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        flags &= ~(kPathDeferAnalytic | kPathDeferEnvironment);
+        const V3 tp = F4(ps.throughput[path]);
+        const V3 rad = F4(ps.radiance[path]) + Mul(tp, sum);
+        ContinuePath(sc, ps, q, path, depth, m, material, p, n, wo, tp, rad, flags, smp, rng);
+    }
+}
+
+// Empties the shadow queue between the two shadow stages of a bounce (the
+// first stage's results stay in their slots).
+__global__ void ResetShadowQueueKernel(Queues q) {
+    if (threadIdx.x == 0) {
+        q.counters[kCtrShadow] = 0;
+        q.counters[kCtrShadowTrace] = 0;
+        q.counters[kCtrShadowOverflow] = 0;
     }
 }
 
@@ -1761,6 +2006,23 @@ void LaunchCacheResolve(const PathState& ps, const CacheArgs& cache, int64_t cap
 }
 void LaunchCacheTargets(const PathState& ps, const CacheArgs& cache, int sm_count, cudaStream_t st) {
     CacheTargetsKernel<<<Grid(cache.train_paths, sm_count), kThreads, 0, st>>>(ps, cache);
+}
+void LaunchLayeredNee(const DevScene& sc, const PathState& ps, const Queues& q, const float4* transmittance,
+                      int depth, int64_t capacity, int sm_count, cudaStream_t st) {
+    ResetShadowQueueKernel<<<1, 32, 0, st>>>(q);
+    if (transmittance) {
+        LayeredNeeKernel<true><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, transmittance, depth);
+    } else {
+        LayeredNeeKernel<false><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, transmittance, depth);
+    }
+}
+void LaunchLayeredContinue(const DevScene& sc, const PathState& ps, const Queues& q, const float4* transmittance,
+                           int depth, int64_t capacity, int sm_count, cudaStream_t st) {
+    if (transmittance) {
+        LayeredContinueKernel<true><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, transmittance, depth);
+    } else {
+        LayeredContinueKernel<false><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, transmittance, depth);
+    }
 }
 void LaunchNeeResolve(const PathState& ps, const Queues& q, const float4* transmittance, int64_t capacity,
                       int sm_count, cudaStream_t st) {

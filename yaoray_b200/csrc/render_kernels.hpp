@@ -53,6 +53,16 @@ void LaunchSubsurfaceExit(const DevScene& sc, const PathState& ps, const Queues&
 void LaunchCacheResolve(const PathState& ps, const CacheArgs& cache, int64_t capacity, int sm_count,
                         cudaStream_t st);
 void LaunchCacheTargets(const PathState& ps, const CacheArgs& cache, int sm_count, cudaStream_t st);
+// Coated (layered) vertices deferred by the shade stage: their emissive next
+// events and the analytic / environment samples after the first shadow stage
+// (LaunchLayeredNee, which also empties the shadow queue for the second
+// stage), their analytic / environment results and continuation after the
+// second (LaunchLayeredContinue). `transmittance` is null in scenes whose
+// shadow stage is the any-hit kernel.
+void LaunchLayeredNee(const DevScene& sc, const PathState& ps, const Queues& q, const float4* transmittance,
+                      int depth, int64_t capacity, int sm_count, cudaStream_t st);
+void LaunchLayeredContinue(const DevScene& sc, const PathState& ps, const Queues& q, const float4* transmittance,
+                           int depth, int64_t capacity, int sm_count, cudaStream_t st);
 void LaunchNeeResolve(const PathState& ps, const Queues& q, const float4* transmittance, int64_t capacity,
                       int sm_count, cudaStream_t st);
 void LaunchFilm(const DevScene& sc, const PathState& ps, const BatchArgs& b, const FilmArgs& f, int64_t pixels,

@@ -157,6 +157,7 @@ struct DevScene {
     int32_t measured_count;
     int32_t any_alpha;      // a material can cut surfaces out (alpha < 0.5 or an alpha texture)
     int32_t exact_shadows;  // shadow rays take the per-thread reference loop (cut-outs, textured thin glass)
+    int32_t any_layered;    // scene has coated (layered) materials, whose vertices defer their next events
 };
 
 // Path state, structure of arrays over `capacity` slots.
@@ -176,6 +177,13 @@ struct PathState {
     float4* nee_tp;       // throughput at the vertex that made the NEE samples
     float* nee_vis;       // 3 per path: shadow transmittance (1 visible, 0 occluded)
     float2* spread;       // radiance cache: primary footprint a0, running spread sum
+    // Coated (layered) vertices, whose BSDF draws from the PCG32 stream: 5 per
+    // path, the vertex kept across the deferred next-event stages
+    // (LayeredNeeKernel, LayeredContinueKernel): [0] position + material
+    // index bits, [1] shading normal, [2] direction to the viewer, [3]
+    // reflectance (texture scale applied), [4] the pending light direction +
+    // its pdf (emissive) or cosine (environment).
+    float4* defer;
 };
 
 // Radiance-cache stage of the path tracer (device pointers; all counts live
@@ -210,6 +218,11 @@ constexpr uint32_t kPathMedium = 1u << 2;
 constexpr uint32_t kPathPrimary = 1u << 3;
 constexpr uint32_t kPathNee = 1u << 5;  // pending next-event contributions
 constexpr uint32_t kPathCacheQueued = 1u << 6;  // the path's image estimate already ended at the cache
+// A deferred coated vertex's pending shadow rays: emissive (slot 0),
+// analytic (slot 1), environment (slot 2).
+constexpr uint32_t kPathDeferEmissive = 1u << 7;
+constexpr uint32_t kPathDeferAnalytic = 1u << 8;
+constexpr uint32_t kPathDeferEnvironment = 1u << 9;
 
 // Work queues (device counters live in a small array).
 struct Queues {
@@ -223,6 +236,8 @@ struct Queues {
     int32_t* shadow_slot; // path * 3 + light type
     uint8_t* shadow_occluded;
     int32_t* shadow_overflow;  // shadow entries the exact loop traces (see ShadowArgs::overflow)
+    int32_t* defer_paths;      // coated vertices awaiting their emissive shadow ray (kCtrDefer)
+    int32_t* defer_paths2;     // ... and then their analytic / environment shadow rays (kCtrDefer2)
     int32_t* nee_paths;   // paths with pending NEE
     // Subsurface probes (BSSRDF entry -> probe traversal -> exit), one per
     // path at most: probe_ray 2 per entry (base.xyz + t_min, direction.xyz +
@@ -249,9 +264,11 @@ enum CounterIndex {
     kCtrNee = 3,
     kCtrClass0 = 4,  // entries per shading class (kShadeClasses of them)
     kCtrProbe = 10,  // subsurface probes queued at this depth
+    kCtrDefer = 11,  // entries in defer_paths
     kCtrTrace = 12,  // traversal work counter
     kCtrShadowTrace = 13,
     kCtrShadowOverflow = 14,  // entries in shadow_overflow
+    kCtrDefer2 = 15,  // entries in defer_paths2
     kCtrStatsBase = 16,  // rays, shadow rays, occluded, hits, misses, bad
     kCtrCursor0 = 24,  // scatter cursors per shading class
     kCtrCount = 32,
