@@ -854,6 +854,13 @@ yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t count, const
 yrc_status yrc_render_scene_shadow_eval(yrc_render_scene* scene, const yrc_ray* rays, int64_t n,
                                         float* transmittance);
 
+/* A new camera and sampler seed (RenderSettings::seed) for a prepared scene,
+ * e.g. the next frame of a camera path: the next yrc_render draws that view.
+ * The scene's working memory and captured batch are kept, so that render
+ * pays no allocation or capture. An attached radiance cache stays attached.
+ * No counterpart in the reference (its prepared scene is immutable). */
+yrc_status yrc_render_scene_set_view(yrc_render_scene* scene, const yrc_camera* camera, uint64_t seed);
+
 /* Wait for all work the library queued on `stream` (NULL = legacy default). */
 yrc_status yrc_stream_synchronize(void* stream);
 

@@ -19,7 +19,9 @@ forward pass, gradients and optimiser step can be checked value by value:
 * loss: relative L2, mean over samples and channels of
   (rgb - target)^2 / (stop_grad(rgb)^2 + 0.01);
 * optimiser: Adam (lr 1e-2, betas 0.9 / 0.99, eps 1e-15) on fp32 master
-  copies of the weights and of the grid, with bias correction.
+  copies of the weights and of the grid, with bias correction; on the grid
+  lazily (the sparse-Adam variant, e.g. PyTorch's SparseAdam): only the
+  entries a step's samples touched update, as does their moving average.
 
 Only tests import this module.
 """
@@ -199,8 +201,26 @@ def grid_backward(dx: np.ndarray, corners) -> np.ndarray:
     return grad.astype(np.float32)
 
 
-def adam(param: np.ndarray, grad: np.ndarray, m: np.ndarray, v: np.ndarray, step: int):
-    """One Adam step in place (fp32); step counts from 1."""
+def touched(corners) -> np.ndarray:
+    """(LEVELS, TABLE) bool: the grid entries a batch's samples read (all
+    eight corners on every level, whatever their trilinear weight)."""
+    mask = np.zeros((LEVELS, TABLE), bool)
+    for l, (idx, _) in enumerate(corners):
+        mask[l, idx.reshape(-1)] = True
+    return mask
+
+
+def adam(param: np.ndarray, grad: np.ndarray, m: np.ndarray, v: np.ndarray, step: int, mask=None):
+    """One Adam step in place (fp32); step counts from 1. With `mask` (the
+    shape of the parameters' leading axes, e.g. touched()), lazy Adam: only
+    the masked entries update their moments and parameters; the others keep
+    theirs (the bias corrections still use the global step)."""
+    if mask is not None:
+        sub = [a[mask] for a in (param, grad, m, v)]
+        adam(*sub, step)
+        for a, b in zip((param, m, v), (sub[0], sub[2], sub[3])):
+            a[mask] = b
+        return
     m *= np.float32(BETA1)
     m += np.float32(1 - BETA1) * grad
     v *= np.float32(BETA2)
@@ -210,12 +230,16 @@ def adam(param: np.ndarray, grad: np.ndarray, m: np.ndarray, v: np.ndarray, step
     param -= np.float32(LR) * mhat / (np.sqrt(vhat) + np.float32(EPS))
 
 
-def average(avg: np.ndarray, param: np.ndarray, step: int, decay_max: float = 0.99):
+def average(avg: np.ndarray, param: np.ndarray, step: int, decay_max: float = 0.99, mask=None):
     """Moving average of the parameters after optimiser step `step` (counted
     from 1), in place: decay = min(decay_max, (1 + t) / (10 + t)) rounded to
-    fp32, avg = decay * avg + (1 - decay) * param in fp32."""
+    fp32, avg = decay * avg + (1 - decay) * param in fp32; with `mask`, only
+    the masked entries (the lazy optimiser's updated ones)."""
     decay = np.float32(min(float(np.float32(decay_max)), (1.0 + step) / (10.0 + step)))
     keep = np.float32(1.0 - float(decay))
+    if mask is not None:
+        avg[mask] = (decay * avg[mask]).astype(np.float32) + (keep * param[mask]).astype(np.float32)
+        return
     avg[...] = (decay * avg).astype(np.float32) + (keep * param).astype(np.float32)
 
 

@@ -108,7 +108,7 @@ def test_adam_step_matches_oracle(cuda, cache):
     q, flat = queries(2048, 3)
     target = np.full((2048, 4), 0.5, np.float32)
     qt, tt = torch.from_numpy(flat).to(cuda), torch.from_numpy(target).to(cuda)
-    wg, _, _ = cache.gradients(qt, tt)
+    wg, gg, _ = cache.gradients(qt, tt)
     fresh = RadianceCache(LO, EXTENT, seed=3)  # step counter 0, zero moments
     fresh.set_params(w, grid)
     fresh.train_step(qt, tt)
@@ -121,6 +121,15 @@ def test_adam_step_matches_oracle(cuda, cache):
     N.adam(p, wg, m, v, 1)
     diff = np.abs(w_after - p)
     assert (diff > 1e-5).mean() < 1e-3, (diff > 1e-5).mean()
+    # the grid: lazy Adam over the entries the batch touched, the rest untouched
+    p01 = np.clip((q["pos"] - LO) * np.float32(1.0 / EXTENT), 0.0, 1.0).astype(np.float32)
+    mask = N.touched(N.grid_corners(p01))
+    assert np.array_equal(g_after[~mask], grid[~mask])
+    gp, gm, gv = grid.copy(), np.zeros_like(grid), np.zeros_like(grid)
+    N.adam(gp, gg, gm, gv, 1, mask)
+    gdiff = np.abs(g_after - gp)[mask]
+    assert (gdiff > 1e-5).mean() < 1e-3, (gdiff > 1e-5).mean()
+    assert (g_after[mask] != grid[mask]).mean() > 0.5  # the touched entries did move
 
 
 def test_parameter_average_matches_oracle(cuda):
@@ -135,11 +144,13 @@ def test_parameter_average_matches_oracle(cuda):
     qt = torch.from_numpy(flat).to(cuda)
     tt = torch.from_numpy(np.full((1024, 4), 0.3, np.float32)).to(cuda)
     avg_w, avg_g = w.copy(), grid.copy()
+    p01 = np.clip((q["pos"] - LO) * np.float32(1.0 / EXTENT), 0.0, 1.0).astype(np.float32)
+    mask = N.touched(N.grid_corners(p01))  # the lazy grid optimiser updates these entries only
     for step in range(1, 5):
         c.train_step(qt, tt)
         pw, pg = c.get_params()
         N.average(avg_w, pw, step, 0.9)
-        N.average(avg_g, pg, step, 0.9)
+        N.average(avg_g, pg, step, 0.9, mask)
     c.check()
     aw, ag = c.get_averaged_params()
     c.close()

@@ -246,3 +246,26 @@ def test_subsurface_scene_matches_reference_cpu(cuda, ref):
     alb = res.film["albedo_sum"] / np.maximum(res.film["aov_samples"], 1)[..., None]
     box = np.abs(alb[..., 0] - 0.5) < 1e-3
     assert box.sum() > 100 and g.reshape(-1, 3)[box.reshape(-1)].mean() > 0
+
+
+def test_set_view_equals_a_fresh_scene(cuda):
+    """yrc_render_scene_set_view on a scene that has rendered (working memory
+    and captured batch in place) renders exactly what a scene prepared with
+    that camera and seed renders."""
+    import dataclasses
+    from yaoray_b200 import instanced
+
+    base = instanced.scene(width=64, height=48, spp=4, mesh_scale=0.02, instances=12, env_width=128)
+    other = dataclasses.replace(base, seed=5, camera=instanced.camera(orbit=0.3))
+    backend = CudaBackend()
+    resident = backend.prepare(base)
+    first = backend.render(resident)
+    assert first.ok, first.error
+    resident.set_view(other.camera, other.seed)
+    moved = backend.render(resident)
+    fresh = backend.render(backend.prepare(other))
+    assert moved.ok and fresh.ok
+    assert moved.film.tobytes() == fresh.film.tobytes()
+    assert moved.film.tobytes() != first.film.tobytes()
+    resident.set_view(base.camera, base.seed)
+    assert backend.render(resident).film.tobytes() == first.film.tobytes()

@@ -9,8 +9,9 @@
 //   CacheTrainKernel  encode + forward + loss + 6 x (dW, dX) backward GEMMs,
 //                     weight gradients accumulated in TMEM across the CTA's
 //                     tiles and flushed once, grid gradients scattered with
-//                     float2 atomics
-//   AdamKernel        fp32 master weights/grid -> bf16 weights / fp16 grid
+//                     float2 atomics, the touched entries listed once each
+//   AdamKernel        fp32 master weights -> bf16 weights (all of them)
+//   SparseGridAdamKernel  lazy Adam over the listed grid entries -> fp16 grid
 //
 // The reference renderer has no radiance cache; this file has no counterpart
 // in it.
@@ -70,6 +71,11 @@ constexpr uint32_t kInferTmemCols = 64;
 struct GridArgs {
     const __half2* table;  // [kLevels * kTable]
     float2* grad;          // same shape, training only
+    // Training only: the entries this step's samples touched, as a bitmask
+    // over [kLevels * kTable] and a compacted list (each entry once).
+    uint32_t* touched;
+    int32_t* touched_list;
+    unsigned long long* touched_count;
     float scale[kLevels];
     int32_t side[kLevels];  // dense grid side, 0 when the level is hashed
     float lo[3];
@@ -450,8 +456,14 @@ __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const _
                     const float d0 = dx[2 * lv], d1 = dx[2 * lv + 1];
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
-                        atomicAdd(g.grad + static_cast<int64_t>(lv) * kTable + idx[c],
-                                  make_float2(w[c] * d0, w[c] * d1));
+                        const int64_t e = static_cast<int64_t>(lv) * kTable + idx[c];
+                        atomicAdd(g.grad + e, make_float2(w[c] * d0, w[c] * d1));
+                        // First touch of the entry this step: list it for the optimiser.
+                        const uint32_t bit = 1u << (e & 31);
+                        uint32_t* word = g.touched + (e >> 5);
+                        if (!(*word & bit) && !(atomicOr(word, bit) & bit)) {
+                            g.touched_list[atomicAdd(g.touched_count, 1ull)] = static_cast<int32_t>(e);
+                        }
                     }
                 }
             }
@@ -483,40 +495,87 @@ __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const _
 
 // ---------------------------------------------------------------- Adam
 
-// One Adam step with bias correction (c1 = 1 - beta1^t, c2 = 1 - beta2^t,
-// t read from the device so that a captured graph replays correctly), in
-// the operation order of the oracle; `half_out` / `bf16_out` receive the
-// rounded copy read by the kernels. The same pass updates the exponential
-// moving average of the parameters (Polyak averaging, decay
-// min(avg_decay, (1 + t) / (10 + t))) and its rounded copy.
+// The step's constants: bias corrections c1 = 1 - beta1^t, c2 = 1 - beta2^t
+// (t read from the device so that a captured graph replays correctly) and
+// the moving average's decay min(avg_decay, (1 + t) / (10 + t)).
+struct AdamStep {
+    float c1, c2, decay, keep;
+};
+
+__device__ inline AdamStep MakeAdamStep(const int64_t* step, float avg_decay) {
+    const double t = static_cast<double>(*step);
+    AdamStep a;
+    a.c1 = static_cast<float>(1.0 - pow(kBeta1, t));
+    a.c2 = static_cast<float>(1.0 - pow(kBeta2, t));
+    a.decay = static_cast<float>(fmin(static_cast<double>(avg_decay), (1.0 + t) / (10.0 + t)));
+    a.keep = static_cast<float>(1.0 - static_cast<double>(a.decay));
+    return a;
+}
+
+// One parameter's Adam update in the operation order of the oracle, then
+// its moving average (Polyak averaging); returns (parameter, average).
+__device__ __forceinline__ float2 AdamUpdate(const AdamStep& a, float& p, float& m, float& v, float g, float& avg) {
+    const float b1 = static_cast<float>(kBeta1), b2 = static_cast<float>(kBeta2);
+    const float nb1 = static_cast<float>(1.0 - kBeta1), nb2 = static_cast<float>(1.0 - kBeta2);
+    const float mi = __fadd_rn(__fmul_rn(m, b1), __fmul_rn(nb1, g));
+    const float vi = __fadd_rn(__fmul_rn(v, b2), __fmul_rn(__fmul_rn(nb2, g), g));
+    m = mi;
+    v = vi;
+    const float mhat = __fdiv_rn(mi, a.c1);
+    const float vhat = __fdiv_rn(vi, a.c2);
+    const float step = __fdiv_rn(__fmul_rn(kLr, mhat), __fadd_rn(__fsqrt_rn(vhat), kAdamEps));
+    p = __fsub_rn(p, step);
+    avg = __fadd_rn(__fmul_rn(a.decay, avg), __fmul_rn(a.keep, p));
+    return make_float2(p, avg);
+}
+
+// Adam over every parameter (the network weights); `half_out` / `bf16_out`
+// receive the rounded copy read by the kernels, likewise for the average.
 __global__ void AdamKernel(float* p, float* m, float* v, const float* grad, int64_t count, const int64_t* step,
                            __half* half_out, __nv_bfloat16* bf16_out, float* avg, __half* avg_half,
                            __nv_bfloat16* avg_bf16, float avg_decay) {
-    const double t = static_cast<double>(*step);
-    const float c1 = static_cast<float>(1.0 - pow(kBeta1, t));
-    const float c2 = static_cast<float>(1.0 - pow(kBeta2, t));
-    const float decay = static_cast<float>(fmin(static_cast<double>(avg_decay), (1.0 + t) / (10.0 + t)));
-    const float keep = static_cast<float>(1.0 - static_cast<double>(decay));
-    const float b1 = static_cast<float>(kBeta1), b2 = static_cast<float>(kBeta2);
-    const float nb1 = static_cast<float>(1.0 - kBeta1), nb2 = static_cast<float>(1.0 - kBeta2);
+    const AdamStep a = MakeAdamStep(step, avg_decay);
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const float gi = grad[i];
-        const float mi = __fadd_rn(__fmul_rn(m[i], b1), __fmul_rn(nb1, gi));
-        const float vi = __fadd_rn(__fmul_rn(v[i], b2), __fmul_rn(__fmul_rn(nb2, gi), gi));
+        float pi = p[i], mi = m[i], vi = v[i], ai = avg[i];
+        AdamUpdate(a, pi, mi, vi, grad[i], ai);
+        p[i] = pi;
         m[i] = mi;
         v[i] = vi;
-        const float mhat = __fdiv_rn(mi, c1);
-        const float vhat = __fdiv_rn(vi, c2);
-        const float step = __fdiv_rn(__fmul_rn(kLr, mhat), __fadd_rn(__fsqrt_rn(vhat), kAdamEps));
-        const float pi = __fsub_rn(p[i], step);
-        p[i] = pi;
+        avg[i] = ai;
         if (half_out) half_out[i] = __float2half_rn(pi);
         if (bf16_out) bf16_out[i] = __float2bfloat16_rn(pi);
-        const float ai = __fadd_rn(__fmul_rn(decay, avg[i]), __fmul_rn(keep, pi));
-        avg[i] = ai;
         if (avg_half) avg_half[i] = __float2half_rn(ai);
         if (avg_bf16) avg_bf16[i] = __float2bfloat16_rn(ai);
+    }
+}
+
+// Lazy Adam over the grid: only the entries this step's samples touched
+// (the compacted list the training kernel wrote) update their two features,
+// moments and averages, with the dense kernel's arithmetic; an entry no
+// sample reached keeps its state, as sparse Adam variants do (PyTorch's
+// SparseAdam). Each listed entry's gradient and touched bit are cleared for
+// the next step, so no pass over the whole table is needed.
+__global__ void SparseGridAdamKernel(float2* p, float2* m, float2* v, float2* grad, uint32_t* touched,
+                                     const int32_t* list, const unsigned long long* count, const int64_t* step,
+                                     __half2* half_out, float2* avg, __half2* avg_half, float avg_decay) {
+    const AdamStep a = MakeAdamStep(step, avg_decay);
+    const int64_t n = static_cast<int64_t>(*count);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t e = list[i];
+        touched[e >> 5] = 0u;  // every listed entry of the word clears it alike
+        float2 pe = p[e], me = m[e], ve = v[e], ae = avg[e];
+        const float2 ge = grad[e];
+        AdamUpdate(a, pe.x, me.x, ve.x, ge.x, ae.x);
+        AdamUpdate(a, pe.y, me.y, ve.y, ge.y, ae.y);
+        p[e] = pe;
+        m[e] = me;
+        v[e] = ve;
+        avg[e] = ae;
+        grad[e] = make_float2(0.0f, 0.0f);
+        half_out[e] = __floats2half2_rn(pe.x, pe.y);
+        avg_half[e] = __floats2half2_rn(ae.x, ae.y);
     }
 }
 
@@ -556,7 +615,10 @@ struct yrc_nrc {
     float* table_master = nullptr;  // fp32 master
     float* table_m = nullptr;
     float* table_v = nullptr;
-    float* table_grad = nullptr;
+    float* table_grad = nullptr;    // zero between steps (the grid optimiser clears what it used)
+    uint32_t* touched_mask = nullptr;       // entries touched this step, zero between steps
+    int32_t* touched_list = nullptr;        // kLevels * kTable
+    unsigned long long* touched_count = nullptr;
     __nv_bfloat16* w = nullptr;  // kWeightCount
     float* w_master = nullptr;
     float* w_m = nullptr;
@@ -595,20 +657,25 @@ void FreeAll(yrc_nrc* c) {
     void* ptrs[] = {c->table,  c->table_master,     c->table_m,   c->table_v,      c->table_grad,
                     c->w,      c->w_master,         c->w_m,       c->w_v,          c->w_grad,
                     c->table_avg_master, c->table_avg, c->w_avg_master, c->w_avg, c->loss,
-                    c->error,  c->step};
+                    c->error,  c->step, c->touched_mask, c->touched_list, c->touched_count};
     for (void* p : ptrs) cudaFree(p);
 }
 
 // Gradients of n pairs (n_ptr: the count on the device, at most n).
 yrc_status LaunchTrain(yrc_nrc* c, const float* queries, const float* targets, int64_t n,
                        const unsigned long long* n_ptr, cudaStream_t st) {
-    cudaError_t err = cudaMemsetAsync(c->table_grad, 0, sizeof(float) * kGridParams, st);
+    // The grid gradients and touched bits are zero already (cleared per
+    // entry by the grid optimiser); the compacted list starts empty.
+    cudaError_t err = cudaMemsetAsync(c->touched_count, 0, sizeof(unsigned long long), st);
     if (err == cudaSuccess) err = cudaMemsetAsync(c->w_grad, 0, sizeof(float) * kWeightCount, st);
     if (err == cudaSuccess) err = cudaMemsetAsync(c->loss, 0, sizeof(float), st);
     if (err != cudaSuccess) return CudaFailN(err, "clearing gradients");
     if (n <= 0) return Ok();
     GridArgs g = c->grid;
     g.grad = reinterpret_cast<float2*>(c->table_grad);
+    g.touched = c->touched_mask;
+    g.touched_list = c->touched_list;
+    g.touched_count = c->touched_count;
     const int64_t tiles = (n + kTile - 1) / kTile;
     const int64_t blocks = tiles < c->sm_count ? tiles : c->sm_count;  // one CTA per SM (TMEM, smem)
     CacheTrainKernel<<<static_cast<unsigned>(blocks), kThreads, kTrainSmem, st>>>(
@@ -623,10 +690,11 @@ yrc_status LaunchAdam(yrc_nrc* c, cudaStream_t st) {
     AdamKernel<<<Blocks(kWeightCount, c->sm_count), 256, 0, st>>>(c->w_master, c->w_m, c->w_v, c->w_grad,
                                                                   kWeightCount, c->step, nullptr, c->w,
                                                                   c->w_avg_master, nullptr, c->w_avg, c->avg_decay);
-    AdamKernel<<<Blocks(kGridParams, c->sm_count), 256, 0, st>>>(c->table_master, c->table_m, c->table_v,
-                                                                 c->table_grad, kGridParams, c->step, c->table,
-                                                                 nullptr, c->table_avg_master, c->table_avg,
-                                                                 nullptr, c->avg_decay);
+    SparseGridAdamKernel<<<static_cast<unsigned>(c->sm_count) * 8, 256, 0, st>>>(
+        reinterpret_cast<float2*>(c->table_master), reinterpret_cast<float2*>(c->table_m),
+        reinterpret_cast<float2*>(c->table_v), reinterpret_cast<float2*>(c->table_grad), c->touched_mask,
+        c->touched_list, c->touched_count, c->step, reinterpret_cast<__half2*>(c->table),
+        reinterpret_cast<float2*>(c->table_avg_master), reinterpret_cast<__half2*>(c->table_avg), c->avg_decay);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return CudaFailN(err, "optimiser launch");
     return Ok();
@@ -724,6 +792,9 @@ yrc_status yrc_nrc_create(const float box_lo[3], float box_extent, uint64_t seed
     alloc(&c->table_m, sizeof(float) * kGridParams);
     alloc(&c->table_v, sizeof(float) * kGridParams);
     alloc(&c->table_grad, sizeof(float) * kGridParams);
+    alloc(&c->touched_mask, sizeof(uint32_t) * (kLevels * kTable / 32));
+    alloc(&c->touched_list, sizeof(int32_t) * kLevels * kTable);
+    alloc(&c->touched_count, sizeof(unsigned long long));
     alloc(&c->w, sizeof(__nv_bfloat16) * kWeightCount);
     alloc(&c->w_master, sizeof(float) * kWeightCount);
     alloc(&c->w_m, sizeof(float) * kWeightCount);
@@ -762,6 +833,9 @@ yrc_status yrc_nrc_create(const float box_lo[3], float box_extent, uint64_t seed
     if (err == cudaSuccess) err = cudaMemset(c->w_v, 0, sizeof(float) * kWeightCount);
     if (err == cudaSuccess) err = cudaMemset(c->table_m, 0, sizeof(float) * kGridParams);
     if (err == cudaSuccess) err = cudaMemset(c->table_v, 0, sizeof(float) * kGridParams);
+    if (err == cudaSuccess) err = cudaMemset(c->table_grad, 0, sizeof(float) * kGridParams);
+    if (err == cudaSuccess) err = cudaMemset(c->touched_mask, 0, sizeof(uint32_t) * (kLevels * kTable / 32));
+    if (err == cudaSuccess) err = cudaMemset(c->touched_count, 0, sizeof(unsigned long long));
     if (err == cudaSuccess) err = cudaMemset(c->error, 0, sizeof(int));
     if (err == cudaSuccess) err = cudaMemset(c->step, 0, sizeof(int64_t));
     if (err == cudaSuccess) {
@@ -907,6 +981,10 @@ yrc_status yrc_nrc_gradients(yrc_nrc* c, const float* queries, const float* targ
         err = cudaMemcpy(&sum, c->loss, sizeof(float), cudaMemcpyDeviceToHost);
         *loss = n > 0 ? sum / (3.0f * static_cast<float>(n)) : 0.0f;
     }
+    // No optimiser step follows: restore the zero gradients and touched bits
+    // the next training step starts from.
+    if (err == cudaSuccess) err = cudaMemset(c->table_grad, 0, sizeof(float) * kGridParams);
+    if (err == cudaSuccess) err = cudaMemset(c->touched_mask, 0, sizeof(uint32_t) * (kLevels * kTable / 32));
     if (err != cudaSuccess) return CudaFailN(err, "reading gradients");
     return Ok();
 }

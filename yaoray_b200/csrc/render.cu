@@ -84,6 +84,17 @@ float HostLuminance(const float* c) { return std::max(0.0f, 0.2126f * c[0] + 0.7
 
 constexpr int kMaxBatch = 64;
 
+DevView MakeView(const yrc_camera& c, uint64_t seed) {
+    DevView v{};
+    std::memcpy(v.cam_origin, c.origin, sizeof(v.cam_origin));
+    std::memcpy(v.cam_forward, c.forward, sizeof(v.cam_forward));
+    std::memcpy(v.cam_right, c.right, sizeof(v.cam_right));
+    std::memcpy(v.cam_up, c.up, sizeof(v.cam_up));
+    v.cam_half_height = std::tan(c.fov_y_radians * 0.5f);
+    v.seed = seed;
+    return v;
+}
+
 }  // namespace
 }  // namespace yrc
 
@@ -121,6 +132,7 @@ struct yrc_render_scene {
     yrc::TextureSet textures;  // scene textures and their mip chains
     yrc::MeasuredSet measured;  // measured BRDF warps
     yrc::CacheArgs cargs{};
+    yrc::DevView* view = nullptr;  // camera and seed (device), see yrc_render_scene_set_view
     std::mutex mutex;
 };
 
@@ -623,18 +635,14 @@ yrc_status yrc_render_scene_create(const yrc_scene_desc* desc, yrc_render_scene*
     }
 
     // Camera and settings.
-    const yrc_camera& c = desc->camera;
-    std::memcpy(d.cam_origin, c.origin, sizeof(d.cam_origin));
-    std::memcpy(d.cam_forward, c.forward, sizeof(d.cam_forward));
-    std::memcpy(d.cam_right, c.right, sizeof(d.cam_right));
-    std::memcpy(d.cam_up, c.up, sizeof(d.cam_up));
-    d.cam_half_height = std::tan(c.fov_y_radians * 0.5f);
+    const DevView view = MakeView(desc->camera, st.seed);
+    s->view = A.Upload(&view, 1);
+    d.view = s->view;
     d.width = st.width;
     d.height = st.height;
     d.spp = std::max(1, st.spp);
     d.max_depth = std::max(1, st.max_depth);
     d.sampler = st.sampler;
-    d.seed = st.seed;
     d.radiance_clamp = st.radiance_clamp;
 
     if (A.err != cudaSuccess) {
@@ -1519,4 +1527,21 @@ extern "C" yrc_status yrc_render_scene_shadow_eval(yrc_render_scene* s, const yr
     a.Release();
     if (err != cudaSuccess) return CudaError(err, "yrc_render_scene_shadow_eval");
     return CheckDeviceError(s->accel);
+}
+
+// A new camera and sampler seed for a resident scene (a camera path, frames
+// of an animation): one small copy into the scene's view record. The scene's
+// working memory and captured batch stay as they are, so the next render
+// pays neither allocation nor capture. No counterpart in the reference (its
+// RenderJob is immutable once prepared).
+extern "C" yrc_status yrc_render_scene_set_view(yrc_render_scene* s, const yrc_camera* camera, uint64_t seed) {
+    using namespace yrc;
+    if (!s || !camera) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_scene_set_view: bad argument");
+    std::lock_guard<std::mutex> lock(s->mutex);
+    cudaSetDevice(s->device);
+    const DevView v = MakeView(*camera, seed);
+    const cudaError_t err = cudaMemcpy(s->view, &v, sizeof(v), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) return CudaError(err, "yrc_render_scene_set_view");
+    s->settings.seed = seed;
+    return Ok();
 }

@@ -66,9 +66,10 @@ __device__ inline V3 CameraDirection(const DevScene& sc, float fx, float fy) {
     const float w = static_cast<float>(sc.width < 1 ? 1 : sc.width);
     const float h = static_cast<float>(sc.height < 1 ? 1 : sc.height);
     const float aspect = w / h;
-    const float sx = (2.0f * fx / w - 1.0f) * aspect * sc.cam_half_height;
-    const float sy = (1.0f - 2.0f * fy / h) * sc.cam_half_height;
-    return Normalize(Ld3(sc.cam_forward) + Ld3(sc.cam_right) * sx + Ld3(sc.cam_up) * sy);
+    const DevView& v = *sc.view;
+    const float sx = (2.0f * fx / w - 1.0f) * aspect * v.cam_half_height;
+    const float sy = (1.0f - 2.0f * fy / h) * v.cam_half_height;
+    return Normalize(Ld3(v.cam_forward) + Ld3(v.cam_right) * sx + Ld3(v.cam_up) * sy);
 }
 
 }  // namespace
@@ -97,14 +98,14 @@ __global__ void GenerateKernel(DevScene sc, PathState ps, Queues q, BatchArgs b,
         const int x = pixel % sc.width, y = pixel / sc.width;
         const int32_t sample = static_cast<int32_t>(b.film[pixel].samples) + j;
         PixelSampler smp;
-        smp.Init(sc.sampler, sc.seed, x, y, sample, sc.spp);
+        smp.Init(sc.sampler, sc.view->seed, x, y, sample, sc.spp);
         float sx, sy;
         smp.Sample2D(kDimPixel, 0, sx, sy);
         const float fx = static_cast<float>(x) + sx;
         const float fy = static_cast<float>(y) + sy;
         const V3 d = CameraDirection(sc, fx, fy);
         Pcg32 rng;
-        rng.Seed(SeedForPixelSample(sc.seed, x, y, sample) ^ kDefaultSeed);
+        rng.Seed(SeedForPixelSample(sc.view->seed, x, y, sample) ^ kDefaultSeed);
         ps.pixel[i] = pixel;
         ps.sample[i] = sample;
         ps.throughput[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -115,7 +116,7 @@ __global__ void GenerateKernel(DevScene sc, PathState ps, Queues q, BatchArgs b,
         ps.aov_albedo[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         ps.aov_normal[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         ps.nee[3 * i] = ps.nee[3 * i + 1] = ps.nee[3 * i + 2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        q.ray_in[2 * i] = make_float4(sc.cam_origin[0], sc.cam_origin[1], sc.cam_origin[2], 1.0e-5f);
+        q.ray_in[2 * i] = make_float4(sc.view->cam_origin[0], sc.view->cam_origin[1], sc.view->cam_origin[2], 1.0e-5f);
         q.ray_in[2 * i + 1] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
         q.path_in[i] = static_cast<int32_t>(i);
         if (cache.enabled) {
@@ -309,7 +310,7 @@ __device__ __forceinline__ V3 TransformVectorV(const float* m, V3 v) {
 __device__ inline void CameraDifferentials(const DevScene& sc, int32_t pixel, int32_t sample, V3& dx, V3& dy) {
     const int x = pixel % sc.width, y = pixel / sc.width;
     PixelSampler smp;
-    smp.Init(sc.sampler, sc.seed, x, y, sample, sc.spp);
+    smp.Init(sc.sampler, sc.view->seed, x, y, sample, sc.spp);
     float sx, sy;
     smp.Sample2D(kDimPixel, 0, sx, sy);
     const float fx = static_cast<float>(x) + sx;
@@ -1372,7 +1373,7 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
 
         PixelSampler smp;
         const int32_t pixel = ps.pixel[path];
-        smp.Init(sc.sampler, sc.seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
+        smp.Init(sc.sampler, sc.view->seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
         Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
 
         // --- coated vertex: next events and continuation in the reference's
@@ -1562,7 +1563,7 @@ __global__ void __launch_bounds__(256, 2) LayeredNeeKernel(DevScene sc, PathStat
         Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
         PixelSampler smp;
         const int32_t pixel = ps.pixel[path];
-        smp.Init(sc.sampler, sc.seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
+        smp.Init(sc.sampler, sc.view->seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
         V3 sum{0.0f, 0.0f, 0.0f};
         if (flags & kPathDeferEmissive) {
             const float4 vis = SlotVisibility<kTransmittance>(q, transmittance, 3 * path + 0);
@@ -1649,7 +1650,7 @@ __global__ void __launch_bounds__(256, 2) LayeredContinueKernel(DevScene sc, Pat
         Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
         PixelSampler smp;
         const int32_t pixel = ps.pixel[path];
-        smp.Init(sc.sampler, sc.seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
+        smp.Init(sc.sampler, sc.view->seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
         V3 sum{0.0f, 0.0f, 0.0f};
         if (flags & kPathDeferAnalytic) {
             const float4 vis = SlotVisibility<kTransmittance>(q, transmittance, 3 * path + 1);
@@ -1732,7 +1733,7 @@ __global__ void __launch_bounds__(256, 2) SubsurfaceExitKernel(DevScene sc, Path
         uint32_t flags = ps.flags[path];
         PixelSampler smp;
         const int32_t pixel = ps.pixel[path];
-        smp.Init(sc.sampler, sc.seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
+        smp.Init(sc.sampler, sc.view->seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
         Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
         NextEvent(sc, ps, q, path, smp, rng, depth, mx, pi, ni, ni, tp, flags);
         float bx, by;

@@ -34,6 +34,14 @@ struct DevEnvironment {
     float total_weight;
 };
 
+// The view a render draws: RenderCamera (include/yaoray/scene/camera.hpp:
+// 7-13) with tan(fov_y / 2) computed on the host, and RenderSettings::seed.
+struct alignas(16) DevView {
+    float cam_origin[3], cam_forward[3], cam_right[3], cam_up[3];
+    float cam_half_height;
+    uint64_t seed;
+};
+
 struct alignas(16) DevMaterial {
     int32_t kind;
     float reflectance[3];
@@ -138,12 +146,11 @@ struct DevScene {
     // subsurface
     const DevBssrdf* bssrdf;
     int32_t bssrdf_count;
-    // camera
-    float cam_origin[3], cam_forward[3], cam_right[3], cam_up[3];
-    float cam_half_height;  // tan(fov_y / 2), computed on the host
+    // camera and sampler seed: device memory, so that a new view of a
+    // resident scene is one small copy and the captured batch stays valid
+    const DevView* view;
     // settings
     int32_t width, height, spp, max_depth, sampler;
-    uint64_t seed;
     float radiance_clamp;
     int32_t any_transparent;  // scene has Dielectric / ThinDielectric materials
     int32_t any_subsurface;   // scene has Subsurface materials (probe stage needed)

@@ -13,6 +13,8 @@ structs; programming errors raise `YrcError`.
 """
 from __future__ import annotations
 
+import dataclasses
+
 import ctypes as C
 from dataclasses import dataclass, field
 
@@ -199,6 +201,7 @@ def _bind():
         ("yrc_render_autotune", C.c_int, [P, C.c_int32, P]),
         ("yrc_render_scene_set_tuning", C.c_int, [P, P]),
         ("yrc_render_scene_shadow_eval", C.c_int, [P, P, C.c_int64, P]),
+        ("yrc_render_scene_set_view", C.c_int, [P, P, C.c_uint64]),
         ("yrc_render_many", C.c_int, [P, C.c_int32, P, P, P, P, P]),
         ("yrc_bssrdf_table_build", C.c_int, [C.c_float, C.c_float, C.c_int32, C.c_int32, P, P, P, P, P]),
         ("yrc_alias_table_build", C.c_int, [P, C.c_int32, P, P, P]),
@@ -466,6 +469,17 @@ class PreparedScene:
         e.g. one found on a scene of the same image size and spp."""
         t = RenderTuning(int(tuning["capacity"]), int(tuning["trace_shape"]), 0, 0.0)
         check(_bind().yrc_render_scene_set_tuning(self._handle, C.byref(t)))
+
+    def set_view(self, camera: dict, seed: int) -> None:
+        """A new camera (origin, forward, right, up, fov_y_radians) and
+        sampler seed for the next render; the scene's working memory and
+        captured batch are kept."""
+        cam = Camera()
+        for k in ("origin", "forward", "right", "up"):
+            getattr(cam, k)[:] = [float(x) for x in camera[k]]
+        cam.fov_y_radians = float(camera["fov_y_radians"])
+        check(_bind().yrc_render_scene_set_view(self._handle, C.byref(cam), C.c_uint64(seed)))
+        self.scene = dataclasses.replace(self.scene, camera=dict(camera), seed=int(seed))
 
     def shadow_visibility(self, rays: np.ndarray) -> np.ndarray:
         """TraceShadowVisibility through this scene's shadow stage for (n, 8)
