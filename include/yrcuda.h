@@ -144,10 +144,12 @@ void yrc_bvh_options_default(yrc_bvh_options* options);
 yrc_status yrc_bvh_build(const yrc_geometry* geometry, const yrc_bvh_options* options, yrc_bvh** out);
 /*
  * The same build with the hierarchy built on the current CUDA device: the
- * same nodes, primitive_indices and primitives, byte for byte. Ranges the
- * reference splits at the median (std::nth_element, used only when every
- * centroid extent of a range is below 1e-8 or its box has no area) and
- * median-split options are built by the host builder instead;
+ * same nodes, primitive_indices and primitives, byte for byte. Where the
+ * reference splits a range at the median (std::nth_element, used only when
+ * every centroid extent of a range is below 1e-8 or its box has no area),
+ * the host's own std::nth_element permutes that range (a subtree of at most
+ * 64 refs that meets one is built by the host's serial builder) and the
+ * device builds the rest. The median-split option is built on the host;
  * *built_on_device (optional) is 1 when the device built the hierarchy.
  * Synchronous. No counterpart in the reference (its builder is CPU-only).
  */

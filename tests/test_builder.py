@@ -132,6 +132,23 @@ def test_flat_build_matches_live_reference(ref):
             assert ours.max_depth == md
 
 
+def test_median_splits_match_live_reference(ref):
+    """Nearly coincident centroids (extents below the reference's 1e-8, keys
+    still distinct): the median split's std::nth_element permutation, which
+    the host builder and the device builder's host step both take from the
+    standard library, gives the reference's bytes."""
+    rng = np.random.default_rng(4)
+    base = np.array([[0.0, 0.0, 0.0], [1e-9, 0.0, 0.0], [0.0, 1e-9, 0.0]], np.float32)
+    tris = (base[None] + (rng.random((3000, 1, 3)) * 4e-10).astype(np.float32)).reshape(-1, 3).astype(np.float32)
+    mesh = scenes.traversal_scene(seed=9, spheres=3)
+    g = SceneGeometry.from_meshes([(tris, np.arange(len(tris), dtype=np.uint32).reshape(-1, 3)),
+                                   (mesh.positions, mesh.indices.reshape(-1, 3))])
+    b = accel.build_bvh(g)
+    nodes, pi, prims, depth = ref.RefScene(g).flat_bvh()
+    assert b.nodes.tobytes() == nodes.tobytes() and b.primitive_indices.tobytes() == pi.tobytes()
+    assert b.primitives.tobytes() == prims.tobytes() and b.max_depth == depth
+
+
 def test_two_level_build_matches_live_reference(ref):
     f, g = golden_geometry("trace_two_level")
     ours = accel.build_two_level_bvh(g)

@@ -1,8 +1,8 @@
 """Device BVH build: the hierarchy built on the GPU is the reference
 builder's, byte for byte (nodes, primitive slots, primitives, max depth),
 on the traversal set, a Cornell box, spheres, signed zeros, large leaves,
-and a soup with coincident centroids (which the median split of the
-reference sends to the host builder)."""
+and soups with coincident or nearly coincident centroids (the reference's
+median split, whose std::nth_element permutation the host computes)."""
 import time
 
 import numpy as np
@@ -63,11 +63,15 @@ def test_signed_zeros_and_spheres_match_host():
     same(host, dev)
 
 
-def test_coincident_centroids_fall_back_to_host():
+def test_coincident_centroids_build_on_device():
+    """Degenerate ranges (the reference's median split, std::nth_element):
+    200 copies of one triangle give ranges above and below the 64-ref small
+    subtree size whose centroid extents are all 0. The device build asks the
+    host's std::nth_element for the large ones and the host's serial builder
+    for the small subtrees, and stays byte-identical to the host builder."""
     geom = scenes.traversal_scene(seed=6, spheres=2)
     pos = geom.positions.copy()
     idx = geom.indices.copy()
-    # Many copies of one triangle: every centroid extent of their range is 0.
     tri = idx[:3]
     idx = np.concatenate([idx, np.tile(tri, 200)])
     prims = geom.primitives.copy()
@@ -75,7 +79,25 @@ def test_coincident_centroids_fall_back_to_host():
     g2 = SceneGeometry(pos, idx, prims)
     host = accel.build_bvh(g2)
     dev, on_device = accel.build_bvh_device(g2)
-    assert not on_device
+    assert on_device
+    same(host, dev)
+
+
+def test_nearly_coincident_centroids_build_on_device():
+    """Centroids a few 1e-10 apart near the origin: every extent below the
+    1e-8 threshold, yet the keys differ, so the median split's permutation
+    depends on std::nth_element's own pivoting. 3000 such triangles next to
+    an ordinary mesh, byte-identical to the host builder."""
+    rng = np.random.default_rng(4)
+    base = np.array([[0.0, 0.0, 0.0], [1e-9, 0.0, 0.0], [0.0, 1e-9, 0.0]], np.float32)
+    jitter = (rng.random((3000, 1, 3)) * 4e-10).astype(np.float32)
+    tris = (base[None] + jitter).reshape(-1, 3).astype(np.float32)
+    mesh = scenes.traversal_scene(seed=9, spheres=3)
+    g = SceneGeometry.from_meshes([(tris, np.arange(len(tris), dtype=np.uint32).reshape(-1, 3)),
+                                   (mesh.positions, mesh.indices.reshape(-1, 3))])
+    host = accel.build_bvh(g)
+    dev, on_device = accel.build_bvh_device(g)
+    assert on_device
     same(host, dev)
 
 

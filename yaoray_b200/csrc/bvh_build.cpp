@@ -116,6 +116,18 @@ public:
         return true;
     }
 
+    // Builds the whole of refs_ serially as one subtree rooted at `depth`
+    // (a range of the device builder): subtree-local node indices, leaf
+    // payloads relative to the range.
+    bool RunSubtree(int depth, Subtree& out, std::string& error) {
+        const int r = Build(0, static_cast<int>(refs_.size()), depth, 1, out);
+        if (r != 0 || !error_.empty()) {
+            error = error_.empty() ? "BVH build produced an empty primitive range" : error_;
+            return false;
+        }
+        return true;
+    }
+
 private:
     void SetError(const char* message) {
         std::lock_guard<std::mutex> lock(error_mutex_);
@@ -324,6 +336,28 @@ bool ValidOptions(const yrc_bvh_options& o, std::string& error) {
 }
 
 }  // namespace
+
+void MedianPartitionRange(std::vector<BuildRef>& refs) {
+    Box centroid_box;
+    for (const BuildRef& r : refs) centroid_box = Grow(centroid_box, r.centroid);
+    const int axis = WidestAxis(centroid_box);
+    const auto mid = refs.begin() + static_cast<std::ptrdiff_t>(refs.size() / 2);
+    std::nth_element(refs.begin(), mid, refs.end(), [axis](const BuildRef& a, const BuildRef& b) {
+        return Comp(a.centroid, axis) < Comp(b.centroid, axis);
+    });
+}
+
+bool BuildSubtreeHost(std::vector<BuildRef>& refs, const yrc_bvh_options& options, int depth,
+                      std::vector<yrc_bvh_node>& nodes, int32_t& max_depth, std::string& error) {
+    yrc_bvh_options serial = options;
+    serial.thread_count = 1;
+    HierarchyBuilder builder(refs, serial);
+    Subtree out;
+    if (!builder.RunSubtree(depth, out, error)) return false;
+    nodes = std::move(out.nodes);
+    max_depth = out.max_depth;
+    return true;
+}
 
 bool BuildHierarchy(std::vector<BuildRef>& refs, const yrc_bvh_options& options, HostBvh& bvh,
                     std::string& error) {

@@ -18,10 +18,13 @@
 //    inside [begin, begin + T) (counted from the left) is swapped with the
 //    i-th element that satisfies it inside [begin + T, end) (counted from the
 //    right) and nothing else moves, which is a pair of prefix counts.
-// The median fallback (std::nth_element) has no order-free description; it
-// only occurs for degenerate ranges (every centroid extent below 1e-8 or a
-// zero-area box), and when the device builder meets one it reports it so the
-// caller builds on the host instead.
+// The median split (std::nth_element) has no order-free description; it only
+// occurs for degenerate ranges (every centroid extent below 1e-8 or a
+// zero-area box). Its permutation is by definition the standard library's,
+// so the host computes it with its own std::nth_element: between levels for
+// large ranges (the device lists them, the host permutes them before their
+// children are read), and by the host's serial builder for a small subtree
+// that meets one. Everything else stays on the device.
 //
 // Execution: ranges larger than kSmall are processed level by level, one
 // 512-thread block per range (bounds, buckets with per-warp bins, decision,
@@ -47,7 +50,7 @@ constexpr int kBlock = 512;  // threads per large range
 constexpr int kWarps = kBlock / 32;
 constexpr int kMaxSmallDepth = 64;  // explicit stack of the one-thread subtree build (depth <= kSmall)
 
-enum BuildFlag : int { kFlagMedian = 1, kFlagNonFinite = 2, kFlagEmpty = 4 };
+enum BuildFlag : int { kFlagNonFinite = 2, kFlagEmpty = 4, kFlagHostSubtree = 8 };
 
 // One ref in the device layout: lo.w carries the flat index.
 struct DevRef {
@@ -196,6 +199,8 @@ struct LevelArgs {
     int* flags;
     const int32_t* wide_of;  // per range of this level: its WideResult, -1 none (nullptr: none at all)
     const WideResult* wide;
+    int2* median;            // ranges split at their median: (begin, end), permuted by the host
+    unsigned* median_count;
 };
 
 // Warp-level min / max of 64-bit keys.
@@ -347,8 +352,14 @@ __global__ void __launch_bounds__(kBlock) LevelKernel(LevelArgs a) {
             if (found && best_cost >= __int2float_rn(count)) {
                 leaf = 1;
             } else if (!found) {
-                atomicOr(a.flags, kFlagMedian);  // std::nth_element: the host builds this BVH
-                leaf = 1;
+                // The reference's median split (std::nth_element): an
+                // interior node at begin + count / 2 whose range the host
+                // permutes with its own std::nth_element before the next
+                // level reads it.
+                leaf = 0;
+                axis = -1;
+                left_count = count / 2;
+                a.median[atomicAdd(a.median_count, 1u)] = make_int2(begin, end);
             } else {
                 leaf = 0;
                 for (int b = 0; b <= split; ++b) left_count += counts[axis * kBuckets + b];
@@ -373,6 +384,13 @@ __global__ void __launch_bounds__(kBlock) LevelKernel(LevelArgs a) {
     if (s_decision[0]) return;
     const int axis = s_decision[1], split = s_decision[2];
     const int mid = begin + s_decision[3];
+    if (axis < 0) {  // median split: no partition here
+        if (tid == 0) {
+            SpawnChild(a, r.id, 0, begin, mid, r.depth + 1);
+            SpawnChild(a, r.id, 1, mid, end, r.depth + 1);
+        }
+        return;
+    }
     const float lo = clo[axis], extent = cext[axis];
 
     // --- two-pointer partition: the i-th left-side failure (from the left)
@@ -637,6 +655,7 @@ struct SmallArgs {
     int32_t max_leaf;
     int* max_depth;
     int* flags;
+    int32_t* host;  // per task: 1 when the host builds it (a median split)
 };
 
 // One thread builds the whole subtree of a range of at most kSmall refs, in
@@ -712,8 +731,15 @@ __global__ void SmallKernel(SmallArgs a) {
             if (found && best_cost >= __int2float_rn(n)) {
                 leaf = true;
             } else if (!found) {
-                atomicOr(a.flags, kFlagMedian);
-                leaf = true;
+                // A median split (std::nth_element): the host builds this
+                // whole subtree with its serial builder. The partitions done
+                // so far are kept; repeating a two-pointer partition on a
+                // partitioned range moves nothing, so the host's build from
+                // here equals a build from the start.
+                a.host[t] = 1;
+                atomicOr(a.flags, kFlagHostSubtree);
+                a.size[t] = 0;
+                return;
             }
         }
         if (leaf) {
@@ -737,10 +763,10 @@ __global__ void SmallKernel(SmallArgs a) {
         }
         const int mid = first;
         if (mid == b || mid == e) {  // cannot happen when the SAH found both sides non-empty
-            atomicOr(a.flags, kFlagMedian);
-            self.payload_offset = b;
-            self.primitive_count = n;
-            continue;
+            a.host[t] = 1;
+            atomicOr(a.flags, kFlagHostSubtree);
+            a.size[t] = 0;
+            return;
         }
         self.primitive_count = 0;
         self.payload_offset = -1;
@@ -858,6 +884,38 @@ struct Buffers {
 namespace {
 
 // The hierarchy over n refs already in `d_refs` (reordered in place).
+DevRef ToDevRef(const BuildRef& r) {
+    float flat;
+    std::memcpy(&flat, &r.flat_index, sizeof(flat));
+    return DevRef{make_float4(r.bounds.lo.x, r.bounds.lo.y, r.bounds.lo.z, flat),
+                  make_float4(r.bounds.hi.x, r.bounds.hi.y, r.bounds.hi.z, 0.0f),
+                  make_float4(r.centroid.x, r.centroid.y, r.centroid.z, 0.0f)};
+}
+
+BuildRef ToBuildRef(const DevRef& d) {
+    BuildRef r;
+    std::memcpy(&r.flat_index, &d.lo.w, sizeof(r.flat_index));
+    r.bounds.lo = Vec3{d.lo.x, d.lo.y, d.lo.z};
+    r.bounds.hi = Vec3{d.hi.x, d.hi.y, d.hi.z};
+    r.centroid = Vec3{d.c.x, d.c.y, d.c.z};
+    return r;
+}
+
+// Copies device refs [begin, end) to the host as BuildRefs.
+cudaError_t DownloadRefs(const DevRef* d_refs, int64_t begin, int64_t end, std::vector<BuildRef>& out) {
+    std::vector<DevRef> dev(static_cast<size_t>(end - begin));
+    const cudaError_t err = cudaMemcpy(dev.data(), d_refs + begin, sizeof(DevRef) * dev.size(), cudaMemcpyDeviceToHost);
+    out.resize(dev.size());
+    for (size_t i = 0; i < dev.size(); ++i) out[i] = ToBuildRef(dev[i]);
+    return err;
+}
+
+cudaError_t UploadRefs(DevRef* d_refs, int64_t begin, const std::vector<BuildRef>& refs) {
+    std::vector<DevRef> dev(refs.size());
+    for (size_t i = 0; i < refs.size(); ++i) dev[i] = ToDevRef(refs[i]);
+    return cudaMemcpy(d_refs + begin, dev.data(), sizeof(DevRef) * dev.size(), cudaMemcpyHostToDevice);
+}
+
 int BuildOnDevice(Buffers& B, DevRef* d_refs, int64_t n, const yrc_bvh_options& options, HostBvh& bvh,
                   std::string& error) {
     int32_t* d_tmp = B.Alloc<int32_t>(n);
@@ -881,6 +939,8 @@ int BuildOnDevice(Buffers& B, DevRef* d_refs, int64_t n, const yrc_bvh_options& 
     const int64_t max_chunks = n / kChunk + kMaxWideRanges + 1;
     WideChunk* d_chunks = B.Alloc<WideChunk>(max_chunks);
     int* d_flags = B.Alloc<int>(2);             // flags, max depth
+    int2* d_median = B.Alloc<int2>(big_cap);     // median ranges of a level
+    int32_t* d_small_host = B.Alloc<int32_t>(n);  // per small task: built by the host
     if (B.err != cudaSuccess) {
         error = std::string("device BVH build: ") + cudaGetErrorString(B.err);
         return -1;
@@ -888,7 +948,7 @@ int BuildOnDevice(Buffers& B, DevRef* d_refs, int64_t n, const yrc_bvh_options& 
     cudaError_t err = cudaSuccess;
     const int max_leaf = options.max_leaf_triangles;
     // Root: a big range (id 0), or a single small subtree.
-    unsigned counts[4] = {0, 0, 0, 0};
+    unsigned counts[4] = {0, 0, 0, 0};  // next ranges, big nodes, small tasks, median ranges
     std::vector<int> level_lo, level_hi;
     if (err == cudaSuccess) err = cudaMemset(d_flags, 0, 2 * sizeof(int));
     if (n > kSmall) {
@@ -934,13 +994,28 @@ int BuildOnDevice(Buffers& B, DevRef* d_refs, int64_t n, const yrc_bvh_options& 
                     }
                 }
             }
+            if (err == cudaSuccess) err = cudaMemcpy(d_counts + 3, &zero, sizeof(unsigned), cudaMemcpyHostToDevice);
             LevelArgs a{d_refs, d_tmp, d_ranges[cur], ranges, d_ranges[cur ^ 1], d_counts, d_big, d_counts + 1,
-                        d_small, d_counts + 2, max_leaf, d_flags, use_wide ? d_wide_of : nullptr, d_wide};
+                        d_small, d_counts + 2, max_leaf, d_flags, use_wide ? d_wide_of : nullptr, d_wide,
+                        d_median, d_counts + 3};
             if (err == cudaSuccess) {
                 LevelKernel<<<static_cast<unsigned>(ranges), kBlock>>>(a);
                 err = cudaGetLastError();
             }
-            if (err == cudaSuccess) err = cudaMemcpy(counts, d_counts, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost);
+            if (err == cudaSuccess) err = cudaMemcpy(counts, d_counts, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost);
+            // Median splits of this level (degenerate ranges): the host's
+            // std::nth_element permutes each range before its children run.
+            if (err == cudaSuccess && counts[3] > 0) {
+                std::vector<int2> med(counts[3]);
+                err = cudaMemcpy(med.data(), d_median, sizeof(int2) * med.size(), cudaMemcpyDeviceToHost);
+                std::vector<BuildRef> range;
+                for (size_t q = 0; q < med.size() && err == cudaSuccess; ++q) {
+                    err = DownloadRefs(d_refs, med[q].x, med[q].y, range);
+                    if (err != cudaSuccess) break;
+                    MedianPartitionRange(range);
+                    err = UploadRefs(d_refs, med[q].x, range);
+                }
+            }
             level_lo.push_back(lo);
             level_hi.push_back(lo + ranges);
             lo += ranges;
@@ -955,17 +1030,49 @@ int BuildOnDevice(Buffers& B, DevRef* d_refs, int64_t n, const yrc_bvh_options& 
     const int big_total = static_cast<int>(counts[1]);
     const int small_total = static_cast<int>(counts[2]);
     if (err == cudaSuccess && small_total > 0) {
-        SmallArgs s{d_refs, d_small, small_total, d_local, d_small_size, max_leaf, d_flags + 1, d_flags};
-        SmallKernel<<<Grid(small_total, 128), 128>>>(s);
-        err = cudaGetLastError();
+        err = cudaMemset(d_small_host, 0, sizeof(int32_t) * small_total);
+        SmallArgs s{d_refs, d_small, small_total, d_local, d_small_size, max_leaf, d_flags + 1, d_flags, d_small_host};
+        if (err == cudaSuccess) {
+            SmallKernel<<<Grid(small_total, 128), 128>>>(s);
+            err = cudaGetLastError();
+        }
     }
     int flags[2] = {0, 0};
     if (err == cudaSuccess) err = cudaMemcpy(flags, d_flags, 2 * sizeof(int), cudaMemcpyDeviceToHost);
+    int32_t host_depth = 0;
+    if (err == cudaSuccess && (flags[0] & kFlagHostSubtree)) {
+        // Subtrees that met a median split: the host's serial builder, from
+        // the refs as the device left them, into the task's local node slots.
+        std::vector<SmallTask> tasks(static_cast<size_t>(small_total));
+        std::vector<int32_t> host(static_cast<size_t>(small_total));
+        err = cudaMemcpy(tasks.data(), d_small, sizeof(SmallTask) * tasks.size(), cudaMemcpyDeviceToHost);
+        if (err == cudaSuccess) err = cudaMemcpy(host.data(), d_small_host, sizeof(int32_t) * host.size(), cudaMemcpyDeviceToHost);
+        std::vector<BuildRef> range;
+        std::vector<yrc_bvh_node> nodes;
+        for (int t = 0; t < small_total && err == cudaSuccess; ++t) {
+            if (!host[static_cast<size_t>(t)]) continue;
+            const SmallTask& task = tasks[static_cast<size_t>(t)];
+            err = DownloadRefs(d_refs, task.begin, task.begin + task.count, range);
+            int32_t depth = 0;
+            if (err == cudaSuccess && !BuildSubtreeHost(range, options, task.depth, nodes, depth, error)) return -1;
+            for (yrc_bvh_node& node : nodes) {
+                if (node.primitive_count > 0) node.payload_offset += task.begin;  // leaf: global first slot
+            }
+            if (err == cudaSuccess) err = UploadRefs(d_refs, task.begin, range);
+            if (err == cudaSuccess) {
+                err = cudaMemcpy(d_local + 2 * static_cast<int64_t>(task.begin), nodes.data(),
+                                 sizeof(yrc_bvh_node) * nodes.size(), cudaMemcpyHostToDevice);
+            }
+            const int32_t size = static_cast<int32_t>(nodes.size());
+            if (err == cudaSuccess) err = cudaMemcpy(d_small_size + t, &size, sizeof(int32_t), cudaMemcpyHostToDevice);
+            host_depth = std::max(host_depth, depth);
+        }
+        flags[0] &= ~kFlagHostSubtree;
+    }
     if (err != cudaSuccess) {
         error = std::string("device BVH build: ") + cudaGetErrorString(err);
         return -1;
     }
-    if (flags[0] & kFlagMedian) return 0;  // a degenerate range: the host builder decides
     if (flags[0] != 0) {
         error = "device BVH build: subtree stack exhausted";
         return -1;
@@ -1020,11 +1127,11 @@ int BuildOnDevice(Buffers& B, DevRef* d_refs, int64_t n, const yrc_bvh_options& 
         error = std::string("device BVH build: ") + cudaGetErrorString(err);
         return -1;
     }
-    if (flags[0] != 0) {
+    if (flags[0] & ~kFlagHostSubtree) {
         error = "device BVH build: inconsistent node layout";
         return -1;
     }
-    bvh.max_depth = flags[1];
+    bvh.max_depth = std::max(flags[1], host_depth);
     return 1;
 }
 
@@ -1043,14 +1150,7 @@ int BuildHierarchyDevice(std::vector<BuildRef>& refs, const yrc_bvh_options& opt
         return -1;
     }
     std::vector<DevRef> host(static_cast<size_t>(n));
-    for (int64_t i = 0; i < n; ++i) {
-        const BuildRef& r = refs[static_cast<size_t>(i)];
-        float flat;
-        std::memcpy(&flat, &r.flat_index, sizeof(flat));
-        host[static_cast<size_t>(i)] = DevRef{make_float4(r.bounds.lo.x, r.bounds.lo.y, r.bounds.lo.z, flat),
-                                              make_float4(r.bounds.hi.x, r.bounds.hi.y, r.bounds.hi.z, 0.0f),
-                                              make_float4(r.centroid.x, r.centroid.y, r.centroid.z, 0.0f)};
-    }
+    for (int64_t i = 0; i < n; ++i) host[static_cast<size_t>(i)] = ToDevRef(refs[static_cast<size_t>(i)]);
     const cudaError_t err = cudaMemcpy(d_refs, host.data(), sizeof(DevRef) * n, cudaMemcpyHostToDevice);
     if (err != cudaSuccess) {
         error = std::string("device BVH build: ") + cudaGetErrorString(err);

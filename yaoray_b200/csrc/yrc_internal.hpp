@@ -64,6 +64,21 @@ bool BuildHierarchy(std::vector<BuildRef>& refs, const yrc_bvh_options& options,
 bool BuildFlatBvh(const yrc_geometry& geometry, const yrc_bvh_options& options, HostBvh& bvh,
                   std::string& error, bool device = false, bool* on_device = nullptr);
 
+// The reference's MedianPartition (bvh_split_policy.cpp:98-113) of a whole
+// range held as its own vector: std::nth_element by centroid on the range's
+// widest centroid axis at mid = size / 2. The device builder asks the host
+// for it on degenerate ranges, so its permutation is the standard library's
+// own, as in the reference.
+void MedianPartitionRange(std::vector<BuildRef>& refs);
+
+// The host builder's serial build of a whole range (refs permuted to slot
+// order) as one subtree rooted at `depth`: nodes with subtree-local indices
+// (an interior node's payload is its right child's local index, a leaf's its
+// first slot relative to the range). For device subtrees that meet a median
+// split. Returns false with `error` set on a build error.
+bool BuildSubtreeHost(std::vector<BuildRef>& refs, const yrc_bvh_options& options, int depth,
+                      std::vector<yrc_bvh_node>& nodes, int32_t& max_depth, std::string& error);
+
 // The hierarchy of BuildHierarchy built on the current CUDA device, byte for
 // byte the same. Returns 1 when built, 0 when a range needs the median split
 // (std::nth_element) or the options ask for median splits — the caller then
