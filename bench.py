@@ -420,12 +420,20 @@ RENDER_WORKLOADS = {
 }
 
 
-def render_scene(workload: str, spp: int):
+def render_scene(workload: str, spp: int, size=None, max_depth=None):
+    """The workload's scene; `size` (W, H) and `max_depth` override the
+    configured ones (smaller cases for profiler captures only)."""
+    kw = {}
+    if size:
+        kw.update(width=size[0], height=size[1])
+    if max_depth:
+        kw.update(max_depth=max_depth)
     if workload in ("cornell", "textured", "cutout"):
         from yaoray_b200 import cornell
-        return {"cornell": cornell.scene, "textured": cornell.textured_scene, "cutout": cornell.cutout_scene}[workload]()
+        return {"cornell": cornell.scene, "textured": cornell.textured_scene,
+                "cutout": cornell.cutout_scene}[workload](**kw)
     from yaoray_b200 import instanced
-    return instanced.scene(spp=spp)
+    return instanced.scene(spp=spp, **kw)
 
 
 def run_render(args):
@@ -446,11 +454,18 @@ def run_render(args):
     import torch
     from yaoray_b200.render import CudaBackend
 
-    scene = render_scene(args.workload, args.render_spp)
+    size = tuple(int(v) for v in args.size.split("x")) if args.size else None
+    scene = render_scene(args.workload, args.render_spp, size, args.max_depth)
     backend = CudaBackend()
     t0 = time.perf_counter()
     prepared = backend.prepare(scene)
     prepare_s = time.perf_counter() - t0
+    cache = None
+    if args.cache:  # radiance cache attached (profiler captures of its kernels)
+        from yaoray_b200.nrc import RadianceCache
+        lo = scene.geometry.positions.min(0)
+        cache = RadianceCache(lo, float((scene.geometry.positions.max(0) - lo).max()), seed=1)
+        prepared.set_radiance_cache(cache, spread_threshold=1.0e-4, train_steps=2, averaged=True)
     tuning = None
     if args.tuning:  # capacity,shape fixed by the caller (e.g. to profile what a plain run chose)
         cap, shape = (int(x) for x in args.tuning.split(","))
@@ -489,7 +504,9 @@ def run_render(args):
                     "cores": os.cpu_count(), "kind": "reference",
                     "sample": f"reference CpuBackend, same scene at {base_spp} spp ({secs:.2f} s)"}
     metric, workload = RENDER_WORKLOADS[args.workload]
-    config = {"workload": workload, "triangles": scene.geometry.triangle_count,
+    config = {"workload": workload + (" (size/depth override)" if args.size or args.max_depth else "")
+                          + (" (radiance cache attached)" if args.cache else ""),
+              "triangles": scene.geometry.triangle_count,
               "width": scene.width, "height": scene.height, "spp_per_step": scene.spp,
               "max_depth": scene.max_depth,
               "path_segments_per_step": int(res.stats["rays_traced"]),
@@ -773,6 +790,9 @@ def main():
     ap.add_argument("--four-wide", action="store_true", help="traversal: the opt-in four-wide traversal")
     ap.add_argument("--tuning", default=None, help="render workloads: 'capacity,shape' instead of the autotuner")
     ap.add_argument("--render-spp", type=int, default=16, help="spp per step of --workload instanced")
+    ap.add_argument("--size", default=None, help="render workloads: WxH instead of the configured size (profiling)")
+    ap.add_argument("--max-depth", type=int, default=None, help="render workloads: max depth override (profiling)")
+    ap.add_argument("--cache", action="store_true", help="render workloads: attach a radiance cache (profiling)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)

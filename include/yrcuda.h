@@ -340,7 +340,9 @@ yrc_status yrc_trace_stats_device_noalloc(yrc_accel* accel, const yrc_ray* rays,
 /*
  * Autotuner: times every compiled launch shape of the flat closest-hit (or,
  * with YRC_TRACE_ANY, any-hit) kernel on `count` device rays (results are
- * discarded) and keeps the fastest for this accelerator. `times_ms`
+ * discarded) and keeps, for this accelerator, the lowest-numbered shape
+ * within 2 % of the fastest (a choice that stays the same from run to run
+ * when shapes time alike). `times_ms`
  * (optional, YRC_TRACE_SHAPES floats) receives the measured time per shape.
  * Synchronises `stream`.
  */

@@ -849,8 +849,7 @@ yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t cou
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    float best = 0.0f;
-    int best_shape = 0;
+    float totals[kTraceShapes] = {};
     yrc_status status = Ok();
     for (int shape = 0; shape < kTraceShapes && status == YRC_OK; ++shape) {
         accel->trace_shape[any ? 1 : 0] = shape;
@@ -867,11 +866,15 @@ yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t cou
             if (rep > 0) total += ms;
         }
         if (times_ms) times_ms[shape] = total / 2.0f;
-        if (shape == 0 || total < best) {
-            best = total;
-            best_shape = shape;
-        }
+        totals[shape] = total;
     }
+    // The lowest-index shape within 2 % of the fastest: the shapes often time
+    // within run-to-run noise of each other, and a stable choice keeps the
+    // kernel a caller tuned for (and profiled) the same from run to run.
+    float best = totals[0];
+    for (int shape = 1; shape < kTraceShapes; ++shape) best = totals[shape] < best ? totals[shape] : best;
+    int best_shape = 0;
+    while (best_shape + 1 < kTraceShapes && totals[best_shape] > 1.02f * best) ++best_shape;
     accel->trace_shape[any ? 1 : 0] = best_shape;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
