@@ -722,6 +722,8 @@ def run_jobs(args):
     conc_lat = conc.latency_quantiles()
     shared = runner.run_shared_launch(jobs, concurrency=args.concurrency)
     shared_lat = shared.latency_quantiles()
+    pooled = runner.run_shared_launch(jobs, concurrency=args.concurrency, pooled=True)
+    pooled_lat = pooled.latency_quantiles()
     failed = [j.name for j in jobs if not j.ok]
     runner.close(jobs)
     tris = [j.scene.geometry.triangle_count for j in jobs]
@@ -761,6 +763,9 @@ def run_jobs(args):
                            "latency_p50_s": conc_lat["p50"], "latency_p99_s": conc_lat["p99"]},
             "shared_launch": {"samples_per_s": round(shared.samples_per_s, 1), "wall_s": round(shared.wall_s, 3),
                               "latency_p50_s": shared_lat["p50"], "latency_p99_s": shared_lat["p99"],
+                              "groups_of": args.concurrency},
+            "pooled_launch": {"samples_per_s": round(pooled.samples_per_s, 1), "wall_s": round(pooled.wall_s, 3),
+                              "latency_p50_s": pooled_lat["p50"], "latency_p99_s": pooled_lat["p99"],
                               "groups_of": args.concurrency},
             "failed_jobs": failed,
             "gpu_launches": sum(j.kernels for j in jobs),

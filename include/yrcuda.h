@@ -369,6 +369,33 @@ int32_t yrc_accel_get_trace_shape(const yrc_accel* accel, int32_t any_hit);
 yrc_status yrc_accel_set_wide(yrc_accel* accel, int32_t enable);
 int32_t yrc_accel_get_wide(const yrc_accel* accel);
 
+/* Ray reordering (opt-in) for yrc_trace_device and the autotuner: before a
+ * closest- or any-hit trace of at least 65,536 rays, the rays are sorted by
+ * a spatial key (a counting sort on the device, in the same stream) and the
+ * traversal takes them in that order, so that rays which start close
+ * together and head the same way share a warp. Hits are written per ray as
+ * before and do not depend on the order. Modes: YRC_RAY_ORDER_OFF;
+ * YRC_RAY_ORDER_DIRECTION (key: origin in the root box and direction);
+ * YRC_RAY_ORDER_TWO_POINT (key: origin and the point `length` x the root
+ * box diagonal along the ray). `key_bits` (8..24, 0 = about eight rays per
+ * bin) sets the number of bins. The sort's buffers (8 bytes per ray plus 4
+ * per bin) are allocated on the first trace that needs them and kept by the
+ * accelerator. Statistics traces, probes and yrc_trace_host keep the
+ * caller's order. No counterpart in the reference (its CPU traversal takes
+ * rays one at a time, src/accel/bvh_traversal.cpp:253-345). */
+#define YRC_RAY_ORDER_OFF 0
+#define YRC_RAY_ORDER_DIRECTION 1
+#define YRC_RAY_ORDER_TWO_POINT 2
+yrc_status yrc_accel_set_ray_order(yrc_accel* accel, int32_t mode, int32_t key_bits, float length);
+int32_t yrc_accel_get_ray_order(const yrc_accel* accel);
+
+/* Per-launch device timing of yrc_trace_device: with timing on, each trace
+ * records CUDA events in its stream around the reordering and around the
+ * traversal kernel; last_timing waits for the last trace and returns both
+ * durations in milliseconds (order_ms = 0 when the launch did not sort). */
+yrc_status yrc_accel_set_timing(yrc_accel* accel, int32_t enable);
+yrc_status yrc_accel_last_timing(yrc_accel* accel, float* order_ms, float* trace_ms);
+
 /* ------------------------------------------------------------------ probe */
 
 #define YRC_PROBE_MAX_HITS 64 /* BvhProbeHits::MaxHits (bvh.hpp:122-127) */
@@ -845,6 +872,24 @@ yrc_status yrc_render(yrc_render_scene* scene, const yrc_render_request* request
 yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t count, const yrc_render_request* requests,
                            yrc_film_pixel* const* films_out, uint64_t* bad_samples_out, yrc_render_stats* stats,
                            double* device_seconds);
+
+/*
+ * yrc_render_many with pooled traversal: every step is ONE graph launch in
+ * which, per bounce, the extend rays of all scenes still rendering are
+ * traced by ONE persistent traversal kernel and their shadow rays by ONE
+ * shadow kernel (each lane takes a ray from any scene's queue through a
+ * device job table and works with that scene's BVH and outputs), while the
+ * scenes' generate, shading, next-event and film stages run as parallel
+ * branches of the graph. Scenes in one pooled launch share the BVH kind and
+ * stack class; a call with both kinds makes one launch per kind. At most
+ * 128 scenes per call; otherwise the arguments, results (films byte for
+ * byte equal to yrc_render's) and limits are yrc_render_many's. No
+ * counterpart in the reference (its CpuWorkerPool renders one job per
+ * pass loop, src/backends/cpu/cpu_path_tracer.cpp:109-160).
+ */
+yrc_status yrc_render_pooled(yrc_render_scene* const* scenes, int32_t count, const yrc_render_request* requests,
+                             yrc_film_pixel* const* films_out, uint64_t* bad_samples_out, yrc_render_stats* stats,
+                             double* device_seconds);
 
 /*
  * TraceShadowVisibility (src/integrators/path_direct_lighting.cpp:23-113) for

@@ -69,3 +69,46 @@ def test_oversized_job_runs_alone():
     r = _StubRunner()
     res = r.run_concurrent(jobs, concurrency=4, budget_bytes=1)
     assert all(j.ok for j in jobs) and res.peak_concurrency == 1
+
+
+class _StubPrepared:
+    """A prepared scene's queue-capacity rules without a device: the
+    capacity is a whole number of passes between one pass and min(spp, 64)."""
+
+    def __init__(self, scene, capacity):
+        self.scene = scene
+        self._cap = capacity
+
+    @property
+    def capacity(self):
+        pixels = self.scene.width * self.scene.height
+        return min(max(self._cap, pixels), pixels * min(self.scene.spp, 64))
+
+    def set_tuning(self, tuning):
+        self._cap = int(tuning["capacity"])
+
+
+def test_fit_capacities_brings_the_working_sets_under_the_budget(monkeypatch):
+    """All jobs stay resident once rendered, so preparation halves the
+    largest jobs' queue capacities (whole passes, never below one) until
+    every job's working memory fits the device at once."""
+    jobs = batch.job_set(12, seed=5, spp_scale=1.0, max_triangles=50_000)
+    for j in jobs:
+        pixels = j.scene.width * j.scene.height
+        j.prepared = _StubPrepared(j.scene, pixels * min(j.scene.spp, 64))
+        j.tuning = {"capacity": j.prepared.capacity, "trace_shape": 2}
+    before = sum(batch._working_set(j) for j in jobs)
+    budget = before // 3
+    r = batch.JobRunner(reserve_bytes=0)
+    monkeypatch.setattr(batch, "_free_device_bytes", lambda: budget)
+    r.fit_capacities(jobs)
+    after = sum(batch._working_set(j) for j in jobs)
+    assert after <= budget < before
+    for j in jobs:
+        pixels = j.scene.width * j.scene.height
+        assert j.prepared.capacity % pixels == 0 and j.prepared.capacity >= pixels
+        assert j.tuning["trace_shape"] == 2
+    # A budget below one pass of every job leaves each job at one pass.
+    monkeypatch.setattr(batch, "_free_device_bytes", lambda: 1)
+    r.fit_capacities(jobs)
+    assert all(j.prepared.capacity == j.scene.width * j.scene.height for j in jobs)

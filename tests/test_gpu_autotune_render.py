@@ -5,7 +5,7 @@ and later renders use it."""
 import numpy as np
 import pytest
 
-from yaoray_b200 import batch, cornell
+from yaoray_b200 import accel, batch, cornell
 from yaoray_b200.render import CudaBackend
 
 pytestmark = pytest.mark.gpu
@@ -36,7 +36,7 @@ def test_autotune_chooses_a_candidate_and_keeps_it():
     t = p.autotune()
     pixels = job.scene.width * job.scene.height
     assert t["capacity"] % pixels == 0 and pixels <= t["capacity"] <= pixels * min(job.scene.spp, 64)
-    assert 0 <= t["trace_shape"] < 7 and t["candidates"] >= 2 and t["seconds_per_sample"] > 0
+    assert 0 <= t["trace_shape"] < accel.TRACE_SHAPES and t["candidates"] >= 2 and t["seconds_per_sample"] > 0
     assert p.capacity == t["capacity"]
     again = b.render(p)
     assert again.ok, again.error

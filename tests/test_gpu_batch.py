@@ -98,3 +98,48 @@ def test_shared_launch_renders_every_scene_kind():
     for k, (one, shared) in enumerate(zip(singles, many)):
         assert one.ok and shared.ok, (k, one.error, shared.error)
         assert shared.film.tobytes() == one.film.tobytes(), k
+
+
+def test_pooled_launch_matches_single_renders():
+    """yrc_render_pooled: per bounce one persistent traversal launch serves
+    the extend rays of every unfinished job and one their shadow rays; the
+    films equal one-at-a-time renders byte for byte for the jobs without a
+    cache (a ray's hit does not depend on which launch traced it)."""
+    jobs = batch.job_set(6, seed=13, spp_scale=1 / 64, max_triangles=100_000)
+    runner = batch.JobRunner(keep_films=True)
+    try:
+        runner.prepare(jobs)
+        runner.run_sequential(jobs)
+        films = {j.name: j.film.copy() for j in jobs}
+        res = runner.run_shared_launch(jobs, concurrency=6, pooled=True)
+        assert all(j.ok for j in jobs), [j.error for j in jobs if not j.ok]
+        assert res.peak_concurrency > 1
+        for j in jobs:
+            assert (j.film["samples"] == j.scene.spp).all()
+            if not j.use_cache:
+                assert j.film.tobytes() == films[j.name].tobytes(), j.name
+    finally:
+        runner.close(jobs)
+
+
+def test_pooled_launch_renders_every_scene_kind():
+    """Pooled launches over scenes of every kind: flat and two-level BVHs
+    (one pooled launch per kind), exact-loop shadows (traced per scene),
+    transmittance and any-hit shadows (pooled); films equal one-at-a-time
+    renders."""
+    from yaoray_b200 import cornell
+    from yaoray_b200.render import CudaBackend
+
+    scenes = [cornell.textured_scene(48, 48, 8, 6), cornell.cutout_scene(48, 48, 8, 6),
+              cornell.instanced_cutout_scene(48, 48, 8, 6), cornell.measured_scene(48, 48, 8, 6),
+              cornell.analytic_scene(48, 48, 8, 6, many=True), cornell.scene(48, 48, 8, 6),
+              cornell.scene(32, 40, 4, 3)]
+    b = CudaBackend()
+    prepared = [b.prepare(s) for s in scenes]
+    singles = [b.render(p) for p in prepared]
+    pooled = b.render_many(prepared, pooled=True)
+    for k, (one, shared) in enumerate(zip(singles, pooled)):
+        assert one.ok and shared.ok, (k, one.error, shared.error)
+        assert shared.film.tobytes() == one.film.tobytes(), k
+        assert shared.stats["rays_traced"] == one.stats["rays_traced"], k
+        assert shared.stats["occluded_shadow_rays"] == one.stats["occluded_shadow_rays"], k

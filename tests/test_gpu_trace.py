@@ -326,13 +326,13 @@ def test_every_launch_shape_is_bit_identical(cuda, full_set):
     rays = torch.from_numpy(scenes.incoherent_rays(500_000, seed=77)).to(cuda)
     base_hits = dev.intersect(rays).clone()
     base_occ = dev.intersect(rays, any_hit=True).clone()
-    for shape in range(7):
+    for shape in range(accel.TRACE_SHAPES):
         dev.set_trace_shape(shape)
         dev.set_trace_shape(shape, any_hit=True)
         assert torch.equal(dev.intersect(rays).view(torch.int32), base_hits.view(torch.int32)), shape
         assert torch.equal(dev.intersect(rays, any_hit=True), base_occ), shape
     tuned = dev.autotune(rays)
-    assert 0 <= tuned["shape"] < 7 and min(tuned["times_ms"]) > 0
+    assert 0 <= tuned["shape"] < accel.TRACE_SHAPES and min(tuned["times_ms"]) > 0
     dev.check()
 
 
@@ -356,7 +356,7 @@ def test_four_wide_traversal_matches_binary(cuda, full_set):
     wide_occ = dev.intersect(rays, any_hit=True)
     assert torch.equal(wide_hits.view(torch.int32), bin_hits.view(torch.int32))
     assert torch.equal(wide_occ, bin_occ)
-    for shape in range(7):
+    for shape in range(accel.TRACE_SHAPES):
         dev.set_trace_shape(shape)
         assert torch.equal(dev.intersect(rays).view(torch.int32), bin_hits.view(torch.int32)), shape
     dev.check()
@@ -364,6 +364,40 @@ def test_four_wide_traversal_matches_binary(cuda, full_set):
     assert gs.spheres.size > 0
     with pytest.raises(Exception):
         accel.DeviceAccelerator(gs, accel.build_bvh(gs)).set_wide(True)
+
+
+def test_ray_order_keeps_every_hit(cuda, full_set):
+    """Reordering the rays before a trace (both key kinds, several key
+    sizes) changes only which lanes share a warp: closest and any hits are
+    those of the unordered trace, bit for bit, for incoherent, coherent
+    (many rays per key bin) and shadow rays, and the timing entry point
+    reports both stages."""
+    import torch
+
+    g, b = full_set
+    dev = accel.DeviceAccelerator(g, b)
+    assert dev.ray_order == "off"
+    rays = torch.from_numpy(np.concatenate([scenes.incoherent_rays(300_000, seed=93),
+                                            scenes.coherent_rays(400, 400),
+                                            scenes.shadow_rays(200_000, seed=94)])).to(cuda)
+    ref_hits = dev.intersect(rays).clone()
+    ref_occ = dev.intersect(rays, any_hit=True).clone()
+    dev.set_timing(True)
+    for mode, bits, length in (("direction", 0, 0.05), ("direction", 8, 0.05), ("two-point", 19, 0.15),
+                               ("two-point", 24, 0.02)):
+        dev.set_ray_order(mode, bits, length)
+        assert dev.ray_order == mode
+        hits = dev.intersect(rays)
+        order_ms, trace_ms = dev.last_timing()
+        assert order_ms > 0.0 and trace_ms > 0.0
+        assert torch.equal(hits.view(torch.int32), ref_hits.view(torch.int32)), (mode, bits)
+        assert torch.equal(dev.intersect(rays, any_hit=True), ref_occ), (mode, bits)
+    dev.set_ray_order("off")
+    dev.intersect(rays)
+    assert dev.last_timing()[0] == 0.0
+    dev.check()
+    with pytest.raises(Exception):
+        dev.set_ray_order("two-point", 25, 0.1)
 
 
 @pytest.mark.parametrize("name", ["trace_two_level", "trace_spheres"])
@@ -377,7 +411,7 @@ def test_every_launch_shape_matches_golden(cuda, name):
     dev = accel.DeviceAccelerator(g, b)
     rays = torch.from_numpy(f["rays"]).to(cuda)
     exp = {k[4:]: v for k, v in f.items() if k.startswith("out_")}
-    for shape in range(7):
+    for shape in range(accel.TRACE_SHAPES):
         dev.set_trace_shape(shape)
         dev.set_trace_shape(shape, any_hit=True)
         inst = torch.empty(rays.shape[0], dtype=torch.int32, device=cuda)

@@ -185,6 +185,10 @@ def lib() -> C.CDLL:
         "yrc_accel_get_trace_shape": (I32, [P, I32]),
         "yrc_accel_set_wide": (C.c_int, [P, I32]),
         "yrc_accel_get_wide": (I32, [P]),
+        "yrc_accel_set_ray_order": (C.c_int, [P, I32, I32, C.c_float]),
+        "yrc_accel_get_ray_order": (I32, [P]),
+        "yrc_accel_set_timing": (C.c_int, [P, I32]),
+        "yrc_accel_last_timing": (C.c_int, [P, P, P]),
         "yrc_stream_synchronize": (C.c_int, [P]),
         "yrc_nrc_create": (C.c_int, [P, C.c_float, C.c_uint64, P]),
         "yrc_nrc_destroy": (None, [P]),

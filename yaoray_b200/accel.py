@@ -23,6 +23,10 @@ import numpy as np
 from . import _lib
 from ._lib import check, lib, ptr
 
+# Compiled launch shapes of the closest / any-hit traversal kernel
+# (YRC_TRACE_SHAPES): the autotuner's candidates.
+TRACE_SHAPES = 7
+
 
 # ------------------------------------------------------------------ geometry
 
@@ -314,7 +318,7 @@ class DeviceAccelerator:
     def autotune(self, rays, any_hit: bool = False, stream=None) -> dict:
         """Times every launch shape on `rays` (CUDA tensor) and keeps the
         fastest; returns {shape: milliseconds} and the chosen shape."""
-        times = (C.c_float * 7)()
+        times = (C.c_float * TRACE_SHAPES)()
         n = rays.numel() // 8
         check(lib().yrc_accel_autotune(self._handle, ptr(rays), n, _lib.YRC_TRACE_ANY if any_hit else 0,
                                        _stream_handle(stream), times))
@@ -332,6 +336,30 @@ class DeviceAccelerator:
 
     def set_wide(self, enable: bool) -> None:
         check(lib().yrc_accel_set_wide(self._handle, int(enable)))
+
+    RAY_ORDER_MODES = {"off": 0, "direction": 1, "two-point": 2}
+
+    @property
+    def ray_order(self) -> str:
+        """Reordering applied before device traces: "off", "direction" (key:
+        origin and direction) or "two-point" (key: origin and a point along
+        the ray)."""
+        mode = int(lib().yrc_accel_get_ray_order(self._handle))
+        return {v: k for k, v in self.RAY_ORDER_MODES.items()}[mode]
+
+    def set_ray_order(self, mode: str, key_bits: int = 0, length: float = 0.05) -> None:
+        check(lib().yrc_accel_set_ray_order(self._handle, self.RAY_ORDER_MODES[mode], key_bits, length))
+
+    def set_timing(self, enable: bool) -> None:
+        """Records CUDA events around each device trace's reordering and
+        traversal kernel (read back with last_timing)."""
+        check(lib().yrc_accel_set_timing(self._handle, int(enable)))
+
+    def last_timing(self) -> tuple[float, float]:
+        """(reordering ms, traversal kernel ms) of the last device trace."""
+        order_ms, trace_ms = C.c_float(), C.c_float()
+        check(lib().yrc_accel_last_timing(self._handle, C.byref(order_ms), C.byref(trace_ms)))
+        return float(order_ms.value), float(trace_ms.value)
 
     def check(self) -> None:
         """Synchronises and raises if a kernel recorded an error status."""

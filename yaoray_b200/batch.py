@@ -122,14 +122,16 @@ def _working_set(job: Job) -> int:
     """Device bytes a job's render still has to allocate: none once it has
     rendered (its working memory stays allocated), else the path state and queues
     for its queue capacity (the prepared scene's, else max(2^21, pixels))
-    at ~400 B per path (~700 B with a cache), plus the film and, with a
-    cache, its grid (~300 MB)."""
+    at ~640 B per path for these scenes (path state 196 B, coated-vertex
+    state 80 B, extend / shadow / subsurface queues and transmittance
+    ~350 B), ~760 B with a cache (its query queues), plus the film and,
+    with a cache, its grid, optimiser state and training records (~450 MB)."""
     if job.resident:
         return 0
     pixels = job.scene.width * job.scene.height
     paths = job.prepared.capacity if job.prepared is not None else max(1 << 21, pixels)
-    per = 700 if job.use_cache else 400
-    return paths * per + pixels * 80 + (300 << 20 if job.use_cache else 0)
+    per = 760 if job.use_cache else 640
+    return paths * per + pixels * 80 + (450 << 20 if job.use_cache else 0)
 
 
 @dataclass
@@ -186,6 +188,26 @@ class JobRunner:
                 job.cache.set_average_decay(0.995)
                 job.prepared.set_radiance_cache(job.cache, spread_threshold=1e-4, train_steps=2, averaged=True)
             job.prepare_s = time.perf_counter() - t0
+        self.fit_capacities(jobs)
+
+    def fit_capacities(self, jobs: list[Job]) -> None:
+        """Every schedule here keeps a job's working memory once it has
+        rendered, so all the jobs' working sets must fit the device at once:
+        while their sum exceeds free device memory less the reserve, the
+        largest job's queue capacity is halved (in whole passes of its
+        image, never below one pass). The films do not depend on it."""
+        budget = max(_free_device_bytes() - self.reserve, 0)
+        while sum(_working_set(j) for j in jobs) > budget:
+            cands = [j for j in jobs if not j.resident and j.prepared is not None
+                     and j.prepared.capacity >= 2 * j.scene.width * j.scene.height]
+            if not cands:
+                break
+            job = max(cands, key=_working_set)
+            pixels = job.scene.width * job.scene.height
+            cap = max(pixels, job.prepared.capacity // 2 // pixels * pixels)
+            shape = job.tuning["trace_shape"] if job.tuning else 0
+            job.prepared.set_tuning({"capacity": cap, "trace_shape": shape})
+            job.tuning = dict(job.tuning or {}, capacity=cap, trace_shape=shape, fitted=True)
 
     def _render(self, job: Job) -> None:
         t0 = time.perf_counter()
@@ -241,12 +263,15 @@ class JobRunner:
         wall = time.perf_counter() - t0
         return BatchResult(list(jobs), wall, sum(j.samples for j in jobs), peak[0], {"budget_bytes": budget})
 
-    def run_shared_launch(self, jobs: list[Job], concurrency: int = 8, budget_bytes: int | None = None) -> BatchResult:
+    def run_shared_launch(self, jobs: list[Job], concurrency: int = 8, budget_bytes: int | None = None,
+                          pooled: bool = False) -> BatchResult:
         """Renders the jobs in groups of up to `concurrency` (largest first,
         admitted against the budget like run_concurrent), each group with
         one yrc_render_many call: every step of a group is ONE graph launch
-        holding all of its unfinished jobs. A job's latency is its group's
-        call."""
+        holding all of its unfinished jobs. With `pooled`, yrc_render_pooled:
+        per bounce one persistent traversal launch serves the extend rays of
+        every job of the group and one the shadow rays. A job's latency is
+        its group's call."""
         budget = budget_bytes if budget_bytes is not None else max(_free_device_bytes() - self.reserve, 0)
         order = sorted(jobs, key=lambda j: -j.scene.width * j.scene.height * j.scene.spp)
         peak = 0
@@ -261,7 +286,7 @@ class JobRunner:
                 i += 1
             peak = max(peak, len(group))
             g0 = time.perf_counter()
-            results = self.backend.render_many([j.prepared for j in group])
+            results = self.backend.render_many([j.prepared for j in group], pooled=pooled)
             dt = time.perf_counter() - g0
             for job, res in zip(group, results):
                 job.latency_s = dt

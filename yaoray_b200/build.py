@@ -79,10 +79,22 @@ def build(force: bool = False, ptxas_verbose: bool = False, jobs: int | None = N
     if not force and LIB.exists() and LIB.stat().st_mtime >= newest:
         return LIB
     logs = []
+    # An object is reused when it is newer than its source, every header and
+    # this script (a header change rebuilds every unit).
+    common = max(_headers_mtime(), Path(__file__).stat().st_mtime)
+
+    def fresh(src: Path) -> bool:
+        obj = OBJ / (src.name + ".o")
+        return (not force and not ptxas_verbose and obj.exists()
+                and obj.stat().st_mtime >= max(src.stat().st_mtime, common))
+
     with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 4)) as ex:
-        futs = [ex.submit(_compile, s, ptxas_verbose) for s in srcs]
+        futs = [None if fresh(s) else ex.submit(_compile, s, ptxas_verbose) for s in srcs]
         objs = []
-        for f in futs:
+        for src, f in zip(srcs, futs):
+            if f is None:
+                objs.append(OBJ / (src.name + ".o"))
+                continue
             obj, log = f.result()
             objs.append(obj)
             if log.strip():

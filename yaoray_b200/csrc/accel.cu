@@ -325,6 +325,17 @@ struct yrc_accel {
     int trace_shape[2] = {0, 0};  // launch shape for closest / any hit (autotuned)
     int64_t device_bytes = 0;
     yrc::HostPipeline pipe;
+    // Ray reordering ahead of device traces (yrc_accel_set_ray_order).
+    int order_mode = 0;
+    int order_bits = 0;          // 0: chosen from the ray count
+    float order_length = 0.05f;  // two-point key distance, fraction of the root box diagonal
+    yrc::RayOrderScratch order{};
+    int64_t order_capacity = 0;  // rays the key / permutation buffers hold
+    int order_hist_bits = 0;     // bins the histogram holds (log2)
+    // Per-launch timing of device traces (yrc_accel_set_timing).
+    bool timing = false;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    bool timed_order = false;
     std::mutex mutex;
 };
 
@@ -364,7 +375,43 @@ void FreeAccel(yrc_accel* a) {
         if (p.streams[s]) cudaStreamDestroy(p.streams[s]);
     }
     cudaFree(p.d_counters);
+    cudaFree(a->order.keys);
+    cudaFree(a->order.order);
+    cudaFree(a->order.hist);
+    cudaFree(a->order.tile_sums);
+    for (cudaEvent_t e : a->ev) {
+        if (e) cudaEventDestroy(e);
+    }
     delete a;
+}
+
+// Grows the reordering buffers to `count` rays and 2^bits bins.
+cudaError_t EnsureOrderScratch(yrc_accel* a, int64_t count, int bits) {
+    cudaError_t err = cudaSuccess;
+    if (count > a->order_capacity) {
+        cudaFree(a->order.keys);
+        cudaFree(a->order.order);
+        a->order.keys = a->order.order = nullptr;
+        a->order_capacity = 0;
+        err = cudaMalloc(reinterpret_cast<void**>(&a->order.keys), static_cast<size_t>(count) * sizeof(uint32_t));
+        if (err == cudaSuccess)
+            err = cudaMalloc(reinterpret_cast<void**>(&a->order.order), static_cast<size_t>(count) * sizeof(uint32_t));
+        if (err != cudaSuccess) return err;
+        a->order_capacity = count;
+    }
+    if (bits > a->order_hist_bits) {
+        cudaFree(a->order.hist);
+        cudaFree(a->order.tile_sums);
+        a->order.hist = a->order.tile_sums = nullptr;
+        a->order_hist_bits = 0;
+        err = cudaMalloc(reinterpret_cast<void**>(&a->order.hist), (size_t{1} << bits) * sizeof(uint32_t));
+        if (err == cudaSuccess)
+            err = cudaMalloc(reinterpret_cast<void**>(&a->order.tile_sums),
+                             static_cast<size_t>(RayOrderTiles(bits)) * sizeof(uint32_t));
+        if (err != cudaSuccess) return err;
+        a->order_hist_bits = bits;
+    }
+    return cudaSuccess;
 }
 
 yrc_status Finalize(Layout& layout, int32_t root_ref, const float lo[3], const float hi[3], int32_t two_level,
@@ -406,9 +453,15 @@ yrc_status Finalize(Layout& layout, int32_t root_ref, const float lo[3], const f
     return Ok();
 }
 
+// Rays below this count are traced in the caller's order: sorting them
+// costs more than the coherence it buys.
+constexpr int64_t kOrderMinRays = int64_t{1} << 16;
+
+// `reorder`: the launch may sort the rays first (the accelerator's
+// reordering buffers are not shared with another stream at the time).
 yrc_status LaunchInternal(yrc_accel* a, const yrc_ray* rays, int64_t count, int32_t flags, yrc_hit* hits,
                           int32_t* instances, uint8_t* occluded, uint32_t* nt, uint32_t* tt, uint32_t* st,
-                          unsigned long long* counter, cudaStream_t stream) {
+                          unsigned long long* counter, cudaStream_t stream, bool reorder = false) {
     if (count <= 0) return Ok();
     TraceArgs args{};
     args.accel = a->params;
@@ -422,12 +475,31 @@ yrc_status LaunchInternal(yrc_accel* a, const yrc_ray* rays, int64_t count, int3
     args.sphere_tests = st;
     args.counter = counter;
     args.error = a->d_error;
-    cudaError_t err = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
-    if (err != cudaSuccess) return CudaFail(err, "trace counter reset");
     const bool any = (flags & YRC_TRACE_ANY) != 0;
     const bool stats = (flags & YRC_TRACE_STATS) != 0;
+    const bool order = reorder && !stats && a->order_mode != kRayOrderOff && count >= kOrderMinRays &&
+                       count < (int64_t{1} << 32);
+    cudaError_t err = cudaSuccess;
+    if (a->timing) err = cudaEventRecord(a->ev[0], stream);
+    if (order && err == cudaSuccess) {
+        const int bits = RayOrderBits(count, a->order_bits);
+        err = EnsureOrderScratch(a, count, bits);
+        if (err != cudaSuccess) return CudaFail(err, "ray order scratch");
+        err = OrderRays(args.rays, count, a->params, a->order_mode, bits, a->order_length, a->order, stream,
+                        a->sm_count);
+        if (err != cudaSuccess) return CudaFail(err, "ray order");
+        args.order = a->order.order;
+    }
+    if (a->timing && err == cudaSuccess) err = cudaEventRecord(a->ev[1], stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
+    if (err != cudaSuccess) return CudaFail(err, "trace counter reset");
     err = LaunchTrace(args, any, stats, a->trace_shape[any ? 1 : 0], stream, a->sm_count);
     if (err != cudaSuccess) return CudaFail(err, "trace launch");
+    if (a->timing) {
+        err = cudaEventRecord(a->ev[2], stream);
+        if (err != cudaSuccess) return CudaFail(err, "trace timing event");
+        a->timed_order = order;
+    }
     return Ok();
 }
 
@@ -627,7 +699,7 @@ yrc_status yrc_trace_device(yrc_accel* accel, const yrc_ray* rays, int64_t count
     std::lock_guard<std::mutex> lock(accel->mutex);
     cudaSetDevice(accel->device);
     return LaunchInternal(accel, rays, count, flags & ~YRC_TRACE_STATS, hits, instances, occluded, nullptr, nullptr,
-                          nullptr, accel->d_counter, static_cast<cudaStream_t>(stream));
+                          nullptr, accel->d_counter, static_cast<cudaStream_t>(stream), true);
 }
 
 yrc_status yrc_trace_stats_device(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags,
@@ -835,6 +907,50 @@ yrc_status yrc_accel_set_wide(yrc_accel* accel, int32_t enable) {
 
 int32_t yrc_accel_get_wide(const yrc_accel* accel) { return accel && accel->wide_enabled ? 1 : 0; }
 
+yrc_status yrc_accel_set_ray_order(yrc_accel* accel, int32_t mode, int32_t key_bits, float length) {
+    using namespace yrc;
+    if (!accel || mode < YRC_RAY_ORDER_OFF || mode > YRC_RAY_ORDER_TWO_POINT || key_bits < 0 ||
+        key_bits > kRayOrderMaxBits || !(length >= 0.0f) || !(length <= 16.0f)) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_set_ray_order: bad argument");
+    }
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    accel->order_mode = mode;
+    accel->order_bits = key_bits;
+    accel->order_length = length;
+    return Ok();
+}
+
+int32_t yrc_accel_get_ray_order(const yrc_accel* accel) { return accel ? accel->order_mode : -1; }
+
+yrc_status yrc_accel_set_timing(yrc_accel* accel, int32_t enable) {
+    using namespace yrc;
+    if (!accel) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_set_timing: null accelerator");
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    cudaSetDevice(accel->device);
+    if (enable && !accel->ev[0]) {
+        for (cudaEvent_t& e : accel->ev) {
+            const cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) return CudaFail(err, "yrc_accel_set_timing");
+        }
+    }
+    accel->timing = enable != 0;
+    return Ok();
+}
+
+yrc_status yrc_accel_last_timing(yrc_accel* accel, float* order_ms, float* trace_ms) {
+    using namespace yrc;
+    if (!accel || !order_ms || !trace_ms) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_last_timing: bad argument");
+    std::lock_guard<std::mutex> lock(accel->mutex);
+    if (!accel->timing) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_last_timing: timing is off");
+    cudaSetDevice(accel->device);
+    cudaError_t err = cudaEventSynchronize(accel->ev[2]);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(order_ms, accel->ev[0], accel->ev[1]);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(trace_ms, accel->ev[1], accel->ev[2]);
+    if (err != cudaSuccess) return CudaFail(err, "yrc_accel_last_timing");
+    if (!accel->timed_order) *order_ms = 0.0f;
+    return Ok();
+}
+
 yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags, void* stream,
                               float* times_ms) {
     using namespace yrc;
@@ -858,7 +974,7 @@ yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t cou
             cudaEventRecord(e0, st);
             status = LaunchInternal(accel, rays, count, flags & YRC_TRACE_ANY, any ? nullptr : static_cast<yrc_hit*>(out),
                                     nullptr, any ? static_cast<uint8_t*>(out) : nullptr, nullptr, nullptr, nullptr,
-                                    accel->d_counter, st);
+                                    accel->d_counter, st, true);
             cudaEventRecord(e1, st);
             cudaEventSynchronize(e1);
             float ms = 0.0f;

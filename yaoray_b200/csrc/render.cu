@@ -138,55 +138,80 @@ struct yrc_render_scene {
 
 namespace yrc {
 namespace {
-// The shadow stage of a bounce over the queued shadow rays: the exact
-// per-thread loop (cut-outs, textured thin glass), the single-pass
-// transmittance kernel with its exact-loop overflow (surfaces that pass
-// light), or the any-hit kernel.
-cudaError_t ShadowStage(yrc_render_scene* s, const Queues& q, int64_t C, int* error, cudaStream_t st) {
+// How a scene traces its shadow rays: the exact per-thread loop (cut-outs,
+// textured thin glass), the single-pass transmittance kernel with its
+// exact-loop overflow (surfaces that pass light), or the any-hit kernel.
+enum class ShadowKind { kExact, kTransmittance, kAnyHit };
+
+ShadowKind ShadowKindOf(const yrc_render_scene* s) {
+    if (s->dev.exact_shadows) return ShadowKind::kExact;
+    return s->dev.any_transparent ? ShadowKind::kTransmittance : ShadowKind::kAnyHit;
+}
+
+ShadowArgs TransmittanceArgs(yrc_render_scene* s, const Queues& q, int64_t C, int* error) {
     const DevScene& sc = s->dev;
+    ShadowArgs sa{};
+    sa.accel = sc.accel;
+    sa.rays = q.shadow_ray;
+    sa.count_ptr = q.counters + kCtrShadow;
+    sa.capacity = 2 * C;
+    sa.out_index = q.shadow_slot;
+    sa.transmittance = s->transmittance;
+    sa.tri_prim = sc.tri_prim;
+    sa.prim_material = sc.prim_material;
+    sa.sphere_material = sc.sphere_material;
+    sa.materials = sc.materials;
+    sa.tri_clear = sc.tri_clear;
+    sa.sphere_clear = sc.sphere_clear;
+    sa.counter = q.counters + kCtrShadowTrace;
+    sa.occluded_count = q.counters + kCtrStatsBase + 2;
+    sa.overflow = q.shadow_overflow;
+    sa.overflow_count = q.counters + kCtrShadowOverflow;
+    sa.error = error;
+    return sa;
+}
+
+TraceArgs AnyHitShadowArgs(const Queues& q, const AccelParams& accel, int64_t C, int* error) {
+    TraceArgs sh{};
+    sh.accel = accel;
+    sh.rays = q.shadow_ray;
+    sh.count = 2 * C;
+    sh.count_ptr = q.counters + kCtrShadow;
+    sh.occluded = q.shadow_occluded;
+    sh.out_index = q.shadow_slot;
+    sh.counter = q.counters + kCtrShadowTrace;
+    sh.occluded_count = q.counters + kCtrStatsBase + 2;
+    sh.error = error;
+    return sh;
+}
+
+// Rays that passed more than 16 clear surfaces in the transmittance kernel:
+// the exact loop.
+void ShadowOverflow(yrc_render_scene* s, const Queues& q, int64_t C, int* error, cudaStream_t st) {
+    LaunchShadowExact(s->dev, q, s->transmittance, q.counters + kCtrStatsBase + 2, 2 * C, s->sm_count, error, st,
+                      q.shadow_overflow);
+}
+
+// The shadow stage of a bounce over the queued shadow rays.
+cudaError_t ShadowStage(yrc_render_scene* s, const Queues& q, int64_t C, int* error, cudaStream_t st) {
     cudaError_t err = cudaSuccess;
-    if (sc.exact_shadows) {
-        LaunchShadowExact(sc, q, s->transmittance, q.counters + kCtrStatsBase + 2, 2 * C, s->sm_count, error,
-                          st);
-        err = cudaGetLastError();
-    } else if (sc.any_transparent) {
-        ShadowArgs sa{};
-        sa.accel = sc.accel;
-        sa.rays = q.shadow_ray;
-        sa.count_ptr = q.counters + kCtrShadow;
-        sa.capacity = 2 * C;
-        sa.out_index = q.shadow_slot;
-        sa.transmittance = s->transmittance;
-        sa.tri_prim = sc.tri_prim;
-        sa.prim_material = sc.prim_material;
-        sa.sphere_material = sc.sphere_material;
-        sa.materials = sc.materials;
-        sa.tri_clear = sc.tri_clear;
-        sa.sphere_clear = sc.sphere_clear;
-        sa.counter = q.counters + kCtrShadowTrace;
-        sa.occluded_count = q.counters + kCtrStatsBase + 2;
-        sa.overflow = q.shadow_overflow;
-        sa.overflow_count = q.counters + kCtrShadowOverflow;
-        sa.error = error;
-        err = LaunchShadowTransmittance(sa, st, s->sm_count);
-        // Rays past more than 16 clear surfaces: the exact loop.
-        if (err == cudaSuccess) {
-            LaunchShadowExact(sc, q, s->transmittance, q.counters + kCtrStatsBase + 2, 2 * C, s->sm_count,
-                              error, st, q.shadow_overflow);
+    switch (ShadowKindOf(s)) {
+        case ShadowKind::kExact:
+            LaunchShadowExact(s->dev, q, s->transmittance, q.counters + kCtrStatsBase + 2, 2 * C, s->sm_count, error,
+                              st);
             err = cudaGetLastError();
-        }
-    } else {
-        TraceArgs sh{};
-        sh.accel = sc.accel;
-        sh.rays = q.shadow_ray;
-        sh.count = 2 * C;
-        sh.count_ptr = q.counters + kCtrShadow;
-        sh.occluded = q.shadow_occluded;
-        sh.out_index = q.shadow_slot;
-        sh.counter = q.counters + kCtrShadowTrace;
-        sh.occluded_count = q.counters + kCtrStatsBase + 2;
-        sh.error = error;
-        err = LaunchTrace(sh, true, false, TraceShapeOf(s->accel, 1), st, s->sm_count);
+            break;
+        case ShadowKind::kTransmittance:
+            err = LaunchShadowTransmittance(TransmittanceArgs(s, q, C, error), st, s->sm_count);
+            if (err == cudaSuccess) {
+                ShadowOverflow(s, q, C, error, st);
+                err = cudaGetLastError();
+            }
+            break;
+        case ShadowKind::kAnyHit:
+            err = LaunchTrace(AnyHitShadowArgs(q, s->dev.accel, C, error), true, false, TraceShapeOf(s->accel, 1), st,
+                              s->sm_count);
+            break;
     }
     return err;
 }
@@ -813,68 +838,91 @@ yrc_status EnsureCache(yrc_render_scene* s) {
     return Ok();
 }
 
-// Records one batch (generate, max_depth bounces, film, next active list).
-yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
-    const DevScene& sc = s->dev;
-    const int64_t C = s->capacity;
-    const int64_t pixels = static_cast<int64_t>(sc.width) * sc.height;
-    cudaStream_t st = s->stream;
-    BatchArgs b{s->active, s->scalars + 0, s->scalars + 1, s->batch, s->film};
-    FilmArgs f{s->attempts, s->scalars + 2, s->scalars + 3, s->settings.adaptive_enabled, s->settings.adaptive_min_spp,
-               s->settings.adaptive_relative_error, s->settings.adaptive_absolute_error,
-               s->settings.adaptive_confidence};
+// One batch of a scene in stages (generate; per bounce: counters, extend
+// trace, shading, shadow trace, next-event resolve; film), so that a pooled
+// batch of several scenes can interleave them with shared traversal
+// launches. Queues `q` are the scene's queues at this bounce (the extend
+// queues alternate between bounces).
+
+yrc_status BatchPrologue(yrc_render_scene* s, cudaStream_t st) {
     const CacheArgs& cache = s->cargs;
     if (cache.enabled) {
         const cudaError_t err = cudaMemsetAsync(cache.counters, 0, 4 * sizeof(unsigned long long), st);
         if (err != cudaSuccess) return CudaError(err, "cache counters");
     }
-    LaunchGenerate(sc, s->ps, s->q, b, cache, C, s->sm_count, st);
-    Queues q = s->q;
-    for (int depth = 0; depth < sc.max_depth; ++depth) {
-        LaunchResetCounters(q, st);
-        TraceArgs ta{};
-        ta.accel = sc.accel;
-        ta.rays = q.ray_in;
-        ta.count = C;
-        ta.count_ptr = q.counters + kCtrIn;
-        ta.hits = reinterpret_cast<yrc_hit*>(q.hits);
-        ta.instances = q.inst;
-        ta.counter = q.counters + kCtrTrace;
-        ta.error = AccelErrorWord(s->accel);
-        cudaError_t err = LaunchTrace(ta, false, false, TraceShapeOf(s->accel, 0), st, s->sm_count);
-        if (err != cudaSuccess) return CudaError(err, "extend trace");
-        if (sc.any_alpha) LaunchAlphaExtend(sc, s->ps, q, depth, C, s->sm_count, ta.error, st);
-        LaunchShade(sc, s->ps, q, cache, depth, C, s->sm_count, st);
-        if (sc.any_subsurface) {
-            RenderProbeArgs pa{};
-            pa.accel = sc.accel;
-            pa.rays = q.probe_ray;
-            pa.targets = q.probe_target;
-            pa.selection = q.probe_entry;
-            pa.count_ptr = q.counters + kCtrProbe;
-            pa.capacity = C;
-            pa.hit = q.probe_hit;
-            pa.hits = q.probe_count;
-            pa.error = AccelErrorWord(s->accel);
-            const cudaError_t perr = LaunchRenderProbe(pa, st, s->sm_count);
-            if (perr != cudaSuccess) return CudaError(perr, "subsurface probe");
-            LaunchSubsurfaceExit(sc, s->ps, q, depth, C, s->sm_count, st);
-        }
-        err = ShadowStage(s, q, C, ta.error, st);
-        if (err != cudaSuccess) return CudaError(err, "shadow trace");
-        LaunchNeeResolve(s->ps, q, s->transmittance, C, s->sm_count, st);
-        if (sc.any_layered) {
-            // Coated vertices: their next events in the reference's PCG32
-            // order, with a second shadow stage in between.
-            LaunchLayeredNee(sc, s->ps, q, s->transmittance, depth, C, s->sm_count, st);
-            err = ShadowStage(s, q, C, ta.error, st);
-            if (err != cudaSuccess) return CudaError(err, "coated-vertex shadow trace");
-            LaunchLayeredContinue(sc, s->ps, q, s->transmittance, depth, C, s->sm_count, st);
-        }
-        LaunchAdvanceQueue(q, st);
-        std::swap(q.ray_in, q.ray_out);
-        std::swap(q.path_in, q.path_out);
+    BatchArgs b{s->active, s->scalars + 0, s->scalars + 1, s->batch, s->film};
+    LaunchGenerate(s->dev, s->ps, s->q, b, cache, s->capacity, s->sm_count, st);
+    return Ok();
+}
+
+// The extend trace's arguments (closest hit over the current queue).
+TraceArgs ExtendTraceArgs(yrc_render_scene* s, const Queues& q) {
+    TraceArgs ta{};
+    ta.accel = s->dev.accel;
+    ta.rays = q.ray_in;
+    ta.count = s->capacity;
+    ta.count_ptr = q.counters + kCtrIn;
+    ta.hits = reinterpret_cast<yrc_hit*>(q.hits);
+    ta.instances = q.inst;
+    ta.counter = q.counters + kCtrTrace;
+    ta.error = AccelErrorWord(s->accel);
+    return ta;
+}
+
+// Shading after the extend trace: alpha skips, the class shade kernels,
+// subsurface probes and exits.
+yrc_status BounceShade(yrc_render_scene* s, const Queues& q, int depth, cudaStream_t st) {
+    const DevScene& sc = s->dev;
+    const int64_t C = s->capacity;
+    if (sc.any_alpha) LaunchAlphaExtend(sc, s->ps, q, depth, C, s->sm_count, AccelErrorWord(s->accel), st);
+    LaunchShade(sc, s->ps, q, s->cargs, depth, C, s->sm_count, st);
+    if (sc.any_subsurface) {
+        RenderProbeArgs pa{};
+        pa.accel = sc.accel;
+        pa.rays = q.probe_ray;
+        pa.targets = q.probe_target;
+        pa.selection = q.probe_entry;
+        pa.count_ptr = q.counters + kCtrProbe;
+        pa.capacity = C;
+        pa.hit = q.probe_hit;
+        pa.hits = q.probe_count;
+        pa.error = AccelErrorWord(s->accel);
+        const cudaError_t perr = LaunchRenderProbe(pa, st, s->sm_count);
+        if (perr != cudaSuccess) return CudaError(perr, "subsurface probe");
+        LaunchSubsurfaceExit(sc, s->ps, q, depth, C, s->sm_count, st);
     }
+    return Ok();
+}
+
+// After the shadow trace: next-event resolve, coated vertices (with their
+// own second shadow stage), and the next bounce's queue.
+yrc_status BounceResolve(yrc_render_scene* s, const Queues& q, int depth, cudaStream_t st) {
+    const DevScene& sc = s->dev;
+    const int64_t C = s->capacity;
+    LaunchNeeResolve(s->ps, q, s->transmittance, C, s->sm_count, st);
+    if (sc.any_layered) {
+        // Coated vertices: their next events in the reference's PCG32
+        // order, with a second shadow stage in between.
+        LaunchLayeredNee(sc, s->ps, q, s->transmittance, depth, C, s->sm_count, st);
+        const cudaError_t err = ShadowStage(s, q, C, AccelErrorWord(s->accel), st);
+        if (err != cudaSuccess) return CudaError(err, "coated-vertex shadow trace");
+        LaunchLayeredContinue(sc, s->ps, q, s->transmittance, depth, C, s->sm_count, st);
+    }
+    LaunchAdvanceQueue(q, st);
+    return Ok();
+}
+
+// After the last bounce: the radiance cache's inference and training, the
+// film, and the next batch's active list.
+yrc_status BatchEpilogue(yrc_render_scene* s, int32_t max_batch, cudaStream_t st) {
+    const DevScene& sc = s->dev;
+    const int64_t C = s->capacity;
+    const int64_t pixels = static_cast<int64_t>(sc.width) * sc.height;
+    BatchArgs b{s->active, s->scalars + 0, s->scalars + 1, s->batch, s->film};
+    FilmArgs f{s->attempts, s->scalars + 2, s->scalars + 3, s->settings.adaptive_enabled, s->settings.adaptive_min_spp,
+               s->settings.adaptive_relative_error, s->settings.adaptive_absolute_error,
+               s->settings.adaptive_confidence};
+    const CacheArgs& cache = s->cargs;
     if (cache.enabled) {
         // Training targets from the unbiased training paths' full radiance;
         // then every path that ended at the cache (training paths at their
@@ -899,6 +947,28 @@ yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return CudaError(err, "batch launch");
     return Ok();
+}
+
+// Records one batch (generate, max_depth bounces, film, next active list).
+yrc_status EnqueueBatch(yrc_render_scene* s, int32_t max_batch) {
+    cudaStream_t st = s->stream;
+    yrc_status status = BatchPrologue(s, st);
+    Queues q = s->q;
+    for (int depth = 0; depth < s->dev.max_depth && status == YRC_OK; ++depth) {
+        LaunchResetCounters(q, st);
+        const TraceArgs ta = ExtendTraceArgs(s, q);
+        cudaError_t err = LaunchTrace(ta, false, false, TraceShapeOf(s->accel, 0), st, s->sm_count);
+        if (err != cudaSuccess) return CudaError(err, "extend trace");
+        status = BounceShade(s, q, depth, st);
+        if (status != YRC_OK) return status;
+        err = ShadowStage(s, q, s->capacity, ta.error, st);
+        if (err != cudaSuccess) return CudaError(err, "shadow trace");
+        status = BounceResolve(s, q, depth, st);
+        std::swap(q.ray_in, q.ray_out);
+        std::swap(q.path_in, q.path_out);
+    }
+    if (status != YRC_OK) return status;
+    return BatchEpilogue(s, max_batch, st);
 }
 
 // Captures one batch as a CUDA graph (all sizes are read on the device),
@@ -1203,32 +1273,224 @@ extern "C" yrc_status yrc_render(yrc_render_scene* s, const yrc_render_request* 
     return FinishRender(run, device_ms / 1e3);
 }
 
-extern "C" yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t count,
-                                      const yrc_render_request* requests, yrc_film_pixel* const* films_out,
-                                      uint64_t* bad_samples_out, yrc_render_stats* stats, double* device_seconds) {
-    using namespace yrc;
+namespace yrc {
+namespace {
+
+// Pooled batch of several scenes: per bounce, the extend rays of every
+// scene go through ONE persistent traversal launch and the shadow rays
+// through ONE transmittance (or any-hit) launch, the lanes taking rays from
+// all scenes' queues (TracePool / ShadowPool); each scene's generate,
+// shading, next-event and film stages run as parallel branches of the same
+// graph. Holds the instantiated graph and the device job tables it reads.
+struct PooledBatch {
+    cudaGraphExec_t exec = nullptr;
+    DeviceArena mem;
+    std::vector<cudaEvent_t> events;
+    void Release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        mem.Release();
+        mem.err = cudaSuccess;
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+        events.clear();
+    }
+    ~PooledBatch() { Release(); }
+};
+
+// The scene's queues at bounce `depth` (the extend queues alternate).
+Queues QueuesAt(const yrc_render_scene* s, int depth) {
+    Queues q = s->q;
+    if (depth & 1) {
+        std::swap(q.ray_in, q.ray_out);
+        std::swap(q.path_in, q.path_out);
+    }
+    return q;
+}
+
+// Pool group of a scene: scenes in one pooled launch share the BVH kind
+// and the traversal stack class.
+int PoolGroup(const yrc_render_scene* s) {
+    return (s->dev.accel.two_level ? 2 : 0) + (s->dev.accel.stack_limit > 64 ? 1 : 0);
+}
+
+// Makes `side` wait for the work recorded on `main` so far (fork), or
+// `main` wait for each of `side` (join); inside a capture these become the
+// graph's dependencies.
+cudaError_t Fork(cudaStream_t main, const std::vector<cudaStream_t>& side, PooledBatch& pb) {
+    cudaEvent_t e = nullptr;
+    cudaError_t err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    if (err != cudaSuccess) return err;
+    pb.events.push_back(e);
+    err = cudaEventRecord(e, main);
+    for (size_t i = 0; i < side.size() && err == cudaSuccess; ++i) err = cudaStreamWaitEvent(side[i], e, 0);
+    return err;
+}
+cudaError_t Join(cudaStream_t main, const std::vector<cudaStream_t>& side, PooledBatch& pb) {
+    cudaError_t err = cudaSuccess;
+    for (size_t i = 0; i < side.size() && err == cudaSuccess; ++i) {
+        cudaEvent_t e = nullptr;
+        err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        if (err != cudaSuccess) break;
+        pb.events.push_back(e);
+        err = cudaEventRecord(e, side[i]);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(main, e, 0);
+    }
+    return err;
+}
+
+struct PoolLaunch {
+    int kind;  // 0 extend (closest hit), 1 shadow transmittance, 2 shadow any hit
+    int group;
+    size_t first;  // into the trace or shadow job table
+    int32_t count;
+    int64_t capacity;
+};
+
+// Records the pooled batch of `ss` (every scene set up by BeginRender) on
+// `main` under stream capture and instantiates it.
+yrc_status CapturePooledBatch(const std::vector<yrc_render_scene*>& ss, cudaStream_t main, PooledBatch& pb) {
+    pb.Release();
+    int max_depth = 0;
+    for (const yrc_render_scene* s : ss) max_depth = std::max(max_depth, s->dev.max_depth);
+    std::vector<TraceArgs> trace_jobs;
+    std::vector<ShadowArgs> shadow_jobs;
+    std::vector<std::vector<PoolLaunch>> launches(static_cast<size_t>(max_depth));
+    for (int d = 0; d < max_depth; ++d) {
+        for (int kind = 0; kind < 3; ++kind) {
+            for (int g = 0; g < 4; ++g) {
+                PoolLaunch L{kind, g, kind == 1 ? shadow_jobs.size() : trace_jobs.size(), 0, 0};
+                for (yrc_render_scene* s : ss) {
+                    if (d >= s->dev.max_depth || PoolGroup(s) != g) continue;
+                    const Queues q = QueuesAt(s, d);
+                    int* error = AccelErrorWord(s->accel);
+                    if (kind == 0) {
+                        trace_jobs.push_back(ExtendTraceArgs(s, q));
+                        L.capacity += s->capacity;
+                    } else if (kind == 1 && ShadowKindOf(s) == ShadowKind::kTransmittance) {
+                        shadow_jobs.push_back(TransmittanceArgs(s, q, s->capacity, error));
+                        L.capacity += 2 * s->capacity;
+                    } else if (kind == 2 && ShadowKindOf(s) == ShadowKind::kAnyHit) {
+                        trace_jobs.push_back(AnyHitShadowArgs(q, s->dev.accel, s->capacity, error));
+                        L.capacity += 2 * s->capacity;
+                    } else {
+                        continue;
+                    }
+                    ++L.count;
+                }
+                if (L.count > 0) launches[static_cast<size_t>(d)].push_back(L);
+            }
+        }
+    }
+    size_t n_launches = 0;
+    for (const auto& v : launches) n_launches += v.size();
+    const TraceArgs* d_trace = pb.mem.Upload(trace_jobs);
+    const ShadowArgs* d_shadow = pb.mem.Upload(shadow_jobs);
+    unsigned long long* counters = pb.mem.Alloc<unsigned long long>(n_launches);
+    if (pb.mem.err != cudaSuccess) return CudaError(pb.mem.err, "pooled batch tables");
+    const int sm_count = ss.front()->sm_count;
+
+    std::vector<cudaStream_t> side;
+    for (yrc_render_scene* s : ss) side.push_back(s->stream);
+    cudaError_t err = cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal);
+    if (err != cudaSuccess) return CudaError(err, "pooled batch capture");
+    yrc_status status = Ok();
+    auto run = [&](cudaError_t e, const char* what) {
+        if (status == YRC_OK && e != cudaSuccess) status = CudaError(e, what);
+        return status == YRC_OK;
+    };
+    auto per_scene = [&](auto&& body) {
+        if (!run(Fork(main, side, pb), "pooled batch fork")) return;
+        for (size_t i = 0; i < ss.size() && status == YRC_OK; ++i) status = body(ss[i]);
+        run(Join(main, side, pb), "pooled batch join");
+    };
+    per_scene([&](yrc_render_scene* s) { return BatchPrologue(s, s->stream); });
+    size_t k = 0;
+    auto pooled = [&](int d, bool shadow) {
+        for (const PoolLaunch& L : launches[static_cast<size_t>(d)]) {
+            if ((L.kind != 0) != shadow || status != YRC_OK) continue;
+            unsigned long long* counter = counters + k++;
+            if (!run(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), main), "pooled counter")) return;
+            const bool two = (L.group & 2) != 0, deep = (L.group & 1) != 0;
+            cudaError_t e;
+            if (L.kind == 1) {
+                e = LaunchPooledShadowTransmittance(ShadowPool{d_shadow + L.first, L.count, L.capacity, counter}, two,
+                                                    deep, main, sm_count);
+            } else {
+                e = LaunchPooledTrace(TracePool{d_trace + L.first, L.count, L.capacity, counter}, L.kind == 2, two,
+                                      deep, main, sm_count);
+            }
+            run(e, L.kind == 0 ? "pooled extend trace" : "pooled shadow trace");
+        }
+    };
+    for (int d = 0; d < max_depth && status == YRC_OK; ++d) {
+        per_scene([&](yrc_render_scene* s) {
+            if (d < s->dev.max_depth) LaunchResetCounters(QueuesAt(s, d), s->stream);
+            return Ok();
+        });
+        pooled(d, false);
+        per_scene([&](yrc_render_scene* s) {
+            return d < s->dev.max_depth ? BounceShade(s, QueuesAt(s, d), d, s->stream) : Ok();
+        });
+        pooled(d, true);
+        per_scene([&](yrc_render_scene* s) {
+            if (d >= s->dev.max_depth) return Ok();
+            const Queues q = QueuesAt(s, d);
+            int* error = AccelErrorWord(s->accel);
+            const ShadowKind kind = ShadowKindOf(s);
+            if (kind == ShadowKind::kExact) {
+                const cudaError_t e = ShadowStage(s, q, s->capacity, error, s->stream);
+                if (e != cudaSuccess) return CudaError(e, "shadow trace");
+            } else if (kind == ShadowKind::kTransmittance) {
+                ShadowOverflow(s, q, s->capacity, error, s->stream);
+            }
+            return BounceResolve(s, q, d, s->stream);
+        });
+    }
+    per_scene([&](yrc_render_scene* s) { return BatchEpilogue(s, s->graph_max_batch, s->stream); });
+    cudaGraph_t graph = nullptr;
+    err = cudaStreamEndCapture(main, &graph);
+    if (status == YRC_OK && err != cudaSuccess) status = CudaError(err, "pooled batch capture");
+    if (status == YRC_OK) {
+        err = cudaGraphInstantiate(&pb.exec, graph, 0);
+        if (err != cudaSuccess) status = CudaError(err, "pooled batch instantiate");
+    }
+    if (graph) cudaGraphDestroy(graph);
+    return status;
+}
+
+// yrc_render_many / yrc_render_pooled: every step launches one graph for
+// the scenes still rendering, rebuilt when a scene finishes.
+yrc_status RenderMany(yrc_render_scene* const* scenes, int32_t count, const yrc_render_request* requests,
+                      yrc_film_pixel* const* films_out, uint64_t* bad_samples_out, yrc_render_stats* stats,
+                      double* device_seconds, bool pooled, const char* name) {
     if (count < 0 || (count > 0 && (!scenes || !films_out))) {
-        return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: bad argument");
+        return Fail(YRC_ERR_INVALID_ARGUMENT, std::string(name) + ": bad argument");
     }
     if (count == 0) return Ok();
+    if (pooled && count > kMaxPoolJobs) {
+        return Fail(YRC_ERR_INVALID_ARGUMENT,
+                    std::string(name) + ": at most " + std::to_string(kMaxPoolJobs) + " scenes per call");
+    }
     // One lock per scene, taken in address order; every scene on one device.
     std::vector<yrc_render_scene*> order(scenes, scenes + count);
     for (int32_t i = 0; i < count; ++i) {
-        if (!order[static_cast<size_t>(i)] || !films_out[i]) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: null scene or film");
+        if (!order[static_cast<size_t>(i)] || !films_out[i]) {
+            return Fail(YRC_ERR_INVALID_ARGUMENT, std::string(name) + ": null scene or film");
+        }
         for (int32_t j = 0; j < i; ++j) {
             if (order[static_cast<size_t>(j)] == order[static_cast<size_t>(i)]) {
-                return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: a scene appears twice");
+                return Fail(YRC_ERR_INVALID_ARGUMENT, std::string(name) + ": a scene appears twice");
             }
         }
         if (order[static_cast<size_t>(i)]->device != order[0]->device) {
-            return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: scenes on different devices");
+            return Fail(YRC_ERR_INVALID_ARGUMENT, std::string(name) + ": scenes on different devices");
         }
         if (requests && requests[i].progress) {
-            return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: progress callbacks are not supported");
+            return Fail(YRC_ERR_INVALID_ARGUMENT, std::string(name) + ": progress callbacks are not supported");
         }
         for (int32_t j = 0; j < i; ++j) {
             if (scenes[i]->cache && scenes[i]->cache == scenes[j]->cache) {
-                return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_render_many: two scenes share a radiance cache");
+                return Fail(YRC_ERR_INVALID_ARGUMENT, std::string(name) + ": two scenes share a radiance cache");
             }
         }
     }
@@ -1254,10 +1516,8 @@ extern "C" yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t c
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, stream);
-    // Each step launches one graph holding the batch graph of every scene
-    // still rendering (child graphs, independent of one another); the
-    // combined graph is rebuilt when a scene finishes.
-    cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec = nullptr;  // child-graph form
+    PooledBatch pb;                  // pooled form
     std::vector<int32_t> members;
     yrc_status status = YRC_OK;
     for (;;) {
@@ -1276,27 +1536,34 @@ extern "C" yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t c
             break;
         }
         if (live != members) {
-            if (exec) cudaGraphExecDestroy(exec);
-            exec = nullptr;
-            cudaGraph_t combined = nullptr;
-            err = cudaGraphCreate(&combined, 0);
-            for (int32_t i : live) {
-                cudaGraphNode_t node = nullptr;
-                if (err == cudaSuccess) {
-                    err = cudaGraphAddChildGraphNode(&node, combined, nullptr, 0,
-                                                     runs[static_cast<size_t>(i)].s->graph_template);
+            if (pooled) {
+                std::vector<yrc_render_scene*> ss;
+                for (int32_t i : live) ss.push_back(runs[static_cast<size_t>(i)].s);
+                status = CapturePooledBatch(ss, stream, pb);
+                if (status != YRC_OK) break;
+            } else {
+                if (exec) cudaGraphExecDestroy(exec);
+                exec = nullptr;
+                cudaGraph_t combined = nullptr;
+                err = cudaGraphCreate(&combined, 0);
+                for (int32_t i : live) {
+                    cudaGraphNode_t node = nullptr;
+                    if (err == cudaSuccess) {
+                        err = cudaGraphAddChildGraphNode(&node, combined, nullptr, 0,
+                                                         runs[static_cast<size_t>(i)].s->graph_template);
+                    }
                 }
-            }
-            if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, combined, 0);
-            if (combined) cudaGraphDestroy(combined);
-            if (err != cudaSuccess) {
-                status = CudaError(err, "combined batch graph");
-                break;
+                if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, combined, 0);
+                if (combined) cudaGraphDestroy(combined);
+                if (err != cudaSuccess) {
+                    status = CudaError(err, "combined batch graph");
+                    break;
+                }
             }
             members = live;
         }
         for (int32_t i : live) QueueBatchPrologue(runs[static_cast<size_t>(i)], stream);
-        err = cudaGraphLaunch(exec, stream);
+        err = cudaGraphLaunch(pooled ? pb.exec : exec, stream);
         if (err != cudaSuccess) {
             status = CudaError(err, "combined batch launch");
             break;
@@ -1316,6 +1583,7 @@ extern "C" yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t c
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (exec) cudaGraphExecDestroy(exec);
+    pb.Release();
     cudaStreamDestroy(stream);
     if (status != YRC_OK) return status;
     if (device_seconds) *device_seconds = device_ms / 1e3;
@@ -1323,6 +1591,23 @@ extern "C" yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t c
         status = FinishRender(runs[static_cast<size_t>(i)], device_ms / 1e3);
     }
     return status;
+}
+
+}  // namespace
+}  // namespace yrc
+
+extern "C" yrc_status yrc_render_many(yrc_render_scene* const* scenes, int32_t count,
+                                      const yrc_render_request* requests, yrc_film_pixel* const* films_out,
+                                      uint64_t* bad_samples_out, yrc_render_stats* stats, double* device_seconds) {
+    return yrc::RenderMany(scenes, count, requests, films_out, bad_samples_out, stats, device_seconds, false,
+                           "yrc_render_many");
+}
+
+extern "C" yrc_status yrc_render_pooled(yrc_render_scene* const* scenes, int32_t count,
+                                        const yrc_render_request* requests, yrc_film_pixel* const* films_out,
+                                        uint64_t* bad_samples_out, yrc_render_stats* stats, double* device_seconds) {
+    return yrc::RenderMany(scenes, count, requests, films_out, bad_samples_out, stats, device_seconds, true,
+                           "yrc_render_pooled");
 }
 
 extern "C" yrc_status yrc_render_scene_set_capacity(yrc_render_scene* s, int64_t capacity) {

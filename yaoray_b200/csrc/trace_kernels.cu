@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args
                 if (idx >= count) {
                     exhausted = true;
                 } else {
-                    ray = static_cast<int64_t>(idx);
+                    ray = args.order ? static_cast<int64_t>(__ldg(args.order + idx)) : static_cast<int64_t>(idx);
                     const float4 b = Ld(args.rays + 2 * ray + 1);
                     const float tmin = Ld(args.rays + 2 * ray).w;
                     alive = Begin(args.accel, args.rays, ray, tmin, b.w, s);
@@ -94,6 +94,93 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args
             alive = Step<kAny, kStats, kTwo, StackStore<kTotal, kBlock>, false, kWide>(args.accel, args.rays, ray, s, st,
                                                                                        col, args.error);
             if (!alive) WriteResult<kAny, kStats>(args, ray, s);
+        }
+    }
+}
+
+// Loads the pooled jobs' ray counts (written on the device by the stage
+// that filled the queues) into `ends` as an inclusive prefix sum; returns
+// the total. Called by the whole block.
+template <typename Job>
+__device__ __forceinline__ unsigned long long LoadPoolEnds(const Job* jobs, int njobs, unsigned long long* ends) {
+    for (int j = threadIdx.x; j < njobs; j += blockDim.x) ends[j] = *jobs[j].count_ptr;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int j = 1; j < njobs; ++j) ends[j] += ends[j - 1];
+    }
+    __syncthreads();
+    return njobs > 0 ? ends[njobs - 1] : 0ull;
+}
+
+// The job that pooled work item idx (< the total) belongs to: the first
+// whose queue ends past it.
+__device__ __forceinline__ int PoolJobOf(const unsigned long long* ends, int njobs, unsigned long long idx) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (ends[mid] > idx) {
+            hi = mid;
+        } else {
+            lo = mid + 1;
+        }
+    }
+    return lo;
+}
+
+// TraceKernel over the ray queues of several jobs at once (TracePool): the
+// same traversal and refill, with the accelerator, rays and outputs of the
+// job each lane's ray came from.
+template <bool kAny, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) PooledTraceKernel(TracePool pool) {
+    __shared__ int2 s_stack[kShortStack * kBlock];
+    __shared__ unsigned long long s_ends[kMaxPoolJobs];
+    const unsigned long long count = LoadPoolEnds(pool.jobs, pool.njobs, s_ends);
+    int2* col = s_stack + threadIdx.x;
+    StackStore<kTotal, kBlock> st;
+    Traversal s;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const TraceArgs* job = pool.jobs;
+    AccelParams acc = job->accel;
+    const float4* rays = job->rays;
+    int64_t ray = -1;
+    bool alive = false;
+    bool exhausted = false;
+
+    for (;;) {
+        const unsigned need = __ballot_sync(kFull, !alive && !exhausted);
+        if (need) {
+            unsigned long long base = 0;
+            const int leader = __ffs(need) - 1;
+            if (static_cast<int>(lane) == leader) {
+                base = atomicAdd(pool.counter, static_cast<unsigned long long>(__popc(need)));
+            }
+            base = __shfl_sync(kFull, base, leader);
+            if (!alive && !exhausted) {
+                const unsigned long long idx = base + __popc(need & lt_mask);
+                if (idx >= count) {
+                    exhausted = true;
+                } else {
+                    const int j = PoolJobOf(s_ends, pool.njobs, idx);
+                    job = pool.jobs + j;
+                    acc = job->accel;
+                    rays = job->rays;
+                    ray = static_cast<int64_t>(idx - (j ? s_ends[j - 1] : 0ull));
+                    const float4 b = Ld(rays + 2 * ray + 1);
+                    const float tmin = Ld(rays + 2 * ray).w;
+                    alive = Begin(acc, rays, ray, tmin, b.w, s);
+                    if (!alive) WriteResult<kAny, false>(*job, ray, s);
+                }
+            }
+        }
+        if (!__any_sync(kFull, alive)) {
+            if (__all_sync(kFull, exhausted)) break;
+            continue;
+        }
+#pragma unroll 1
+        for (int k = 0; k < kStepsPerRefill && alive; ++k) {
+            alive = Step<kAny, false, kTwo, StackStore<kTotal, kBlock>>(acc, rays, ray, s, st, col, job->error);
+            if (!alive) WriteResult<kAny, false>(*job, ray, s);
         }
     }
 }
@@ -220,11 +307,20 @@ __global__ void __launch_bounds__(kTraceBlock) RenderProbeKernel(RenderProbeArgs
 // is the traversal's t from the ray origin less the distance already
 // advanced, not a new intersection from the re-spawned origin. Persistent
 // warps with per-lane refill, like TraceKernel.
-template <bool kTwo, int kTotal>
-__global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmittanceKernel(ShadowArgs args) {
+//
+// kPooled: the launch serves the shadow queues of several jobs (ShadowPool);
+// each lane works with the job of the ray it holds.
+template <bool kTwo, int kTotal, bool kPooled = false>
+__global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm)
+    ShadowTransmittanceKernel(const __grid_constant__ ShadowArgs args, const __grid_constant__ ShadowPool pool) {
     __shared__ int2 s_stack[kShadowShortStack * kTraceBlock];
     __shared__ float s_clear_t[kClearHits * kTraceBlock];
     __shared__ int32_t s_clear_id[kClearHits * kTraceBlock];
+    __shared__ unsigned long long s_ends[kPooled ? kMaxPoolJobs : 1];
+    const ShadowArgs* A = kPooled ? pool.jobs : &args;
+    AccelParams acc = A->accel;
+    const unsigned long long count = kPooled ? LoadPoolEnds(pool.jobs, pool.njobs, s_ends) : *args.count_ptr;
+    unsigned long long* const counter = kPooled ? pool.counter : args.counter;
     int2* col = s_stack + threadIdx.x;
     StackStore<kTotal, kTraceBlock, kShadowShortStack> st;
     Traversal s;
@@ -236,13 +332,12 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmi
     int64_t ray = -1;
     bool alive = false;
     bool exhausted = false;
-    const unsigned long long count = *args.count_ptr;
 
     // The reference loop over the kept clear surfaces; returns the RGB
     // transmittance, w = 1 when visible, all 0 when occluded.
     auto replay = [&]() -> float4 {
-        const float4 ra = Ld(args.rays + 2 * ray);
-        const float4 rb = Ld(args.rays + 2 * ray + 1);
+        const float4 ra = Ld(A->rays + 2 * ray);
+        const float4 rb = Ld(A->rays + 2 * ray + 1);
         float o[3] = {ra.x, ra.y, ra.z};
         const float d[3] = {rb.x, rb.y, rb.z};
         float remaining = rb.w;
@@ -290,11 +385,11 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmi
                 beer(t);
                 if (black()) return occluded;
             }
-            const int32_t material = id >= 0 ? args.prim_material[args.tri_prim[id]] : args.sphere_material[-2 - id];
-            if (material < 0 || (args.materials[material].kind != 2 && args.materials[material].kind != 3)) {
+            const int32_t material = id >= 0 ? A->prim_material[A->tri_prim[id]] : A->sphere_material[-2 - id];
+            if (material < 0 || (A->materials[material].kind != 2 && A->materials[material].kind != 3)) {
                 return occluded;
             }
-            const DevMaterial& m = args.materials[material];
+            const DevMaterial& m = A->materials[material];
             float hp[3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) hp[c] = __fadd_rn(o[c], __fmul_rn(d[c], t));
@@ -326,7 +421,7 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmi
         return occluded;  // the reference gives up after 16 queries
     };
     auto finish = [&]() {
-        const int32_t slot = args.out_index[ray];
+        const int32_t slot = A->out_index[ray];
         float4 tr;
         if (s.best.hit) {
             tr = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -335,13 +430,13 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmi
         } else {
             tr = replay();
             if (tr.w < 0.0f) {
-                const unsigned long long o = atomicAdd(args.overflow_count, 1ull);
-                args.overflow[o] = static_cast<int32_t>(ray);
+                const unsigned long long o = atomicAdd(A->overflow_count, 1ull);
+                A->overflow[o] = static_cast<int32_t>(ray);
                 return;
             }
         }
-        args.transmittance[slot] = tr;
-        if (tr.w == 0.0f) CountLanes(args.occluded_count);
+        A->transmittance[slot] = tr;
+        if (tr.w == 0.0f) CountLanes(A->occluded_count);
     };
     for (;;) {
         const unsigned need = __ballot_sync(kFull, !alive && !exhausted);
@@ -349,7 +444,7 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmi
             unsigned long long base = 0;
             const int leader = __ffs(need) - 1;
             if (static_cast<int>(lane) == leader) {
-                base = atomicAdd(args.counter, static_cast<unsigned long long>(__popc(need)));
+                base = atomicAdd(counter, static_cast<unsigned long long>(__popc(need)));
             }
             base = __shfl_sync(kFull, base, leader);
             if (!alive && !exhausted) {
@@ -358,11 +453,17 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmi
                     exhausted = true;
                 } else {
                     ray = static_cast<int64_t>(idx);
-                    const float4 b = Ld(args.rays + 2 * ray + 1);
-                    const float tmin = Ld(args.rays + 2 * ray).w;
+                    if (kPooled) {
+                        const int j = PoolJobOf(s_ends, pool.njobs, idx);
+                        A = pool.jobs + j;
+                        acc = A->accel;
+                        ray -= static_cast<int64_t>(j ? s_ends[j - 1] : 0ull);
+                    }
+                    const float4 b = Ld(A->rays + 2 * ray + 1);
+                    const float tmin = Ld(A->rays + 2 * ray).w;
                     clear.n = 0;
                     clear.dropped = false;
-                    alive = Begin(args.accel, args.rays, ray, tmin, b.w, s);
+                    alive = Begin(acc, A->rays, ray, tmin, b.w, s);
                     if (!alive) finish();
                 }
             }
@@ -374,7 +475,7 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm) ShadowTransmi
 #pragma unroll 1
         for (int k = 0; k < 8 && alive; ++k) {
             alive = Step<true, false, kTwo, StackStore<kTotal, kTraceBlock, kShadowShortStack>, true>(
-                args.accel, args.rays, ray, s, st, col, args.error, args.tri_clear, args.sphere_clear, &clear);
+                acc, A->rays, ray, s, st, col, A->error, A->tri_clear, A->sphere_clear, &clear);
             if (!alive) finish();
         }
     }
@@ -444,13 +545,25 @@ cudaError_t LaunchProbeOne(const ProbeArgs& args, cudaStream_t stream, int sm_co
     return cudaGetLastError();
 }
 
-template <bool kTwo, int kTotal>
-cudaError_t LaunchShadowOne(const ShadowArgs& args, cudaStream_t stream, int sm_count) {
-    auto kernel = ShadowTransmittanceKernel<kTwo, kTotal>;
+template <bool kTwo, int kTotal, bool kPooled = false>
+cudaError_t LaunchShadowOne(const ShadowArgs& args, const ShadowPool& pool, cudaStream_t stream, int sm_count) {
+    auto kernel = ShadowTransmittanceKernel<kTwo, kTotal, kPooled>;
     int64_t blocks = 0;
-    const cudaError_t err = PersistentGrid(kernel, kTraceBlock, args.capacity, sm_count, blocks);
+    const cudaError_t err =
+        PersistentGrid(kernel, kTraceBlock, kPooled ? pool.capacity : args.capacity, sm_count, blocks);
     if (err != cudaSuccess) return err;
-    kernel<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args);
+    kernel<<<static_cast<unsigned>(blocks), kTraceBlock, 0, stream>>>(args, pool);
+    return cudaGetLastError();
+}
+
+template <bool kAny, bool kTwo, int kTotal>
+cudaError_t LaunchPooledOne(const TracePool& pool, cudaStream_t stream, int sm_count) {
+    constexpr int kBlock = 128;
+    auto kernel = PooledTraceKernel<kAny, kTwo, kTotal, kBlock, 8, 1>;
+    int64_t blocks = 0;
+    const cudaError_t err = PersistentGrid(kernel, kBlock, pool.capacity, sm_count, blocks);
+    if (err != cudaSuccess) return err;
+    kernel<<<static_cast<unsigned>(blocks), kBlock, 0, stream>>>(pool);
     return cudaGetLastError();
 }
 
@@ -478,10 +591,38 @@ cudaError_t LaunchRenderProbe(const RenderProbeArgs& args, cudaStream_t stream, 
 cudaError_t LaunchShadowTransmittance(const ShadowArgs& args, cudaStream_t stream, int sm_count) {
     const bool two = args.accel.two_level != 0;
     const bool deep = args.accel.stack_limit > 64;
-    if (two) return deep ? LaunchShadowOne<true, kMaxTraceStack>(args, stream, sm_count)
-                         : LaunchShadowOne<true, 64>(args, stream, sm_count);
-    return deep ? LaunchShadowOne<false, kMaxTraceStack>(args, stream, sm_count)
-                : LaunchShadowOne<false, 64>(args, stream, sm_count);
+    const ShadowPool none{};
+    if (two) return deep ? LaunchShadowOne<true, kMaxTraceStack>(args, none, stream, sm_count)
+                         : LaunchShadowOne<true, 64>(args, none, stream, sm_count);
+    return deep ? LaunchShadowOne<false, kMaxTraceStack>(args, none, stream, sm_count)
+                : LaunchShadowOne<false, 64>(args, none, stream, sm_count);
+}
+
+cudaError_t LaunchPooledShadowTransmittance(const ShadowPool& pool, bool two, bool deep, cudaStream_t stream,
+                                            int sm_count) {
+    if (pool.njobs <= 0) return cudaSuccess;
+    if (pool.njobs > kMaxPoolJobs) return cudaErrorInvalidValue;
+    const ShadowArgs none{};
+    if (two) return deep ? LaunchShadowOne<true, kMaxTraceStack, true>(none, pool, stream, sm_count)
+                         : LaunchShadowOne<true, 64, true>(none, pool, stream, sm_count);
+    return deep ? LaunchShadowOne<false, kMaxTraceStack, true>(none, pool, stream, sm_count)
+                : LaunchShadowOne<false, 64, true>(none, pool, stream, sm_count);
+}
+
+cudaError_t LaunchPooledTrace(const TracePool& pool, bool any, bool two, bool deep, cudaStream_t stream,
+                              int sm_count) {
+    if (pool.njobs <= 0) return cudaSuccess;
+    if (pool.njobs > kMaxPoolJobs) return cudaErrorInvalidValue;
+    if (any) {
+        if (two) return deep ? LaunchPooledOne<true, true, kMaxTraceStack>(pool, stream, sm_count)
+                             : LaunchPooledOne<true, true, 64>(pool, stream, sm_count);
+        return deep ? LaunchPooledOne<true, false, kMaxTraceStack>(pool, stream, sm_count)
+                    : LaunchPooledOne<true, false, 64>(pool, stream, sm_count);
+    }
+    if (two) return deep ? LaunchPooledOne<false, true, kMaxTraceStack>(pool, stream, sm_count)
+                         : LaunchPooledOne<false, true, 64>(pool, stream, sm_count);
+    return deep ? LaunchPooledOne<false, false, kMaxTraceStack>(pool, stream, sm_count)
+                : LaunchPooledOne<false, false, 64>(pool, stream, sm_count);
 }
 
 cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, int shape, cudaStream_t stream,

@@ -33,6 +33,7 @@ struct TraceArgs {
     const unsigned long long* count_ptr;  // optional: ray count read on the device (count = capacity)
     const int32_t* out_index;             // optional: any-hit output slot per ray
     unsigned long long* occluded_count;   // optional: any-hit rays that hit something (RenderStats)
+    const uint32_t* order;                // optional: ray index per traversal slot (OrderRays)
 };
 
 constexpr int kProbeMaxHits = YRC_PROBE_MAX_HITS;  // BvhProbeHits::MaxHits
@@ -92,6 +93,35 @@ struct RenderProbeArgs {
 
 cudaError_t LaunchRenderProbe(const RenderProbeArgs& args, cudaStream_t stream, int sm_count);
 
+// Pooled traversal: one persistent launch over the ray queues of several
+// render jobs. Each job's rays keep their own queue, accelerator and
+// outputs (its TraceArgs / ShadowArgs entry in a device-resident table,
+// with the ray count read from count_ptr on the device); the launch's lanes
+// take rays from one work counter over the jobs' queues laid end to end, so
+// that no job's tail leaves the GPU idle while another's rays wait.
+constexpr int kMaxPoolJobs = 128;
+
+struct TracePool {
+    const TraceArgs* jobs;          // njobs entries (count_ptr required; counter unused)
+    int32_t njobs;
+    int64_t capacity;               // bound on the total rays, for grid sizing
+    unsigned long long* counter;    // work counter, zeroed before the launch
+};
+
+struct ShadowPool {
+    const ShadowArgs* jobs;         // njobs entries (counter unused)
+    int32_t njobs;
+    int64_t capacity;
+    unsigned long long* counter;
+};
+
+// Every job of a pool must share the BVH kind (flat or two-level) and
+// depth class (stack limit <= 64 or not) given here.
+cudaError_t LaunchPooledTrace(const TracePool& pool, bool any_hit, bool two_level, bool deep, cudaStream_t stream,
+                              int sm_count);
+cudaError_t LaunchPooledShadowTransmittance(const ShadowPool& pool, bool two_level, bool deep, cudaStream_t stream,
+                                            int sm_count);
+
 // Accessors of accelerator internals used by the render stages (accel.cu).
 AccelParams AccelParamsOf(const yrc_accel* a);
 int TraceShapeOf(const yrc_accel* a, int any_hit);
@@ -103,6 +133,29 @@ cudaError_t LaunchShadowTransmittance(const ShadowArgs& args, cudaStream_t strea
 cudaError_t LaunchTrace(const TraceArgs& args, bool any_hit, bool stats, int shape, cudaStream_t stream,
                         int sm_count);
 cudaError_t LaunchProbe(const ProbeArgs& args, cudaStream_t stream, int sm_count);
+
+// Ray reordering ahead of a traversal launch (ray_order.cu).
+constexpr int kRayOrderOff = 0;
+constexpr int kRayOrderDirection = 1;  // key: origin and direction
+constexpr int kRayOrderTwoPoint = 2;   // key: origin and a point along the ray
+constexpr int kRayOrderMinBits = 8;
+constexpr int kRayOrderMaxBits = 24;
+
+struct RayOrderScratch {
+    uint32_t* keys;       // one per ray
+    uint32_t* order;      // one per ray: the permutation
+    uint32_t* hist;       // 2^bits bin counters
+    uint32_t* tile_sums;  // RayOrderTiles(bits)
+};
+
+// Key bits for `count` rays (`requested` > 0 is clamped to the supported range).
+int RayOrderBits(int64_t count, int requested);
+int64_t RayOrderTiles(int bits);
+// Writes scratch.order[0..count) = ray indices sorted by their key bin.
+// `length` is the two-point key's distance as a fraction of the root box
+// diagonal. count must be below 2^32.
+cudaError_t OrderRays(const float4* rays, int64_t count, const AccelParams& accel, int mode, int bits, float length,
+                      const RayOrderScratch& scratch, cudaStream_t stream, int sm_count);
 // Loads the code of the two statistics traversal kernels (closest and any
 // hit) that a BVH of this kind and stack limit uses, so that their first
 // launch under lazy module loading does not take device memory.

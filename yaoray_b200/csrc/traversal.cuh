@@ -55,11 +55,14 @@ __device__ __forceinline__ float4 LdNode(const float4* p, unsigned long long pol
     return v;
 }
 
-// Warp-aggregated increment of a statistics counter by the calling lanes.
+// Warp-aggregated increment of a statistics counter by the calling lanes;
+// lanes that hold different counters (a pooled launch's lanes may serve
+// different jobs) count into their own.
 __device__ __forceinline__ void CountLanes(unsigned long long* counter) {
     const unsigned mask = __activemask();
-    if ((threadIdx.x & 31u) == static_cast<unsigned>(__ffs(mask) - 1)) {
-        atomicAdd(counter, static_cast<unsigned long long>(__popc(mask)));
+    const unsigned peers = __match_any_sync(mask, reinterpret_cast<unsigned long long>(counter));
+    if ((threadIdx.x & 31u) == static_cast<unsigned>(__ffs(peers) - 1)) {
+        atomicAdd(counter, static_cast<unsigned long long>(__popc(peers)));
     }
 }
 

@@ -203,6 +203,7 @@ def _bind():
         ("yrc_render_scene_shadow_eval", C.c_int, [P, P, C.c_int64, P]),
         ("yrc_render_scene_set_view", C.c_int, [P, P, C.c_uint64]),
         ("yrc_render_many", C.c_int, [P, C.c_int32, P, P, P, P, P]),
+        ("yrc_render_pooled", C.c_int, [P, C.c_int32, P, P, P, P, P]),
         ("yrc_bssrdf_table_build", C.c_int, [C.c_float, C.c_float, C.c_int32, C.c_int32, P, P, P, P, P]),
         ("yrc_alias_table_build", C.c_int, [P, C.c_int32, P, P, P]),
         ("yrc_environment_distribution_build", C.c_int, [P, C.c_int32, C.c_int32, P, P, P, P, P]),
@@ -587,10 +588,12 @@ class CudaBackend:
         stats = {f[0]: getattr(st, f[0]) for f in Stats._fields_}
         return RenderResult(True, "", film, int(bad.value), stats)
 
-    def render_many(self, prepared: list) -> list:
+    def render_many(self, prepared: list, pooled: bool = False) -> list:
         """Renders several prepared scenes together (yrc_render_many): each
         step is one launch of a graph holding every unfinished scene's batch.
-        Films equal render()'s; stats["device_seconds"] is the whole call's."""
+        With `pooled` (yrc_render_pooled), each bounce traces the extend and
+        shadow rays of all scenes in one persistent launch each. Films equal
+        render()'s; stats["device_seconds"] is the whole call's."""
         L = _bind()
         n = len(prepared)
         if n == 0:
@@ -601,7 +604,8 @@ class CudaBackend:
         bads = (C.c_uint64 * n)()
         stats = (Stats * n)()
         secs = C.c_double()
-        status = L.yrc_render_many(handles, n, None, film_ptrs, bads, stats, C.byref(secs))
+        call = L.yrc_render_pooled if pooled else L.yrc_render_many
+        status = call(handles, n, None, film_ptrs, bads, stats, C.byref(secs))
         if status != _lib.YRC_OK:
             msg = L.yrc_last_error().decode(errors="replace")
             if status in (_lib.YRC_ERR_CANCELLED, _lib.YRC_ERR_INVALID_ARGUMENT):
