@@ -346,11 +346,18 @@ yrc_status yrc_trace_stats_device_noalloc(yrc_accel* accel, const yrc_ray* rays,
  * (optional, YRC_TRACE_SHAPES floats) receives the measured time per shape.
  * Synchronises `stream`.
  */
-#define YRC_TRACE_SHAPES 7
+#define YRC_TRACE_SHAPES 12
 yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags, void* stream,
                               float* times_ms);
 /* Set / get the launch shape (0..YRC_TRACE_SHAPES-1) used for closest-hit
- * (any_hit = 0) or any-hit (any_hit = 1) traces; 0 is the default shape. */
+ * (any_hit = 0) or any-hit (any_hit = 1) traces; 0 is the default shape.
+ * Shapes 0-6 differ in block size, node visits between ray refills and
+ * register budget; shapes 7, 8 and 9 let a lane that reaches a leaf wait
+ * until 4, 8 or 16 lanes of its warp are at leaves (or none is at an
+ * interior node), so that the leaf tests run for many lanes at once;
+ * shapes 10 and 11 are shape 8 with a 40-register budget (12 blocks of 128
+ * per SM) and with blocks of 256. No
+ * shape changes a hit: every ray keeps the reference's visiting order. */
 yrc_status yrc_accel_set_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t shape);
 int32_t yrc_accel_get_trace_shape(const yrc_accel* accel, int32_t any_hit);
 
@@ -827,8 +834,9 @@ int64_t yrc_render_scene_capacity(const yrc_render_scene* scene);
 /* Render autotuner: times short probe renders of this scene (sample indices
  * 0..P-1 of every pixel, P = two batches of the largest candidate) for each
  * candidate queue capacity (whole passes of the image between 2^17 and 2^23
- * paths) and each closest-hit traversal
- * launch shape of the extend stage at the best capacity; keeps the fastest
+ * paths) and each traversal launch shape at the best capacity (one shape
+ * for the extend and the shadow traversals; shapes 7-11 batch the leaf tests
+ * of a warp, in the shadow-transmittance kernel too); keeps the fastest
  * for later yrc_render calls. The traversal stack depth is not a candidate:
  * it follows the BVH's measured depth (64 or 256 entries). Probes run
  * without an attached radiance cache (they do not train it). Synchronous.
@@ -837,12 +845,12 @@ int64_t yrc_render_scene_capacity(const yrc_render_scene* scene);
 #define YRC_TUNE_TRACE_SHAPE 2
 typedef struct yrc_render_tuning {
     int64_t capacity;          /* chosen queue capacity */
-    int32_t trace_shape;       /* chosen closest-hit launch shape */
+    int32_t trace_shape;       /* chosen traversal launch shape (extend and shadow rays) */
     int32_t candidates;        /* configurations timed */
     double seconds_per_sample; /* device time per sample of the chosen configuration */
 } yrc_render_tuning;
 yrc_status yrc_render_autotune(yrc_render_scene* scene, int32_t flags, yrc_render_tuning* result);
-/* Applies a tuning (capacity and closest-hit launch shape; the other fields
+/* Applies a tuning (capacity and traversal launch shape; the other fields
  * are ignored), e.g. one found by yrc_render_autotune on a scene of the same
  * image size and spp. */
 yrc_status yrc_render_scene_set_tuning(yrc_render_scene* scene, const yrc_render_tuning* tuning);

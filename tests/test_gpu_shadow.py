@@ -78,12 +78,16 @@ def shadow_rays(n, seed):
     return rays, np.clip(pairs, 0, PAIRS)
 
 
-def test_shadow_visibility_matches_reference_per_ray(cuda, ref):
+@pytest.mark.parametrize("shape", [0, 8])
+def test_shadow_visibility_matches_reference_per_ray(cuda, ref, shape):
+    """Per-ray parity of the shadow stage; launch shape 8 batches the leaf
+    tests of each warp in the transmittance kernel."""
     scene = slab_stack_scene()
     rays, pairs = shadow_rays(60000, seed=5)
     want = ref.RefJob.from_scene(scene).shadow_visibility(rays)
     backend = CudaBackend()
     prepared = backend.prepare(scene)
+    prepared.set_tuning({"capacity": 0, "trace_shape": shape})
     got = prepared.shadow_visibility(rays)
     vis_w = want[:, 3] == 1.0
     vis_g = got[:, 3] == 1.0

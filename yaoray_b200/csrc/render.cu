@@ -168,6 +168,7 @@ ShadowArgs TransmittanceArgs(yrc_render_scene* s, const Queues& q, int64_t C, in
     sa.overflow = q.shadow_overflow;
     sa.overflow_count = q.counters + kCtrShadowOverflow;
     sa.error = error;
+    sa.leaf_batch = LeafBatchOfShape(TraceShapeOf(s->accel, 1));
     return sa;
 }
 
@@ -869,13 +870,19 @@ TraceArgs ExtendTraceArgs(yrc_render_scene* s, const Queues& q) {
     return ta;
 }
 
-// Shading after the extend trace: alpha skips, the class shade kernels,
-// subsurface probes and exits.
-yrc_status BounceShade(yrc_render_scene* s, const Queues& q, int depth, cudaStream_t st) {
+// Shading after the extend trace, in three parts: alpha skips and the sort
+// of the extend queue by shading class; the class shade kernels (pooled
+// over several scenes in a pooled batch); subsurface probes and exits.
+void BounceShadeSort(yrc_render_scene* s, const Queues& q, int depth, cudaStream_t st) {
     const DevScene& sc = s->dev;
     const int64_t C = s->capacity;
     if (sc.any_alpha) LaunchAlphaExtend(sc, s->ps, q, depth, C, s->sm_count, AccelErrorWord(s->accel), st);
-    LaunchShade(sc, s->ps, q, s->cargs, depth, C, s->sm_count, st);
+    LaunchShadeSort(sc, s->ps, q, depth, C, s->sm_count, st);
+}
+
+yrc_status BounceSubsurface(yrc_render_scene* s, const Queues& q, int depth, cudaStream_t st) {
+    const DevScene& sc = s->dev;
+    const int64_t C = s->capacity;
     if (sc.any_subsurface) {
         RenderProbeArgs pa{};
         pa.accel = sc.accel;
@@ -892,6 +899,12 @@ yrc_status BounceShade(yrc_render_scene* s, const Queues& q, int depth, cudaStre
         LaunchSubsurfaceExit(sc, s->ps, q, depth, C, s->sm_count, st);
     }
     return Ok();
+}
+
+yrc_status BounceShade(yrc_render_scene* s, const Queues& q, int depth, cudaStream_t st) {
+    BounceShadeSort(s, q, depth, st);
+    LaunchShadeClasses(s->dev, s->ps, q, s->cargs, depth, s->capacity, s->sm_count, st);
+    return BounceSubsurface(s, q, depth, st);
 }
 
 // After the shadow trace: next-event resolve, coated vertices (with their
@@ -1381,8 +1394,28 @@ yrc_status CapturePooledBatch(const std::vector<yrc_render_scene*>& ss, cudaStre
             }
         }
     }
+    // Per bounce, the shade jobs of the scenes that reach it.
+    std::vector<ShadeJob> shade_jobs;
+    std::vector<size_t> shade_first(static_cast<size_t>(max_depth) + 1, 0);
+    std::vector<int64_t> shade_capacity(static_cast<size_t>(max_depth), 0);
+    for (int d = 0; d < max_depth; ++d) {
+        shade_first[static_cast<size_t>(d)] = shade_jobs.size();
+        for (yrc_render_scene* s : ss) {
+            if (d >= s->dev.max_depth) continue;
+            ShadeJob j{};
+            j.sc = s->dev;
+            j.ps = s->ps;
+            j.q = QueuesAt(s, d);
+            j.cache = s->cargs;
+            j.depth = d;
+            shade_jobs.push_back(j);
+            shade_capacity[static_cast<size_t>(d)] += s->capacity;
+        }
+    }
+    shade_first[static_cast<size_t>(max_depth)] = shade_jobs.size();
     size_t n_launches = 0;
     for (const auto& v : launches) n_launches += v.size();
+    const ShadeJob* d_shade = pb.mem.Upload(shade_jobs);
     const TraceArgs* d_trace = pb.mem.Upload(trace_jobs);
     const ShadowArgs* d_shadow = pb.mem.Upload(shadow_jobs);
     unsigned long long* counters = pb.mem.Alloc<unsigned long long>(n_launches);
@@ -1429,7 +1462,15 @@ yrc_status CapturePooledBatch(const std::vector<yrc_render_scene*>& ss, cudaStre
         });
         pooled(d, false);
         per_scene([&](yrc_render_scene* s) {
-            return d < s->dev.max_depth ? BounceShade(s, QueuesAt(s, d), d, s->stream) : Ok();
+            if (d < s->dev.max_depth) BounceShadeSort(s, QueuesAt(s, d), d, s->stream);
+            return Ok();
+        });
+        const size_t first = shade_first[static_cast<size_t>(d)];
+        LaunchPooledShade(d_shade + first, static_cast<int>(shade_first[static_cast<size_t>(d) + 1] - first),
+                          shade_capacity[static_cast<size_t>(d)], sm_count, main);
+        run(cudaGetLastError(), "pooled shade");
+        per_scene([&](yrc_render_scene* s) {
+            return d < s->dev.max_depth ? BounceSubsurface(s, QueuesAt(s, d), d, s->stream) : Ok();
         });
         pooled(d, true);
         per_scene([&](yrc_render_scene* s) {
@@ -1650,14 +1691,18 @@ extern "C" yrc_status yrc_render_autotune(yrc_render_scene* s, int32_t flags, yr
     EnsureCache(s);
     const int64_t saved_choice = s->capacity_choice;
     const int saved_shape = yrc_accel_get_trace_shape(s->accel, 0);
+    const int saved_any_shape = yrc_accel_get_trace_shape(s->accel, 1);
     int tried = 0;
     double best = 0.0;
     int64_t best_cap = RenderCapacity(s);
     int best_shape = saved_shape;
     yrc_status status = YRC_OK;
+    // One launch shape for the extend (closest-hit) and shadow (any-hit and
+    // transmittance) traversals.
     auto time_config = [&](int64_t cap, int shape, double* sec) -> yrc_status {
         s->capacity_choice = cap;
         yrc_accel_set_trace_shape(s->accel, 0, shape);
+        yrc_accel_set_trace_shape(s->accel, 1, shape);
         DropGraph(s);
         double first = 0.0;
         yrc_status st = ProbeRender(s, passes, &first);  // allocation, graph capture, warm-up
@@ -1693,6 +1738,7 @@ extern "C" yrc_status yrc_render_autotune(yrc_render_scene* s, int32_t flags, yr
     }
     s->capacity_choice = status == YRC_OK ? best_cap : saved_choice;
     yrc_accel_set_trace_shape(s->accel, 0, status == YRC_OK ? best_shape : saved_shape);
+    yrc_accel_set_trace_shape(s->accel, 1, status == YRC_OK ? best_shape : saved_any_shape);
     DropGraph(s);
     s->cache = cache;
     s->cache_capacity = 0;  // re-allocated for the chosen capacity on the next render
@@ -1714,7 +1760,8 @@ extern "C" yrc_status yrc_render_scene_set_tuning(yrc_render_scene* s, const yrc
     std::lock_guard<std::mutex> lock(s->mutex);
     cudaSetDevice(s->device);
     s->capacity_choice = tuning->capacity;
-    const yrc_status st = yrc_accel_set_trace_shape(s->accel, 0, tuning->trace_shape);
+    yrc_status st = yrc_accel_set_trace_shape(s->accel, 0, tuning->trace_shape);
+    if (st == YRC_OK) st = yrc_accel_set_trace_shape(s->accel, 1, tuning->trace_shape);
     if (st != YRC_OK) return st;
     DropGraph(s);
     return Ok();
@@ -1778,6 +1825,7 @@ extern "C" yrc_status yrc_render_scene_shadow_eval(yrc_render_scene* s, const yr
             sa.overflow = q.shadow_overflow;
             sa.overflow_count = q.counters + kCtrShadowOverflow;
             sa.error = error;
+            sa.leaf_batch = LeafBatchOfShape(TraceShapeOf(s->accel, 1));
             err = LaunchShadowTransmittance(sa, st, s->sm_count);
             if (err == cudaSuccess) {
                 LaunchShadowExact(sc, q, tr, q.counters + kCtrStatsBase + 2, n, s->sm_count, error, st,

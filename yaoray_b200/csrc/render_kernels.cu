@@ -41,9 +41,11 @@ __device__ __forceinline__ float ShadowBias(V3 o, V3 t, float dist) {
 __device__ __forceinline__ V3 F4(const float4& v) { return V3{v.x, v.y, v.z}; }
 __device__ __forceinline__ float4 ToF4(V3 v, float w = 0.0f) { return make_float4(v.x, v.y, v.z, w); }
 
-// Warp-aggregated append to a device queue; returns this lane's slot.
+// Warp-aggregated append to a device queue; returns this lane's slot. The
+// lanes that append to the same queue are aggregated together (in a pooled
+// launch the lanes of a warp may serve different jobs' queues).
 __device__ __forceinline__ unsigned long long QueueAppend(unsigned long long* counter) {
-    const unsigned mask = __activemask();
+    const unsigned mask = __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(counter));
     const int leader = __ffs(mask) - 1;
     const unsigned lane = threadIdx.x & 31u;
     unsigned long long base = 0;
@@ -53,7 +55,7 @@ __device__ __forceinline__ unsigned long long QueueAppend(unsigned long long* co
 }
 
 __device__ __forceinline__ void CountStat(unsigned long long* counters, int which) {
-    const unsigned mask = __activemask();
+    const unsigned mask = __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(counters));
     if ((threadIdx.x & 31u) == static_cast<unsigned>(__ffs(mask) - 1)) {
         atomicAdd(counters + kCtrStatsBase + which, static_cast<unsigned long long>(__popc(mask)));
     }
@@ -1234,6 +1236,230 @@ __global__ void __launch_bounds__(kTraceBlock) ShadowExactKernel(DevScene sc, Qu
 
 // IntegratePathSample's per-bounce body (src/integrators/path_integrator.cpp:23-197)
 // for the entries of one shading class.
+// One extend-queue entry `e` of shading class kClass.
+template <int kClass>
+__device__ __forceinline__ void ShadeEntry(const DevScene& sc, PathState& ps, Queues& q, int depth,
+                                           const CacheArgs& cache, int64_t e) {
+    const int32_t path = q.path_in[e];
+    const float4 ra = q.ray_in[2 * e], rb = q.ray_in[2 * e + 1];
+    const V3 o = F4(ra), d = F4(rb);
+    const float4 hit = q.hits[e];
+    const int32_t inst = q.inst[e];
+    const int32_t id = __float_as_int(hit.y);
+    V3 tp = F4(ps.throughput[path]);
+    V3 rad = F4(ps.radiance[path]);
+    uint32_t flags = ps.flags[path];
+    const float4 prev = ps.prev[path];
+    CountStat(q.counters, kStatRays);
+
+    // --- miss: environment with the BSDF-sampling MIS weight
+    if (kClass == kClassMiss || id == -1) {
+        CountStat(q.counters, kStatMisses);
+        float w = 1.0f;
+        if ((flags & kPathPrevValid) && !(flags & kPathPrevDelta)) {
+            w = PowerHeuristic(1, prev.w, 1, PdfEnvironment(sc.env, d));
+        }
+        rad = rad + Mul(tp, EvalEnvironment(sc.env, d)) * w;
+        ps.radiance[path] = ToF4(rad);
+        return;
+    }
+    CountStat(q.counters, kStatHits);
+
+    // --- medium attenuation (Beer-Lambert inside a thick dielectric)
+    if (flags & kPathMedium) {
+        const float4 md = ps.medium[path];
+        if (hit.x > 0.0f && md.w > 0.0f) {
+            const float inv = 1.0f / md.w;
+            const float c[3] = {Clampf(md.x, 1.0e-6f, 1.0f), Clampf(md.y, 1.0e-6f, 1.0f), Clampf(md.z, 1.0e-6f, 1.0f)};
+            tp = V3{tp.x * expf(logf(c[0]) * hit.x * inv), tp.y * expf(logf(c[1]) * hit.x * inv),
+                    tp.z * expf(logf(c[2]) * hit.x * inv)};
+        }
+    }
+    if (IsBlack(tp)) {
+        ps.throughput[path] = ToF4(tp);
+        return;
+    }
+
+    Surface s;
+    if (!ResolveSurface<false>(sc, o, d, hit, inst, s, depth, 0, 0)) {
+        rad = rad + Mul(tp, V3{1.0f, 0.0f, 1.0f});  // invalid material marker
+        ps.radiance[path] = ToF4(rad);
+        return;
+    }
+    if (sc.texture_count > 0 && s.triangle) {  // the texture stage's result for this entry
+        const float4 tn = q.tex_normal[e];
+        if (tn.w != 0.0f) {
+            s.n = F4(tn);
+            s.reflectance_scale = F4(q.tex_scale[e]);
+        }
+    }
+    Mat m;
+    V3 emission{0.0f, 0.0f, 0.0f};
+    if (s.material >= 0) {
+        const DevMaterial& dm = sc.materials[s.material];
+        m = LoadMat(dm);
+        m.reflectance = Mul(m.reflectance, s.reflectance_scale);
+        m.measured = dm.measured_index >= 0 ? sc.measured + dm.measured_index : nullptr;
+        emission = Ld3(dm.emission);
+    } else {  // default RenderMaterial: diffuse 0.5
+        m = Mat{kDiffuse, {0.5f, 0.5f, 0.5f}, 1.5f, 0.0f, 0.0f, 1.5f, 0.01f, {0, 0, 0}, 10, 1};
+    }
+    if constexpr (ClassKind<kClass>() >= 0) m.kind = ClassKind<kClass>();  // the class fixes the kind
+    const V3 wo = -d;
+    if (depth == 0) {
+        flags |= kPathPrimary;
+        ps.aov_albedo[path] = ToF4(m.reflectance, hit.x);
+        ps.aov_normal[path] = ToF4(s.n);
+    }
+
+    // --- emission with the BSDF-sampling MIS weight (triangle lights only)
+    if (!IsBlack(emission) && s.triangle) {
+        float w = 1.0f;
+        if ((flags & kPathPrevValid) && !(flags & kPathPrevDelta)) {
+            const int32_t ei = sc.prim_emissive[s.prim];
+            const float pl = PdfEmissiveSolidAngle(sc, F4(prev), s.p, s.ng_obj, ei);
+            w = PowerHeuristic(1, prev.w, 1, pl);
+        }
+        rad = rad + Mul(tp, emission) * w;
+    }
+
+    // --- radiance cache: path spread (footprint heuristic), training
+    // records, early termination into the cache
+    if (cache.enabled) {
+        const float cv = fmaxf(fabsf(Dot(d, s.n)), 1.0e-4f);
+        float2 sp = ps.spread[path];
+        if (depth == 0) {
+            sp.x = hit.x * hit.x / (4.0f * kPi * cv);
+            sp.y = 0.0f;
+        } else if (!(flags & kPathPrevDelta)) {
+            sp.y += sqrtf(hit.x * hit.x / (fmaxf(prev.w, 1.0e-12f) * cv));
+        }
+        ps.spread[path] = sp;
+        const int32_t slot = cache.train_slot[path];
+        if (slot >= 0) {
+            const int32_t k = cache.slot_len[slot];
+            if (k < cache.max_depth) {
+                const int64_t v = static_cast<int64_t>(slot) * cache.max_depth + k;
+                WriteCacheQuery(cache.slot_q + 16 * v, s.p, wo, s.n, m);
+                cache.slot_lt[2 * v] = ToF4(rad);
+                cache.slot_lt[2 * v + 1] = ToF4(tp);
+                cache.slot_len[slot] = k + 1;
+            }
+        }
+        const bool fires = depth >= 1 && !(flags & kPathCacheQueued) && (cache.delta_vertices || !IsDelta(m)) &&
+                           sp.y * sp.y > cache.spread_c * sp.x;
+        if (fires) {
+            // The image estimate of the path ends here: radiance so far
+            // plus throughput x cache. A training path goes on as an
+            // unbiased suffix whose radiance only trains the cache.
+            const unsigned long long k = QueueAppend(cache.counters + 0);
+            WriteCacheQuery(cache.queries + 16 * k, s.p, wo, s.n, m);
+            cache.query_path[k] = path;
+            cache.query_tp[k] = ToF4(tp);
+            cache.query_base[k] = ToF4(rad);
+            if (slot < 0) {
+                ps.throughput[path] = ToF4(tp);
+                ps.radiance[path] = ToF4(rad);
+                ps.flags[path] = flags;
+                return;
+            }
+            flags |= kPathCacheQueued;
+        }
+    }
+
+    PixelSampler smp;
+    const int32_t pixel = ps.pixel[path];
+    smp.Init(sc.sampler, sc.view->seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
+    Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
+
+    // --- coated vertex: next events and continuation in the reference's
+    // PCG32 order, after the shadow stages (DeferLayeredVertex)
+    if ((kClass == kClassCoatedDiffuse || kClass == kClassGeneric) && IsLayered(m.kind) && !IsDelta(m)) {
+        DeferLayeredVertex(sc, ps, q, path, smp, depth, m, s.material, s.p, s.n, wo, flags);
+        ps.throughput[path] = ToF4(tp);
+        ps.radiance[path] = ToF4(rad);
+        ps.flags[path] = flags;
+        return;
+    }
+
+    // --- next-event estimation: samples now, visibility in the shadow stage
+    if (!IsDelta(m)) NextEvent(sc, ps, q, path, smp, rng, depth, m, s.p, s.n, wo, tp, flags);
+
+    // --- subsurface entry (path_integrator.cpp:103-135): Fresnel split at
+    // the interface; the transmitted part becomes a probe ray that the
+    // subsurface stage traces and closes (SubsurfaceExitKernel).
+    if (kClass == kClassGeneric && m.kind == kSubsurface && s.material >= 0 &&
+        sc.materials[s.material].bssrdf_index >= 0 && sc.materials[s.material].bssrdf_index < sc.bssrdf_count) {
+        if (depth + 1 < sc.max_depth) {
+            const DevMaterial& dm = sc.materials[s.material];
+            const V3 ns = s.n;
+            V3 ss, ts;
+            BssrdfFrame(ns, ss, ts);
+            const float fr = FrDielectric(fabsf(Dot(wo, ns)), dm.bssrdf_eta);
+            if (smp.Sample1D(kDimBssrdfReflect, depth) < fr) {
+                // Specular reflection (the selection probability cancels Fresnel).
+                const V3 wr = ns * (2.0f * Dot(wo, ns)) - wo;
+                flags |= kPathPrevValid | kPathPrevDelta;
+                ps.prev[path] = ToF4(s.p, 1.0f);
+                const V3 bn = Dot(wr, ns) >= 0.0f ? ns : -ns;
+                const V3 no = s.p + bn * SurfaceBias(s.p);
+                const unsigned long long k = QueueAppend(q.counters + kCtrOut);
+                q.ray_out[2 * k] = make_float4(no.x, no.y, no.z, 1.0e-5f);
+                q.ray_out[2 * k + 1] = make_float4(wr.x, wr.y, wr.z, __int_as_float(0x7f800000));
+                q.path_out[k] = path;
+            } else {
+                // SampleBssrdfProbe (src/integrators/bssrdf_probe.cpp:17-60): projection
+                // axis, colour channel, radius, and the probe segment through the disk.
+                const TabBssrdf tab = MakeTabBssrdf(dm, sc.bssrdf[dm.bssrdf_index]);
+                float u1 = smp.Sample1D(kDimBssrdfAxis, depth);
+                float ux, uy;
+                smp.Sample2D(kDimBssrdfDisk, depth, ux, uy);
+                V3 vx, vy, vz;
+                if (u1 < 0.5f) {
+                    vx = ss, vy = ts, vz = ns;
+                    u1 *= 2.0f;
+                } else if (u1 < 0.75f) {
+                    vx = ts, vy = ns, vz = ss;
+                    u1 = (u1 - 0.5f) * 4.0f;
+                } else {
+                    vx = ns, vy = ss, vz = ts;
+                    u1 = (u1 - 0.75f) * 4.0f;
+                }
+                const int channel = min(max(static_cast<int>(u1 * 3.0f), 0), 2);
+                u1 = u1 * 3.0f - static_cast<float>(channel);
+                const float radius = BssrdfSampleSr(tab, channel, ux);
+                if (radius >= 0.0f) {
+                    const float phi = 2.0f * kPi * uy;
+                    const float max_radius = BssrdfSampleSr(tab, channel, 0.999f);
+                    if (radius < max_radius) {
+                        const float length = 2.0f * sqrtf(fmaxf(0.0f, max_radius * max_radius - radius * radius));
+                        // cos/sin rounded from double precision: the correctly rounded
+                        // float values, as the host libm's float cos/sin return them.
+                        const float cphi = static_cast<float>(cos(static_cast<double>(phi)));
+                        const float sphi = static_cast<float>(sin(static_cast<double>(phi)));
+                        const V3 disk = vx * (radius * cphi) + vy * (radius * sphi);
+                        const V3 base = s.p + disk - vz * (length * 0.5f);
+                        const unsigned long long k = QueueAppend(q.counters + kCtrProbe);
+                        q.probe_ray[2 * k] = make_float4(base.x, base.y, base.z, 1.0e-5f);
+                        q.probe_ray[2 * k + 1] = make_float4(vz.x, vz.y, vz.z, length);
+                        q.probe_target[k] = make_int4(s.triangle ? s.prim : -1, s.triangle ? inst : -1,
+                                                      s.triangle ? -1 : -2 - id, path);
+                        q.probe_entry[2 * k] = ToF4(s.p, u1);
+                        q.probe_entry[2 * k + 1] = ToF4(ns, __int_as_float(s.material));
+                    }
+                }
+            }
+        }
+        ps.throughput[path] = ToF4(tp);
+        ps.radiance[path] = ToF4(rad);
+        ps.flags[path] = flags;
+        ps.rng_state[path] = rng.state;
+        return;
+    }
+
+    ContinuePath(sc, ps, q, path, depth, m, s.material, s.p, s.n, wo, tp, rad, flags, smp, rng);
+}
+
 template <int kClass>
 __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps, Queues q, int depth,
                                                        CacheArgs cache) {
@@ -1243,225 +1469,40 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
     const int64_t count = static_cast<int64_t>(q.counters[kCtrClass0 + kClass]);
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t e = q.order[begin + i];
-        const int32_t path = q.path_in[e];
-        const float4 ra = q.ray_in[2 * e], rb = q.ray_in[2 * e + 1];
-        const V3 o = F4(ra), d = F4(rb);
-        const float4 hit = q.hits[e];
-        const int32_t inst = q.inst[e];
-        const int32_t id = __float_as_int(hit.y);
-        V3 tp = F4(ps.throughput[path]);
-        V3 rad = F4(ps.radiance[path]);
-        uint32_t flags = ps.flags[path];
-        const float4 prev = ps.prev[path];
-        CountStat(q.counters, kStatRays);
+        ShadeEntry<kClass>(sc, ps, q, depth, cache, q.order[begin + i]);
+    }
+}
 
-        // --- miss: environment with the BSDF-sampling MIS weight
-        if (kClass == kClassMiss || id == -1) {
-            CountStat(q.counters, kStatMisses);
-            float w = 1.0f;
-            if ((flags & kPathPrevValid) && !(flags & kPathPrevDelta)) {
-                w = PowerHeuristic(1, prev.w, 1, PdfEnvironment(sc.env, d));
-            }
-            rad = rad + Mul(tp, EvalEnvironment(sc.env, d)) * w;
-            ps.radiance[path] = ToF4(rad);
-            continue;
-        }
-        CountStat(q.counters, kStatHits);
-
-        // --- medium attenuation (Beer-Lambert inside a thick dielectric)
-        if (flags & kPathMedium) {
-            const float4 md = ps.medium[path];
-            if (hit.x > 0.0f && md.w > 0.0f) {
-                const float inv = 1.0f / md.w;
-                const float c[3] = {Clampf(md.x, 1.0e-6f, 1.0f), Clampf(md.y, 1.0e-6f, 1.0f), Clampf(md.z, 1.0e-6f, 1.0f)};
-                tp = V3{tp.x * expf(logf(c[0]) * hit.x * inv), tp.y * expf(logf(c[1]) * hit.x * inv),
-                        tp.z * expf(logf(c[2]) * hit.x * inv)};
-            }
-        }
-        if (IsBlack(tp)) {
-            ps.throughput[path] = ToF4(tp);
-            continue;
-        }
-
-        Surface s;
-        if (!ResolveSurface<false>(sc, o, d, hit, inst, s, depth, 0, 0)) {
-            rad = rad + Mul(tp, V3{1.0f, 0.0f, 1.0f});  // invalid material marker
-            ps.radiance[path] = ToF4(rad);
-            continue;
-        }
-        if (sc.texture_count > 0 && s.triangle) {  // the texture stage's result for this entry
-            const float4 tn = q.tex_normal[e];
-            if (tn.w != 0.0f) {
-                s.n = F4(tn);
-                s.reflectance_scale = F4(q.tex_scale[e]);
-            }
-        }
-        Mat m;
-        V3 emission{0.0f, 0.0f, 0.0f};
-        if (s.material >= 0) {
-            const DevMaterial& dm = sc.materials[s.material];
-            m = LoadMat(dm);
-            m.reflectance = Mul(m.reflectance, s.reflectance_scale);
-            m.measured = dm.measured_index >= 0 ? sc.measured + dm.measured_index : nullptr;
-            emission = Ld3(dm.emission);
-        } else {  // default RenderMaterial: diffuse 0.5
-            m = Mat{kDiffuse, {0.5f, 0.5f, 0.5f}, 1.5f, 0.0f, 0.0f, 1.5f, 0.01f, {0, 0, 0}, 10, 1};
-        }
-        if constexpr (ClassKind<kClass>() >= 0) m.kind = ClassKind<kClass>();  // the class fixes the kind
-        const V3 wo = -d;
-        if (depth == 0) {
-            flags |= kPathPrimary;
-            ps.aov_albedo[path] = ToF4(m.reflectance, hit.x);
-            ps.aov_normal[path] = ToF4(s.n);
-        }
-
-        // --- emission with the BSDF-sampling MIS weight (triangle lights only)
-        if (!IsBlack(emission) && s.triangle) {
-            float w = 1.0f;
-            if ((flags & kPathPrevValid) && !(flags & kPathPrevDelta)) {
-                const int32_t ei = sc.prim_emissive[s.prim];
-                const float pl = PdfEmissiveSolidAngle(sc, F4(prev), s.p, s.ng_obj, ei);
-                w = PowerHeuristic(1, prev.w, 1, pl);
-            }
-            rad = rad + Mul(tp, emission) * w;
-        }
-
-        // --- radiance cache: path spread (footprint heuristic), training
-        // records, early termination into the cache
-        if (cache.enabled) {
-            const float cv = fmaxf(fabsf(Dot(d, s.n)), 1.0e-4f);
-            float2 sp = ps.spread[path];
-            if (depth == 0) {
-                sp.x = hit.x * hit.x / (4.0f * kPi * cv);
-                sp.y = 0.0f;
-            } else if (!(flags & kPathPrevDelta)) {
-                sp.y += sqrtf(hit.x * hit.x / (fmaxf(prev.w, 1.0e-12f) * cv));
-            }
-            ps.spread[path] = sp;
-            const int32_t slot = cache.train_slot[path];
-            if (slot >= 0) {
-                const int32_t k = cache.slot_len[slot];
-                if (k < cache.max_depth) {
-                    const int64_t v = static_cast<int64_t>(slot) * cache.max_depth + k;
-                    WriteCacheQuery(cache.slot_q + 16 * v, s.p, wo, s.n, m);
-                    cache.slot_lt[2 * v] = ToF4(rad);
-                    cache.slot_lt[2 * v + 1] = ToF4(tp);
-                    cache.slot_len[slot] = k + 1;
-                }
-            }
-            const bool fires = depth >= 1 && !(flags & kPathCacheQueued) && (cache.delta_vertices || !IsDelta(m)) &&
-                               sp.y * sp.y > cache.spread_c * sp.x;
-            if (fires) {
-                // The image estimate of the path ends here: radiance so far
-                // plus throughput x cache. A training path goes on as an
-                // unbiased suffix whose radiance only trains the cache.
-                const unsigned long long k = QueueAppend(cache.counters + 0);
-                WriteCacheQuery(cache.queries + 16 * k, s.p, wo, s.n, m);
-                cache.query_path[k] = path;
-                cache.query_tp[k] = ToF4(tp);
-                cache.query_base[k] = ToF4(rad);
-                if (slot < 0) {
-                    ps.throughput[path] = ToF4(tp);
-                    ps.radiance[path] = ToF4(rad);
-                    ps.flags[path] = flags;
-                    continue;
-                }
-                flags |= kPathCacheQueued;
-            }
-        }
-
-        PixelSampler smp;
-        const int32_t pixel = ps.pixel[path];
-        smp.Init(sc.sampler, sc.view->seed, pixel % sc.width, pixel / sc.width, ps.sample[path], sc.spp);
-        Pcg32 rng{ps.rng_state[path], ps.rng_inc[path]};
-
-        // --- coated vertex: next events and continuation in the reference's
-        // PCG32 order, after the shadow stages (DeferLayeredVertex)
-        if ((kClass == kClassCoatedDiffuse || kClass == kClassGeneric) && IsLayered(m.kind) && !IsDelta(m)) {
-            DeferLayeredVertex(sc, ps, q, path, smp, depth, m, s.material, s.p, s.n, wo, flags);
-            ps.throughput[path] = ToF4(tp);
-            ps.radiance[path] = ToF4(rad);
-            ps.flags[path] = flags;
-            continue;
-        }
-
-        // --- next-event estimation: samples now, visibility in the shadow stage
-        if (!IsDelta(m)) NextEvent(sc, ps, q, path, smp, rng, depth, m, s.p, s.n, wo, tp, flags);
-
-        // --- subsurface entry (path_integrator.cpp:103-135): Fresnel split at
-        // the interface; the transmitted part becomes a probe ray that the
-        // subsurface stage traces and closes (SubsurfaceExitKernel).
-        if (kClass == kClassGeneric && m.kind == kSubsurface && s.material >= 0 &&
-            sc.materials[s.material].bssrdf_index >= 0 && sc.materials[s.material].bssrdf_index < sc.bssrdf_count) {
-            if (depth + 1 < sc.max_depth) {
-                const DevMaterial& dm = sc.materials[s.material];
-                const V3 ns = s.n;
-                V3 ss, ts;
-                BssrdfFrame(ns, ss, ts);
-                const float fr = FrDielectric(fabsf(Dot(wo, ns)), dm.bssrdf_eta);
-                if (smp.Sample1D(kDimBssrdfReflect, depth) < fr) {
-                    // Specular reflection (the selection probability cancels Fresnel).
-                    const V3 wr = ns * (2.0f * Dot(wo, ns)) - wo;
-                    flags |= kPathPrevValid | kPathPrevDelta;
-                    ps.prev[path] = ToF4(s.p, 1.0f);
-                    const V3 bn = Dot(wr, ns) >= 0.0f ? ns : -ns;
-                    const V3 no = s.p + bn * SurfaceBias(s.p);
-                    const unsigned long long k = QueueAppend(q.counters + kCtrOut);
-                    q.ray_out[2 * k] = make_float4(no.x, no.y, no.z, 1.0e-5f);
-                    q.ray_out[2 * k + 1] = make_float4(wr.x, wr.y, wr.z, __int_as_float(0x7f800000));
-                    q.path_out[k] = path;
-                } else {
-                    // SampleBssrdfProbe (src/integrators/bssrdf_probe.cpp:17-60): projection
-                    // axis, colour channel, radius, and the probe segment through the disk.
-                    const TabBssrdf tab = MakeTabBssrdf(dm, sc.bssrdf[dm.bssrdf_index]);
-                    float u1 = smp.Sample1D(kDimBssrdfAxis, depth);
-                    float ux, uy;
-                    smp.Sample2D(kDimBssrdfDisk, depth, ux, uy);
-                    V3 vx, vy, vz;
-                    if (u1 < 0.5f) {
-                        vx = ss, vy = ts, vz = ns;
-                        u1 *= 2.0f;
-                    } else if (u1 < 0.75f) {
-                        vx = ts, vy = ns, vz = ss;
-                        u1 = (u1 - 0.5f) * 4.0f;
-                    } else {
-                        vx = ns, vy = ss, vz = ts;
-                        u1 = (u1 - 0.75f) * 4.0f;
-                    }
-                    const int channel = min(max(static_cast<int>(u1 * 3.0f), 0), 2);
-                    u1 = u1 * 3.0f - static_cast<float>(channel);
-                    const float radius = BssrdfSampleSr(tab, channel, ux);
-                    if (radius >= 0.0f) {
-                        const float phi = 2.0f * kPi * uy;
-                        const float max_radius = BssrdfSampleSr(tab, channel, 0.999f);
-                        if (radius < max_radius) {
-                            const float length = 2.0f * sqrtf(fmaxf(0.0f, max_radius * max_radius - radius * radius));
-                            // cos/sin rounded from double precision: the correctly rounded
-                            // float values, as the host libm's float cos/sin return them.
-                            const float cphi = static_cast<float>(cos(static_cast<double>(phi)));
-                            const float sphi = static_cast<float>(sin(static_cast<double>(phi)));
-                            const V3 disk = vx * (radius * cphi) + vy * (radius * sphi);
-                            const V3 base = s.p + disk - vz * (length * 0.5f);
-                            const unsigned long long k = QueueAppend(q.counters + kCtrProbe);
-                            q.probe_ray[2 * k] = make_float4(base.x, base.y, base.z, 1.0e-5f);
-                            q.probe_ray[2 * k + 1] = make_float4(vz.x, vz.y, vz.z, length);
-                            q.probe_target[k] = make_int4(s.triangle ? s.prim : -1, s.triangle ? inst : -1,
-                                                          s.triangle ? -1 : -2 - id, path);
-                            q.probe_entry[2 * k] = ToF4(s.p, u1);
-                            q.probe_entry[2 * k + 1] = ToF4(ns, __int_as_float(s.material));
-                        }
-                    }
-                }
-            }
-            ps.throughput[path] = ToF4(tp);
-            ps.radiance[path] = ToF4(rad);
-            ps.flags[path] = flags;
-            ps.rng_state[path] = rng.state;
-            continue;
-        }
-
-        ContinuePath(sc, ps, q, path, depth, m, s.material, s.p, s.n, wo, tp, rad, flags, smp, rng);
+// ShadeKernel over the class-kClass entries of several jobs' extend queues
+// at once (ShadeJob table): each thread takes an entry from the jobs'
+// class ranges laid end to end and shades it with its job's scene, path
+// state and queues.
+template <int kClass>
+__global__ void __launch_bounds__(256, 2) PooledShadeKernel(const ShadeJob* __restrict__ jobs, int njobs) {
+    __shared__ unsigned long long s_ends[kMaxPoolJobs];
+    __shared__ unsigned long long s_begin[kMaxPoolJobs];
+    for (int j = threadIdx.x; j < njobs; j += blockDim.x) {
+        const unsigned long long* c = jobs[j].q.counters;
+        unsigned long long b = 0;
+#pragma unroll
+        for (int k = 0; k < kClass; ++k) b += c[kCtrClass0 + k];
+        s_begin[j] = b;
+        s_ends[j] = c[kCtrClass0 + kClass];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int j = 1; j < njobs; ++j) s_ends[j] += s_ends[j - 1];
+    }
+    __syncthreads();
+    const unsigned long long total = njobs > 0 ? s_ends[njobs - 1] : 0ull;
+    for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        const int j = PoolJobOf(s_ends, njobs, i);
+        const ShadeJob& job = jobs[j];
+        PathState ps = job.ps;
+        Queues q = job.q;
+        const unsigned long long local = i - (j ? s_ends[j - 1] : 0ull);
+        ShadeEntry<kClass>(job.sc, ps, q, job.depth, job.cache, q.order[s_begin[j] + local]);
     }
 }
 
@@ -1948,9 +1989,27 @@ void LaunchResetCounters(const Queues& q, cudaStream_t st) { ResetCountersKernel
 void LaunchAdvanceQueue(const Queues& q, cudaStream_t st) { AdvanceQueueKernel<<<1, 32, 0, st>>>(q); }
 void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, const CacheArgs& cache, int depth,
                  int64_t capacity, int sm_count, cudaStream_t st) {
+    LaunchShadeSort(sc, ps, q, depth, capacity, sm_count, st);
+    LaunchShadeClasses(sc, ps, q, cache, depth, capacity, sm_count, st);
+}
+void LaunchShadeSort(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
+                     int sm_count, cudaStream_t st) {
     if (sc.texture_count > 0) SurfaceTextureKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth);
     ClassifyKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, q);
     ScatterByClassKernel<<<Grid(capacity, sm_count), kThreads, 0, st>>>(q);
+}
+void LaunchPooledShade(const ShadeJob* jobs, int njobs, int64_t capacity, int sm_count, cudaStream_t st) {
+    if (njobs <= 0) return;
+    const unsigned grid = Grid(capacity, sm_count);
+    PooledShadeKernel<kClassMiss><<<grid, kThreads, 0, st>>>(jobs, njobs);
+    PooledShadeKernel<kClassDiffuse><<<grid, kThreads, 0, st>>>(jobs, njobs);
+    PooledShadeKernel<kClassConductor><<<grid, kThreads, 0, st>>>(jobs, njobs);
+    PooledShadeKernel<kClassDielectric><<<grid, kThreads, 0, st>>>(jobs, njobs);
+    PooledShadeKernel<kClassCoatedDiffuse><<<grid, kThreads, 0, st>>>(jobs, njobs);
+    PooledShadeKernel<kClassGeneric><<<grid, kThreads, 0, st>>>(jobs, njobs);
+}
+void LaunchShadeClasses(const DevScene& sc, const PathState& ps, const Queues& q, const CacheArgs& cache, int depth,
+                        int64_t capacity, int sm_count, cudaStream_t st) {
     ShadeKernel<kClassMiss><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
     ShadeKernel<kClassDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
     ShadeKernel<kClassConductor><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);

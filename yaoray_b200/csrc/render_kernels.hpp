@@ -36,6 +36,24 @@ void LaunchResetCounters(const Queues& q, cudaStream_t st);
 void LaunchAdvanceQueue(const Queues& q, cudaStream_t st);
 void LaunchShade(const DevScene& sc, const PathState& ps, const Queues& q, const CacheArgs& cache, int depth,
                  int64_t capacity, int sm_count, cudaStream_t st);
+// LaunchShade in two parts: the texture stage and the sort of the extend
+// queue by shading class, then the shade kernel of every class.
+void LaunchShadeSort(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
+                     int sm_count, cudaStream_t st);
+void LaunchShadeClasses(const DevScene& sc, const PathState& ps, const Queues& q, const CacheArgs& cache, int depth,
+                        int64_t capacity, int sm_count, cudaStream_t st);
+// One job of a pooled shade launch: its scene, path state, queues at this
+// bounce (sorted by LaunchShadeSort), cache arguments and bounce.
+struct ShadeJob {
+    DevScene sc;
+    PathState ps;
+    Queues q;
+    CacheArgs cache;
+    int32_t depth;
+};
+// The shade kernel of every class, each launch over the class's entries of
+// all `njobs` jobs (a device array); `capacity` bounds their sum.
+void LaunchPooledShade(const ShadeJob* jobs, int njobs, int64_t capacity, int sm_count, cudaStream_t st);
 // Subsurface: close the probes traced by LaunchRenderProbe (exit point,
 // Sp / pdf, NEE at the exit, continuation).
 // Scenes with cut-out (alpha) materials: the extend stage's skip loop over

@@ -47,8 +47,15 @@ __device__ __forceinline__ void WriteResult(const TraceArgs& args, int64_t ray, 
     }
 }
 
+// kLeafBatch > 0: a lane that reaches a leaf waits (its ray keeps its place
+// in its own visiting order) until at least kLeafBatch lanes of the warp
+// are at leaves or no lane is at an interior node, so that the leaf tests,
+// the longest branch of a step, run for many lanes at once instead of for
+// the one or two lanes that reached a leaf at each step. Interior steps go
+// on meanwhile; every ray's visiting order, and so every hit and count,
+// is unchanged.
 template <bool kAny, bool kStats, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks,
-          bool kWide = false>
+          bool kWide = false, int kLeafBatch = 0>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args) {
     __shared__ int2 s_stack[kShortStack * kBlock];
     int2* col = s_stack + threadIdx.x;
@@ -89,6 +96,24 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args
             if (__all_sync(kFull, exhausted)) break;
             continue;
         }
+        if (kLeafBatch > 0) {
+            // Uniform loop: every lane runs every iteration, so the votes
+            // see the whole warp.
+#pragma unroll 1
+            for (int k = 0; k < kStepsPerRefill; ++k) {
+                const unsigned at_leaf = __ballot_sync(kFull, alive && s.cur < 0);
+                const unsigned at_node = __ballot_sync(kFull, alive && s.cur >= 0);
+                if (!(at_leaf | at_node)) break;
+                const bool leaves = at_node == 0u || __popc(at_leaf) >= kLeafBatch;
+                if (alive && (s.cur >= 0 || leaves)) {
+                    alive = Step<kAny, kStats, kTwo, StackStore<kTotal, kBlock>, false, kWide>(args.accel, args.rays,
+                                                                                               ray, s, st, col,
+                                                                                               args.error);
+                    if (!alive) WriteResult<kAny, kStats>(args, ray, s);
+                }
+            }
+            continue;
+        }
 #pragma unroll 1
         for (int k = 0; k < kStepsPerRefill && alive; ++k) {
             alive = Step<kAny, kStats, kTwo, StackStore<kTotal, kBlock>, false, kWide>(args.accel, args.rays, ray, s, st,
@@ -98,39 +123,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args
     }
 }
 
-// Loads the pooled jobs' ray counts (written on the device by the stage
-// that filled the queues) into `ends` as an inclusive prefix sum; returns
-// the total. Called by the whole block.
-template <typename Job>
-__device__ __forceinline__ unsigned long long LoadPoolEnds(const Job* jobs, int njobs, unsigned long long* ends) {
-    for (int j = threadIdx.x; j < njobs; j += blockDim.x) ends[j] = *jobs[j].count_ptr;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int j = 1; j < njobs; ++j) ends[j] += ends[j - 1];
-    }
-    __syncthreads();
-    return njobs > 0 ? ends[njobs - 1] : 0ull;
-}
-
-// The job that pooled work item idx (< the total) belongs to: the first
-// whose queue ends past it.
-__device__ __forceinline__ int PoolJobOf(const unsigned long long* ends, int njobs, unsigned long long idx) {
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (ends[mid] > idx) {
-            hi = mid;
-        } else {
-            lo = mid + 1;
-        }
-    }
-    return lo;
-}
-
 // TraceKernel over the ray queues of several jobs at once (TracePool): the
 // same traversal and refill, with the accelerator, rays and outputs of the
 // job each lane's ray came from.
-template <bool kAny, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks>
+template <bool kAny, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks, int kLeafBatch>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) PooledTraceKernel(TracePool pool) {
     __shared__ int2 s_stack[kShortStack * kBlock];
     __shared__ unsigned long long s_ends[kMaxPoolJobs];
@@ -178,9 +174,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) PooledTraceKernel(TracePoo
             continue;
         }
 #pragma unroll 1
-        for (int k = 0; k < kStepsPerRefill && alive; ++k) {
-            alive = Step<kAny, false, kTwo, StackStore<kTotal, kBlock>>(acc, rays, ray, s, st, col, job->error);
-            if (!alive) WriteResult<kAny, false>(*job, ray, s);
+        for (int k = 0; k < kStepsPerRefill; ++k) {
+            const unsigned at_leaf = __ballot_sync(kFull, alive && s.cur < 0);
+            const unsigned at_node = __ballot_sync(kFull, alive && s.cur >= 0);
+            if (!(at_leaf | at_node)) break;
+            const bool leaves = at_node == 0u || __popc(at_leaf) >= kLeafBatch;
+            if (alive && (s.cur >= 0 || leaves)) {
+                alive = Step<kAny, false, kTwo, StackStore<kTotal, kBlock>>(acc, rays, ray, s, st, col, job->error);
+                if (!alive) WriteResult<kAny, false>(*job, ray, s);
+            }
         }
     }
 }
@@ -310,7 +312,8 @@ __global__ void __launch_bounds__(kTraceBlock) RenderProbeKernel(RenderProbeArgs
 //
 // kPooled: the launch serves the shadow queues of several jobs (ShadowPool);
 // each lane works with the job of the ray it holds.
-template <bool kTwo, int kTotal, bool kPooled = false>
+// kLeafBatch: leaf tests batched across the warp, as in TraceKernel.
+template <bool kTwo, int kTotal, bool kPooled = false, int kLeafBatch = 0>
 __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm)
     ShadowTransmittanceKernel(const __grid_constant__ ShadowArgs args, const __grid_constant__ ShadowPool pool) {
     __shared__ int2 s_stack[kShadowShortStack * kTraceBlock];
@@ -472,6 +475,21 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm)
             if (__all_sync(kFull, exhausted)) break;
             continue;
         }
+        if (kLeafBatch > 0) {
+#pragma unroll 1
+            for (int k = 0; k < 8; ++k) {
+                const unsigned at_leaf = __ballot_sync(kFull, alive && s.cur < 0);
+                const unsigned at_node = __ballot_sync(kFull, alive && s.cur >= 0);
+                if (!(at_leaf | at_node)) break;
+                const bool leaves = at_node == 0u || __popc(at_leaf) >= kLeafBatch;
+                if (alive && (s.cur >= 0 || leaves)) {
+                    alive = Step<true, false, kTwo, StackStore<kTotal, kTraceBlock, kShadowShortStack>, true>(
+                        acc, A->rays, ray, s, st, col, A->error, A->tri_clear, A->sphere_clear, &clear);
+                    if (!alive) finish();
+                }
+            }
+            continue;
+        }
 #pragma unroll 1
         for (int k = 0; k < 8 && alive; ++k) {
             alive = Step<true, false, kTwo, StackStore<kTotal, kTraceBlock, kShadowShortStack>, true>(
@@ -494,9 +512,9 @@ cudaError_t PersistentGrid(Kernel kernel, int block, int64_t count, int sm_count
 }
 
 template <bool kAny, bool kStats, bool kTwo, int kTotal, int kBlock, int kStepsPerRefill, int kMinBlocks,
-          bool kWide = false>
+          bool kWide = false, int kLeafBatch = 0>
 cudaError_t LaunchOne(const TraceArgs& args, cudaStream_t stream, int sm_count) {
-    auto kernel = TraceKernel<kAny, kStats, kTwo, kTotal, kBlock, kStepsPerRefill, kMinBlocks, kWide>;
+    auto kernel = TraceKernel<kAny, kStats, kTwo, kTotal, kBlock, kStepsPerRefill, kMinBlocks, kWide, kLeafBatch>;
     int64_t blocks = 0;
     const cudaError_t err = PersistentGrid(kernel, kBlock, args.count, sm_count, blocks);
     if (err != cudaSuccess) return err;
@@ -516,6 +534,11 @@ cudaError_t LaunchShape(const TraceArgs& args, int shape, cudaStream_t stream, i
         case 4: return LaunchOne<kAny, kStats, kTwo, kTotal, 64, 8, 1, kWide>(args, stream, sm_count);
         case 5: return LaunchOne<kAny, kStats, kTwo, kTotal, 256, 8, 1, kWide>(args, stream, sm_count);
         case 6: return LaunchOne<kAny, kStats, kTwo, kTotal, 64, 8, 24, kWide>(args, stream, sm_count);
+        case 7: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1, kWide, 4>(args, stream, sm_count);
+        case 8: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1, kWide, 8>(args, stream, sm_count);
+        case 9: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1, kWide, 16>(args, stream, sm_count);
+        case 10: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 12, kWide, 8>(args, stream, sm_count);
+        case 11: return LaunchOne<kAny, kStats, kTwo, kTotal, 256, 8, 1, kWide, 8>(args, stream, sm_count);
         default: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1, kWide>(args, stream, sm_count);
     }
 }
@@ -547,7 +570,9 @@ cudaError_t LaunchProbeOne(const ProbeArgs& args, cudaStream_t stream, int sm_co
 
 template <bool kTwo, int kTotal, bool kPooled = false>
 cudaError_t LaunchShadowOne(const ShadowArgs& args, const ShadowPool& pool, cudaStream_t stream, int sm_count) {
-    auto kernel = ShadowTransmittanceKernel<kTwo, kTotal, kPooled>;
+    // A pooled launch batches leaf tests; a single one when its shape asks.
+    auto kernel = (kPooled || args.leaf_batch > 0) ? ShadowTransmittanceKernel<kTwo, kTotal, kPooled, 8>
+                                                   : ShadowTransmittanceKernel<kTwo, kTotal, kPooled, 0>;
     int64_t blocks = 0;
     const cudaError_t err =
         PersistentGrid(kernel, kTraceBlock, kPooled ? pool.capacity : args.capacity, sm_count, blocks);
@@ -559,7 +584,7 @@ cudaError_t LaunchShadowOne(const ShadowArgs& args, const ShadowPool& pool, cuda
 template <bool kAny, bool kTwo, int kTotal>
 cudaError_t LaunchPooledOne(const TracePool& pool, cudaStream_t stream, int sm_count) {
     constexpr int kBlock = 128;
-    auto kernel = PooledTraceKernel<kAny, kTwo, kTotal, kBlock, 8, 1>;
+    auto kernel = PooledTraceKernel<kAny, kTwo, kTotal, kBlock, 8, 1, 8>;
     int64_t blocks = 0;
     const cudaError_t err = PersistentGrid(kernel, kBlock, pool.capacity, sm_count, blocks);
     if (err != cudaSuccess) return err;

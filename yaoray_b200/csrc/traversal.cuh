@@ -66,6 +66,35 @@ __device__ __forceinline__ void CountLanes(unsigned long long* counter) {
     }
 }
 
+// Loads the pooled jobs' work counts (written on the device by the stage
+// that filled their queues) into `ends` as an inclusive prefix sum;
+// returns the total. Called by the whole block.
+template <typename Job>
+__device__ __forceinline__ unsigned long long LoadPoolEnds(const Job* jobs, int njobs, unsigned long long* ends) {
+    for (int j = threadIdx.x; j < njobs; j += blockDim.x) ends[j] = *jobs[j].count_ptr;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int j = 1; j < njobs; ++j) ends[j] += ends[j - 1];
+    }
+    __syncthreads();
+    return njobs > 0 ? ends[njobs - 1] : 0ull;
+}
+
+// The job that pooled work item idx (< the total) belongs to: the first
+// whose queue ends past it.
+__device__ __forceinline__ int PoolJobOf(const unsigned long long* ends, int njobs, unsigned long long idx) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (ends[mid] > idx) {
+            hi = mid;
+        } else {
+            lo = mid + 1;
+        }
+    }
+    return lo;
+}
+
 // Traversal stack of kTotal entries per thread: the first kShortStack in the
 // block's shared memory (column `col`, stride kBlock), the rest local.
 template <int kTotal, int kBlock = kTraceBlock, int kShort = kShortStack>
