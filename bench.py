@@ -298,6 +298,12 @@ def run_gpu(args):
     # End to end through the C ABI host path (pinned host buffers).
     host_rays = torch.from_numpy(rays_np).pin_memory().numpy()
     host_hits = torch.empty((n, 4), dtype=torch.float32).pin_memory().numpy()
+    # The host path's own launch shape (its kernels share the GPU with its
+    # copies), tuned untimed on a 2M-ray slice of the step's host rays.
+    host_tune = {"shape": args.trace_shape} if args.trace_shape is not None else \
+        acc.autotune_host(host_rays[: min(n, 1 << 21)])
+    if args.trace_shape is not None:
+        acc.set_host_trace_shape(args.trace_shape)
     for _ in range(max(1, args.warmup // 2)):
         acc.intersect_host(host_rays, out=host_hits)
     e_steps = max(1, args.steps // 2)
@@ -355,6 +361,7 @@ def run_gpu(args):
                        "l2": f"inputs larger than L2 (rays {n * 32 >> 20} MiB + hits {n * 16 >> 20} MiB + "
                              f"BVH {bvh_mib} MiB, L2 126 MB), no flush",
                        "parallelism": f"replicas x{ws}", "launch_shape": tune["shape"],
+                       "host_path_launch_shape": host_tune["shape"], "host_path_autotune_ms": host_tune.get("times_ms"),
                        "hierarchy": "four-wide copy of the reference BVH" if acc.wide else "binary reference BVH",
                        "autotune_ms": tune["times_ms"],
                        "bvh_build_s": {"device": round(build_device_s, 3), "host": round(build_host_s, 3),

@@ -361,6 +361,22 @@ yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t cou
 yrc_status yrc_accel_set_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t shape);
 int32_t yrc_accel_get_trace_shape(const yrc_accel* accel, int32_t any_hit);
 
+/* The launch shape of yrc_trace_host's traversal kernels: its chunks'
+ * kernels run beside the chunks' host<->device copies, and the shape that
+ * is fastest alone is not always the fastest there (on the 2M-triangle
+ * set the leaf-batched shape 8 traverses 1.31x faster alone but the host
+ * pipeline runs 8 % slower with it than with shape 10). autotune_host
+ * times yrc_trace_host on `count` HOST rays (pinned memory, as the caller's
+ * own) once per shape and keeps the lowest-numbered shape within 2 % of the
+ * fastest; set_host_trace_shape(-1) makes the host path follow
+ * yrc_accel_set_trace_shape again (the default). `times_ms` (optional,
+ * YRC_TRACE_SHAPES floats) receives the wall time per call and shape.
+ * Synchronous. No counterpart in the reference. */
+yrc_status yrc_accel_autotune_host(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags,
+                                   float* times_ms);
+yrc_status yrc_accel_set_host_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t shape);
+int32_t yrc_accel_get_host_trace_shape(const yrc_accel* accel, int32_t any_hit);
+
 /* Four-wide traversal (opt-in). set_wide(1) builds, for a flat BVH of
  * triangles only, a four-wide copy of its hierarchy (the binary tree
  * collapsed two levels at a time, same node boxes and leaves) that later

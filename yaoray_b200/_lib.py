@@ -183,6 +183,9 @@ def lib() -> C.CDLL:
         "yrc_accel_autotune": (C.c_int, [P, P, I64, I32, P, P]),
         "yrc_accel_set_trace_shape": (C.c_int, [P, I32, I32]),
         "yrc_accel_get_trace_shape": (I32, [P, I32]),
+        "yrc_accel_autotune_host": (C.c_int, [P, P, I64, I32, P]),
+        "yrc_accel_set_host_trace_shape": (C.c_int, [P, I32, I32]),
+        "yrc_accel_get_host_trace_shape": (I32, [P, I32]),
         "yrc_accel_set_wide": (C.c_int, [P, I32]),
         "yrc_accel_get_wide": (I32, [P]),
         "yrc_accel_set_ray_order": (C.c_int, [P, I32, I32, C.c_float]),

@@ -328,6 +328,20 @@ class DeviceAccelerator:
     def set_trace_shape(self, shape: int, any_hit: bool = False) -> None:
         check(lib().yrc_accel_set_trace_shape(self._handle, int(any_hit), shape))
 
+    def autotune_host(self, rays: np.ndarray, any_hit: bool = False) -> dict:
+        """Times yrc_trace_host on host rays (N, 8) float32 (pinned memory,
+        like the caller's) per launch shape and keeps the fastest for the
+        host path; returns {shape: milliseconds per call} and the choice."""
+        times = (C.c_float * TRACE_SHAPES)()
+        n = rays.size // 8
+        check(lib().yrc_accel_autotune_host(self._handle, ptr(rays), n, _lib.YRC_TRACE_ANY if any_hit else 0, times))
+        return {"times_ms": [round(float(t), 3) for t in times],
+                "shape": int(lib().yrc_accel_get_host_trace_shape(self._handle, int(any_hit)))}
+
+    def set_host_trace_shape(self, shape: int, any_hit: bool = False) -> None:
+        """Launch shape of the host-buffer path (-1: follow set_trace_shape)."""
+        check(lib().yrc_accel_set_host_trace_shape(self._handle, int(any_hit), shape))
+
     @property
     def wide(self) -> bool:
         """True while closest / any-hit traces use the four-wide copy of the

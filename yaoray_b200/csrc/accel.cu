@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <array>
 #include <cstring>
+#include <chrono>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -323,6 +324,10 @@ struct yrc_accel {
     int* d_error = nullptr;
     yrc::AccelParams params{};
     int trace_shape[2] = {0, 0};  // launch shape for closest / any hit (autotuned)
+    // Launch shape of yrc_trace_host's chunks (closest / any hit), -1: the
+    // device shape. Its kernels share the GPU with the chunks' copies, so
+    // the fastest device shape need not be the fastest there.
+    int host_shape[2] = {-1, -1};
     int64_t device_bytes = 0;
     yrc::HostPipeline pipe;
     // Ray reordering ahead of device traces (yrc_accel_set_ray_order).
@@ -461,7 +466,8 @@ constexpr int64_t kOrderMinRays = int64_t{1} << 16;
 // reordering buffers are not shared with another stream at the time).
 yrc_status LaunchInternal(yrc_accel* a, const yrc_ray* rays, int64_t count, int32_t flags, yrc_hit* hits,
                           int32_t* instances, uint8_t* occluded, uint32_t* nt, uint32_t* tt, uint32_t* st,
-                          unsigned long long* counter, cudaStream_t stream, bool reorder = false) {
+                          unsigned long long* counter, cudaStream_t stream, bool reorder = false,
+                          int shape = -1) {
     if (count <= 0) return Ok();
     TraceArgs args{};
     args.accel = a->params;
@@ -493,7 +499,7 @@ yrc_status LaunchInternal(yrc_accel* a, const yrc_ray* rays, int64_t count, int3
     if (a->timing && err == cudaSuccess) err = cudaEventRecord(a->ev[1], stream);
     if (err == cudaSuccess) err = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
     if (err != cudaSuccess) return CudaFail(err, "trace counter reset");
-    err = LaunchTrace(args, any, stats, a->trace_shape[any ? 1 : 0], stream, a->sm_count);
+    err = LaunchTrace(args, any, stats, shape >= 0 ? shape : a->trace_shape[any ? 1 : 0], stream, a->sm_count);
     if (err != cudaSuccess) return CudaFail(err, "trace launch");
     if (a->timing) {
         err = cudaEventRecord(a->ev[2], stream);
@@ -805,7 +811,7 @@ yrc_status yrc_trace_host(yrc_accel* accel, const yrc_ray* rays, int64_t count, 
                                        any ? nullptr : static_cast<yrc_hit*>(p.d_out[s]), instances ? p.d_inst[s] : nullptr,
                                        any ? static_cast<uint8_t*>(p.d_out[s]) : nullptr, want_stats ? ds : nullptr,
                                        want_stats ? ds + n : nullptr, want_stats ? ds + 2 * n : nullptr,
-                                       p.d_counters + s, st);
+                                       p.d_counters + s, st, false, accel->host_shape[any ? 1 : 0]);
         if (ls != YRC_OK) return ls;
         if (any) {
             err = cudaMemcpyAsync(occluded + done, p.d_out[s], static_cast<size_t>(n), cudaMemcpyDeviceToHost, st);
@@ -868,6 +874,60 @@ yrc_status yrc_accel_set_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t 
     }
     accel->trace_shape[any_hit ? 1 : 0] = shape;
     return yrc::Ok();
+}
+
+yrc_status yrc_accel_set_host_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t shape) {
+    if (!accel || shape < -1 || shape >= yrc::kTraceShapes) {
+        return yrc::Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_set_host_trace_shape: bad argument");
+    }
+    accel->host_shape[any_hit ? 1 : 0] = shape;
+    return yrc::Ok();
+}
+
+int32_t yrc_accel_get_host_trace_shape(const yrc_accel* accel, int32_t any_hit) {
+    return accel ? accel->host_shape[any_hit ? 1 : 0] : -2;
+}
+
+yrc_status yrc_accel_autotune_host(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags,
+                                   float* times_ms) {
+    using namespace yrc;
+    if (!accel || count <= 0 || !rays) return Fail(YRC_ERR_INVALID_ARGUMENT, "yrc_accel_autotune_host: bad argument");
+    const bool any = (flags & YRC_TRACE_ANY) != 0;
+    const int32_t trace_flags = flags & YRC_TRACE_ANY;
+    // Pinned output, as a caller that cares about this path's speed has.
+    uint8_t* out = nullptr;
+    cudaSetDevice(accel->device);
+    const cudaError_t aerr = cudaMallocHost(reinterpret_cast<void**>(&out),
+                                            static_cast<size_t>(count) * (any ? 1 : sizeof(yrc_hit)));
+    if (aerr != cudaSuccess) return CudaFail(aerr, "yrc_accel_autotune_host output");
+    float totals[kTraceShapes] = {};
+    const int saved = accel->host_shape[any ? 1 : 0];
+    yrc_status status = Ok();
+    for (int shape = 0; shape < kTraceShapes && status == YRC_OK; ++shape) {
+        accel->host_shape[any ? 1 : 0] = shape;
+        double total = 0.0;
+        for (int rep = 0; rep < 3 && status == YRC_OK; ++rep) {  // first repetition warms up
+            const auto t0 = std::chrono::steady_clock::now();
+            status = yrc_trace_host(accel, rays, count, trace_flags, any ? nullptr : reinterpret_cast<yrc_hit*>(out),
+                                    nullptr, any ? out : nullptr, nullptr);
+            const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            if (rep > 0) total += ms;
+        }
+        totals[shape] = static_cast<float>(total);
+        if (times_ms) times_ms[shape] = static_cast<float>(total / 2.0);
+    }
+    cudaFreeHost(out);
+    if (status != YRC_OK) {
+        accel->host_shape[any ? 1 : 0] = saved;
+        return status;
+    }
+    // As the device autotuner: the lowest-index shape within 2 % of the fastest.
+    float best = totals[0];
+    for (int shape = 1; shape < kTraceShapes; ++shape) best = totals[shape] < best ? totals[shape] : best;
+    int best_shape = 0;
+    while (best_shape + 1 < kTraceShapes && totals[best_shape] > 1.02f * best) ++best_shape;
+    accel->host_shape[any ? 1 : 0] = best_shape;
+    return Ok();
 }
 
 int32_t yrc_accel_get_trace_shape(const yrc_accel* accel, int32_t any_hit) {
