@@ -78,10 +78,10 @@ def shadow_rays(n, seed):
     return rays, np.clip(pairs, 0, PAIRS)
 
 
-@pytest.mark.parametrize("shape", [0, 8])
+@pytest.mark.parametrize("shape", [0, 8, 9])
 def test_shadow_visibility_matches_reference_per_ray(cuda, ref, shape):
-    """Per-ray parity of the shadow stage; launch shape 8 batches the leaf
-    tests of each warp in the transmittance kernel."""
+    """Per-ray parity of the shadow stage; launch shapes 8 and 9 batch the
+    leaf tests of each warp in the transmittance kernel by 8 and 16."""
     scene = slab_stack_scene()
     rays, pairs = shadow_rays(60000, seed=5)
     want = ref.RefJob.from_scene(scene).shadow_visibility(rays)

@@ -462,8 +462,9 @@ yrc_status Finalize(Layout& layout, int32_t root_ref, const float lo[3], const f
 // costs more than the coherence it buys.
 constexpr int64_t kOrderMinRays = int64_t{1} << 16;
 
-// `reorder`: the launch may sort the rays first (the accelerator's
-// reordering buffers are not shared with another stream at the time).
+// `reorder`: a yrc_trace_device launch, which may sort the rays first (the
+// accelerator's reordering buffers are not shared with another stream at
+// the time) and records the timing events when timing is on.
 yrc_status LaunchInternal(yrc_accel* a, const yrc_ray* rays, int64_t count, int32_t flags, yrc_hit* hits,
                           int32_t* instances, uint8_t* occluded, uint32_t* nt, uint32_t* tt, uint32_t* st,
                           unsigned long long* counter, cudaStream_t stream, bool reorder = false,
@@ -486,7 +487,8 @@ yrc_status LaunchInternal(yrc_accel* a, const yrc_ray* rays, int64_t count, int3
     const bool order = reorder && !stats && a->order_mode != kRayOrderOff && count >= kOrderMinRays &&
                        count < (int64_t{1} << 32);
     cudaError_t err = cudaSuccess;
-    if (a->timing) err = cudaEventRecord(a->ev[0], stream);
+    const bool timed = a->timing && reorder;
+    if (timed) err = cudaEventRecord(a->ev[0], stream);
     if (order && err == cudaSuccess) {
         const int bits = RayOrderBits(count, a->order_bits);
         err = EnsureOrderScratch(a, count, bits);
@@ -496,12 +498,12 @@ yrc_status LaunchInternal(yrc_accel* a, const yrc_ray* rays, int64_t count, int3
         if (err != cudaSuccess) return CudaFail(err, "ray order");
         args.order = a->order.order;
     }
-    if (a->timing && err == cudaSuccess) err = cudaEventRecord(a->ev[1], stream);
+    if (timed && err == cudaSuccess) err = cudaEventRecord(a->ev[1], stream);
     if (err == cudaSuccess) err = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
     if (err != cudaSuccess) return CudaFail(err, "trace counter reset");
     err = LaunchTrace(args, any, stats, shape >= 0 ? shape : a->trace_shape[any ? 1 : 0], stream, a->sm_count);
     if (err != cudaSuccess) return CudaFail(err, "trace launch");
-    if (a->timing) {
+    if (timed) {
         err = cudaEventRecord(a->ev[2], stream);
         if (err != cudaSuccess) return CudaFail(err, "trace timing event");
         a->timed_order = order;

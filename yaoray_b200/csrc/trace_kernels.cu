@@ -539,6 +539,7 @@ cudaError_t LaunchShape(const TraceArgs& args, int shape, cudaStream_t stream, i
         case 9: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1, kWide, 16>(args, stream, sm_count);
         case 10: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 12, kWide, 8>(args, stream, sm_count);
         case 11: return LaunchOne<kAny, kStats, kTwo, kTotal, 256, 8, 1, kWide, 8>(args, stream, sm_count);
+        case 12: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 8, kWide, 16>(args, stream, sm_count);
         default: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1, kWide>(args, stream, sm_count);
     }
 }
@@ -570,9 +571,12 @@ cudaError_t LaunchProbeOne(const ProbeArgs& args, cudaStream_t stream, int sm_co
 
 template <bool kTwo, int kTotal, bool kPooled = false>
 cudaError_t LaunchShadowOne(const ShadowArgs& args, const ShadowPool& pool, cudaStream_t stream, int sm_count) {
-    // A pooled launch batches leaf tests; a single one when its shape asks.
-    auto kernel = (kPooled || args.leaf_batch > 0) ? ShadowTransmittanceKernel<kTwo, kTotal, kPooled, 8>
-                                                   : ShadowTransmittanceKernel<kTwo, kTotal, kPooled, 0>;
+    // A pooled launch batches leaf tests by 8; a single one as its shape asks
+    // (leaf batch 4 runs as 8).
+    auto kernel = kPooled                  ? ShadowTransmittanceKernel<kTwo, kTotal, kPooled, 8>
+                  : args.leaf_batch >= 16 ? ShadowTransmittanceKernel<kTwo, kTotal, kPooled, 16>
+                  : args.leaf_batch > 0   ? ShadowTransmittanceKernel<kTwo, kTotal, kPooled, 8>
+                                          : ShadowTransmittanceKernel<kTwo, kTotal, kPooled, 0>;
     int64_t blocks = 0;
     const cudaError_t err =
         PersistentGrid(kernel, kTraceBlock, kPooled ? pool.capacity : args.capacity, sm_count, blocks);
