@@ -459,7 +459,7 @@ def run_render(args):
     e2e from the host wall clock around the call. The CPU baseline renders the
     same scene with the reference CPU backend on all host threads at a few spp."""
     import torch
-    from yaoray_b200.render import CudaBackend
+    from yaoray_b200.render import CudaBackend, pinned_film
 
     size = tuple(int(v) for v in args.size.split("x")) if args.size else None
     scene = render_scene(args.workload, args.render_spp, size, args.max_depth)
@@ -487,11 +487,12 @@ def run_render(args):
         assert res.ok, res.error
     gpu_index = 0
     times, devs, launches = [], [], 0
+    film_buf = pinned_film(scene.width, scene.height)  # the caller's pinned film, kept across steps
     with ClockSampler(gpu_index) as clocks:
         for _ in range(args.steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            res = backend.render(prepared)
+            res = backend.render(prepared, film_out=film_buf)
             times.append(time.perf_counter() - t0)
             devs.append(res.stats["device_seconds"])
             launches += int(res.stats["kernel_launches"])
@@ -531,6 +532,7 @@ def run_render(args):
             "e2e": {"value": round(samples / dt, 1), "unit": "samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": scene.width * scene.height * 56},
             "path_segments_per_s": round(res.stats["rays_traced"] / ddt, 1),
+            "shadow_rays_per_s": round(res.stats["shadow_rays"] / ddt, 1),
             "gpu_launches": launches,
             "cpu_baseline": base, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
@@ -567,7 +569,7 @@ def run_nrc(args):
     import torch
     from yaoray_b200 import instanced
     from yaoray_b200.nrc import RadianceCache
-    from yaoray_b200.render import CudaBackend, build_two_level_bvh
+    from yaoray_b200.render import CudaBackend, build_two_level_bvh, pinned_film
 
     W, H, CLAMP, C_SPREAD, DECAY, ORBIT_DEG = args.nrc_width, args.nrc_height, 20.0, 1.0e-4, 0.995, 0.5
     FRAMES, EVAL, SPP = args.nrc_frames, args.nrc_eval_frames, args.nrc_spp
@@ -604,10 +606,15 @@ def run_nrc(args):
             p.set_tuning(tunings[spp])
         return p
 
+    # One pinned film buffer for every timed frame, as an interactive
+    # renderer keeps its framebuffer (the image is taken from it before the
+    # next render).
+    film_buf = pinned_film(W, H)
+
     def timed_render(p):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = backend.render(p)
+        r = backend.render(p, film_out=film_buf)
         wall = time.perf_counter() - t0
         return r.linear(), r.stats, wall
 

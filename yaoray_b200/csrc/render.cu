@@ -1186,8 +1186,15 @@ yrc_status FinishRender(RenderRun& run, double device_seconds) {
     yrc_render_scene* s = run.s;
     cudaStream_t stream = s->stream;
     const int64_t pixels = run.pixels;
-    cudaError_t err = cudaMemcpyAsync(run.film_out, s->film, sizeof(yrc_film_pixel) * pixels, cudaMemcpyDeviceToHost,
-                                      stream);
+    // samples_rendered: summed on the device rather than over the host film.
+    cudaError_t err = cudaMemsetAsync(s->q.counters + kCtrSamplesDone, 0, sizeof(unsigned long long), stream);
+    if (err == cudaSuccess) {
+        LaunchSumSamples(s->film, pixels, s->q.counters + kCtrSamplesDone, s->sm_count, stream);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) {
+        err = cudaMemcpyAsync(run.film_out, s->film, sizeof(yrc_film_pixel) * pixels, cudaMemcpyDeviceToHost, stream);
+    }
     unsigned long long counters[kCtrCount];
     if (err == cudaSuccess) {
         err = cudaMemcpyAsync(counters, s->q.counters, sizeof(counters), cudaMemcpyDeviceToHost, stream);
@@ -1202,9 +1209,7 @@ yrc_status FinishRender(RenderRun& run, double device_seconds) {
     if (run.stats) {
         yrc_render_stats* stats = run.stats;
         std::memset(stats, 0, sizeof(*stats));
-        uint64_t done = 0;
-        for (int64_t i = 0; i < pixels; ++i) done += run.film_out[i].samples;
-        stats->samples_rendered = done;
+        stats->samples_rendered = counters[kCtrSamplesDone];
         stats->converged_pixels = run.converged;
         stats->rays_traced = counters[kCtrStatsBase + 0];
         stats->shadow_rays = counters[kCtrStatsBase + 1];

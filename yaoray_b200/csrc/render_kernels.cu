@@ -1869,6 +1869,19 @@ __global__ void CacheTargetsKernel(PathState ps, CacheArgs cache) {
 // assumption that every sample is finite; accepting stops at the first
 // non-finite one (the reference re-uses that sample index on its next pass)
 // or when adaptive sampling declares the pixel converged.
+// The film's sample count summed over the pixels (RenderStats::samples_rendered)
+// into *out, one atomic per warp.
+__global__ void SumSamplesKernel(const yrc_film_pixel* film, int64_t pixels, unsigned long long* out) {
+    unsigned long long n = 0;
+    for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < pixels;
+         p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        n += film[p].samples;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31u) == 0 && n) atomicAdd(out, n);
+}
+
 __global__ void FilmKernel(DevScene sc, PathState ps, BatchArgs b, FilmArgs f) {
     const int64_t n_active = static_cast<int64_t>(*b.active_count);
     const int32_t batch = *b.batch;
@@ -2112,6 +2125,11 @@ void LaunchActivePixels(const DevScene& sc, const BatchArgs& b, const FilmArgs& 
 void LaunchFinishActive(unsigned long long* active_count, unsigned long long* active_count_next, int32_t* batch,
                         int32_t max_batch, int64_t capacity, cudaStream_t st) {
     FinishActiveKernel<<<1, 32, 0, st>>>(active_count, active_count_next, batch, max_batch, capacity);
+}
+
+void LaunchSumSamples(const yrc_film_pixel* film, int64_t pixels, unsigned long long* out, int sm_count,
+                      cudaStream_t st) {
+    SumSamplesKernel<<<Grid(pixels, sm_count), kThreads, 0, st>>>(film, pixels, out);
 }
 
 }  // namespace yrc

@@ -89,6 +89,9 @@ void LaunchActivePixels(const DevScene& sc, const BatchArgs& b, const FilmArgs& 
                         cudaStream_t st);
 // dst[0..n) = value.
 void LaunchFillInt32(int32_t* dst, int64_t n, int32_t value, int sm_count, cudaStream_t st);
+// Sums the film's per-pixel sample counts into *out (zeroed by the caller).
+void LaunchSumSamples(const yrc_film_pixel* film, int64_t pixels, unsigned long long* out, int sm_count,
+                      cudaStream_t st);
 void LaunchFinishActive(unsigned long long* active_count, unsigned long long* active_count_next, int32_t* batch,
                         int32_t max_batch, int64_t capacity, cudaStream_t st);
 

@@ -278,6 +278,7 @@ enum CounterIndex {
     kCtrDefer2 = 15,  // entries in defer_paths2
     kCtrStatsBase = 16,  // rays, shadow rays, occluded, hits, misses, bad
     kCtrCursor0 = 24,  // scatter cursors per shading class
+    kCtrSamplesDone = 30,  // film samples summed over the pixels after a render
     kCtrCount = 32,
 };
 

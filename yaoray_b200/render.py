@@ -530,6 +530,16 @@ class RenderRequestPy:
     progress_callback: object | None = None    # f(progress dict, film) -> (cancel, error)
 
 
+def pinned_film(width: int, height: int) -> np.ndarray:
+    """A (height, width) FILM_PIXEL_DTYPE array in pinned host memory, for
+    CudaBackend.render(..., film_out=...): the film's device-to-host copy
+    then runs at full link speed and touches no fresh pages."""
+    import torch
+
+    buf = torch.empty(width * height * FILM_PIXEL_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    return buf.numpy().view(FILM_PIXEL_DTYPE).reshape(height, width)
+
+
 class CudaBackend:
     """RenderBackend for RenderBackendKind::Cuda over libyrcuda."""
 
@@ -550,7 +560,13 @@ class CudaBackend:
                 accel = build_bvh_device(scene.geometry)[0]
         return PreparedScene(scene, accel)
 
-    def render(self, prepared: PreparedScene, request: RenderRequestPy | None = None) -> RenderResult:
+    def render(self, prepared: PreparedScene, request: RenderRequestPy | None = None,
+               film_out: np.ndarray | None = None) -> RenderResult:
+        """CudaBackend::Render. `film_out` (optional) is a caller-owned
+        (height, width) FILM_PIXEL_DTYPE array that receives the film, e.g. a
+        pinned buffer kept across the frames of an interactive renderer
+        (the copy into pinned memory is direct; a fresh array is allocated
+        and page-faulted in on every call otherwise)."""
         L = _bind()
         sc = prepared.scene
         req = request or RenderRequestPy()
@@ -576,7 +592,13 @@ class CudaBackend:
                 return 1 if cancel else 0
             r.progress = PROGRESS_FN(cb)
             keep.append(r.progress)
-        film = np.zeros((sc.height, sc.width), FILM_PIXEL_DTYPE)
+        if film_out is not None:
+            if (film_out.dtype != FILM_PIXEL_DTYPE or film_out.shape != (sc.height, sc.width)
+                    or not film_out.flags.c_contiguous):
+                raise ValueError("film_out must be a C-contiguous (height, width) FILM_PIXEL_DTYPE array")
+            film = film_out
+        else:
+            film = np.zeros((sc.height, sc.width), FILM_PIXEL_DTYPE)
         bad = C.c_uint64()
         st = Stats()
         status = L.yrc_render(prepared._handle, C.byref(r), ptr(film), C.byref(bad), C.byref(st))
