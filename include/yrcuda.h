@@ -358,7 +358,8 @@ yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t cou
  * shapes 10 and 11 are shape 8 with a 40-register budget (12 blocks of 128
  * per SM) and with blocks of 256, shape 12 is shape 9 with a 64-register
  * budget (8 blocks of 128 per SM; the two-level kernel needs more), and
- * shapes 13 and 14 are shape 8 refilling lanes every 2 and 4 steps. No
+ * shapes 13 and 14 are shape 8 refilling lanes every 16 and 32 steps
+ * (every 2 and 4 steps measured slower). No
  * shape changes a hit: every ray keeps the reference's visiting order. */
 yrc_status yrc_accel_set_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t shape);
 int32_t yrc_accel_get_trace_shape(const yrc_accel* accel, int32_t any_hit);

@@ -540,8 +540,8 @@ cudaError_t LaunchShape(const TraceArgs& args, int shape, cudaStream_t stream, i
         case 10: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 12, kWide, 8>(args, stream, sm_count);
         case 11: return LaunchOne<kAny, kStats, kTwo, kTotal, 256, 8, 1, kWide, 8>(args, stream, sm_count);
         case 12: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 8, kWide, 16>(args, stream, sm_count);
-        case 13: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 2, 1, kWide, 8>(args, stream, sm_count);
-        case 14: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 4, 1, kWide, 8>(args, stream, sm_count);
+        case 13: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 16, 1, kWide, 8>(args, stream, sm_count);
+        case 14: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 32, 1, kWide, 8>(args, stream, sm_count);
         default: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1, kWide>(args, stream, sm_count);
     }
 }
