@@ -397,7 +397,8 @@ def run_gpu(args):
 # scene, and the radiance cache's equal-relMSE ratio.
 EXTRA_LEGS = (("cornell", ["--workload", "cornell", "--steps", "10", "--warmup", "3"]),
               ("instanced", ["--workload", "instanced", "--steps", "4", "--warmup", "3"]),
-              ("nrc", ["--workload", "nrc"]))
+              ("nrc", ["--workload", "nrc"]),
+              ("jobs", ["--workload", "jobs", "--schedules", "one_at_a_time,shared,pooled"]))
 
 
 def run_extra_legs():
@@ -712,12 +713,15 @@ def run_jobs(args):
     """--workload jobs: 48 uneven render jobs (resolutions 128^2..1024^2, spp
     16..1024 scaled by --spp-scale, 10K-2M-triangle sphere-mesh scenes with
     the instanced material mix plus subsurface, half with a radiance cache),
-    rendered once untimed (allocation and graph capture), then one at a time,
-    concurrently from --concurrency worker threads (one stream per job), and
-    in shared launches (groups of --concurrency jobs, one graph launch per
-    step for all unfinished jobs of a group; device-memory admission).
-    value = aggregate samples/s of the shared-launch run; the line also
-    carries per-job latency p50/p99 of all three."""
+    rendered once untimed (allocation and graph capture), then under each of
+    --schedules: one at a time, concurrently from --concurrency worker
+    threads (one stream per job), in shared launches (groups of
+    --concurrency jobs, one graph launch per step for all unfinished jobs of
+    a group; device-memory admission) and in pooled launches (the same
+    groups, with one traversal launch per bounce over every job's rays and
+    one shade launch per material class). value = aggregate samples/s of
+    the shared-launch run (the pooled run without it); the line carries
+    per-job latency p50/p99 of each."""
     import torch
     from yaoray_b200 import batch
 
@@ -726,18 +730,26 @@ def run_jobs(args):
     runner = batch.JobRunner()
     runner.prepare(jobs, autotune=not args.no_autotune)
     prepare_s = time.perf_counter() - t0
+    schedules = set(args.schedules.split(","))
     runner.run_sequential(jobs)  # warm-up: allocates and captures every job's batch graph
-    seq = runner.run_sequential(jobs)
-    seq_lat = seq.latency_quantiles()
-    seq_sps = seq.samples_per_s
     torch.cuda.synchronize()
+    runs, lat = {}, {}  # latencies are per job and overwritten by the next schedule: keep each run's
     with ClockSampler(0) as clocks:
-        conc = runner.run_concurrent(jobs, concurrency=args.concurrency)
-    conc_lat = conc.latency_quantiles()
-    shared = runner.run_shared_launch(jobs, concurrency=args.concurrency)
-    shared_lat = shared.latency_quantiles()
-    pooled = runner.run_shared_launch(jobs, concurrency=args.concurrency, pooled=True)
-    pooled_lat = pooled.latency_quantiles()
+        if "one_at_a_time" in schedules:
+            runs["one_at_a_time"] = runner.run_sequential(jobs)
+            lat["one_at_a_time"] = runs["one_at_a_time"].latency_quantiles()
+        if "concurrent" in schedules:
+            runs["concurrent"] = runner.run_concurrent(jobs, concurrency=args.concurrency)
+            lat["concurrent"] = runs["concurrent"].latency_quantiles()
+        if "shared" in schedules:
+            runs["shared_launch"] = runner.run_shared_launch(jobs, concurrency=args.concurrency)
+            lat["shared_launch"] = runs["shared_launch"].latency_quantiles()
+        runs["pooled_launch"] = runner.run_shared_launch(jobs, concurrency=args.concurrency, pooled=True)
+        lat["pooled_launch"] = runs["pooled_launch"].latency_quantiles()
+    pooled = runs["pooled_launch"]
+    # value: the shared launch (one graph launch per step holding every job's
+    # batch graph), measured 1-2 % faster than the pooled form on this job set.
+    main = runs.get("shared_launch", pooled)
     failed = [j.name for j in jobs if not j.ok]
     runner.close(jobs)
     tris = [j.scene.geometry.triangle_count for j in jobs]
@@ -757,33 +769,30 @@ def run_jobs(args):
             base = {"value": round(n / secs, 1), "unit": "samples/s", "cores": os.cpu_count(), "kind": "reference",
                     "sample": f"reference CpuBackend, the first {len(plain)} jobs without a cache, 32 spp each, "
                               f"one after another ({secs:.2f} s)"}
-    line = {"metric": "samples/s (48 batched uneven render jobs)", "value": round(shared.samples_per_s, 1),
+    line = {"metric": "samples/s (48 batched uneven render jobs)", "value": round(main.samples_per_s, 1),
             "unit": "samples/s", "n_gpus": 1, "steps": 1, "warmup": 1,
-            "ms_per_step": round(shared.wall_s * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": round(main.wall_s * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "jobs48-128..1024px-16..1024spp-10K..2M-tris", "jobs": len(jobs),
                        "spp_scale": args.spp_scale, "concurrency": args.concurrency,
-                       "scheduling": "shared launch: groups of up to --concurrency jobs, one yrc_render_many call "
-                                     "per group, one graph launch per step for all unfinished jobs of the group",
+                       "scheduling": ("shared launch: groups of up to --concurrency jobs, one yrc_render_many call "
+                                      "per group, one graph launch per step for all unfinished jobs of the group"
+                                      if main is not pooled else
+                                      "pooled launch: groups of up to --concurrency jobs, one yrc_render_pooled call "
+                                      "per group; per bounce one persistent traversal launch over every job's extend "
+                                      "rays, one shade launch per material class and one shadow launch"),
                        "triangles_min_max": [min(tris), max(tris)], "with_radiance_cache": sum(j.use_cache for j in jobs),
-                       "samples_total": conc.samples, "prepare_seconds": round(prepare_s, 2),
+                       "samples_total": main.samples, "prepare_seconds": round(prepare_s, 2),
                        "autotune_seconds": round(sum(j.tune_s for j in jobs), 2),
                        "capacities": sorted({j.tuning["capacity"] for j in jobs if j.tuning}),
-                       "admission_budget_gb": round(conc.extra.get("budget_bytes", 0) / 2**30, 1),
-                       "peak_concurrent_jobs": shared.peak_concurrency},
-            "one_at_a_time": {"samples_per_s": round(seq_sps, 1), "wall_s": round(seq.wall_s, 3),
-                              "latency_p50_s": seq_lat["p50"], "latency_p99_s": seq_lat["p99"]},
-            "concurrent": {"samples_per_s": round(conc.samples_per_s, 1), "wall_s": round(conc.wall_s, 3),
-                           "latency_p50_s": conc_lat["p50"], "latency_p99_s": conc_lat["p99"]},
-            "shared_launch": {"samples_per_s": round(shared.samples_per_s, 1), "wall_s": round(shared.wall_s, 3),
-                              "latency_p50_s": shared_lat["p50"], "latency_p99_s": shared_lat["p99"],
-                              "groups_of": args.concurrency},
-            "pooled_launch": {"samples_per_s": round(pooled.samples_per_s, 1), "wall_s": round(pooled.wall_s, 3),
-                              "latency_p50_s": pooled_lat["p50"], "latency_p99_s": pooled_lat["p99"],
-                              "groups_of": args.concurrency},
+                       "admission_budget_gb": round(main.extra.get("budget_bytes", 0) / 2**30, 1),
+                       "peak_concurrent_jobs": main.peak_concurrency},
+            **{name: {"samples_per_s": round(r.samples_per_s, 1), "wall_s": round(r.wall_s, 3),
+                      "latency_p50_s": lat[name]["p50"], "latency_p99_s": lat[name]["p99"]}
+               for name, r in runs.items()},
             "failed_jobs": failed,
             "gpu_launches": sum(j.kernels for j in jobs),
-            "e2e": {"value": round(shared.samples_per_s, 1), "unit": "samples/s", "h2d_bytes_per_step": 0,
+            "e2e": {"value": round(main.samples_per_s, 1), "unit": "samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": film_bytes,
                     "note": "value is already host wall clock around the CudaBackend.render calls, films read back"},
             "cpu_baseline": base, "clocks": clocks.summary()}
@@ -802,6 +811,8 @@ def main():
     ap.add_argument("--nrc-spp", type=int, default=4, help="--workload nrc: spp per orbit frame")
     ap.add_argument("--nrc-train-steps", type=int, default=2, help="--workload nrc: optimiser steps per batch")
     ap.add_argument("--spp-scale", type=float, default=1.0, help="spp scale of --workload jobs")
+    ap.add_argument("--schedules", default="one_at_a_time,concurrent,shared,pooled",
+                    help="--workload jobs: the schedules to time (the default bench line's leg skips 'concurrent')")
     ap.add_argument("--concurrency", type=int, default=16,
                     help="--workload jobs: jobs per shared launch (and concurrent streams)")
     ap.add_argument("--no-autotune", action="store_true", help="render workloads: keep the default queue capacity")

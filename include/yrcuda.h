@@ -346,7 +346,7 @@ yrc_status yrc_trace_stats_device_noalloc(yrc_accel* accel, const yrc_ray* rays,
  * (optional, YRC_TRACE_SHAPES floats) receives the measured time per shape.
  * Synchronises `stream`.
  */
-#define YRC_TRACE_SHAPES 15
+#define YRC_TRACE_SHAPES 17
 yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags, void* stream,
                               float* times_ms);
 /* Set / get the launch shape (0..YRC_TRACE_SHAPES-1) used for closest-hit
@@ -359,7 +359,8 @@ yrc_status yrc_accel_autotune(yrc_accel* accel, const yrc_ray* rays, int64_t cou
  * per SM) and with blocks of 256, shape 12 is shape 9 with a 64-register
  * budget (8 blocks of 128 per SM; the two-level kernel needs more), and
  * shapes 13 and 14 are shape 8 refilling lanes every 16 and 32 steps
- * (every 2 and 4 steps measured slower). No
+ * (every 2 and 4 steps measured slower), shapes 15 and 16 shape 8 with
+ * register budgets for 9 and 10 blocks of 128 per SM. No
  * shape changes a hit: every ray keeps the reference's visiting order. */
 yrc_status yrc_accel_set_trace_shape(yrc_accel* accel, int32_t any_hit, int32_t shape);
 int32_t yrc_accel_get_trace_shape(const yrc_accel* accel, int32_t any_hit);
@@ -854,7 +855,7 @@ int64_t yrc_render_scene_capacity(const yrc_render_scene* scene);
  * 0..P-1 of every pixel, P = two batches of the largest candidate) for each
  * candidate queue capacity (whole passes of the image between 2^17 and 2^23
  * paths) and each traversal launch shape at the best capacity (one shape
- * for the extend and the shadow traversals; shapes 7-14 batch the leaf tests
+ * for the extend and the shadow traversals; shapes 7-16 batch the leaf tests
  * of a warp, in the shadow-transmittance kernel too); keeps the fastest
  * for later yrc_render calls. The traversal stack depth is not a candidate:
  * it follows the BVH's measured depth (64 or 256 entries). Probes run

@@ -25,7 +25,7 @@ from ._lib import check, lib, ptr
 
 # Compiled launch shapes of the closest / any-hit traversal kernel
 # (YRC_TRACE_SHAPES): the autotuner's candidates.
-TRACE_SHAPES = 15
+TRACE_SHAPES = 17
 
 
 # ------------------------------------------------------------------ geometry

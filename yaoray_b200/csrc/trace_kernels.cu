@@ -542,6 +542,8 @@ cudaError_t LaunchShape(const TraceArgs& args, int shape, cudaStream_t stream, i
         case 12: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 8, kWide, 16>(args, stream, sm_count);
         case 13: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 16, 1, kWide, 8>(args, stream, sm_count);
         case 14: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 32, 1, kWide, 8>(args, stream, sm_count);
+        case 15: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 9, kWide, 8>(args, stream, sm_count);
+        case 16: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 10, kWide, 8>(args, stream, sm_count);
         default: return LaunchOne<kAny, kStats, kTwo, kTotal, 128, 8, 1, kWide>(args, stream, sm_count);
     }
 }

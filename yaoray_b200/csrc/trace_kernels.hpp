@@ -12,7 +12,7 @@ namespace yrc {
 
 constexpr int kTraceBlock = 128;    // threads per block
 constexpr int kShortStack = 12;     // stack entries per thread kept in shared memory
-constexpr int kTraceShapes = 15;     // launch shapes the autotuner may choose from
+constexpr int kTraceShapes = 17;     // launch shapes the autotuner may choose from
 constexpr int kMaxTraceStack = 256; // deepest traversal stack any kernel supports
 
 // Status bits a kernel may set in the accelerator's device error word.
@@ -76,7 +76,7 @@ struct ShadowArgs {
     int32_t leaf_batch;                   // > 0: leaf tests batched across the warp (TraceKernel's kLeafBatch)
 };
 
-// The leaf batch of a launch shape (TraceKernel's kLeafBatch; shapes 7-14).
+// The leaf batch of a launch shape (TraceKernel's kLeafBatch; shapes 7-16).
 constexpr int LeafBatchOfShape(int shape) {
     return shape == 7 ? 4 : (shape == 9 || shape == 12) ? 16 : (shape == 8 || shape == 10 || shape == 11 || shape >= 13) ? 8 : 0;
 }
