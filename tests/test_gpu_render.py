@@ -17,7 +17,7 @@ import pytest
 
 import oracle
 from yaoray_b200 import cornell
-from yaoray_b200.render import CudaBackend, RenderRequestPy
+from yaoray_b200.render import CudaBackend, RenderRequestPy, pinned_film
 
 pytestmark = pytest.mark.gpu
 
@@ -131,6 +131,14 @@ def test_render_is_deterministic_and_resumable(cuda):
     resumed = backend.render(prepared, RenderRequestPy(resume_film=first.film, resume_completed_spp=6))
     assert resumed.ok
     assert resumed.film.tobytes() == a.film.tobytes()
+    # a caller-owned pinned film receives the same bytes, and the sample
+    # count (summed on the device) is the film's
+    film = pinned_film(scene.width, scene.height)
+    c = backend.render(prepared, film_out=film)
+    assert c.film is film and film.tobytes() == a.film.tobytes()
+    assert c.stats["samples_rendered"] == int(a.film["samples"].sum()) == 48 * 40 * 16
+    with pytest.raises(ValueError):
+        backend.render(prepared, film_out=np.zeros((40, 48), np.float32))
 
 
 def test_progress_callback_cancel_and_stop(cuda):

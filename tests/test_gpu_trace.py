@@ -105,6 +105,30 @@ def test_golden_host_path_matches(cuda, name):
     assert np.array_equal(occ.astype(bool), exp["hit"].astype(bool))
 
 
+@pytest.mark.parametrize("name", ["trace_spheres", "trace_two_level"])
+def test_host_path_autotune_keeps_the_reference_hits(cuda, name):
+    """The host path's own launch shape (tuned on the host pipeline) changes
+    no hit: after autotune_host, and with every shape set explicitly, the
+    host path returns the reference's hits and occlusion."""
+    import torch
+
+    f = load(name)
+    g, b = golden_accel(f, name)
+    dev = accel.DeviceAccelerator(g, b)
+    rays = torch.from_numpy(np.ascontiguousarray(f["rays"])).pin_memory().numpy()
+    exp = {k[4:]: v for k, v in f.items() if k.startswith("out_")}
+    tuned = dev.autotune_host(rays)
+    assert 0 <= tuned["shape"] < accel.TRACE_SHAPES and min(tuned["times_ms"]) > 0
+    check_closest(dev.intersect_host(rays), None, exp)
+    for shape in (0, 8, 12):
+        dev.set_host_trace_shape(shape)
+        check_closest(dev.intersect_host(rays), None, exp)
+        assert np.array_equal(dev.intersect_host(rays, any_hit=True).astype(bool), exp["hit"].astype(bool))
+    dev.set_host_trace_shape(-1)
+    with pytest.raises(Exception):
+        dev.set_host_trace_shape(accel.TRACE_SHAPES)
+
+
 def test_probe_matches_golden(cuda):
     import torch
 
