@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args
             if (__all_sync(kFull, exhausted)) break;
             continue;
         }
-        if (kLeafBatch > 0) {
+        if constexpr (kLeafBatch > 0) {
             // Uniform loop: every lane runs every iteration, so the votes
             // see the whole warp.
 #pragma unroll 1
@@ -112,13 +112,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) TraceKernel(TraceArgs args
                     if (!alive) WriteResult<kAny, kStats>(args, ray, s);
                 }
             }
-            continue;
-        }
+        } else {
 #pragma unroll 1
-        for (int k = 0; k < kStepsPerRefill && alive; ++k) {
-            alive = Step<kAny, kStats, kTwo, StackStore<kTotal, kBlock>, false, kWide>(args.accel, args.rays, ray, s, st,
-                                                                                       col, args.error);
-            if (!alive) WriteResult<kAny, kStats>(args, ray, s);
+            for (int k = 0; k < kStepsPerRefill && alive; ++k) {
+                alive = Step<kAny, kStats, kTwo, StackStore<kTotal, kBlock>, false, kWide>(args.accel, args.rays, ray,
+                                                                                           s, st, col, args.error);
+                if (!alive) WriteResult<kAny, kStats>(args, ray, s);
+            }
         }
     }
 }
@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm)
             if (__all_sync(kFull, exhausted)) break;
             continue;
         }
-        if (kLeafBatch > 0) {
+        if constexpr (kLeafBatch > 0) {
 #pragma unroll 1
             for (int k = 0; k < 8; ++k) {
                 const unsigned at_leaf = __ballot_sync(kFull, alive && s.cur < 0);
@@ -488,13 +488,13 @@ __global__ void __launch_bounds__(kTraceBlock, kShadowBlocksPerSm)
                     if (!alive) finish();
                 }
             }
-            continue;
-        }
+        } else {
 #pragma unroll 1
-        for (int k = 0; k < 8 && alive; ++k) {
-            alive = Step<true, false, kTwo, StackStore<kTotal, kTraceBlock, kShadowShortStack>, true>(
-                acc, A->rays, ray, s, st, col, A->error, A->tri_clear, A->sphere_clear, &clear);
-            if (!alive) finish();
+            for (int k = 0; k < 8 && alive; ++k) {
+                alive = Step<true, false, kTwo, StackStore<kTotal, kTraceBlock, kShadowShortStack>, true>(
+                    acc, A->rays, ray, s, st, col, A->error, A->tri_clear, A->sphere_clear, &clear);
+                if (!alive) finish();
+            }
         }
     }
 }
