@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cstring>
 #include <chrono>
 #include <mutex>
@@ -327,7 +328,9 @@ struct yrc_accel {
     // Launch shape of yrc_trace_host's chunks (closest / any hit), -1: the
     // device shape. Its kernels share the GPU with the chunks' copies, so
     // the fastest device shape need not be the fastest there.
-    int host_shape[2] = {-1, -1};
+    // Atomic: the host autotuner sets it between its own yrc_trace_host
+    // calls, which take the accelerator's lock themselves.
+    std::atomic<int> host_shape[2] = {-1, -1};
     int64_t device_bytes = 0;
     yrc::HostPipeline pipe;
     // Ray reordering ahead of device traces (yrc_accel_set_ray_order).
@@ -813,7 +816,7 @@ yrc_status yrc_trace_host(yrc_accel* accel, const yrc_ray* rays, int64_t count, 
                                        any ? nullptr : static_cast<yrc_hit*>(p.d_out[s]), instances ? p.d_inst[s] : nullptr,
                                        any ? static_cast<uint8_t*>(p.d_out[s]) : nullptr, want_stats ? ds : nullptr,
                                        want_stats ? ds + n : nullptr, want_stats ? ds + 2 * n : nullptr,
-                                       p.d_counters + s, st, false, accel->host_shape[any ? 1 : 0]);
+                                       p.d_counters + s, st, false, accel->host_shape[any ? 1 : 0].load());
         if (ls != YRC_OK) return ls;
         if (any) {
             err = cudaMemcpyAsync(occluded + done, p.d_out[s], static_cast<size_t>(n), cudaMemcpyDeviceToHost, st);
@@ -887,7 +890,7 @@ yrc_status yrc_accel_set_host_trace_shape(yrc_accel* accel, int32_t any_hit, int
 }
 
 int32_t yrc_accel_get_host_trace_shape(const yrc_accel* accel, int32_t any_hit) {
-    return accel ? accel->host_shape[any_hit ? 1 : 0] : -2;
+    return accel ? accel->host_shape[any_hit ? 1 : 0].load() : -2;
 }
 
 yrc_status yrc_accel_autotune_host(yrc_accel* accel, const yrc_ray* rays, int64_t count, int32_t flags,
@@ -903,7 +906,7 @@ yrc_status yrc_accel_autotune_host(yrc_accel* accel, const yrc_ray* rays, int64_
                                             static_cast<size_t>(count) * (any ? 1 : sizeof(yrc_hit)));
     if (aerr != cudaSuccess) return CudaFail(aerr, "yrc_accel_autotune_host output");
     float totals[kTraceShapes] = {};
-    const int saved = accel->host_shape[any ? 1 : 0];
+    const int saved = accel->host_shape[any ? 1 : 0].load();
     yrc_status status = Ok();
     for (int shape = 0; shape < kTraceShapes && status == YRC_OK; ++shape) {
         accel->host_shape[any ? 1 : 0] = shape;
