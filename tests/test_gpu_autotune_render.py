@@ -42,3 +42,26 @@ def test_autotune_chooses_a_candidate_and_keeps_it():
     assert again.ok, again.error
     assert again.film.tobytes() == ref.film.tobytes()
     p.close()
+
+
+@pytest.mark.parametrize("make", [lambda: batch.job_set(2, seed=5, spp_scale=1 / 64, max_triangles=60_000)[0].scene,
+                                  lambda: cornell.instanced_cutout_scene(48, 48, 8, 6)],
+                         ids=["flat-glass-subsurface", "two-level-cutout"])
+def test_film_independent_of_launch_shape(make):
+    """Every launch shape the render autotuner may choose (leaf batching in
+    the extend, shadow-transmittance and any-hit traversals included) gives
+    the film of the default shape byte for byte, on a flat scene with glass,
+    coated and subsurface materials and on a two-level scene with cut-outs."""
+    b = CudaBackend()
+    scene = make()
+    p = b.prepare(scene)
+    cap = scene.width * scene.height * min(scene.spp, 4)
+    films = []
+    for shape in range(accel.TRACE_SHAPES):
+        p.set_tuning({"capacity": cap, "trace_shape": shape})
+        r = b.render(p)
+        assert r.ok, (shape, r.error)
+        films.append(r.film.copy())
+    p.close()
+    for shape, f in enumerate(films[1:], 1):
+        assert f.tobytes() == films[0].tobytes(), shape
