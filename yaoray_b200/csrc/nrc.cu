@@ -358,6 +358,9 @@ __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const _
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
         const int64_t row = t * kTile + r;
         const bool valid = row < n;
+        // The lanes of this warp with a sample (all but in the last tile),
+        // for the warp-wide steps of the grid-gradient scatter.
+        const unsigned valid_mask = __ballot_sync(0xffffffffu, valid);
         {
             float x[kWidth];
             if (valid) {
@@ -445,24 +448,54 @@ __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const _
                 StoreRow(sg, r, dx);
             } else if (valid) {
                 // Grid features: scatter d input / d feature with the
-                // trilinear weights.
+                // trilinear weights. Per level, the eight corners' gradient
+                // reductions, touched-bit reads and bit sets are issued
+                // together (eight requests in flight instead of one round
+                // trip per corner), and the entries touched first this step
+                // are appended to the optimiser's list with one counter
+                // atomic per warp.
+                const unsigned warp_mask = valid_mask;
+                const unsigned lane = threadIdx.x & 31u;
                 float p[3];
                 NormalisedPosition(g, queries + row * kQueryFloats, p);
-#pragma unroll
+#pragma unroll 1
                 for (int lv = 0; lv < kLevels; ++lv) {
                     uint32_t idx[8];
                     float w[8];
                     LevelCorners(g, lv, p, idx, w);
                     const float d0 = dx[2 * lv], d1 = dx[2 * lv + 1];
+                    int64_t e[8];
+                    uint32_t seen[8];
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
-                        const int64_t e = static_cast<int64_t>(lv) * kTable + idx[c];
-                        atomicAdd(g.grad + e, make_float2(w[c] * d0, w[c] * d1));
-                        // First touch of the entry this step: list it for the optimiser.
-                        const uint32_t bit = 1u << (e & 31);
-                        uint32_t* word = g.touched + (e >> 5);
-                        if (!(*word & bit) && !(atomicOr(word, bit) & bit)) {
-                            g.touched_list[atomicAdd(g.touched_count, 1ull)] = static_cast<int32_t>(e);
+                        e[c] = static_cast<int64_t>(lv) * kTable + idx[c];
+                        atomicAdd(g.grad + e[c], make_float2(w[c] * d0, w[c] * d1));
+                    }
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) seen[c] = g.touched[e[c] >> 5];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        // A bit already set was listed by whoever set it;
+                        // of the threads that set it now, atomicOr tells
+                        // exactly one that it came first.
+                        const uint32_t bit = 1u << (e[c] & 31);
+                        if (!(seen[c] & bit)) seen[c] = atomicOr(g.touched + (e[c] >> 5), bit);
+                        else seen[c] = bit;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const bool first_touch = !(seen[c] & (1u << (e[c] & 31)));
+                        const unsigned fresh = __ballot_sync(warp_mask, first_touch);
+                        if (fresh) {
+                            const int leader = __ffs(fresh) - 1;
+                            unsigned long long base = 0;
+                            if (static_cast<int>(lane) == leader) {
+                                base = atomicAdd(g.touched_count, static_cast<unsigned long long>(__popc(fresh)));
+                            }
+                            base = __shfl_sync(warp_mask, base, leader);
+                            if (first_touch) {
+                                g.touched_list[base + __popc(fresh & ((1u << lane) - 1u))] = static_cast<int32_t>(e[c]);
+                            }
                         }
                     }
                 }
