@@ -358,9 +358,6 @@ __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const _
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
         const int64_t row = t * kTile + r;
         const bool valid = row < n;
-        // The lanes of this warp with a sample (all but in the last tile),
-        // for the warp-wide steps of the grid-gradient scatter.
-        const unsigned valid_mask = __ballot_sync(0xffffffffu, valid);
         {
             float x[kWidth];
             if (valid) {
@@ -446,18 +443,20 @@ __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const _
                     for (int k = 0; k < 8; ++k) dx[8 * c + k] = a8[k] > 0.0f ? dx[8 * c + k] : 0.0f;
                 }
                 StoreRow(sg, r, dx);
-            } else if (valid) {
+            } else {
                 // Grid features: scatter d input / d feature with the
                 // trilinear weights. Per level, the eight corners' gradient
                 // reductions, touched-bit reads and bit sets are issued
                 // together (eight requests in flight instead of one round
                 // trip per corner), and the entries touched first this step
                 // are appended to the optimiser's list with one counter
-                // atomic per warp.
-                const unsigned warp_mask = valid_mask;
+                // atomic per warp and level: the list counter is a single
+                // address that every CTA updates, so its atomics serialise.
+                // Every lane of the warp runs the loop (the warp-wide steps
+                // need all of them); a lane without a sample touches nothing.
                 const unsigned lane = threadIdx.x & 31u;
-                float p[3];
-                NormalisedPosition(g, queries + row * kQueryFloats, p);
+                float p[3] = {0.0f, 0.0f, 0.0f};
+                if (valid) NormalisedPosition(g, queries + row * kQueryFloats, p);
 #pragma unroll 1
                 for (int lv = 0; lv < kLevels; ++lv) {
                     uint32_t idx[8];
@@ -466,36 +465,43 @@ __global__ void __launch_bounds__(kThreads) CacheTrainKernel(GridArgs g, const _
                     const float d0 = dx[2 * lv], d1 = dx[2 * lv + 1];
                     int64_t e[8];
                     uint32_t seen[8];
+                    uint32_t fresh = 0;  // bit c: corner c's entry was touched first by this lane
+                    if (valid) {
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        e[c] = static_cast<int64_t>(lv) * kTable + idx[c];
-                        atomicAdd(g.grad + e[c], make_float2(w[c] * d0, w[c] * d1));
-                    }
+                        for (int c = 0; c < 8; ++c) {
+                            e[c] = static_cast<int64_t>(lv) * kTable + idx[c];
+                            atomicAdd(g.grad + e[c], make_float2(w[c] * d0, w[c] * d1));
+                        }
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) seen[c] = g.touched[e[c] >> 5];
+                        for (int c = 0; c < 8; ++c) seen[c] = g.touched[e[c] >> 5];
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        // A bit already set was listed by whoever set it;
-                        // of the threads that set it now, atomicOr tells
-                        // exactly one that it came first.
-                        const uint32_t bit = 1u << (e[c] & 31);
-                        if (!(seen[c] & bit)) seen[c] = atomicOr(g.touched + (e[c] >> 5), bit);
-                        else seen[c] = bit;
-                    }
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        const bool first_touch = !(seen[c] & (1u << (e[c] & 31)));
-                        const unsigned fresh = __ballot_sync(warp_mask, first_touch);
-                        if (fresh) {
-                            const int leader = __ffs(fresh) - 1;
-                            unsigned long long base = 0;
-                            if (static_cast<int>(lane) == leader) {
-                                base = atomicAdd(g.touched_count, static_cast<unsigned long long>(__popc(fresh)));
+                        for (int c = 0; c < 8; ++c) {
+                            // A bit already set was listed by whoever set it;
+                            // of the threads that set it now, atomicOr tells
+                            // exactly one that it came first.
+                            const uint32_t bit = 1u << (e[c] & 31);
+                            if (!(seen[c] & bit) && !(atomicOr(g.touched + (e[c] >> 5), bit) & bit)) {
+                                fresh |= 1u << c;
                             }
-                            base = __shfl_sync(warp_mask, base, leader);
-                            if (first_touch) {
-                                g.touched_list[base + __popc(fresh & ((1u << lane) - 1u))] = static_cast<int32_t>(e[c]);
-                            }
+                        }
+                    }
+                    // Warp prefix sum of the new entries, one counter atomic.
+                    const uint32_t mine = static_cast<uint32_t>(__popc(fresh));
+                    uint32_t incl = mine;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= static_cast<unsigned>(o)) incl += y;
+                    }
+                    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+                    if (total) {
+                        unsigned long long base = 0;
+                        if (lane == 0) base = atomicAdd(g.touched_count, static_cast<unsigned long long>(total));
+                        base = __shfl_sync(0xffffffffu, base, 0);
+                        unsigned long long at = base + (incl - mine);
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            if (fresh & (1u << c)) g.touched_list[at++] = static_cast<int32_t>(e[c]);
                         }
                     }
                 }
