@@ -264,6 +264,8 @@ def run_gpu(args):
     # this step's rays (untimed).
     if args.four_wide:  # opt-in four-wide traversal of the same BVH (same hits)
         acc.set_wide(True)
+    if args.ray_order != "off":  # opt-in ray reordering before each trace (same hits)
+        acc.set_ray_order(args.ray_order, 19, 0.05)
     if args.trace_shape is not None:  # a shape fixed by the caller (e.g. to profile the one a plain run chose)
         acc.set_trace_shape(args.trace_shape)
         tune = {"shape": args.trace_shape, "times_ms": None}
@@ -818,6 +820,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="render workloads: keep the default queue capacity")
     ap.add_argument("--trace-shape", type=int, default=None, help="traversal: use this launch shape, no autotune")
     ap.add_argument("--four-wide", action="store_true", help="traversal: the opt-in four-wide traversal")
+    ap.add_argument("--ray-order", choices=["off", "direction", "two-point"], default="off",
+                    help="traversal: the opt-in ray reordering (19-bit key) before each trace")
     ap.add_argument("--tuning", default=None, help="render workloads: 'capacity,shape' instead of the autotuner")
     ap.add_argument("--render-spp", type=int, default=16, help="spp per step of --workload instanced")
     ap.add_argument("--size", default=None, help="render workloads: WxH instead of the configured size (profiling)")
