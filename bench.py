@@ -787,6 +787,7 @@ def run_jobs(args):
                        "samples_total": main.samples, "prepare_seconds": round(prepare_s, 2),
                        "autotune_seconds": round(sum(j.tune_s for j in jobs), 2),
                        "capacities": sorted({j.tuning["capacity"] for j in jobs if j.tuning}),
+                       "capacity_halved_jobs": sum(1 for j in jobs if j.tuning and j.tuning.get("fitted")),
                        "admission_budget_gb": round(main.extra.get("budget_bytes", 0) / 2**30, 1),
                        "peak_concurrent_jobs": main.peak_concurrency},
             **{name: {"samples_per_s": round(r.samples_per_s, 1), "wall_s": round(r.wall_s, 3),

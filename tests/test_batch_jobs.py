@@ -108,6 +108,14 @@ def test_fit_capacities_brings_the_working_sets_under_the_budget(monkeypatch):
         pixels = j.scene.width * j.scene.height
         assert j.prepared.capacity % pixels == 0 and j.prepared.capacity >= pixels
         assert j.tuning["trace_shape"] == 2
+    # Working memory the autotuner's probes already hold is not needed again.
+    j0 = max(jobs, key=batch._working_set)
+    need = batch._working_set(j0)
+    j0.held_bytes = need // 2
+    assert batch._working_set(j0) == need - need // 2
+    j0.held_bytes = 10 * need
+    assert batch._working_set(j0) == 0
+    j0.held_bytes = 0
     # A budget below one pass of every job leaves each job at one pass.
     monkeypatch.setattr(batch, "_free_device_bytes", lambda: 1)
     r.fit_capacities(jobs)

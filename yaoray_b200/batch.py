@@ -50,6 +50,7 @@ class Job:
     tuning: dict | None = None
     tune_s: float = 0.0
     resident: bool = False  # rendered once: its working memory stays allocated
+    held_bytes: int = 0  # working memory its autotuner probes left allocated (already on the device)
     kernels: int = 0  # device kernels the last render launched
     latency_s: float = 0.0
     device_s: float = 0.0
@@ -125,13 +126,18 @@ def _working_set(job: Job) -> int:
     at ~640 B per path for these scenes (path state 196 B, coated-vertex
     state 80 B, extend / shadow / subsurface queues and transmittance
     ~350 B), ~760 B with a cache (its query queues), plus the film and,
-    with a cache, its grid, optimiser state and training records (~450 MB)."""
+    with a cache, its training-path records (~100 MB; the cache's grid and
+    optimiser state were allocated with the cache itself)."""
     if job.resident:
         return 0
     pixels = job.scene.width * job.scene.height
     paths = job.prepared.capacity if job.prepared is not None else max(1 << 21, pixels)
     per = 760 if job.use_cache else 640
-    return paths * per + pixels * 80 + (450 << 20 if job.use_cache else 0)
+    need = paths * per + pixels * 80 + (100 << 20 if job.use_cache else 0)
+    # The working memory the autotuner's probes left allocated is on the
+    # device already (free device memory does not count it); the render
+    # replaces it, so only the rest is still to allocate.
+    return max(0, need - job.held_bytes)
 
 
 @dataclass
@@ -172,6 +178,7 @@ class JobRunner:
         for job in jobs:
             t0 = time.perf_counter()
             job.prepared = self.backend.prepare(job.scene)
+            base_bytes = job.prepared.device_bytes
             if autotune:
                 key = (job.scene.width * job.scene.height, min(job.scene.spp, 64))
                 t1 = time.perf_counter()
@@ -181,6 +188,7 @@ class JobRunner:
                 else:
                     job.tuning = tuned[key] = job.prepared.autotune()
                 job.tune_s = time.perf_counter() - t1
+                job.held_bytes = max(0, job.prepared.device_bytes - base_bytes)
             if job.use_cache:
                 p = job.scene.geometry.positions
                 lo = p.min(0)
