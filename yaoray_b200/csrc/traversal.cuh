@@ -275,10 +275,10 @@ __device__ __forceinline__ int WideStep(const AccelParams& a, Traversal& s, Stac
     bool m0 = true, m1 = true, m2 = true, m3 = true;
     float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, e3 = 0.0f;
     int32_t r0 = rf.x, r1 = rf.y, r2 = rf.z, r3 = rf.w;
-    if (r0 != kAbsentRef) m0 = !SlabTest(s.r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, s.tmin, limit, e0);
-    if (r1 != kAbsentRef) m1 = !SlabTest(s.r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, s.tmin, limit, e1);
-    if (r2 != kAbsentRef) m2 = !SlabTest(s.r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, s.tmin, limit, e2);
-    if (r3 != kAbsentRef) m3 = !SlabTest(s.r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, s.tmin, limit, e3);
+    if (r0 != kAbsentRef) m0 = !SlabTestInterval(s.r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, s.tmin, limit, e0);
+    if (r1 != kAbsentRef) m1 = !SlabTestInterval(s.r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, s.tmin, limit, e1);
+    if (r2 != kAbsentRef) m2 = !SlabTestInterval(s.r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, s.tmin, limit, e2);
+    if (r3 != kAbsentRef) m3 = !SlabTestInterval(s.r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, s.tmin, limit, e3);
     // Sorting network on four.
     OrderPair(m0, e0, r0, m1, e1, r1);
     OrderPair(m2, e2, r2, m3, e3, r3);
@@ -321,11 +321,11 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
         bool hl = false, hr = false;
         if (pd.x != kAbsentRef) {
             if (kStats) ++s.nodes;
-            hl = SlabTest(s.r, pa.x, pa.y, pa.z, pa.w, pb.x, pb.y, s.tmin, limit, le);
+            hl = SlabTestInterval(s.r, pa.x, pa.y, pa.z, pa.w, pb.x, pb.y, s.tmin, limit, le);
         }
         if (pd.y != kAbsentRef) {
             if (kStats) ++s.nodes;
-            hr = SlabTest(s.r, pb.z, pb.w, pc.x, pc.y, pc.z, pc.w, s.tmin, limit, re);
+            hr = SlabTestInterval(s.r, pb.z, pb.w, pc.x, pc.y, pc.z, pc.w, s.tmin, limit, re);
         }
         if (hl && hr) {
             const bool left_first = le <= re;
@@ -440,7 +440,7 @@ __device__ __forceinline__ bool Step(const AccelParams& a, const float4* rays, i
             if (root != kAbsentRef) {
                 if (kStats) ++s.nodes;
                 float entry;
-                if (SlabTest(obj, ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, s.tmin, s.best.t, entry)) {
+                if (SlabTestInterval(obj, ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, s.tmin, s.best.t, entry)) {
                     s.local.t = s.best.t;
                     s.local.id = -1;
                     s.local.prim = -1;
