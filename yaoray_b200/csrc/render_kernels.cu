@@ -750,6 +750,11 @@ __device__ __noinline__ AnalyticSample SampleAnalyticLight(const DevAnalytic* an
 // the viewer wo), stores each contribution without visibility in the path's
 // NEE slots and queues the shadow rays; the shadow stage and NeeResolveKernel
 // finish the estimate.
+//
+// kEmissiveOnly: the scene has neither analytic lights nor a sampleable
+// environment (checked on the host), so those two branches are left out of
+// the instance.
+template <bool kEmissiveOnly = false>
 __device__ inline void NextEvent(const DevScene& sc, PathState& ps, Queues& q, int32_t path, PixelSampler& smp,
                                  Pcg32& rng, int depth, const Mat& m, V3 p, V3 n, V3 wo, V3 tp, uint32_t& flags) {
     bool any = false;
@@ -793,7 +798,7 @@ __device__ inline void NextEvent(const DevScene& sc, PathState& ps, Queues& q, i
             }
         }
     }
-    if (sc.analytic_count > 0) {  // delta lights: no MIS against the BSDF
+    if (!kEmissiveOnly && sc.analytic_count > 0) {  // delta lights: no MIS against the BSDF
         const AnalyticSample as = SampleAnalyticLight(sc.analytic, sc.analytic_count, sc.analytic_alias_prob,
                                                       sc.analytic_alias_index, sc.analytic_alias_pmf,
                                                       sc.analytic_tree, sc.analytic_tree_root, p,
@@ -812,7 +817,7 @@ __device__ inline void NextEvent(const DevScene& sc, PathState& ps, Queues& q, i
             }
         }
     }
-    if (EnvSampleable(sc.env)) {
+    if (!kEmissiveOnly && EnvSampleable(sc.env)) {
         float tx, ty;
         smp.Sample2D(kDimDirectLightSurface, depth, tx, ty);
         const EnvSample es = SampleEnvironment(sc.env, tx, ty);
@@ -1237,7 +1242,7 @@ __global__ void __launch_bounds__(kTraceBlock) ShadowExactKernel(DevScene sc, Qu
 // IntegratePathSample's per-bounce body (src/integrators/path_integrator.cpp:23-197)
 // for the entries of one shading class.
 // One extend-queue entry `e` of shading class kClass.
-template <int kClass>
+template <int kClass, bool kLean = false>
 __device__ __forceinline__ void ShadeEntry(const DevScene& sc, PathState& ps, Queues& q, int depth,
                                            const CacheArgs& cache, int64_t e) {
     const int32_t path = q.path_in[e];
@@ -1325,7 +1330,7 @@ __device__ __forceinline__ void ShadeEntry(const DevScene& sc, PathState& ps, Qu
 
     // --- radiance cache: path spread (footprint heuristic), training
     // records, early termination into the cache
-    if (cache.enabled) {
+    if (!kLean && cache.enabled) {
         const float cv = fmaxf(fabsf(Dot(d, s.n)), 1.0e-4f);
         float2 sp = ps.spread[path];
         if (depth == 0) {
@@ -1383,7 +1388,7 @@ __device__ __forceinline__ void ShadeEntry(const DevScene& sc, PathState& ps, Qu
     }
 
     // --- next-event estimation: samples now, visibility in the shadow stage
-    if (!IsDelta(m)) NextEvent(sc, ps, q, path, smp, rng, depth, m, s.p, s.n, wo, tp, flags);
+    if (!IsDelta(m)) NextEvent<kLean>(sc, ps, q, path, smp, rng, depth, m, s.p, s.n, wo, tp, flags);
 
     // --- subsurface entry (path_integrator.cpp:103-135): Fresnel split at
     // the interface; the transmitted part becomes a probe ray that the
@@ -1460,7 +1465,10 @@ __device__ __forceinline__ void ShadeEntry(const DevScene& sc, PathState& ps, Qu
     ContinuePath(sc, ps, q, path, depth, m, s.material, s.p, s.n, wo, tp, rad, flags, smp, rng);
 }
 
-template <int kClass>
+// kLean: the scene has only emissive-surface lights and no radiance cache
+// (ShadeLean, on the host); the instance leaves the other light kinds' and
+// the cache's code out, which frees registers for the rest.
+template <int kClass, bool kLean>
 __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps, Queues q, int depth,
                                                        CacheArgs cache) {
     unsigned long long begin = 0;
@@ -1469,7 +1477,7 @@ __global__ void __launch_bounds__(256, 2) ShadeKernel(DevScene sc, PathState ps,
     const int64_t count = static_cast<int64_t>(q.counters[kCtrClass0 + kClass]);
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        ShadeEntry<kClass>(sc, ps, q, depth, cache, q.order[begin + i]);
+        ShadeEntry<kClass, kLean>(sc, ps, q, depth, cache, q.order[begin + i]);
     }
 }
 
@@ -2021,14 +2029,30 @@ void LaunchPooledShade(const ShadeJob* jobs, int njobs, int64_t capacity, int sm
     PooledShadeKernel<kClassCoatedDiffuse><<<grid, kThreads, 0, st>>>(jobs, njobs);
     PooledShadeKernel<kClassGeneric><<<grid, kThreads, 0, st>>>(jobs, njobs);
 }
+// Host mirror of the device checks that the lean shading instances drop:
+// no analytic light, no sampleable environment (EnvSampleable), no cache.
+static bool ShadeLean(const DevScene& sc, const CacheArgs& cache) {
+    const bool env = sc.env.active && sc.env.strength > 0.0f && sc.env.texels && sc.env.texel_weights;
+    return sc.analytic_count == 0 && !env && !cache.enabled;
+}
+template <bool kLean>
+static void LaunchShadeClassesOf(const DevScene& sc, const PathState& ps, const Queues& q, const CacheArgs& cache,
+                                 int depth, int64_t capacity, int sm_count, cudaStream_t st) {
+    const unsigned grid = Grid(capacity, sm_count);
+    ShadeKernel<kClassMiss, kLean><<<grid, kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    ShadeKernel<kClassDiffuse, kLean><<<grid, kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    ShadeKernel<kClassConductor, kLean><<<grid, kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    ShadeKernel<kClassDielectric, kLean><<<grid, kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    ShadeKernel<kClassCoatedDiffuse, kLean><<<grid, kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    ShadeKernel<kClassGeneric, kLean><<<grid, kThreads, 0, st>>>(sc, ps, q, depth, cache);
+}
 void LaunchShadeClasses(const DevScene& sc, const PathState& ps, const Queues& q, const CacheArgs& cache, int depth,
                         int64_t capacity, int sm_count, cudaStream_t st) {
-    ShadeKernel<kClassMiss><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
-    ShadeKernel<kClassDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
-    ShadeKernel<kClassConductor><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
-    ShadeKernel<kClassDielectric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
-    ShadeKernel<kClassCoatedDiffuse><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
-    ShadeKernel<kClassGeneric><<<Grid(capacity, sm_count), kThreads, 0, st>>>(sc, ps, q, depth, cache);
+    if (ShadeLean(sc, cache)) {
+        LaunchShadeClassesOf<true>(sc, ps, q, cache, depth, capacity, sm_count, st);
+    } else {
+        LaunchShadeClassesOf<false>(sc, ps, q, cache, depth, capacity, sm_count, st);
+    }
 }
 template <bool kTwo, int kTotal>
 void LaunchAlphaOne(const DevScene& sc, const PathState& ps, const Queues& q, int depth, int64_t capacity,
