@@ -79,7 +79,10 @@ def replica_value(ws: int, rays_per_rank: int, steps: int, max_ms: float) -> flo
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples the SM clock, power and throttle reasons during the timed region:
+    through NVML every 10 ms where its bindings load (so that a timed region of
+    tens of milliseconds still gets several samples), else through nvidia-smi
+    every 0.2 s. Reads only; changes no setting of the GPU."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -90,16 +93,52 @@ class ClockSampler:
         self.rows = []
         self._stop = threading.Event()
         self._thread = None
+        self._nvml = None
+        self._handle = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            self._handle = self._device_handle(gpu_index)
+        except Exception:
+            self._nvml = None
+
+    def _device_handle(self, idx: int):
+        """The NVML handle of CUDA device idx, matched by PCI address (CUDA and
+        NVML may number the visible GPUs differently)."""
+        n = self._nvml
+        try:
+            import torch
+
+            prop = torch.cuda.get_device_properties(idx)
+            bus = f"{prop.pci_domain_id:08x}:{prop.pci_bus_id:02x}:{prop.pci_device_id:02x}.0"
+            return n.nvmlDeviceGetHandleByPciBusId_v2(bus)
+        except Exception:
+            return n.nvmlDeviceGetHandleByIndex(idx)
+
+    def _sample_nvml(self):
+        n, h = self._nvml, self._handle
+        sm = n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM)
+        mx = n.nvmlDeviceGetMaxClockInfo(h, n.NVML_CLOCK_SM)
+        watts = n.nvmlDeviceGetPowerUsage(h) / 1000.0
+        bits = n.nvmlDeviceGetCurrentClocksEventReasons(h)
+        flags = [n.nvmlClocksEventReasonHwSlowdown, n.nvmlClocksEventReasonHwThermalSlowdown,
+                 n.nvmlClocksEventReasonSwThermalSlowdown, n.nvmlClocksEventReasonSwPowerCap]
+        return [str(sm), str(mx), f"{watts:.2f}"] + ["Active" if bits & f else "Not Active" for f in flags]
 
     def _run(self):
         while not self._stop.is_set():
             try:
+                if self._nvml is not None:
+                    self.rows.append(self._sample_nvml())
+                    self._stop.wait(0.01)
+                    continue
                 out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
                 if out.returncode == 0 and out.stdout.strip():
                     self.rows.append([c.strip() for c in out.stdout.strip().split(",")])
             except Exception:
-                pass
+                self._nvml = None  # fall back to nvidia-smi
             self._stop.wait(0.2)
 
     def __enter__(self):
@@ -111,6 +150,11 @@ class ClockSampler:
         self._stop.set()
         if self._thread:
             self._thread.join(timeout=10)
+        if self._nvml is not None:
+            try:
+                self._nvml.nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
         if not self.rows:
@@ -120,7 +164,8 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(self.rows),
+                "source": "nvml" if self._handle is not None and self._nvml is not None else "nvidia-smi"}
 
 
 def measured_peak():
